@@ -1,0 +1,397 @@
+// Solver context of the C ABI: device-resident mesh, operators and state,
+// fused stage launches and CUDA-graph-captured LSRK45 steps.
+//
+// Replaces the module-level OCCA buffers and host driver of the reference
+// (cpp/src/WaveOKL3d.cpp:12-135 globals, WaveInitOCCA3d :1400-1680,
+// InitWADG_subelem :419-915, RK_step_WADG_subelem :2084-2109,
+// Wave_RK :2014-2081, WaveSetData3d / WaveGetData3d :2527-2558).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include "bbwadg.h"
+#include "device_common.cuh"
+#include "fused.h"
+#include "internal.h"
+
+namespace bbw {
+
+// LSRK45 coefficients (Carpenter-Kennedy), cpp/src/StartUp3d.cpp:517-529
+static const double kRK4A[5] = {0.0, -567301805773.0 / 1357537059087.0,
+                                -2404267990393.0 / 2016746695238.0,
+                                -3550918686646.0 / 2091501179385.0,
+                                -1275806237668.0 / 842570457699.0};
+static const double kRK4B[5] = {1432997174477.0 / 9575080441755.0,
+                                5161836677717.0 / 13612068292357.0,
+                                1720146321549.0 / 2090206949498.0,
+                                3134564353537.0 / 4481467310338.0,
+                                2277821191437.0 / 14882151754819.0};
+
+static int round4i(int x) { return (x + 3) & ~3; }
+static int cdivi(int a, int b) { return (a + b - 1) / b; }
+
+}  // namespace bbw
+
+using namespace bbw;
+
+struct bbw_ctx {
+  int N = 0, K = 0, Nq = 0, Np = 0, Nfp = 0, variant = 0, bc = 0, device = 0;
+  cudaStream_t stream = nullptr;
+  float *Q[2] = {nullptr, nullptr};
+  int cur = 0;
+  float *res = nullptr;
+  float *vgeo = nullptr, *fgeo = nullptr, *c2q = nullptr, *ops = nullptr;
+  int *nbr = nullptr, *tables = nullptr;
+  FusedPlan plan;
+  // one graph per starting buffer parity, for one LSRK45 step of size dt
+  cudaGraphExec_t step_graph[2] = {nullptr, nullptr};
+  uint32_t graph_dt_bits[2] = {0, 0};
+};
+
+namespace {
+
+template <class T>
+bbw_status upload(T **dst, const T *src, size_t n, const char *what) {
+  cudaError_t e = cudaMalloc((void **)dst, n * sizeof(T) + 16);
+  if (e != cudaSuccess) return set_cuda_error(e, what);
+  if (src) e = cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice);
+  else e = cudaMemset(*dst, 0, n * sizeof(T));
+  return set_cuda_error(e, what);
+}
+
+void release(bbw_ctx *c) {
+  if (!c) return;
+  for (int i = 0; i < 2; ++i)
+    if (c->step_graph[i]) cudaGraphExecDestroy(c->step_graph[i]);
+  cudaFree(c->Q[0]);
+  cudaFree(c->Q[1]);
+  cudaFree(c->res);
+  cudaFree(c->vgeo);
+  cudaFree(c->fgeo);
+  cudaFree(c->c2q);
+  cudaFree(c->ops);
+  cudaFree(c->nbr);
+  cudaFree(c->tables);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+// vmapP -> per face (neighbour << 8 | permutation id), permutation table
+bbw_status compress_connectivity(int N, int K, const int *Fmask, const int *vmapP,
+                                 std::vector<int> &nbr, std::vector<int> &pats, int &npat) {
+  const int Np = np_of(N), Nfp = nfp_of(N), NF = 4 * Nfp;
+  nbr.assign((size_t)K * 4, 0);
+  pats.clear();
+  npat = 0;
+  std::map<std::vector<int>, int> index;
+  std::vector<int> p(Nfp);
+  for (int k = 0; k < K; ++k)
+    for (int f = 0; f < 4; ++f) {
+      const int *v = vmapP + (size_t)k * NF + f * Nfp;
+      const long long k2 = v[0] / (4 * Np);
+      bool boundary = true;
+      for (int j = 0; j < Nfp; ++j) {
+        if (v[j] < 0 || v[j] / (4 * Np) != k2 || v[j] % (4 * Np) >= Np)
+          return set_error(BBW_ERR_MESH, "vmapP: trace index outside the p field of one element");
+        p[j] = v[j] % (4 * Np);
+        boundary = boundary && k2 == k && p[j] == Fmask[f * Nfp + j];
+      }
+      if (k2 >= K) return set_error(BBW_ERR_MESH, "vmapP: neighbour out of range");
+      if (boundary) {
+        nbr[4 * (size_t)k + f] = (int)(k << 8) | 255;
+        continue;
+      }
+      if (k2 == k)
+        return set_error(BBW_ERR_MESH, "vmapP: face maps partly onto its own element");
+      auto it = index.find(p);
+      int id;
+      if (it == index.end()) {
+        if (npat >= 255) return set_error(BBW_ERR_MESH, "vmapP: too many face permutations");
+        id = npat++;
+        index[p] = id;
+        pats.insert(pats.end(), p.begin(), p.end());
+      } else {
+        id = it->second;
+      }
+      nbr[4 * (size_t)k + f] = (int)(k2 << 8) | id;
+    }
+  return BBW_OK;
+}
+
+}  // namespace
+
+extern "C" bbw_status bbw_create(const bbw_mesh_desc *m, const bbw_ops_desc *o, int variant,
+                                 int bc, bbw_ctx **out) {
+  if (!out) return set_error(BBW_ERR_ARG, "bbw_create: out is NULL");
+  *out = nullptr;
+  if (!m || !o || (variant != BBW_NODAL && variant != BBW_BB) || (bc != 0 && bc != 1))
+    return set_error(BBW_ERR_ARG, "bbw_create: bad argument");
+  const int N = m->N, K = m->K, Nq = m->Nq;
+  if (N < 1 || N > BBW_MAX_N) return set_error(BBW_ERR_UNSUPPORTED, "bbw_create: N out of range");
+  if (K <= 0 || K >= (1 << 23) || Nq <= 0)
+    return set_error(BBW_ERR_ARG, "bbw_create: K must be in [1, 2^23), Nq > 0");
+  if (!m->vgeo || !m->fgeo || !m->Fmask || !m->vmapP || !m->c2q || !o->Vq || !o->Pq)
+    return set_error(BBW_ERR_ARG, "bbw_create: missing mesh or WADG array");
+  const bool bb = variant == BBW_BB;
+  if (!bb && (!o->Dr || !o->Ds || !o->Dt || !o->LIFT))
+    return set_error(BBW_ERR_ARG, "bbw_create: nodal operators missing");
+  if (bb && (!o->D_ids1 || !o->D_ids2 || !o->D_ids3 || !o->D_ids4 || !o->Dvals4 ||
+             !o->EEL_ids || !o->EEL_vals || !o->L0_ids || !o->L0_vals || o->EEL_nnz <= 0 ||
+             o->L0_nnz <= 0))
+    return set_error(BBW_ERR_ARG, "bbw_create: BB operators missing");
+  const int Np = np_of(N), Nfp = nfp_of(N), NF = 4 * Nfp;
+  // the fused stage skips the velocity rows of the WADG update (Pq*Vq = I),
+  // which requires Jq = 1 (affine elements)
+  std::vector<float> c2J((size_t)K * Nq);
+  for (size_t i = 0; i < c2J.size(); ++i) {
+    const float J = m->Jq ? m->Jq[i] : 1.f;
+    if (J != 1.f)
+      return set_error(BBW_ERR_UNSUPPORTED,
+                       "bbw_create: fused stage needs Jq = 1 (affine elements); use the "
+                       "kernel-level entry points for curved Jacobians");
+    c2J[i] = m->c2q[i];
+  }
+  std::vector<int> nbr, pats;
+  int npat = 0;
+  bbw_status s = compress_connectivity(N, K, m->Fmask, m->vmapP, nbr, pats, npat);
+  if (s != BBW_OK) return s;
+
+  // ---- pack operators in the per-warp layouts of kernels_fused.cu
+  const int W = fused_warps(N), R = cdivi(Np, W), PR = round4i(R), P3R = round4i(3 * R);
+  const int RQ = cdivi(Nq, W), PRQ = round4i(RQ);
+  for (int i = 0; i < NF; ++i)
+    if (m->Fmask[i] < 0 || m->Fmask[i] >= Np)
+      return set_error(BBW_ERR_ARG, "bbw_create: Fmask entry out of range");
+  std::vector<float> ops;
+  int off_lift = 0, off_pq = 0, off_vq = 0;
+  if (!bb) {
+    std::vector<float> vol((size_t)W * Np * P3R, 0.f), lift((size_t)W * NF * PR, 0.f);
+    for (int w = 0; w < W; ++w)
+      for (int i = 0; i < R; ++i) {
+        const int r = w * R + i;
+        if (r >= Np) continue;
+        for (int mm = 0; mm < Np; ++mm) {
+          float *d = &vol[((size_t)w * Np + mm) * P3R + 3 * i];
+          d[0] = o->Dr[r + mm * Np], d[1] = o->Ds[r + mm * Np], d[2] = o->Dt[r + mm * Np];
+        }
+        for (int mm = 0; mm < NF; ++mm) lift[((size_t)w * NF + mm) * PR + i] = o->LIFT[r + mm * Np];
+      }
+    ops.insert(ops.end(), vol.begin(), vol.end());
+    off_lift = (int)ops.size();
+    ops.insert(ops.end(), lift.begin(), lift.end());
+  }
+  if (bb) off_lift = 0;
+  off_pq = (int)ops.size();
+  {
+    std::vector<float> pq((size_t)W * Nq * PR, 0.f), vq((size_t)W * Np * PRQ, 0.f);
+    for (int w = 0; w < W; ++w) {
+      for (int i = 0; i < R; ++i) {
+        const int r = w * R + i;
+        if (r < Np)
+          for (int q = 0; q < Nq; ++q) pq[((size_t)w * Nq + q) * PR + i] = o->Pq[r + q * Np];
+      }
+      for (int i = 0; i < RQ; ++i) {
+        const int q = w * RQ + i;
+        if (q < Nq)
+          for (int n = 0; n < Np; ++n) vq[((size_t)w * Np + n) * PRQ + i] = o->Vq[q + n * Nq];
+      }
+    }
+    ops.insert(ops.end(), pq.begin(), pq.end());
+    off_vq = (int)ops.size();
+    ops.insert(ops.end(), vq.begin(), vq.end());
+  }
+  // ---- integer tables: Fmask | patterns | BB tables
+  std::vector<int> tab(m->Fmask, m->Fmask + NF);
+  tab.resize(round4i((int)tab.size()), 0);
+  const int pat_off = (int)tab.size();
+  tab.insert(tab.end(), pats.begin(), pats.end());
+  tab.resize(round4i((int)tab.size()), 0);
+  const int bb_off = (int)tab.size();
+  if (bb) {
+    const int *Dp[4] = {o->D_ids1, o->D_ids2, o->D_ids3, o->D_ids4};
+    for (int d = 0; d < 4; ++d) tab.insert(tab.end(), Dp[d], Dp[d] + 4 * Np);
+    for (int i = 0; i < 4 * Np; ++i) {
+      int bits;
+      std::memcpy(&bits, &o->Dvals4[i], 4);
+      tab.push_back(bits);
+    }
+    const int L0 = o->L0_nnz;
+    tab.push_back(L0);
+    for (int nt = 0; nt < Nfp; ++nt)
+      for (int j = 0; j < L0; ++j) tab.push_back(o->L0_ids[nt + j * Nfp]);
+    for (int nt = 0; nt < Nfp; ++nt)
+      for (int j = 0; j < L0; ++j) {
+        int bits;
+        std::memcpy(&bits, &o->L0_vals[nt + j * Nfp], 4);
+        tab.push_back(bits);
+      }
+    // EEL as CSR with the nonzeros of each row bucketed by face
+    std::vector<int> ptr((size_t)Np * 5), col;
+    std::vector<float> val;
+    for (int n = 0; n < Np; ++n)
+      for (int f = 0; f < 4; ++f) {
+        ptr[(size_t)n * 5 + f] = (int)col.size();
+        for (int j = 0; j < o->EEL_nnz; ++j) {
+          const int c = o->EEL_ids[n + j * Np];
+          const float v = o->EEL_vals[n + j * Np];
+          if (c < 0 || c >= NF) return set_error(BBW_ERR_ARG, "bbw_create: EEL id out of range");
+          if (v != 0.f && c / Nfp == f) col.push_back(c), val.push_back(v);
+        }
+        if (f == 3) ptr[(size_t)n * 5 + 4] = (int)col.size();
+      }
+    tab.insert(tab.end(), ptr.begin(), ptr.end());
+    tab.insert(tab.end(), col.begin(), col.end());
+    for (float v : val) {
+      int bits;
+      std::memcpy(&bits, &v, 4);
+      tab.push_back(bits);
+    }
+    for (int i = 0; i < Np; ++i)
+      for (int d = 0; d < 4; ++d)
+        for (int c = 0; c < 4; ++c) {
+          const int id = Dp[d][4 * i + c];
+          if (id < 0 || id >= Np) return set_error(BBW_ERR_ARG, "bbw_create: D id out of range");
+        }
+    for (int i = 0; i < Nfp * L0; ++i)
+      if (o->L0_ids[i] < 0 || o->L0_ids[i] >= Nfp)
+        return set_error(BBW_ERR_ARG, "bbw_create: L0 id out of range");
+  }
+  tab.resize(round4i((int)tab.size()), 0);
+
+  bbw_ctx *c = new bbw_ctx;
+  c->N = N, c->K = K, c->Nq = Nq, c->Np = Np, c->Nfp = Nfp, c->variant = variant, c->bc = bc;
+  cudaGetDevice(&c->device);
+  const size_t nstate = (size_t)K * 4 * Np;
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    return set_cuda_error(e, "bbw_create: stream");
+  }
+  if ((s = upload<float>(&c->Q[0], nullptr, nstate, "bbw_create: Q")) != BBW_OK ||
+      (s = upload<float>(&c->Q[1], nullptr, nstate, "bbw_create: Q")) != BBW_OK ||
+      (s = upload<float>(&c->res, nullptr, nstate, "bbw_create: res")) != BBW_OK ||
+      (s = upload(&c->vgeo, m->vgeo, (size_t)K * 9, "bbw_create: vgeo")) != BBW_OK ||
+      (s = upload(&c->fgeo, m->fgeo, (size_t)K * 16, "bbw_create: fgeo")) != BBW_OK ||
+      (s = upload(&c->c2q, c2J.data(), c2J.size(), "bbw_create: c2q")) != BBW_OK ||
+      (s = upload(&c->nbr, nbr.data(), nbr.size(), "bbw_create: connectivity")) != BBW_OK ||
+      (s = upload(&c->ops, ops.data(), ops.size(), "bbw_create: operators")) != BBW_OK ||
+      (s = upload(&c->tables, tab.data(), tab.size(), "bbw_create: tables")) != BBW_OK) {
+    release(c);
+    return s;
+  }
+  FusedPlan &pl = c->plan;
+  pl.N = N, pl.K = K, pl.Nq = Nq, pl.RQ = RQ, pl.PRQ = PRQ, pl.bc = bc, pl.npat = npat;
+  pl.bb = bb;
+  pl.vgeo = c->vgeo, pl.fgeo = c->fgeo, pl.c2q = c->c2q, pl.nbr = c->nbr;
+  pl.ops = c->ops, pl.ops_floats = (int)ops.size();
+  pl.off_lift = off_lift, pl.off_pq = off_pq, pl.off_vq = off_vq;
+  pl.tables = c->tables, pl.table_ints = (int)tab.size(), pl.pat_off = pat_off, pl.bb_off = bb_off;
+  if ((s = fused_prepare(pl)) != BBW_OK) {
+    release(c);
+    return s;
+  }
+  *out = c;
+  return BBW_OK;
+}
+
+extern "C" bbw_status bbw_destroy(bbw_ctx *c) {
+  if (!c) return BBW_OK;
+  cudaStreamSynchronize(c->stream);
+  release(c);
+  return BBW_OK;
+}
+
+static bbw_status copy_state(bbw_ctx *c, float *dev, const float *src, float *dst) {
+  if (!c) return set_error(BBW_ERR_ARG, "bbw: ctx is NULL");
+  const size_t bytes = (size_t)c->K * 4 * c->Np * sizeof(float);
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return set_cuda_error(e, "bbw: sync");
+  if (src) e = cudaMemcpy(dev, src, bytes, cudaMemcpyHostToDevice);
+  else e = cudaMemcpy(dst, dev, bytes, cudaMemcpyDeviceToHost);
+  return set_cuda_error(e, "bbw: state copy");
+}
+
+extern "C" bbw_status bbw_set_state(bbw_ctx *c, const float *Q) {
+  if (!c || !Q) return set_error(BBW_ERR_ARG, "bbw_set_state: NULL");
+  return copy_state(c, c->Q[c->cur], Q, nullptr);
+}
+extern "C" bbw_status bbw_get_state(bbw_ctx *c, float *Q) {
+  if (!c || !Q) return set_error(BBW_ERR_ARG, "bbw_get_state: NULL");
+  return copy_state(c, c->Q[c->cur], nullptr, Q);
+}
+extern "C" bbw_status bbw_set_residual(bbw_ctx *c, const float *r) {
+  if (!c || !r) return set_error(BBW_ERR_ARG, "bbw_set_residual: NULL");
+  return copy_state(c, c->res, r, nullptr);
+}
+extern "C" bbw_status bbw_get_residual(bbw_ctx *c, float *r) {
+  if (!c || !r) return set_error(BBW_ERR_ARG, "bbw_get_residual: NULL");
+  return copy_state(c, c->res, nullptr, r);
+}
+
+extern "C" bbw_status bbw_stage(bbw_ctx *c, float fa, float fb, float fdt) {
+  if (!c) return set_error(BBW_ERR_ARG, "bbw_stage: ctx is NULL");
+  bbw_status s = fused_launch(c->plan, c->Q[c->cur], c->Q[c->cur ^ 1], c->res, fa, fb, fdt,
+                              c->stream);
+  if (s == BBW_OK) c->cur ^= 1;
+  return s;
+}
+
+extern "C" bbw_status bbw_steps(bbw_ctx *c, float dt, int nsteps) {
+  if (!c || nsteps < 0) return set_error(BBW_ERR_ARG, "bbw_steps: bad argument");
+  uint32_t bits;
+  std::memcpy(&bits, &dt, 4);
+  for (int step = 0; step < nsteps; ++step) {
+    const int par = c->cur;
+    if (!c->step_graph[par] || c->graph_dt_bits[par] != bits) {
+      if (c->step_graph[par]) cudaGraphExecDestroy(c->step_graph[par]);
+      c->step_graph[par] = nullptr;
+      cudaGraph_t g;
+      cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) return set_cuda_error(e, "bbw_steps: capture");
+      bbw_status s = BBW_OK;
+      for (int i = 0; i < 5 && s == BBW_OK; ++i)
+        s = bbw_stage(c, (float)kRK4A[i], (float)kRK4B[i], dt);
+      e = cudaStreamEndCapture(c->stream, &g);
+      c->cur = par;  // capture recorded the launches without running them
+      if (s != BBW_OK) return s;
+      if (e != cudaSuccess) return set_cuda_error(e, "bbw_steps: end capture");
+      e = cudaGraphInstantiate(&c->step_graph[par], g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return set_cuda_error(e, "bbw_steps: instantiate");
+      c->graph_dt_bits[par] = bits;
+    }
+    cudaError_t e = cudaGraphLaunch(c->step_graph[par], c->stream);
+    if (e != cudaSuccess) return set_cuda_error(e, "bbw_steps: launch");
+    c->cur ^= 1;  // five stages swap the buffers an odd number of times
+  }
+  return BBW_OK;
+}
+
+extern "C" bbw_status bbw_run(bbw_ctx *c, double final_time, float dt) {
+  if (!c || !(dt > 0.f) || final_time < 0) return set_error(BBW_ERR_ARG, "bbw_run: bad argument");
+  double time = 0;
+  while (time < final_time) {
+    if (time + dt > final_time) dt = (float)(final_time - time);  // WaveOKL3d.cpp:2048
+    bbw_status s = bbw_steps(c, dt, 1);
+    if (s != BBW_OK) return s;
+    time += dt;
+  }
+  return BBW_OK;
+}
+
+extern "C" bbw_status bbw_sync(bbw_ctx *c) {
+  if (!c) return set_error(BBW_ERR_ARG, "bbw_sync: ctx is NULL");
+  return set_cuda_error(cudaStreamSynchronize(c->stream), "bbw_sync");
+}
+
+extern "C" bbw_status bbw_device_state(bbw_ctx *c, float **Q, float **res, void **stream) {
+  if (!c) return set_error(BBW_ERR_ARG, "bbw_device_state: ctx is NULL");
+  if (Q) *Q = c->Q[c->cur];
+  if (res) *res = c->res;
+  if (stream) *stream = (void *)c->stream;
+  return BBW_OK;
+}

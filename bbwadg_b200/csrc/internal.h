@@ -1,0 +1,29 @@
+// Internal host-side helpers shared by the setup and runtime translation units.
+#pragma once
+#include <cmath>
+#include <string>
+#include <vector>
+
+namespace bbw {
+
+inline int np_of(int N) { return (N + 1) * (N + 2) * (N + 3) / 6; }
+inline int nfp_of(int N) { return (N + 1) * (N + 2) / 2; }
+
+// Dense row-major matrix for the FP64 operator construction.
+struct Mat {
+  int m = 0, n = 0;
+  std::vector<double> a;
+  Mat() {}
+  Mat(int m_, int n_, double v = 0.0) : m(m_), n(n_), a((size_t)m_ * n_, v) {}
+  double &operator()(int i, int j) { return a[(size_t)i * n + j]; }
+  double operator()(int i, int j) const { return a[(size_t)i * n + j]; }
+};
+
+Mat matmul(const Mat &A, const Mat &B);
+Mat transpose(const Mat &A);
+Mat inverse(const Mat &A);                 // LU with partial pivoting
+Mat mldivide(const Mat &A, const Mat &B);  // A\B: square solve or least squares
+Mat mrdivide(const Mat &A, const Mat &B);  // A/B = (B'\A')'
+double maxabs(const Mat &A);
+
+}  // namespace bbw

@@ -1,0 +1,537 @@
+// Fused LSRK stage for the affine-tet acoustic WADG method (sm_100a).
+//
+// One kernel per stage replaces the reference's three launches
+// (rk_volume + rk_surface + rk_update_WADG, cpp/src/WaveOKL3d.cpp:2084-2106,
+// or their BB counterparts): per element it forms the volume term, the upwind
+// surface flux and lift, projects c^2 * rhs_p with the WADG operators and
+// applies the LSRK45 stage update, reading each element's state once from
+// HBM and writing the new state and residual once.
+//
+// Work decomposition: a persistent CTA owns a tile of E = 32 consecutive
+// elements at a time; lane l of every warp works on element l of the tile,
+// warp w owns a block of R output rows (nodes) or RQ cubature points.  The
+// reference-element operators are staged in shared memory once per CTA in a
+// per-warp packed layout, so every operator read is a warp-uniform broadcast
+// (float4) while the element data is read conflict-free with lane = element.
+// State tiles are moved between HBM and shared memory with coalesced float4
+// traffic and transposed to [row][element] (stride 33) on the way.
+//
+// Double-buffered state: the stage reads Qin (this element and its
+// neighbours' face traces) and writes Qout, so neighbour gathers never race
+// with updates.  res is updated in place.
+//
+// Connectivity: vmapP is compressed at context creation into, per element
+// face, the neighbour element and the index of its face-node permutation
+// (at most 24 distinct permutations exist: 4 faces x 6 orientations), the
+// permutations being kept in a small table; boundary faces are flagged.
+//
+// Simplifications that are exact in exact arithmetic and checked at
+// creation: Uflux = -pflux (both are formed from the same jump with opposite
+// sign, cpp/okl/WaveKernels.okl:215-216), so one lift of pflux per face
+// serves p and, scaled by -n_f, u,v,w; with Jq = 1 (affine tets,
+// cpp/src/WaveOKL3d.cpp:463) the velocity rows of the WADG update are
+// Pq*Vq = I and are skipped.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "bbwadg.h"
+#include "device_common.cuh"
+#include "fused.h"
+
+namespace bbw {
+
+constexpr int TILE_E = 32;
+constexpr int ES = TILE_E + 1;  // shared-memory row stride (floats)
+
+__host__ __device__ constexpr int round4(int x) { return (x + 3) & ~3; }
+__host__ __device__ constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }
+
+template <int N>
+struct FusedCfg {
+  static constexpr int Np = NP(N), Nfp = NFP(N), NF = 4 * NFP(N);
+  static constexpr int W = N <= 3 ? 4 : 8;  // warps per CTA
+  static constexpr int T = 32 * W;
+  static constexpr int R = cdiv(Np, W);     // node rows per warp
+  static constexpr int PR = round4(R);
+  static constexpr int P3R = round4(3 * R);
+};
+
+// ------------------------------------------------------------------ layouts
+// Operators, packed per warp so that warp w reads one contiguous, 16-byte
+// aligned block per reduction index:
+//   vol  [W][Np(m)][P3R]  (Dr, Ds, Dt)[r0+i][m] at 3i + {0,1,2}
+//   lift [W][NF(m)][PR]   LIFT[r0+i][m]
+//   pq   [W][Nq(q)][PR]   Pq[r0+i][q]
+//   vq   [W][Np(n)][PRQ]  Vq[q0+i][n]
+// plus, for BB, the sparse tables.  Built on the host (fused_host.cu).
+struct FusedParams {
+  int K, Nq, RQ, PRQ, bc, npat;
+  int pat_off, bb_off;              // int offsets of the tables (multiples of 4)
+  float fa, fb, fdt;
+  const float *__restrict__ Qin;
+  float *__restrict__ Qout;
+  float *__restrict__ res;
+  const float *__restrict__ vgeo;   // [K][9]
+  const float *__restrict__ fgeo;   // [K][16]
+  const int *__restrict__ nbr;      // [K][4]  (k2 << 8) | pattern, pattern 255 = boundary
+  const float *__restrict__ c2q;    // [K][Nq] c2/J at the cubature points
+  const float *__restrict__ ops;    // packed operators (global copy)
+  int ops_smem;                     // leading floats of ops staged in shared memory
+  int off_lift, off_pq, off_vq, off_end;  // operator offsets in ops (floats)
+  const int *__restrict__ tables;   // Fmask [NF] | patterns [npat][Nfp] | BB tables
+  int table_ints;
+};
+
+template <int N, bool BB>
+struct FusedSmem {
+  using C = FusedCfg<N>;
+  // element data (floats), all with row stride ES
+  static constexpr int sQ = 0;                          // [4Np][ES] old state
+  static constexpr int sR = sQ + 4 * C::Np * ES;        // [4Np][ES] rhs / U scratch
+  static constexpr int sF = sR + 4 * C::Np * ES;        // [NF][ES]  pflux
+  static constexpr int sF2 = sF + C::NF * ES;           // [NF][ES]  BB: L0 * pflux
+  static constexpr int sGeo = sF2 + (BB ? C::NF * ES : 0);  // [E][25] vgeo + fgeo
+  static constexpr int sNbr = sGeo + TILE_E * 25;       // [E][4] ints
+  static constexpr int sQuad = sNbr + TILE_E * 4;       // [Nq][ES] projected p, then c2
+  // followed at run time by [Nq][ES] c2 tile, the operators and int tables
+};
+
+// -------------------------------------------------------------- device code
+template <int N, bool BB>
+__global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P) {
+  using C = FusedCfg<N>;
+  using L = FusedSmem<N, BB>;
+  constexpr int Np = C::Np, Nfp = C::Nfp, NF = C::NF, W = C::W, T = C::T, R = C::R;
+  extern __shared__ __align__(16) float sm[];
+  const int Nq = P.Nq, RQ = P.RQ, PRQ = P.PRQ;
+  float *sQ = sm + L::sQ, *sR = sm + L::sR, *sF = sm + L::sF, *sF2 = sm + L::sF2;
+  float *sGeo = sm + L::sGeo;
+  int *sNbr = (int *)(sm + L::sNbr);
+  float *sQuad = sm + L::sQuad;
+  float *sC2 = sQuad + round4(Nq * ES);
+  int *sTab = (int *)(sC2 + round4(Nq * ES));
+  float *sOps = (float *)(sTab + P.table_ints);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int r0 = warp * R;
+
+  // stage operators and tables once per CTA
+  for (int i = tid; i < P.ops_smem / 4; i += T)
+    reinterpret_cast<float4 *>(sOps)[i] = __ldg(reinterpret_cast<const float4 *>(P.ops) + i);
+  for (int i = tid; i < P.table_ints; i += T) sTab[i] = __ldg(P.tables + i);
+  const int *sFmask = sTab;
+  const int *sPat = sTab + P.pat_off;
+
+  // operator blocks: from shared memory when staged there, otherwise through
+  // the L1 / read-only path (large N or large cubature rules)
+  auto opb = [&](int off, int end) -> const float * {
+    return end <= P.ops_smem ? sOps + off : P.ops + off;
+  };
+  const float *opVol = opb(0, P.off_lift);          // [W][Np][P3R]
+  const float *opLift = opb(P.off_lift, P.off_pq);  // [W][NF][PR]
+  const float *opPq = opb(P.off_pq, P.off_vq);      // [W][Nq][PR]
+  const float *opVq = opb(P.off_vq, P.off_end);     // [W][Np][PRQ]
+  const float *wVol = opVol + warp * Np * C::P3R;
+  const float *wLift = opLift + warp * NF * C::PR;
+  const float *wPq = opPq + warp * Nq * C::PR;
+  const float *wVq = opVq + warp * Np * PRQ;
+  // BB tables after the patterns: D ids int4 x4 [Np], Dvals float4 [Np],
+  // L0 [Nfp][L0nnz] ids/vals, EEL CSR per face
+  const int *bbTab = sTab + P.bb_off;
+
+  const int ntiles = cdiv(P.K, TILE_E);
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int k0 = tile * TILE_E;
+    const int ne = min(TILE_E, P.K - k0);
+    __syncthreads();  // previous tile fully consumed (and operators staged)
+
+    // ---- 1. stage the tile: state (transposed), c2, geometry, neighbours
+    {
+      const float4 *Qg = reinterpret_cast<const float4 *>(P.Qin + (size_t)k0 * 4 * Np);
+      const int n4 = ne * Np;  // float4 per tile = ne * 4Np / 4
+      for (int i = tid; i < TILE_E * Np; i += T) {
+        const int e = (4 * i) / (4 * Np), fn = (4 * i) % (4 * Np);
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (i < n4) v = Qg[i];
+        sQ[(fn + 0) * ES + e] = v.x;
+        sQ[(fn + 1) * ES + e] = v.y;
+        sQ[(fn + 2) * ES + e] = v.z;
+        sQ[(fn + 3) * ES + e] = v.w;
+      }
+      const float *cg = P.c2q + (size_t)k0 * Nq;
+      for (int i = tid; i < TILE_E * Nq; i += T) {
+        const int e = i / Nq, q = i % Nq;
+        sC2[q * ES + e] = i < ne * Nq ? cg[i] : 0.f;
+      }
+      for (int i = tid; i < TILE_E * 9; i += T)
+        sGeo[(i / 9) * 25 + i % 9] = i < ne * 9 ? P.vgeo[(size_t)k0 * 9 + i] : 0.f;
+      for (int i = tid; i < TILE_E * 16; i += T)
+        sGeo[(i / 16) * 25 + 9 + i % 16] = i < ne * 16 ? P.fgeo[(size_t)k0 * 16 + i] : 0.f;
+      for (int i = tid; i < TILE_E * 4; i += T)
+        sNbr[i] = i < ne * 4 ? P.nbr[(size_t)k0 * 4 + i] : 255;
+    }
+    __syncthreads();
+
+    // ---- 2. contravariant velocities Ur, Us, Ut into sR rows [Np, 4Np)
+    for (int i = tid; i < TILE_E * Np; i += T) {
+      const int e = i & 31, n = i >> 5;
+      const float *G = sGeo + e * 25;
+      const float u = sQ[(Np + n) * ES + e], v = sQ[(2 * Np + n) * ES + e],
+                  w = sQ[(3 * Np + n) * ES + e];
+      sR[(Np + n) * ES + e] = u * G[0] + v * G[1] + w * G[2];
+      sR[(2 * Np + n) * ES + e] = u * G[3] + v * G[4] + w * G[5];
+      sR[(3 * Np + n) * ES + e] = u * G[6] + v * G[7] + w * G[8];
+    }
+
+    // ---- 3. upwind flux at the 4Nfp face nodes (Uflux = -pflux)
+    for (int i = tid; i < TILE_E * NF; i += T) {
+      const int e = i & 31, m = i >> 5, f = m / Nfp;
+      const int code = sNbr[e * 4 + f];
+      const int vM = sFmask[m];
+      const float pM = sQ[vM * ES + e], uM = sQ[(Np + vM) * ES + e],
+                  vvM = sQ[(2 * Np + vM) * ES + e], wM = sQ[(3 * Np + vM) * ES + e];
+      const float *fg = sGeo + e * 25 + 9 + 4 * f;
+      const float Fscale = fg[0], nx = fg[1], ny = fg[2], nz = fg[3];
+      float pjump, Unjump;
+      const int pat = code & 255;
+      if (pat == 255) {
+        if (P.bc == BBW_BC_PRESSURE_RELEASE) {
+          pjump = -2.f * pM;
+          Unjump = 0.f;
+        } else {
+          pjump = 0.f;
+          Unjump = -2.f * (uM * nx + vvM * ny + wM * nz);
+        }
+      } else {
+        const int k2 = code >> 8;
+        const float *q2 = P.Qin + (size_t)k2 * 4 * Np + sPat[pat * Nfp + (m - f * Nfp)];
+        const float pP = __ldg(q2), uP = __ldg(q2 + Np), vP = __ldg(q2 + 2 * Np),
+                    wP = __ldg(q2 + 3 * Np);
+        pjump = pP - pM;
+        Unjump = (uP - uM) * nx + (vP - vvM) * ny + (wP - wM) * nz;
+      }
+      sF[m * ES + e] = .5f * (pjump - Unjump) * Fscale;
+    }
+    __syncthreads();
+
+    // ---- 4. volume term (registers: rows r0..r0+R of this warp, lane = element)
+    float rp[R], ru[R], rv[R], rw[R];
+    {
+      const float *G = sGeo + lane * 25;
+      if constexpr (!BB) {
+        float dr[R], ds[R], dt[R], dv[R];
+#pragma unroll
+        for (int i = 0; i < R; ++i) dr[i] = ds[i] = dt[i] = dv[i] = 0.f;
+#pragma unroll 2
+        for (int m = 0; m < Np; ++m) {
+          const float pm = sQ[m * ES + lane];
+          const float ur = sR[(Np + m) * ES + lane], us = sR[(2 * Np + m) * ES + lane],
+                      ut = sR[(3 * Np + m) * ES + lane];
+          const float4 *op = reinterpret_cast<const float4 *>(wVol + m * C::P3R);
+          float o[C::P3R];
+#pragma unroll
+          for (int j = 0; j < C::P3R / 4; ++j) {
+            const float4 t4 = op[j];
+            o[4 * j] = t4.x, o[4 * j + 1] = t4.y, o[4 * j + 2] = t4.z, o[4 * j + 3] = t4.w;
+          }
+#pragma unroll
+          for (int i = 0; i < R; ++i) {
+            dr[i] += o[3 * i] * pm;
+            ds[i] += o[3 * i + 1] * pm;
+            dt[i] += o[3 * i + 2] * pm;
+            dv[i] += o[3 * i] * ur;
+            dv[i] += o[3 * i + 1] * us;
+            dv[i] += o[3 * i + 2] * ut;
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+          rp[i] = -dv[i];
+          ru[i] = -(G[0] * dr[i] + G[3] * ds[i] + G[6] * dt[i]);
+          rv[i] = -(G[1] * dr[i] + G[4] * ds[i] + G[7] * dt[i]);
+          rw[i] = -(G[2] * dr[i] + G[5] * ds[i] + G[8] * dt[i]);
+        }
+      } else {
+        // sparse Bernstein derivative, cpp/okl/WaveKernels.okl:428-467
+        const int4 *Dids = reinterpret_cast<const int4 *>(bbTab);          // [4][Np]
+        const float4 *Dv = reinterpret_cast<const float4 *>(bbTab + 16 * Np);  // [Np]
+        const float *p = sQ + lane, *ur = sR + Np * ES + lane, *us = sR + 2 * Np * ES + lane,
+                    *ut = sR + 3 * Np * ES + lane;
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+          const int n = r0 + i;
+          rp[i] = ru[i] = rv[i] = rw[i] = 0.f;
+          if (n >= Np) continue;
+          const float4 dv = Dv[n];
+          const int4 a = Dids[n], b = Dids[Np + n], c = Dids[2 * Np + n], d = Dids[3 * Np + n];
+          const float p1 = dv.x * p[a.x * ES] + dv.y * p[b.x * ES] + dv.z * p[c.x * ES] +
+                           dv.w * p[d.x * ES];
+          const float p2 = dv.x * p[a.y * ES] + dv.y * p[b.y * ES] + dv.z * p[c.y * ES] +
+                           dv.w * p[d.y * ES];
+          const float p3 = dv.x * p[a.z * ES] + dv.y * p[b.z * ES] + dv.z * p[c.z * ES] +
+                           dv.w * p[d.z * ES];
+          const float p4 = dv.x * p[a.w * ES] + dv.y * p[b.w * ES] + dv.z * p[c.w * ES] +
+                           dv.w * p[d.w * ES];
+          float dU1 = dv.x * (ur[a.y * ES] + us[a.z * ES] + ut[a.w * ES]);
+          dU1 += dv.y * (ur[b.y * ES] + us[b.z * ES] + ut[b.w * ES]);
+          dU1 += dv.z * (ur[c.y * ES] + us[c.z * ES] + ut[c.w * ES]);
+          dU1 += dv.w * (ur[d.y * ES] + us[d.z * ES] + ut[d.w * ES]);
+          float dU2 = dv.x * (ur[a.x * ES] + us[a.x * ES] + ut[a.x * ES]);
+          dU2 += dv.y * (ur[b.x * ES] + us[b.x * ES] + ut[b.x * ES]);
+          dU2 += dv.z * (ur[c.x * ES] + us[c.x * ES] + ut[c.x * ES]);
+          dU2 += dv.w * (ur[d.x * ES] + us[d.x * ES] + ut[d.x * ES]);
+          const float dpdr = .5f * (p2 - p1), dpds = .5f * (p3 - p1), dpdt = .5f * (p4 - p1);
+          rp[i] = -.5f * (dU1 - dU2);
+          ru[i] = -(G[0] * dpdr + G[3] * dpds + G[6] * dpdt);
+          rv[i] = -(G[1] * dpdr + G[4] * dpds + G[7] * dpdt);
+          rw[i] = -(G[2] * dpdr + G[5] * dpds + G[8] * dpdt);
+        }
+      }
+    }
+
+    // ---- 5. lift of the face fluxes
+    {
+      const float *fgl = sGeo + lane * 25 + 9;
+      if constexpr (!BB) {
+#pragma unroll 1
+        for (int f = 0; f < 4; ++f) {
+          float acc[R];
+#pragma unroll
+          for (int i = 0; i < R; ++i) acc[i] = 0.f;
+#pragma unroll 3
+          for (int j = 0; j < Nfp; ++j) {
+            const int m = f * Nfp + j;
+            const float pf = sF[m * ES + lane];
+            const float4 *op = reinterpret_cast<const float4 *>(wLift + m * C::PR);
+            float o[C::PR];
+#pragma unroll
+            for (int q = 0; q < C::PR / 4; ++q) {
+              const float4 t4 = op[q];
+              o[4 * q] = t4.x, o[4 * q + 1] = t4.y, o[4 * q + 2] = t4.z, o[4 * q + 3] = t4.w;
+            }
+#pragma unroll
+            for (int i = 0; i < R; ++i) acc[i] += o[i] * pf;
+          }
+          const float nx = fgl[4 * f + 1], ny = fgl[4 * f + 2], nz = fgl[4 * f + 3];
+#pragma unroll
+          for (int i = 0; i < R; ++i) {
+            rp[i] += acc[i];
+            ru[i] -= nx * acc[i];
+            rv[i] -= ny * acc[i];
+            rw[i] -= nz * acc[i];
+          }
+        }
+      } else {
+        // BB lift: per face L0 (Nfp x Nfp sparse), then degree elevation EEL
+        // applied face by face (cpp/okl/WaveKernels.okl:576-644)
+        const int L0nnz = bbTab[20 * Np];
+        const int *L0ids = bbTab + 20 * Np + 1;
+        const float *L0vals = reinterpret_cast<const float *>(L0ids + Nfp * L0nnz);
+        const int *eelPtr = reinterpret_cast<const int *>(L0vals + Nfp * L0nnz);  // [Np][5]
+        const int *eelCol = eelPtr + 5 * Np;
+        const float *eelVal = reinterpret_cast<const float *>(eelCol + eelPtr[5 * Np - 1]);
+        for (int m = warp; m < NF; m += W) {
+          const int f = m / Nfp, nt = m - f * Nfp;
+          float v = 0.f;
+          for (int j = 0; j < L0nnz; ++j)
+            v += L0vals[nt * L0nnz + j] * sF[(L0ids[nt * L0nnz + j] + f * Nfp) * ES + lane];
+          sF2[m * ES + lane] = v;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+          const int n = r0 + i;
+          if (n >= Np) continue;
+          const int *ptr = eelPtr + 5 * n;
+#pragma unroll 1
+          for (int f = 0; f < 4; ++f) {
+            float acc = 0.f;
+            for (int j = ptr[f]; j < ptr[f + 1]; ++j) acc += eelVal[j] * sF2[eelCol[j] * ES + lane];
+            rp[i] += acc;
+            ru[i] -= fgl[4 * f + 1] * acc;
+            rv[i] -= fgl[4 * f + 2] * acc;
+            rw[i] -= fgl[4 * f + 3] * acc;
+          }
+        }
+      }
+    }
+    __syncthreads();  // all warps done reading Ur/Us/Ut from sR
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int n = r0 + i;
+      if (n < Np) {
+        sR[n * ES + lane] = rp[i];
+        sR[(Np + n) * ES + lane] = ru[i];
+        sR[(2 * Np + n) * ES + lane] = rv[i];
+        sR[(3 * Np + n) * ES + lane] = rw[i];
+      }
+    }
+    __syncthreads();
+
+    // ---- 6. WADG: p at the cubature points, times c2/J
+    {
+      const int q0 = warp * RQ;
+      for (int qb = 0; qb < RQ; qb += 4) {
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+#pragma unroll 4
+        for (int n = 0; n < Np; ++n) {
+          const float x = sR[n * ES + lane];
+          const float4 v = *reinterpret_cast<const float4 *>(wVq + n * PRQ + qb);
+          a0 += v.x * x;
+          a1 += v.y * x;
+          a2 += v.z * x;
+          a3 += v.w * x;
+        }
+        const float av[4] = {a0, a1, a2, a3};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int q = q0 + qb + j;
+          if (qb + j < RQ && q < Nq) sQuad[q * ES + lane] = av[j] * sC2[q * ES + lane];
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---- 7. project back: rhs_p = Pq * (c2 p_q)
+    {
+      float acc[R];
+#pragma unroll
+      for (int i = 0; i < R; ++i) acc[i] = 0.f;
+#pragma unroll 2
+      for (int q = 0; q < Nq; ++q) {
+        const float x = sQuad[q * ES + lane];
+        const float4 *op = reinterpret_cast<const float4 *>(wPq + q * C::PR);
+        float o[C::PR];
+#pragma unroll
+        for (int j = 0; j < C::PR / 4; ++j) {
+          const float4 t4 = op[j];
+          o[4 * j] = t4.x, o[4 * j + 1] = t4.y, o[4 * j + 2] = t4.z, o[4 * j + 3] = t4.w;
+        }
+#pragma unroll
+        for (int i = 0; i < R; ++i) acc[i] += o[i] * x;
+      }
+      __syncthreads();  // everyone has read sR rows [0, Np) in step 6
+#pragma unroll
+      for (int i = 0; i < R; ++i)
+        if (r0 + i < Np) sR[(r0 + i) * ES + lane] = acc[i];
+    }
+    __syncthreads();
+
+    // ---- 8. LSRK stage update, coalesced: res = fa res + fdt rhs; Q += fb res
+    {
+      float4 *resg = reinterpret_cast<float4 *>(P.res + (size_t)k0 * 4 * Np);
+      float4 *qg = reinterpret_cast<float4 *>(P.Qout + (size_t)k0 * 4 * Np);
+      const int n4 = ne * Np;
+      for (int i = tid; i < n4; i += T) {
+        const int e = (4 * i) / (4 * Np), fn = (4 * i) % (4 * Np);
+        float4 r = resg[i], q;
+        r.x = P.fa * r.x + P.fdt * sR[(fn + 0) * ES + e];
+        r.y = P.fa * r.y + P.fdt * sR[(fn + 1) * ES + e];
+        r.z = P.fa * r.z + P.fdt * sR[(fn + 2) * ES + e];
+        r.w = P.fa * r.w + P.fdt * sR[(fn + 3) * ES + e];
+        q.x = sQ[(fn + 0) * ES + e] + P.fb * r.x;
+        q.y = sQ[(fn + 1) * ES + e] + P.fb * r.y;
+        q.z = sQ[(fn + 2) * ES + e] + P.fb * r.z;
+        q.w = sQ[(fn + 3) * ES + e] + P.fb * r.w;
+        resg[i] = r;
+        qg[i] = q;
+      }
+    }
+  }
+}
+
+// --------------------------------------------------------------- host side
+template <int N, bool BB>
+static size_t smem_bytes(int Nq, int ops_smem, int table_ints) {
+  using L = FusedSmem<N, BB>;
+  return sizeof(float) * ((size_t)L::sQuad + 2 * (size_t)round4(Nq * ES) + ops_smem) +
+         sizeof(int) * (size_t)table_ints;
+}
+
+template <int N, bool BB>
+static bbw_status launch_fused(const FusedPlan &pl, const float *Qin, float *Qout, float *res,
+                               float fa, float fb, float fdt, cudaStream_t st) {
+  FusedParams P;
+  P.K = pl.K, P.Nq = pl.Nq, P.RQ = pl.RQ, P.PRQ = pl.PRQ, P.bc = pl.bc, P.npat = pl.npat;
+  P.pat_off = pl.pat_off, P.bb_off = pl.bb_off;
+  P.fa = fa, P.fb = fb, P.fdt = fdt;
+  P.Qin = Qin, P.Qout = Qout, P.res = res;
+  P.vgeo = pl.vgeo, P.fgeo = pl.fgeo, P.nbr = pl.nbr, P.c2q = pl.c2q;
+  P.ops = pl.ops, P.ops_smem = pl.ops_smem;
+  P.off_lift = pl.off_lift, P.off_pq = pl.off_pq, P.off_vq = pl.off_vq, P.off_end = pl.ops_floats;
+  P.tables = pl.tables, P.table_ints = pl.table_ints;
+  const size_t sm = smem_bytes<N, BB>(pl.Nq, pl.ops_smem, pl.table_ints);
+  k_fused_stage<N, BB><<<pl.grid, FusedCfg<N>::T, sm, st>>>(P);
+  return check_launch("fused stage");
+}
+
+template <int N, bool BB>
+static bbw_status prepare(FusedPlan &pl) {
+  int dev = 0, maxsm = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  // stage the longest prefix of whole operators that fits
+  const int bounds[5] = {0, pl.off_lift, pl.off_pq, pl.off_vq, pl.ops_floats};
+  pl.ops_smem = 0;
+  for (int b = 4; b >= 0; --b)
+    if (smem_bytes<N, BB>(pl.Nq, bounds[b], pl.table_ints) <= (size_t)maxsm) {
+      pl.ops_smem = bounds[b];
+      break;
+    }
+  const size_t sm = smem_bytes<N, BB>(pl.Nq, pl.ops_smem, pl.table_ints);
+  if (sm > (size_t)maxsm)
+    return set_error(BBW_ERR_UNSUPPORTED, "fused stage: element tile does not fit in shared memory");
+  cudaError_t e = cudaFuncSetAttribute(k_fused_stage<N, BB>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return set_cuda_error(e, "fused stage attribute");
+  const int ntiles = cdiv(pl.K, TILE_E);
+  pl.grid = std::min(ntiles, nsm > 0 ? nsm : 148);
+  pl.smem = sm;
+  return BBW_OK;
+}
+
+int fused_warps(int N) {
+  switch (N) {
+    case 1: return FusedCfg<1>::W;
+    case 2: return FusedCfg<2>::W;
+    case 3: return FusedCfg<3>::W;
+    case 4: return FusedCfg<4>::W;
+    case 5: return FusedCfg<5>::W;
+    case 6: return FusedCfg<6>::W;
+    case 7: return FusedCfg<7>::W;
+    case 8: return FusedCfg<8>::W;
+  }
+  return 0;
+}
+
+#define FUSED_SWITCH(FN, ...)                                        \
+  switch (pl.N * 2 + (pl.bb ? 1 : 0)) {                              \
+    case 2: return FN<1, false>(__VA_ARGS__);                        \
+    case 3: return FN<1, true>(__VA_ARGS__);                         \
+    case 4: return FN<2, false>(__VA_ARGS__);                        \
+    case 5: return FN<2, true>(__VA_ARGS__);                         \
+    case 6: return FN<3, false>(__VA_ARGS__);                        \
+    case 7: return FN<3, true>(__VA_ARGS__);                         \
+    case 8: return FN<4, false>(__VA_ARGS__);                        \
+    case 9: return FN<4, true>(__VA_ARGS__);                         \
+    case 10: return FN<5, false>(__VA_ARGS__);                       \
+    case 11: return FN<5, true>(__VA_ARGS__);                        \
+    case 12: return FN<6, false>(__VA_ARGS__);                       \
+    case 13: return FN<6, true>(__VA_ARGS__);                        \
+    case 14: return FN<7, false>(__VA_ARGS__);                       \
+    case 15: return FN<7, true>(__VA_ARGS__);                        \
+    case 16: return FN<8, false>(__VA_ARGS__);                       \
+    case 17: return FN<8, true>(__VA_ARGS__);                        \
+  }                                                                  \
+  return set_error(BBW_ERR_UNSUPPORTED, "fused stage: N out of range");
+
+bbw_status fused_prepare(FusedPlan &pl) { FUSED_SWITCH(prepare, pl) }
+
+bbw_status fused_launch(const FusedPlan &pl, const float *Qin, float *Qout, float *res, float fa,
+                        float fb, float fdt, cudaStream_t st) {
+  FUSED_SWITCH(launch_fused, pl, Qin, Qout, res, fa, fb, fdt, st)
+}
+
+}  // namespace bbw

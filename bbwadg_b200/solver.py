@@ -1,0 +1,148 @@
+"""Host API mirroring the reference's solver entry points (cpp/include/fem.h:49-70).
+
+    reference                                 here
+    WaveInitOCCA3d + InitWADG_subelem         WaveSolver(problem)
+    WaveSetData3d(Q)                          solver.set_data(Q)
+    RK_step_WADG_subelem(mesh, rka, rkb, dt)  solver.rk_step(rka, rkb, dt)
+    Wave_RK(mesh, FinalTime, dt, 1)           solver.wave_rk(final_time, dt)
+    WaveGetData3d(mesh, Q)                    solver.get_data()   (raw coefficients)
+
+All work runs in the native library on the GPU (one fused kernel per LSRK
+stage); there is no CPU path.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .problem import np_of
+
+RK4A = (0.0,
+        -567301805773.0 / 1357537059087.0,
+        -2404267990393.0 / 2016746695238.0,
+        -3550918686646.0 / 2091501179385.0,
+        -1275806237668.0 / 842570457699.0)
+RK4B = (1432997174477.0 / 9575080441755.0,
+        5161836677717.0 / 13612068292357.0,
+        1720146321549.0 / 2090206949498.0,
+        3134564353537.0 / 4481467310338.0,
+        2277821191437.0 / 14882151754819.0)
+RK4C = (0.0,
+        1432997174477.0 / 9575080441755.0,
+        2526269341429.0 / 6820363962896.0,
+        2006345519317.0 / 3224310063776.0,
+        2802321613138.0 / 2924317926251.0,
+        1.0)
+
+VARIANTS = {"nodal": 0, "bb": 1}
+BCS = {"pressure_release": 0, "rigid": 1}
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, np.int32)
+
+
+class WaveSolver:
+    """Fused-stage solver context for one mesh / operator set on the current GPU."""
+
+    def __init__(self, problem=None, *, N=None, K=None, Nq=None, variant=None, ops=None,
+                 vgeo=None, fgeo=None, vmapP=None, c2q=None, Jq=None, bc="pressure_release"):
+        if problem is not None:
+            N, K, Nq = problem.N, problem.K, problem.Nq
+            variant = variant or problem.variant
+            ops = problem.ops_dict() if ops is None else ops
+            vgeo, fgeo = problem.mesh["vgeo"], problem.mesh["fgeo"]
+            vmapP, c2q = problem.mesh["vmapP"], problem.c2q
+        self.N, self.K, self.Nq, self.variant = N, K, Nq, variant
+        self.Np = np_of(N)
+        keep = {}
+
+        def f(a):
+            keep[id(a)] = a = _f32(a)
+            return a.ctypes.data
+
+        def i(a):
+            keep[id(a)] = a = _i32(a)
+            return a.ctypes.data
+
+        md = _lib.MeshDesc(N=N, K=K, Nq=Nq, vgeo=f(vgeo), fgeo=f(fgeo), Fmask=i(ops["Fmask"]),
+                           vmapP=i(vmapP), c2q=f(c2q), Jq=f(Jq) if Jq is not None else None)
+        od = _lib.OpsDesc(Vq=f(ops["Vq"]), Pq=f(ops["Pq"]))
+        if variant == "nodal":
+            od.Dr, od.Ds, od.Dt, od.LIFT = f(ops["Dr"]), f(ops["Ds"]), f(ops["Dt"]), f(ops["LIFT"])
+        else:
+            od.D_ids1, od.D_ids2 = i(ops["D_ids1"]), i(ops["D_ids2"])
+            od.D_ids3, od.D_ids4 = i(ops["D_ids3"]), i(ops["D_ids4"])
+            od.Dvals4 = f(ops["Dvals4"])
+            od.EEL_nnz = int(np.asarray(ops["EEL_ids"]).size // self.Np)
+            od.L0_nnz = int(np.asarray(ops["L0_ids"]).size // ((N + 1) * (N + 2) // 2))
+            od.EEL_ids, od.EEL_vals = i(ops["EEL_ids"]), f(ops["EEL_vals"])
+            od.L0_ids, od.L0_vals = i(ops["L0_ids"]), f(ops["L0_vals"])
+        h = ctypes.c_void_p()
+        _lib.call("bbw_create", ctypes.byref(md), ctypes.byref(od), VARIANTS[variant], BCS[bc],
+                  ctypes.byref(h))
+        self._h = h
+        del keep
+
+    # ---- reference-named entry points
+    def set_data(self, Q):
+        """WaveSetData3d: host state [K][4][Np] -> device."""
+        Q = _f32(Q)
+        assert Q.size == self.K * 4 * self.Np
+        _lib.call("bbw_set_state", self._h, Q.ctypes.data)
+
+    def get_data(self):
+        """WaveGetData3d (raw coefficients; BB -> nodal is Problem.to_nodal)."""
+        Q = np.empty(self.K * 4 * self.Np, np.float32)
+        _lib.call("bbw_get_state", self._h, Q.ctypes.data)
+        return Q
+
+    def set_residual(self, r):
+        r = _f32(r)
+        _lib.call("bbw_set_residual", self._h, r.ctypes.data)
+
+    def get_residual(self):
+        r = np.empty(self.K * 4 * self.Np, np.float32)
+        _lib.call("bbw_get_residual", self._h, r.ctypes.data)
+        return r
+
+    def rk_step(self, rka, rkb, fdt):
+        """RK_step_WADG_subelem: one fused LSRK stage (asynchronous)."""
+        _lib.call("bbw_stage", self._h, float(rka), float(rkb), float(fdt))
+
+    def steps(self, dt, nsteps):
+        """nsteps LSRK45 steps of size dt (CUDA-graph replay; asynchronous)."""
+        _lib.call("bbw_steps", self._h, float(dt), int(nsteps))
+
+    def wave_rk(self, final_time, dt):
+        """Wave_RK: steps of dt until final_time, last step shortened."""
+        _lib.call("bbw_run", self._h, float(final_time), float(dt))
+
+    def sync(self):
+        _lib.call("bbw_sync", self._h)
+
+    def device_state(self):
+        q, r, s = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        _lib.call("bbw_device_state", self._h, ctypes.byref(q), ctypes.byref(r), ctypes.byref(s))
+        return q.value, r.value, s.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.call("bbw_destroy", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -1,0 +1,308 @@
+#!/usr/bin/env python3
+"""Benchmark: acoustic WADG LSRK45 step, N=5, 32^3 x 6 affine tets (K=196608).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  Metric: DOF-stage updates per second,
+K * Np * 4 fields * 5 stages * steps / seconds, the reference's own per-DOF
+normalisation (cpp/src/WaveOKL3d.cpp:1763).  Workload (the configuration the
+metric is quoted on): N=5 (Np=56, Nq=95 from the reference's degree-11 tet
+rule), [-1,1]^3 split into 32^3 hexes x 6 tets, c^2 = 1 + 0.5 sin sin sin +
+0.5 U(0,1) per element (seeded), Gaussian pulse, p = 0 walls, FP32 state.
+The state (3 x 176 MB) exceeds the 126 MB L2, so no flush is needed between
+steps.
+
+* value      device-timed throughput of the fused stage kernels, inputs
+             resident in HBM (CUDA events on the solver's stream, max over
+             ranks, weak scaling: each rank advances its own copy of the
+             workload, one shot per GPU);
+* e2e        the same run through the public API with host buffers: the
+             initial state is copied in from pinned host memory and the final
+             state read back inside the timed region;
+* roofline   the fused stage kernel against the measured HBM copy bandwidth;
+             algorithmic bytes per element-stage 64 Np + 4 Nq + 132;
+* cpu_baseline  the reference's own OKL kernels (oracle/_ref, built from the
+             reference sources, OpenMP over elements) on this host's cores,
+             on a bounded sample (16^3 x 6 tets, same N and operators).
+
+--impl reference runs only that CPU path (rank 0; other ranks exit 0).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_ORDER, N_HEX = 5, 32
+SAMPLE_HEX = 16
+
+
+def algorithmic_bytes_per_element(Np, Nq):
+    # Q read + write, res read + write (4 fields, FP32), c2 at cubature
+    # points, vgeo (9) + fgeo (16) floats, neighbour + permutation codes
+    return 64 * Np + 4 * Nq + 132
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def reference_rule(N):
+    """The reference's tabulated degree-2N+1 tet rule (from the golden
+    fixture produced by running the reference), so Nq matches its cost."""
+    p = os.path.join(ROOT, "tests", "golden", "ops_N%d.npz" % N)
+    if not os.path.exists(p):
+        return None, None
+    g = np.load(p)
+    nfq = int(g["Nfq"][0])
+    return (g["rq"], g["sq"], g["tq"], g["wq"]), (g["rfq"][:nfq], g["sfq"][:nfq], g["wfqFace"])
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def reference_cpu(steps, warmup, nhex=SAMPLE_HEX, N=N_ORDER, bern=0, timeout=900):
+    """The reference's own CPU path: oracle/_ref driver (reference host code +
+    OKL kernels translated and JIT-compiled with OpenMP), all host threads."""
+    from bbwadg_b200.mesh import kuhn_box, write_gmsh22
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_N%d_B%d" % (N, bern))
+    if not os.path.exists(exe):
+        return None, "oracle/_ref/ref_N%d_B%d not built" % (N, bern)
+    d = tempfile.mkdtemp()
+    msh = os.path.join(d, "box.msh")
+    write_gmsh22(msh, *kuhn_box(nhex))
+    cores = os.cpu_count() or 1
+    env = dict(os.environ, OMP_NUM_THREADS=str(cores))
+    p = subprocess.run([exe, "bench", msh, "--steps", str(steps), "--warmup", str(warmup),
+                        "--c2", "sine"], capture_output=True, text=True, env=env, timeout=timeout)
+    if p.returncode != 0:
+        return None, "reference run failed: " + p.stderr[-200:]
+    r = json.loads(p.stdout.strip().splitlines()[-1])
+    r["cores"] = cores
+    return r, None
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    r, err = reference_cpu(max(args.steps, 1), max(args.warmup, 0))
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return 0
+    v = r["dof_stage_per_s"]
+    sample = "N=%d, %d^3 x 6 tets (K=%d), %d LSRK45 steps after %d warm-up" % (
+        N_ORDER, SAMPLE_HEX, r["K"], r["steps"], args.warmup)
+    print(json.dumps({
+        "metric": "DOF-stage updates/s (acoustic WADG, affine tets, N=5)", "impl": "reference",
+        "value": v, "unit": "DOF-stage/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * r["seconds"] / r["steps"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": workload_config(args, "nodal"),
+        "cpu_baseline": {"value": v, "unit": "DOF-stage/s", "cores": r["cores"],
+                         "kind": "reference", "sample": sample},
+        "e2e": {"value": v, "unit": "DOF-stage/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0}}))
+    return 0
+
+
+def workload_config(args, variant):
+    nh = getattr(args, "hex", N_HEX)
+    return {"workload": "acoustic WADG LSRK45 step, N=%d, %d^3x6 affine tets, %s" % (
+                N_ORDER, nh, variant),
+            "N": N_ORDER, "K": 6 * nh ** 3, "Np": 56, "Nq": 95, "variant": variant,
+            "global_batch": args.gpus, "parallelism": "replicas (one shot per GPU)",
+            "l2_flush": "state 3x176 MB > L2", "bc": "pressure_release"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--variant", default="nodal", choices=["nodal", "bb"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--hex", type=int, default=N_HEX, help="hexes per direction (profiling cases)")
+    ap.add_argument("--variants", default="nodal,bb", help="variants to run, comma separated")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    args.warmup = max(args.warmup, 3)
+
+    import torch
+    import torch.distributed as dist
+    from bbwadg_b200 import WaveSolver, make_problem
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    cub, tri = reference_rule(N_ORDER)
+
+    results = {}
+    variants = [v for v in args.variants.split(",") if v]
+    if args.variant not in variants:
+        variants.insert(0, args.variant)
+    for variant in variants:
+        prob = make_problem(N_ORDER, args.hex, variant=variant, c2="sine", c2_jitter=0.5,
+                            seed=1234 + rank, cubature=cub, tri_cubature=tri, cfl=0.25)
+        K, Np, Nq = prob.K, prob.Np, prob.Nq
+        s = WaveSolver(prob)
+        s.set_data(prob.Q0)
+        qptr, rptr, stream_ptr = s.device_state()
+        stream = torch.cuda.ExternalStream(stream_ptr)
+        s.steps(prob.dt, args.warmup)
+        s.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        with ClockSampler(local) as clk:
+            e0.record(stream)
+            s.steps(prob.dt, args.steps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        dofs = K * Np * 4 * 5 * args.steps
+        launches = 5 * args.steps
+        # e2e: WaveSetData3d (pinned host -> device), steps, WaveGetData3d
+        pinned = torch.from_numpy(prob.Q0.copy()).pin_memory()
+        out = torch.empty_like(pinned).pin_memory()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.set_data(pinned.numpy())
+        s.steps(prob.dt, args.steps)
+        out.copy_(torch.from_numpy(s.get_data()))
+        t_e2e = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([t_e2e], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            t_e2e = float(t.item())
+        state_bytes = K * 4 * Np * 4
+        results[variant] = dict(ms=ms, K=K, Np=Np, Nq=Nq, dofs=dofs, launches=launches,
+                                clocks=clk.summary(), e2e_s=t_e2e, state_bytes=state_bytes,
+                                finite=bool(np.isfinite(out.numpy()).all()))
+        s.close()
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
+    peak, peak_kind = measured_peak()
+    head = results[args.variant]
+    K, Np, Nq = head["K"], head["Np"], head["Nq"]
+    value = world * head["dofs"] / (head["ms"] / 1e3)
+    per_launch_s = head["ms"] / 1e3 / head["launches"]
+    alg_bytes = K * algorithmic_bytes_per_element(Np, Nq)
+    achieved = alg_bytes / per_launch_s / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "fused_stage_N5_dram.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            t = json.load(f).get("%s_bytes_per_element" % args.variant)
+        traffic = None if t is None else t * K
+    line = {
+        "metric": "DOF-stage updates/s (acoustic WADG, affine tets, N=5)",
+        "value": value, "unit": "DOF-stage/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms"] / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": workload_config(args, args.variant),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "kernel": "k_fused_stage<%d,%s>" % (N_ORDER, args.variant == "bb"),
+                     "peak_kind": peak_kind},
+        "e2e": {"value": world * head["dofs"] / head["e2e_s"], "unit": "DOF-stage/s",
+                "h2d_bytes_per_step": head["state_bytes"] / args.steps,
+                "d2h_bytes_per_step": head["state_bytes"] / args.steps},
+        "gpu_launches": head["launches"],
+        "clocks": head["clocks"],
+        "side_by_side": {v: {"value": world * r["dofs"] / (r["ms"] / 1e3),
+                             "ms_per_step": r["ms"] / args.steps,
+                             "hbm_frac": K * algorithmic_bytes_per_element(Np, Nq) /
+                             (r["ms"] / 1e3 / r["launches"]) / 1e9 / peak,
+                             "finite": r["finite"]} for v, r in results.items()},
+    }
+    if not args.no_cpu_baseline and world == 1:
+        r, err = reference_cpu(1, 0)
+        if r is not None:
+            line["cpu_baseline"] = {
+                "value": r["dof_stage_per_s"], "unit": "DOF-stage/s", "cores": r["cores"],
+                "kind": "reference",
+                "sample": "N=5, %d^3 x 6 tets (K=%d), %d LSRK45 step, reference OKL kernels "
+                          "via oracle/_ref" % (SAMPLE_HEX, r["K"], r["steps"])}
+        else:
+            line["cpu_baseline"] = {"value": None, "unavailable": err}
+    print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,215 @@
+/* bbwadg.h - C ABI of the B200 acoustic WADG time step (affine tetrahedra).
+ *
+ * Drop-in boundary for the reference's time step (jlchan/bbwadg, cpp/):
+ *   - kernel-level entry points replace the OKL kernels the reference builds
+ *     with device.buildKernelFromSource() and launches positionally
+ *     (cpp/src/WaveOKL3d.cpp:1653-1674, 2084-2106); arguments keep the
+ *     reference's order, meaning and array layouts, all pointers are device
+ *     pointers, the polynomial degree N is a runtime argument instead of the
+ *     p_N define;
+ *   - the solver context replaces the module-level device buffers and the
+ *     host API of cpp/include/fem.h:49-70 (WaveInitOCCA3d, InitWADG_subelem,
+ *     WaveSetData3d, RK_step_WADG_subelem, Wave_RK, WaveGetData3d) with a
+ *     fused one-kernel-per-stage path;
+ *   - setup entry points restate the reference's host setup (mesh
+ *     connectivity, geometric factors, operators).
+ *
+ * Layouts (all as in the reference):
+ *   state   Q[k][fld][n] = Q[n + fld*Np + k*Np*4], fld in {p,u,v,w}, FP32
+ *   vgeo    [K][9]  {rx,ry,rz,sx,sy,sz,tx,ty,tz}      (WaveOKL3d.cpp:1561)
+ *   fgeo    [K][4][4] {Fscale=sJ/J, nx, ny, nz}       (WaveOKL3d.cpp:1584)
+ *   Fmask   [4][Nfp] face-major volume node ids       (StartUp3d.cpp:174)
+ *   vmapP   [K][4*Nfp] state index of the + trace     (WaveOKL3d.cpp:1590)
+ *   Dr,Ds,Dt [Np x Np], LIFT [Np x 4Nfp], Vq [Nq x Np], Pq [Np x Nq],
+ *           column-major (Dr[n + m*Np])
+ *   c2q, Jq [K][Nq]                                   (WaveOKL3d.cpp:464)
+ *   BB:     D_ids1..4 int4[Np], Dvals4 float4[Np], EEL_ids/vals [Np x EEL_nnz],
+ *           L0_ids/vals [Nfp x L0_nnz], cEL [N+1], slice_ids int4[Np]
+ *
+ * Every function returns a status code and never throws.  Kernel-level
+ * functions are asynchronous on the given stream (NULL = legacy default
+ * stream), like OCCA kernel launches.
+ */
+#ifndef BBWADG_H
+#define BBWADG_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BBW_MAX_N 8
+
+typedef enum bbw_status {
+  BBW_OK = 0,
+  BBW_ERR_ARG = 1,          /* invalid argument or size */
+  BBW_ERR_CUDA = 2,         /* CUDA runtime error (see bbw_last_error) */
+  BBW_ERR_NOMEM = 3,        /* device or host allocation failed */
+  BBW_ERR_STATE = 4,        /* call out of sequence (e.g. no state set) */
+  BBW_ERR_MESH = 5,         /* inconsistent mesh (orientation, pairing) */
+  BBW_ERR_NUMERIC = 6,      /* operator construction failed */
+  BBW_ERR_UNSUPPORTED = 7,  /* size or option outside the supported range */
+  BBW_ERR_TIMEOUT = 8       /* a bounded device wait gave up */
+} bbw_status;
+
+enum { BBW_NODAL = 0, BBW_BB = 1 };
+/* boundary condition on faces whose + trace is the element itself:
+ * PRESSURE_RELEASE is the reference's (p = 0, WaveKernels.okl:211-214),
+ * RIGID is u.n = 0 */
+enum { BBW_BC_PRESSURE_RELEASE = 0, BBW_BC_RIGID = 1 };
+
+const char *bbw_status_string(bbw_status s);
+/* message of the last error raised on the calling thread ("" if none) */
+const char *bbw_last_error(void);
+/* library version string */
+const char *bbw_version(void);
+
+/* ---------------------------------------------------------------- setup */
+
+/* Element-to-element / element-to-face connectivity from EToV [K][4]
+ * (0-based).  Replaces FacePair3d, cpp/src/Mesh3d.cpp:335-410; boundary
+ * faces map to themselves. */
+bbw_status bbw_mesh_connect(int Nv, int K, const int *EToV, int *EToE, int *EToF);
+
+/* Affine geometric factors.  Writes vgeo [K][9] and fgeo [K][4][4] as packed
+ * in cpp/src/WaveOKL3d.cpp:1530-1589 (FP32), node coordinates x,y,z [K][Np]
+ * (FP64, cpp/src/StartUp3d.cpp:543-574; optional, need r,s,t) and
+ * dt = 0.25/((N+1)^2 max Fscale) (cpp/src/WaveOKL3d.cpp:1677).  Any output
+ * pointer may be NULL.  Returns BBW_ERR_MESH for non-positive Jacobians. */
+bbw_status bbw_mesh_geometry(int N, int K, const double *VX, const double *VY,
+                             const double *VZ, const int *EToV, const double *r,
+                             const double *s, const double *t, float *vgeo, float *fgeo,
+                             double *x, double *y, double *z, float *dt_out);
+
+/* Trace map vmapP [K][4Nfp] in state indexing (cpp/src/StartUp3d.cpp:643-741
+ * followed by the remap of cpp/src/WaveOKL3d.cpp:1590-1603). */
+bbw_status bbw_mesh_vmapP(int N, int K, const int *EToE, const int *EToF, const int *Fmask,
+                          const double *x, const double *y, const double *z, int *vmapP);
+
+/* Reference-element operators for degree N (cpp/src/StartUp3d.cpp:4-510,
+ * cpp/src/WaveOKL3d.cpp:459-483, 894-897).  cub = {rq[Nq], sq, tq, wq} and
+ * tri = {rfq[Nfq], sfq, wfq} select the volume / face cubature; pass NULL to
+ * use a Stroud conical-product rule of degree 2N+1.  Arrays are read back by
+ * name with bbw_ops_get (dtype 0 = FP32 kernel layout, 1 = FP64 column-major,
+ * 2 = int32).  Names: Dr Ds Dt LIFT Vq_nodal Pq_nodal Vq_bb Pq_bb cEL
+ * Dvals4 EEL_vals L0_vals (FP32 and FP64), V VB invVB LIFTB EEL r s t rq sq tq
+ * wq rfq sfq wfq EEL_val_vec (FP64), Fmask D_ids1..4 EEL_ids L0_ids slice_ids
+ * EEL_id_vec faceVolPerm sizes (int32; sizes = {N,Np,Nfp,Nq,Nfq,EEL_nnz,
+ * L0_nnz,EEL_width,L0_width}). */
+typedef struct bbw_ops bbw_ops;
+bbw_status bbw_ops_build(int N, const double *cub, int Nq, const double *tri, int Nfq,
+                         bbw_ops **out);
+/* Copies array `name` into dst (capacity *count elements) and sets *count to
+ * its length; with dst == NULL only the length is returned. */
+bbw_status bbw_ops_get(const bbw_ops *ops, const char *name, int dtype, void *dst,
+                       long long *count);
+void bbw_ops_free(bbw_ops *ops);
+
+/* ------------------------------------------------ kernel-level entry points
+ * One-to-one replacements of the reference's OKL kernels; same argument
+ * order and meaning, device pointers, N at run time. */
+
+/* cpp/okl/WaveKernels.okl:44-153  rk_volume(K, vgeo, Dr, Ds, Dt, Q, rhsQ) */
+bbw_status bbw_rk_volume(int N, int K, const float *vgeo, const float *Dr, const float *Ds,
+                         const float *Dt, const float *Q, float *rhsQ, void *stream);
+
+/* cpp/okl/WaveKernels.okl:156-260  rk_surface(K, fgeo, Fmask, vmapP, LIFT, Q, rhsQ);
+ * rhsQ += LIFT * flux.  bc selects the wall condition (reference: 0). */
+bbw_status bbw_rk_surface(int N, int K, int bc, const float *fgeo, const int *Fmask,
+                          const int *vmapP, const float *LIFT, const float *Q, float *rhsQ,
+                          void *stream);
+
+/* cpp/okl/WaveKernels.okl:262-313  rk_update(K, fa, fb, fdt, rhsQ, resQ, Q) */
+bbw_status bbw_rk_update(int N, int K, float fa, float fb, float fdt, const float *rhsQ,
+                         float *resQ, float *Q, void *stream);
+
+/* cpp/okl/WaveKernelsWADG.okl:1760-1887
+ * rk_update_WADG(K, Vq, Pq, Jq, c2q, fa, fb, fdt, rhsQ, resQ, Q) */
+bbw_status bbw_rk_update_wadg(int N, int K, int Nq, const float *Vq, const float *Pq,
+                              const float *Jq, const float *c2q, float fa, float fb, float fdt,
+                              const float *rhsQ, float *resQ, float *Q, void *stream);
+
+/* cpp/okl/WaveKernels.okl:344-474
+ * rk_volume_bern(K, vgeo, D1_ids, D2_ids, D3_ids, D4_ids, Dvals, Q, rhsQ) */
+bbw_status bbw_rk_volume_bern(int N, int K, const float *vgeo, const int *D_ids1,
+                              const int *D_ids2, const int *D_ids3, const int *D_ids4,
+                              const float *Dvals4, const float *Q, float *rhsQ, void *stream);
+
+/* cpp/okl/WaveKernels.okl:479-647  rk_surface_bern(K, fgeo, Fmask, vmapP,
+ * slice_ids, EEL_ids, EEL_vals, L0_ids, L0_vals, cEL, Q, rhsQ); overwrites
+ * rhsQ with rhsQ + BB lift of the flux.  EEL_nnz / L0_nnz are the p_EEL_nnz
+ * / p_L0_nnz defines (cpp/src/WaveOKL3d.cpp:1625-1626). */
+bbw_status bbw_rk_surface_bern(int N, int K, int bc, const float *fgeo, const int *Fmask,
+                               const int *vmapP, const int *slice_ids, int EEL_nnz,
+                               const int *EEL_ids, const float *EEL_vals, int L0_nnz,
+                               const int *L0_ids, const float *L0_vals, const float *cEL,
+                               const float *Q, float *rhsQ, void *stream);
+
+/* ---------------------------------------------------------- solver context
+ * Owns device copies of the mesh arrays and operators, the state Q (double
+ * buffered) and the LSRK residual res.  One stream per context; contexts
+ * share no state. */
+typedef struct bbw_ctx bbw_ctx;
+
+typedef struct bbw_mesh_desc {
+  int N, K, Nq;
+  const float *vgeo;  /* [K][9]    host */
+  const float *fgeo;  /* [K][4][4] host */
+  const int *Fmask;   /* [4][Nfp]  host */
+  const int *vmapP;   /* [K][4Nfp] host */
+  const float *c2q;   /* [K][Nq]   host */
+  const float *Jq;    /* [K][Nq]   host, NULL = all ones (affine) */
+} bbw_mesh_desc;
+
+typedef struct bbw_ops_desc {
+  /* nodal (variant BBW_NODAL) */
+  const float *Dr, *Ds, *Dt, *LIFT;
+  /* Bernstein-Bezier (variant BBW_BB) */
+  const int *D_ids1, *D_ids2, *D_ids3, *D_ids4;
+  const float *Dvals4;
+  int EEL_nnz, L0_nnz;
+  const int *EEL_ids, *L0_ids;
+  const float *EEL_vals, *L0_vals;
+  /* WADG projection for the chosen basis */
+  const float *Vq, *Pq;
+} bbw_ops_desc;
+
+/* Uploads mesh and operators (cpp/src/WaveOKL3d.cpp:1400-1615 and
+ * :894-909) to the current CUDA device; state and residual start at zero. */
+bbw_status bbw_create(const bbw_mesh_desc *mesh, const bbw_ops_desc *ops, int variant, int bc,
+                      bbw_ctx **out);
+bbw_status bbw_destroy(bbw_ctx *ctx);
+
+/* WaveSetData3d / WaveGetData3d (cpp/src/WaveOKL3d.cpp:2527-2537): copy the
+ * state from / to host memory ([K][4][Np] FP32).  Synchronous. */
+bbw_status bbw_set_state(bbw_ctx *ctx, const float *Q_host);
+bbw_status bbw_get_state(bbw_ctx *ctx, float *Q_host);
+/* Residual res (LSRK45 register) from / to host memory; zero after create. */
+bbw_status bbw_set_residual(bbw_ctx *ctx, const float *res_host);
+bbw_status bbw_get_residual(bbw_ctx *ctx, float *res_host);
+
+/* RK_step_WADG_subelem (cpp/src/WaveOKL3d.cpp:2084-2109): one LSRK stage
+ * res = fa*res + fdt*P(c2 rhs), Q += fb*res, as one fused kernel.
+ * Asynchronous on the context's stream. */
+bbw_status bbw_stage(bbw_ctx *ctx, float fa, float fb, float fdt);
+
+/* nsteps full LSRK45 steps of size dt (the time loop of Wave_RK,
+ * cpp/src/WaveOKL3d.cpp:2030-2079, with coefficients cast to float as at
+ * :2053-2055).  Asynchronous; captured once as a CUDA graph per nsteps. */
+bbw_status bbw_steps(bbw_ctx *ctx, float dt, int nsteps);
+
+/* Wave_RK(mesh, FinalTime, dt) semantics: steps of dt until FinalTime with
+ * the last step shortened to land on it (cpp/src/WaveOKL3d.cpp:2048). */
+bbw_status bbw_run(bbw_ctx *ctx, double final_time, float dt);
+
+/* Waits for the context's stream. */
+bbw_status bbw_sync(bbw_ctx *ctx);
+
+/* Device pointers of the current state and residual ([K][4][Np]) and the
+ * context's cudaStream_t, for zero-copy interop.  Valid until the next
+ * stage. */
+bbw_status bbw_device_state(bbw_ctx *ctx, float **Q, float **res, void **stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BBWADG_H */

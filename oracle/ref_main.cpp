@@ -206,6 +206,8 @@ int main(int argc, char **argv) {
     w.f64v("tq", mesh->tq);
     w.f64v("wq", mesh->wq);
     w.f64v("wfqFace", mesh->wfqFace);
+    w.f64v("rfq", mesh->rfq);
+    w.f64v("sfq", mesh->sfq);
     w.f64("V64", mesh->V);
     w.f64("Dr64", mesh->Dr);
     w.f64("Ds64", mesh->Ds);

@@ -33,7 +33,7 @@ from bbwadg_b200.mesh import kuhn_box, write_gmsh22  # noqa: E402
 REF = os.path.join(ROOT, "oracle", "_ref")
 F32_OPS = ["Dr", "Ds", "Dt", "LIFT", "Fmask", "D_ids1", "D_ids2", "D_ids3", "D_ids4", "Dvals4",
            "EEL_ids", "EEL_vals", "L0_ids", "L0_vals", "cEL", "slice_ids"]
-NODE_OPS = ["r", "s", "t", "rq", "sq", "tq", "wq", "wfqFace", "EEL_val_vec", "EEL_id_vec",
+NODE_OPS = ["r", "s", "t", "rq", "sq", "tq", "wq", "wfqFace", "rfq", "sfq", "EEL_val_vec", "EEL_id_vec",
             "faceVolPerm", "rk"]
 F64_OPS = ["V64", "Dr64", "Ds64", "Dt64", "LIFT64", "VB64", "invVB64", "Vq64"]
 

@@ -1,0 +1,115 @@
+"""Fused one-kernel-per-stage path (bbw_create / bbw_stage / bbw_steps /
+bbw_run) against the reference's own time loop (golden) and the C
+restatement.  FP32 tolerance: 1e-5 relative L2."""
+import numpy as np
+import pytest
+from conftest import golden, ref_ops, rel_l2
+
+from bbwadg_b200 import RK4A, RK4B, WaveSolver, make_problem
+from bbwadg_b200.mesh import kuhn_box
+from bbwadg_b200.problem import build_operators, connect_and_geometry, cavity_mode
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def ref_box4_solver(variant):
+    r = golden("run_N3_box4.npz")
+    ops = ref_ops(3, variant)
+    m = connect_and_geometry(3, *kuhn_box(4), build_operators(3))
+    s = WaveSolver(N=3, K=384, Nq=int(ops["Nq"][0]), variant=variant, ops=ops, vgeo=m["vgeo"],
+                   fgeo=m["fgeo"], vmapP=m["vmapP"], c2q=r["c2q"])
+    return s, r
+
+
+@pytest.mark.parametrize("variant", ["nodal", "bb"])
+def test_one_stage_matches_reference(cuda, variant):
+    s, r = ref_box4_solver(variant)
+    s.set_data(r["Q0_" + variant])
+    dt = float(r["dt"][0])
+    s.rk_step(np.float32(RK4A[0]), np.float32(RK4B[0]), dt)
+    assert rel_l2(s.get_data(), r["Q1stage_" + variant]) < TOL
+    assert rel_l2(s.get_residual(), r["res1stage_" + variant]) < TOL
+    s.close()
+
+
+@pytest.mark.parametrize("variant", ["nodal", "bb"])
+def test_100_steps_match_reference(cuda, variant):
+    """C1-shaped run (N=3, Gaussian pulse, sine c^2, p=0 walls) on 4^3 x 6
+    tets: 100 LSRK45 steps through the CUDA-graph path vs the reference."""
+    s, r = ref_box4_solver(variant)
+    s.set_data(r["Q0_" + variant])
+    s.steps(float(r["dt"][0]), 100)
+    assert rel_l2(s.get_data(), r["Q100_" + variant]) < TOL
+    s.close()
+
+
+@pytest.mark.parametrize("N", [4, 5])
+@pytest.mark.parametrize("variant", ["nodal", "bb"])
+@pytest.mark.parametrize("bc", ["pressure_release", "rigid"])
+def test_fused_matches_oracle(cuda, N, variant, bc):
+    from oracle import Oracle
+    p = make_problem(N, 4, variant=variant, c2="sine", c2_jitter=0.5, seed=3)
+    orc = Oracle(N, p.K, p.ops_dict(), p.geo_dict(), variant=variant, bc=1 if bc == "rigid" else 0)
+    q_ref, _ = orc.run(p.Q0.copy(), p.dt, 50)
+    s = WaveSolver(p, bc=bc)
+    s.set_data(p.Q0)
+    s.steps(p.dt, 10)
+    assert rel_l2(s.get_data(), q_ref) < TOL
+    s.close()
+
+
+def test_graph_steps_equal_stage_loop(cuda):
+    p = make_problem(3, 3, variant="nodal")
+    a = WaveSolver(p)
+    b = WaveSolver(p)
+    a.set_data(p.Q0)
+    b.set_data(p.Q0)
+    a.steps(p.dt, 3)
+    for _ in range(3):
+        for i in range(5):
+            b.rk_step(np.float32(RK4A[i]), np.float32(RK4B[i]), p.dt)
+    assert np.array_equal(a.get_data(), b.get_data())
+    assert np.array_equal(a.get_residual(), b.get_residual())
+
+
+def test_wave_rk_lands_on_final_time(cuda):
+    p = make_problem(3, 2, variant="nodal")
+    a, b = WaveSolver(p), WaveSolver(p)
+    a.set_data(p.Q0)
+    b.set_data(p.Q0)
+    T = 2.5 * p.dt
+    a.wave_rk(T, p.dt)
+    b.steps(p.dt, 2)
+    last = np.float32(T - 2 * np.float64(np.float32(p.dt)))
+    b.steps(float(last), 1)
+    assert rel_l2(a.get_data(), b.get_data()) < 1e-7
+
+
+def test_cavity_mode_converges_at_order_N_plus_1(cuda):
+    """Standing mode cos(pi x)cos(pi y)cos(pi z)cos(sqrt3 pi t), exact for the
+    p = 0 wall on [-0.5,0.5]^3 (cpp/main_subelem.cpp:3-5), c^2 = 1."""
+    N, T = 3, 0.1
+    errs = []
+    for n in (2, 4):
+        p = make_problem(N, n, variant="nodal", c2="one", ic="cavity", lo=-0.5, hi=0.5)
+        s = WaveSolver(p)
+        s.set_data(p.Q0)
+        s.wave_rk(T, p.dt)
+        errs.append(p.l2_error(s.get_data(), T, cavity_mode)[0])
+        s.close()
+    rate = np.log2(errs[0] / errs[1])
+    assert rate > N + 0.5, (errs, rate)
+
+
+def test_nodal_and_bb_agree(cuda):
+    """Same polynomial space: after 5 steps the BB run, mapped to nodal
+    values, matches the nodal run to round-off times cond(VB)."""
+    pn = make_problem(4, 3, variant="nodal")
+    pb = make_problem(4, 3, variant="bb")
+    sn, sb = WaveSolver(pn), WaveSolver(pb)
+    sn.set_data(pn.Q0)
+    sb.set_data(pb.Q0)
+    sn.steps(pn.dt, 5)
+    sb.steps(pb.dt, 5)
+    assert rel_l2(pb.to_nodal(sb.get_data()), sn.get_data()) < 1e-4

@@ -1,0 +1,121 @@
+"""Kernel-level entry points (bbw_rk_*) on the GPU against the reference's
+own kernels (golden vectors from oracle/_ref) and, at larger sizes, against
+the C restatement.  Tolerance: 1e-5 relative L2 (FP32)."""
+import numpy as np
+import pytest
+from conftest import golden, ref_ops, rel_l2
+
+from bbwadg_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def dev(a, dtype=None):
+    import torch
+    a = np.ascontiguousarray(a)
+    t = torch.from_numpy(a.copy())
+    return t.cuda()
+
+
+def host(t):
+    import torch
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+def P(t):
+    return t.data_ptr()
+
+
+@pytest.mark.parametrize("N", [3, 5])
+def test_rk_volume_and_surface_nodal(cuda, N):
+    o, g, k = ref_ops(N, "nodal"), golden("mesh_box2_N%d.npz" % N), golden("kernels_N%d_box2.npz" % N)
+    Q = dev(k["Q_in"])
+    rhs = dev(np.zeros_like(k["Q_in"]))
+    _lib.call("bbw_rk_volume", N, 48, P(dev(g["vgeo"])), P(dev(o["Dr"])), P(dev(o["Ds"])),
+              P(dev(o["Dt"])), P(Q), P(rhs), None)
+    assert rel_l2(host(rhs), k["rk_volume.rhsQ"]) < TOL
+    rhs = dev(k["rhs_in"])
+    _lib.call("bbw_rk_surface", N, 48, 0, P(dev(g["fgeo"])), P(dev(o["Fmask"])), P(dev(g["vmapP"])),
+              P(dev(o["LIFT"])), P(Q), P(rhs), None)
+    assert rel_l2(host(rhs), k["rk_surface.rhsQ"]) < TOL
+
+
+@pytest.mark.parametrize("N", [3, 5])
+def test_rk_volume_and_surface_bern(cuda, N):
+    o, g, k = ref_ops(N, "bb"), golden("mesh_box2_N%d.npz" % N), golden("kernels_N%d_box2.npz" % N)
+    Q = dev(k["Q_in"])
+    rhs = dev(np.zeros_like(k["Q_in"]))
+    _lib.call("bbw_rk_volume_bern", N, 48, P(dev(g["vgeo"])), P(dev(o["D_ids1"])),
+              P(dev(o["D_ids2"])), P(dev(o["D_ids3"])), P(dev(o["D_ids4"])), P(dev(o["Dvals4"])),
+              P(Q), P(rhs), None)
+    assert rel_l2(host(rhs), k["rk_volume_bern.rhsQ"]) < TOL
+    rhs = dev(k["rhs_in"])
+    Np, Nfp = (N + 1) * (N + 2) * (N + 3) // 6, (N + 1) * (N + 2) // 2
+    _lib.call("bbw_rk_surface_bern", N, 48, 0, P(dev(g["fgeo"])), P(dev(o["Fmask"])),
+              P(dev(g["vmapP"])), P(dev(o["slice_ids"])), o["EEL_ids"].size // Np,
+              P(dev(o["EEL_ids"])), P(dev(o["EEL_vals"])), o["L0_ids"].size // Nfp,
+              P(dev(o["L0_ids"])), P(dev(o["L0_vals"])), P(dev(o["cEL"])), P(Q), P(rhs), None)
+    assert rel_l2(host(rhs), k["rk_surface_bern.rhsQ"]) < TOL
+
+
+@pytest.mark.parametrize("N", [3, 5])
+@pytest.mark.parametrize("variant", ["nodal", "bb"])
+def test_rk_update_wadg(cuda, N, variant):
+    o, g, k = ref_ops(N, variant), golden("mesh_box2_N%d.npz" % N), golden("kernels_N%d_box2.npz" % N)
+    rhs, res, Q = dev(k["rhs_in"]), dev(k["res_in"]), dev(k["Q_in"])
+    Nq = int(o["Nq"][0])
+    _lib.call("bbw_rk_update_wadg", N, 48, Nq, P(dev(o["Vq"])), P(dev(o["Pq"])), P(dev(g["Jq"])),
+              P(dev(g["c2q"])), float(k["fa"]), float(k["fb"]), float(k["dt"][0]), P(rhs), P(res),
+              P(Q), None)
+    t = "rk_update_WADG" + ("_bb" if variant == "bb" else "")
+    assert rel_l2(host(res), k[t + ".resQ"]) < TOL
+    assert rel_l2(host(Q), k[t + ".Q"]) < TOL
+
+
+def test_rk_update(cuda):
+    k = golden("kernels_N3_box2.npz")
+    rhs, res, Q = dev(k["rhs_in"]), dev(k["res_in"]), dev(k["Q_in"])
+    _lib.call("bbw_rk_update", 3, 48, float(k["fa"]), float(k["fb"]), float(k["dt"][0]), P(rhs),
+              P(res), P(Q), None)
+    assert rel_l2(host(res), k["rk_update.resQ"]) < TOL
+    assert rel_l2(host(Q), k["rk_update.Q"]) < TOL
+
+
+def test_kernels_against_oracle_larger_mesh(cuda):
+    """N=4 on 6^3 x 6 tets with the product setup: every kernel vs the C
+    restatement (FP32, same summation order)."""
+    from oracle import Oracle
+    from bbwadg_b200 import make_problem
+    for variant in ("nodal", "bb"):
+        p = make_problem(4, 6, variant=variant)
+        ops, geo = p.ops_dict(), p.geo_dict()
+        orc = Oracle(4, p.K, ops, geo, variant=variant)
+        rng = np.random.default_rng(7)
+        q = rng.standard_normal(p.K * 4 * p.Np).astype(np.float32)
+        r0 = np.zeros_like(q)
+        orc.rk_volume(q, r0)
+        orc.rk_surface(q, r0)
+        Q, rhs = dev(q), dev(np.zeros_like(q))
+        if variant == "nodal":
+            _lib.call("bbw_rk_volume", 4, p.K, P(dev(geo["vgeo"])), P(dev(ops["Dr"])),
+                      P(dev(ops["Ds"])), P(dev(ops["Dt"])), P(Q), P(rhs), None)
+            _lib.call("bbw_rk_surface", 4, p.K, 0, P(dev(geo["fgeo"])), P(dev(ops["Fmask"])),
+                      P(dev(geo["vmapP"])), P(dev(ops["LIFT"])), P(Q), P(rhs), None)
+        else:
+            _lib.call("bbw_rk_volume_bern", 4, p.K, P(dev(geo["vgeo"])), P(dev(ops["D_ids1"])),
+                      P(dev(ops["D_ids2"])), P(dev(ops["D_ids3"])), P(dev(ops["D_ids4"])),
+                      P(dev(ops["Dvals4"])), P(Q), P(rhs), None)
+            _lib.call("bbw_rk_surface_bern", 4, p.K, 0, P(dev(geo["fgeo"])), P(dev(ops["Fmask"])),
+                      P(dev(geo["vmapP"])), P(dev(ops["slice_ids"])), ops["EEL_nnz"],
+                      P(dev(ops["EEL_ids"])), P(dev(ops["EEL_vals"])), ops["L0_nnz"],
+                      P(dev(ops["L0_ids"])), P(dev(ops["L0_vals"])), P(dev(ops["cEL"])), P(Q),
+                      P(rhs), None)
+        assert rel_l2(host(rhs), r0) < TOL, variant
+
+
+def test_empty_and_bad_arguments(cuda):
+    assert _lib.lib().bbw_rk_volume(5, 0, None, None, None, None, None, None, None) == 0
+    with pytest.raises(_lib.BBWError):
+        _lib.call("bbw_rk_volume", 11, 4, 1, 1, 1, 1, 1, 1, None)
