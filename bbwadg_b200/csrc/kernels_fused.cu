@@ -78,7 +78,6 @@ struct FusedParams {
   const int *__restrict__ nbr;      // [K][4]  (k2 << 8) | pattern, pattern 255 = boundary
   const float *__restrict__ c2q;    // [K][Nq] c2/J at the cubature points
   const float *__restrict__ ops;    // packed operators (global copy)
-  int ops_smem;                     // leading floats of ops staged in shared memory
   int off_lift, off_pq, off_vq, off_end;  // operator offsets in ops (floats)
   const int *__restrict__ tables;   // Fmask [NF] | patterns [npat][Nfp] | BB tables
   int table_ints;
@@ -99,7 +98,21 @@ struct FusedSmem {
 };
 
 // -------------------------------------------------------------- device code
-template <int N, bool BB>
+__device__ __forceinline__ void cp_async4(float *smem_dst, const float *gmem_src, bool valid) {
+  // 4-byte asynchronous copy; zero-fills the destination when !valid
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(gmem_src),
+               "r"(valid ? 4 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_all;\n" ::: "memory");
+}
+
+// OPS_SMEM: the packed operators are staged in shared memory (every
+// operator read is a shared-memory broadcast); otherwise they are read
+// through the read-only data path (large N or large cubature rules).
+template <int N, bool BB, bool OPS_SMEM>
 __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P) {
   using C = FusedCfg<N>;
   using L = FusedSmem<N, BB>;
@@ -116,28 +129,21 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int r0 = warp * R;
 
-  // stage operators and tables once per CTA
-  for (int i = tid; i < P.ops_smem / 4; i += T)
-    reinterpret_cast<float4 *>(sOps)[i] = __ldg(reinterpret_cast<const float4 *>(P.ops) + i);
+  // stage operators (when they fit) and tables once per CTA
+  if (OPS_SMEM)
+    for (int i = tid; i < P.off_end / 4; i += T)
+      reinterpret_cast<float4 *>(sOps)[i] = __ldg(reinterpret_cast<const float4 *>(P.ops) + i);
   for (int i = tid; i < P.table_ints; i += T) sTab[i] = __ldg(P.tables + i);
   const int *sFmask = sTab;
   const int *sPat = sTab + P.pat_off;
 
-  // operator blocks: from shared memory when staged there, otherwise through
-  // the L1 / read-only path (large N or large cubature rules)
-  auto opb = [&](int off, int end) -> const float * {
-    return end <= P.ops_smem ? sOps + off : P.ops + off;
-  };
-  const float *opVol = opb(0, P.off_lift);          // [W][Np][P3R]
-  const float *opLift = opb(P.off_lift, P.off_pq);  // [W][NF][PR]
-  const float *opPq = opb(P.off_pq, P.off_vq);      // [W][Nq][PR]
-  const float *opVq = opb(P.off_vq, P.off_end);     // [W][Np][PRQ]
-  const float *wVol = opVol + warp * Np * C::P3R;
-  const float *wLift = opLift + warp * NF * C::PR;
-  const float *wPq = opPq + warp * Nq * C::PR;
-  const float *wVq = opVq + warp * Np * PRQ;
-  // BB tables after the patterns: D ids int4 x4 [Np], Dvals float4 [Np],
-  // L0 [Nfp][L0nnz] ids/vals, EEL CSR per face
+  const float *opBase = OPS_SMEM ? (const float *)sOps : P.ops;
+  const float *wVol = opBase + warp * Np * C::P3R;              // [W][Np][P3R]
+  const float *wLift = opBase + P.off_lift + warp * NF * C::PR;  // [W][NF][PR]
+  const float *wPq = opBase + P.off_pq + warp * Nq * C::PR;      // [W][Nq][PR]
+  const float *wVq = opBase + P.off_vq + warp * Np * PRQ;        // [W][Np][PRQ]
+  // BB tables: D ids int4 [4][Np], Dvals float4 [Np], L0 [Nfp][L0nnz]
+  // ids / vals, EEL rows bucketed by face (CSR)
   const int *bbTab = sTab + P.bb_off;
 
   const int ntiles = cdiv(P.K, TILE_E);
@@ -146,55 +152,72 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
     const int ne = min(TILE_E, P.K - k0);
     __syncthreads();  // previous tile fully consumed (and operators staged)
 
-    // ---- 1. stage the tile: state (transposed), c2, geometry, neighbours
+    // ---- 1. per-element geometry and neighbour codes; state and c2 tiles
+    //         as asynchronous copies transposed to [row][element]
+    for (int i = tid; i < TILE_E * 9; i += T)
+      sGeo[(i / 9) * 25 + i % 9] = i < ne * 9 ? __ldg(P.vgeo + (size_t)k0 * 9 + i) : 0.f;
+    for (int i = tid; i < TILE_E * 16; i += T)
+      sGeo[(i / 16) * 25 + 9 + i % 16] = i < ne * 16 ? __ldg(P.fgeo + (size_t)k0 * 16 + i) : 0.f;
+    for (int i = tid; i < TILE_E * 4; i += T)
+      sNbr[i] = i < ne * 4 ? __ldg(P.nbr + (size_t)k0 * 4 + i) : 255;
     {
-      const float4 *Qg = reinterpret_cast<const float4 *>(P.Qin + (size_t)k0 * 4 * Np);
-      const int n4 = ne * Np;  // float4 per tile = ne * 4Np / 4
-      for (int i = tid; i < TILE_E * Np; i += T) {
-        const int e = (4 * i) / (4 * Np), fn = (4 * i) % (4 * Np);
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (i < n4) v = Qg[i];
-        sQ[(fn + 0) * ES + e] = v.x;
-        sQ[(fn + 1) * ES + e] = v.y;
-        sQ[(fn + 2) * ES + e] = v.z;
-        sQ[(fn + 3) * ES + e] = v.w;
+      const float *Qg = P.Qin + (size_t)k0 * 4 * Np;
+      constexpr int QIT = cdiv(TILE_E * 4 * Np, T);
+#pragma unroll 4
+      for (int j = 0; j < QIT; ++j) {
+        const int i = tid + j * T;
+        if (i < TILE_E * 4 * Np) {
+          const int e = i / (4 * Np), fn = i - e * (4 * Np);
+          const bool ok = e < ne;
+          cp_async4(&sQ[fn * ES + e], ok ? Qg + i : P.Qin, ok);
+        }
       }
       const float *cg = P.c2q + (size_t)k0 * Nq;
       for (int i = tid; i < TILE_E * Nq; i += T) {
-        const int e = i / Nq, q = i % Nq;
-        sC2[q * ES + e] = i < ne * Nq ? cg[i] : 0.f;
+        const int e = i / Nq, q = i - e * Nq;
+        const bool ok = e < ne;
+        cp_async4(&sC2[q * ES + e], ok ? cg + i : P.c2q, ok);
       }
-      for (int i = tid; i < TILE_E * 9; i += T)
-        sGeo[(i / 9) * 25 + i % 9] = i < ne * 9 ? P.vgeo[(size_t)k0 * 9 + i] : 0.f;
-      for (int i = tid; i < TILE_E * 16; i += T)
-        sGeo[(i / 16) * 25 + 9 + i % 16] = i < ne * 16 ? P.fgeo[(size_t)k0 * 16 + i] : 0.f;
-      for (int i = tid; i < TILE_E * 4; i += T)
-        sNbr[i] = i < ne * 4 ? P.nbr[(size_t)k0 * 4 + i] : 255;
     }
-    __syncthreads();
+    __syncthreads();  // neighbour codes visible
 
-    // ---- 2. contravariant velocities Ur, Us, Ut into sR rows [Np, 4Np)
-    for (int i = tid; i < TILE_E * Np; i += T) {
-      const int e = i & 31, n = i >> 5;
-      const float *G = sGeo + e * 25;
-      const float u = sQ[(Np + n) * ES + e], v = sQ[(2 * Np + n) * ES + e],
-                  w = sQ[(3 * Np + n) * ES + e];
-      sR[(Np + n) * ES + e] = u * G[0] + v * G[1] + w * G[2];
-      sR[(2 * Np + n) * ES + e] = u * G[3] + v * G[4] + w * G[5];
-      sR[(3 * Np + n) * ES + e] = u * G[6] + v * G[7] + w * G[8];
+    // ---- 2. neighbour face traces into registers (in flight together with
+    //         the asynchronous tile copies)
+    constexpr int FIT = cdiv(TILE_E * NF, T);
+    float nb[FIT][4];
+#pragma unroll
+    for (int j = 0; j < FIT; ++j) {
+      const int i = tid + j * T;
+      nb[j][0] = nb[j][1] = nb[j][2] = nb[j][3] = 0.f;
+      if (i < TILE_E * NF) {
+        const int e = i & 31, m = i >> 5, f = m / Nfp;
+        const int code = sNbr[e * 4 + f];
+        const int pat = code & 255;
+        if (pat != 255) {
+          const float *q2 = P.Qin + (size_t)(code >> 8) * 4 * Np + sPat[pat * Nfp + (m - f * Nfp)];
+          nb[j][0] = __ldg(q2);
+          nb[j][1] = __ldg(q2 + Np);
+          nb[j][2] = __ldg(q2 + 2 * Np);
+          nb[j][3] = __ldg(q2 + 3 * Np);
+        }
+      }
     }
+    cp_async_commit_wait_all();
+    __syncthreads();  // state and c2 tiles landed
 
     // ---- 3. upwind flux at the 4Nfp face nodes (Uflux = -pflux)
-    for (int i = tid; i < TILE_E * NF; i += T) {
+#pragma unroll
+    for (int j = 0; j < FIT; ++j) {
+      const int i = tid + j * T;
+      if (i >= TILE_E * NF) continue;
       const int e = i & 31, m = i >> 5, f = m / Nfp;
-      const int code = sNbr[e * 4 + f];
+      const int pat = sNbr[e * 4 + f] & 255;
       const int vM = sFmask[m];
       const float pM = sQ[vM * ES + e], uM = sQ[(Np + vM) * ES + e],
                   vvM = sQ[(2 * Np + vM) * ES + e], wM = sQ[(3 * Np + vM) * ES + e];
       const float *fg = sGeo + e * 25 + 9 + 4 * f;
       const float Fscale = fg[0], nx = fg[1], ny = fg[2], nz = fg[3];
       float pjump, Unjump;
-      const int pat = code & 255;
       if (pat == 255) {
         if (P.bc == BBW_BC_PRESSURE_RELEASE) {
           pjump = -2.f * pM;
@@ -204,14 +227,21 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
           Unjump = -2.f * (uM * nx + vvM * ny + wM * nz);
         }
       } else {
-        const int k2 = code >> 8;
-        const float *q2 = P.Qin + (size_t)k2 * 4 * Np + sPat[pat * Nfp + (m - f * Nfp)];
-        const float pP = __ldg(q2), uP = __ldg(q2 + Np), vP = __ldg(q2 + 2 * Np),
-                    wP = __ldg(q2 + 3 * Np);
-        pjump = pP - pM;
-        Unjump = (uP - uM) * nx + (vP - vvM) * ny + (wP - wM) * nz;
+        pjump = nb[j][0] - pM;
+        Unjump = (nb[j][1] - uM) * nx + (nb[j][2] - vvM) * ny + (nb[j][3] - wM) * nz;
       }
       sF[m * ES + e] = .5f * (pjump - Unjump) * Fscale;
+    }
+
+    // ---- 3b. contravariant velocities Ur, Us, Ut into sR rows [Np, 4Np)
+    for (int i = tid; i < TILE_E * Np; i += T) {
+      const int e = i & 31, n = i >> 5;
+      const float *G = sGeo + e * 25;
+      const float u = sQ[(Np + n) * ES + e], v = sQ[(2 * Np + n) * ES + e],
+                  w = sQ[(3 * Np + n) * ES + e];
+      sR[(Np + n) * ES + e] = u * G[0] + v * G[1] + w * G[2];
+      sR[(2 * Np + n) * ES + e] = u * G[3] + v * G[4] + w * G[5];
+      sR[(3 * Np + n) * ES + e] = u * G[6] + v * G[7] + w * G[8];
     }
     __syncthreads();
 
@@ -393,7 +423,16 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
     }
     __syncthreads();
 
-    // ---- 7. project back: rhs_p = Pq * (c2 p_q)
+    // ---- 7. project back: rhs_p = Pq * (c2 p_q); the residual tile is
+    //         fetched meanwhile for the stage update
+    constexpr int UIT = cdiv(TILE_E * Np, T);  // float4 per thread
+    const float4 *resg = reinterpret_cast<const float4 *>(P.res + (size_t)k0 * 4 * Np);
+    float4 rpre[UIT];
+#pragma unroll
+    for (int j = 0; j < UIT; ++j) {
+      const int i = tid + j * T;
+      rpre[j] = i < ne * Np ? resg[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
     {
       float acc[R];
 #pragma unroll
@@ -420,12 +459,14 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
 
     // ---- 8. LSRK stage update, coalesced: res = fa res + fdt rhs; Q += fb res
     {
-      float4 *resg = reinterpret_cast<float4 *>(P.res + (size_t)k0 * 4 * Np);
+      float4 *resw = reinterpret_cast<float4 *>(P.res + (size_t)k0 * 4 * Np);
       float4 *qg = reinterpret_cast<float4 *>(P.Qout + (size_t)k0 * 4 * Np);
-      const int n4 = ne * Np;
-      for (int i = tid; i < n4; i += T) {
+#pragma unroll
+      for (int j = 0; j < UIT; ++j) {
+        const int i = tid + j * T;
+        if (i >= ne * Np) continue;
         const int e = (4 * i) / (4 * Np), fn = (4 * i) % (4 * Np);
-        float4 r = resg[i], q;
+        float4 r = rpre[j], q;
         r.x = P.fa * r.x + P.fdt * sR[(fn + 0) * ES + e];
         r.y = P.fa * r.y + P.fdt * sR[(fn + 1) * ES + e];
         r.z = P.fa * r.z + P.fdt * sR[(fn + 2) * ES + e];
@@ -434,7 +475,7 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
         q.y = sQ[(fn + 1) * ES + e] + P.fb * r.y;
         q.z = sQ[(fn + 2) * ES + e] + P.fb * r.z;
         q.w = sQ[(fn + 3) * ES + e] + P.fb * r.w;
-        resg[i] = r;
+        resw[i] = r;
         qg[i] = q;
       }
     }
@@ -452,17 +493,21 @@ static size_t smem_bytes(int Nq, int ops_smem, int table_ints) {
 template <int N, bool BB>
 static bbw_status launch_fused(const FusedPlan &pl, const float *Qin, float *Qout, float *res,
                                float fa, float fb, float fdt, cudaStream_t st) {
+  const bool ops_smem = pl.ops_smem == pl.ops_floats;
   FusedParams P;
   P.K = pl.K, P.Nq = pl.Nq, P.RQ = pl.RQ, P.PRQ = pl.PRQ, P.bc = pl.bc, P.npat = pl.npat;
   P.pat_off = pl.pat_off, P.bb_off = pl.bb_off;
   P.fa = fa, P.fb = fb, P.fdt = fdt;
   P.Qin = Qin, P.Qout = Qout, P.res = res;
   P.vgeo = pl.vgeo, P.fgeo = pl.fgeo, P.nbr = pl.nbr, P.c2q = pl.c2q;
-  P.ops = pl.ops, P.ops_smem = pl.ops_smem;
+  P.ops = pl.ops;
   P.off_lift = pl.off_lift, P.off_pq = pl.off_pq, P.off_vq = pl.off_vq, P.off_end = pl.ops_floats;
   P.tables = pl.tables, P.table_ints = pl.table_ints;
   const size_t sm = smem_bytes<N, BB>(pl.Nq, pl.ops_smem, pl.table_ints);
-  k_fused_stage<N, BB><<<pl.grid, FusedCfg<N>::T, sm, st>>>(P);
+  if (ops_smem)
+    k_fused_stage<N, BB, true><<<pl.grid, FusedCfg<N>::T, sm, st>>>(P);
+  else
+    k_fused_stage<N, BB, false><<<pl.grid, FusedCfg<N>::T, sm, st>>>(P);
   return check_launch("fused stage");
 }
 
@@ -472,19 +517,19 @@ static bbw_status prepare(FusedPlan &pl) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  // stage the longest prefix of whole operators that fits
-  const int bounds[5] = {0, pl.off_lift, pl.off_pq, pl.off_vq, pl.ops_floats};
-  pl.ops_smem = 0;
-  for (int b = 4; b >= 0; --b)
-    if (smem_bytes<N, BB>(pl.Nq, bounds[b], pl.table_ints) <= (size_t)maxsm) {
-      pl.ops_smem = bounds[b];
-      break;
-    }
+  // operators in shared memory when they fit, else through the read-only path
+  pl.ops_smem = smem_bytes<N, BB>(pl.Nq, pl.ops_floats, pl.table_ints) <= (size_t)maxsm
+                    ? pl.ops_floats
+                    : 0;
   const size_t sm = smem_bytes<N, BB>(pl.Nq, pl.ops_smem, pl.table_ints);
   if (sm > (size_t)maxsm)
     return set_error(BBW_ERR_UNSUPPORTED, "fused stage: element tile does not fit in shared memory");
-  cudaError_t e = cudaFuncSetAttribute(k_fused_stage<N, BB>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = pl.ops_smem ? cudaFuncSetAttribute(k_fused_stage<N, BB, true>,
+                                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     (int)sm)
+                              : cudaFuncSetAttribute(k_fused_stage<N, BB, false>,
+                                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     (int)sm);
   if (e != cudaSuccess) return set_cuda_error(e, "fused stage attribute");
   const int ntiles = cdiv(pl.K, TILE_E);
   pl.grid = std::min(ntiles, nsm > 0 ? nsm : 148);

@@ -11,11 +11,22 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-5
 
 
-def dev(a, dtype=None):
+_KEEP = []  # device buffers must outlive the asynchronous launches that use them
+
+
+def dev(a):
     import torch
-    a = np.ascontiguousarray(a)
-    t = torch.from_numpy(a.copy())
-    return t.cuda()
+    t = torch.from_numpy(np.ascontiguousarray(a).copy()).cuda()
+    _KEEP.append(t)
+    return t
+
+
+@pytest.fixture(autouse=True)
+def _release_buffers():
+    yield
+    import torch
+    torch.cuda.synchronize()
+    _KEEP.clear()
 
 
 def host(t):
