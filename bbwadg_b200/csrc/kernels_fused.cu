@@ -51,7 +51,7 @@ __host__ __device__ constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }
 template <int N>
 struct FusedCfg {
   static constexpr int Np = NP(N), Nfp = NFP(N), NF = 4 * NFP(N);
-  static constexpr int W = N <= 3 ? 4 : 8;  // warps per CTA
+  static constexpr int W = N <= 3 ? 8 : 16;  // warps per CTA
   static constexpr int T = 32 * W;
   static constexpr int R = cdiv(Np, W);     // node rows per warp
   static constexpr int PR = round4(R);
