@@ -219,37 +219,40 @@ extern "C" bbw_status bbw_create(const bbw_mesh_desc *m, const bbw_ops_desc *o, 
       std::memcpy(&bits, &o->Dvals4[i], 4);
       tab.push_back(bits);
     }
+    // header, L0 and EEL as (shared-memory offset, value bits) pairs; the
+    // offsets are pre-multiplied by the kernel's element row stride
     const int L0 = o->L0_nnz;
-    tab.push_back(L0);
-    for (int nt = 0; nt < Nfp; ++nt)
-      for (int j = 0; j < L0; ++j) tab.push_back(o->L0_ids[nt + j * Nfp]);
-    for (int nt = 0; nt < Nfp; ++nt)
-      for (int j = 0; j < L0; ++j) {
-        int bits;
-        std::memcpy(&bits, &o->L0_vals[nt + j * Nfp], 4);
-        tab.push_back(bits);
-      }
+    auto bits = [](float v) {
+      int b;
+      std::memcpy(&b, &v, 4);
+      return b;
+    };
     // EEL as CSR with the nonzeros of each row bucketed by face
-    std::vector<int> ptr((size_t)Np * 5), col;
-    std::vector<float> val;
+    std::vector<int> ptr((size_t)Np * 5);
+    std::vector<int> pairs;
     for (int n = 0; n < Np; ++n)
       for (int f = 0; f < 4; ++f) {
-        ptr[(size_t)n * 5 + f] = (int)col.size();
+        ptr[(size_t)n * 5 + f] = (int)pairs.size() / 2;
         for (int j = 0; j < o->EEL_nnz; ++j) {
           const int c = o->EEL_ids[n + j * Np];
           const float v = o->EEL_vals[n + j * Np];
           if (c < 0 || c >= NF) return set_error(BBW_ERR_ARG, "bbw_create: EEL id out of range");
-          if (v != 0.f && c / Nfp == f) col.push_back(c), val.push_back(v);
+          if (v != 0.f && c / Nfp == f) pairs.push_back(c * kFusedRowStride), pairs.push_back(bits(v));
         }
-        if (f == 3) ptr[(size_t)n * 5 + 4] = (int)col.size();
+        if (f == 3) ptr[(size_t)n * 5 + 4] = (int)pairs.size() / 2;
+      }
+    tab.push_back(L0);
+    tab.push_back((int)pairs.size() / 2);
+    tab.push_back(0);
+    tab.push_back(0);
+    for (int nt = 0; nt < Nfp; ++nt)
+      for (int j = 0; j < L0; ++j) {
+        tab.push_back(o->L0_ids[nt + j * Nfp] * kFusedRowStride);
+        tab.push_back(bits(o->L0_vals[nt + j * Nfp]));
       }
     tab.insert(tab.end(), ptr.begin(), ptr.end());
-    tab.insert(tab.end(), col.begin(), col.end());
-    for (float v : val) {
-      int bits;
-      std::memcpy(&bits, &v, 4);
-      tab.push_back(bits);
-    }
+    if (tab.size() % 2) tab.push_back(0);
+    tab.insert(tab.end(), pairs.begin(), pairs.end());
     for (int i = 0; i < Np; ++i)
       for (int d = 0; d < 4; ++d)
         for (int c = 0; c < 4; ++c) {

@@ -8,9 +8,12 @@
 
 namespace bbw {
 
+// element-tile row stride (floats) of the fused kernel's shared-memory arrays
+constexpr int kFusedRowStride = 33;
+
 struct FusedPlan {
   int N = 0, K = 0, Nq = 0, RQ = 0, PRQ = 0, bc = 0, npat = 0;
-  bool bb = false;
+  bool bb = false, pipe = false;
   int grid = 0;
   size_t smem = 0;
   const float *vgeo = nullptr, *fgeo = nullptr, *c2q = nullptr;

@@ -43,7 +43,8 @@
 namespace bbw {
 
 constexpr int TILE_E = 32;
-constexpr int ES = TILE_E + 1;  // shared-memory row stride (floats)
+constexpr int ES = kFusedRowStride;  // shared-memory row stride (floats), TILE_E + 1
+static_assert(ES == TILE_E + 1, "row stride");
 
 __host__ __device__ constexpr int round4(int x) { return (x + 3) & ~3; }
 __host__ __device__ constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }
@@ -83,48 +84,57 @@ struct FusedParams {
   int table_ints;
 };
 
+// Shared-memory map (floats, rows of stride ES).  Input tiles are double
+// buffered when they fit (PIPE): the next tile's copies are in flight while
+// the current one is computed.
 template <int N, bool BB>
 struct FusedSmem {
   using C = FusedCfg<N>;
-  // element data (floats), all with row stride ES
-  static constexpr int sQ = 0;                          // [4Np][ES] old state
-  static constexpr int sR = sQ + 4 * C::Np * ES;        // [4Np][ES] rhs / U scratch
-  static constexpr int sF = sR + 4 * C::Np * ES;        // [NF][ES]  pflux
-  static constexpr int sF2 = sF + C::NF * ES;           // [NF][ES]  BB: L0 * pflux
-  static constexpr int sGeo = sF2 + (BB ? C::NF * ES : 0);  // [E][25] vgeo + fgeo
-  static constexpr int sNbr = sGeo + TILE_E * 25;       // [E][4] ints
-  static constexpr int sQuad = sNbr + TILE_E * 4;       // [Nq][ES] projected p, then c2
-  // followed at run time by [Nq][ES] c2 tile, the operators and int tables
+  static constexpr int inQ = 0;                               // [4Np][ES] state tile
+  static constexpr int inGeo = 4 * C::Np * ES;                // [E][25]  vgeo + fgeo
+  static constexpr int inNbr = inGeo + TILE_E * 25;           // [E][4]   neighbour codes
+  static constexpr int inC2 = inNbr + TILE_E * 4;             // [Nq][ES] c2 (runtime Nq)
+  __host__ __device__ static int in_size(int Nq) { return inC2 + round4(Nq * ES); }
+  static constexpr int sR = 0;                                // [4Np][ES] rhs / U scratch
+  static constexpr int sF = sR + 4 * C::Np * ES;              // [NF][ES]  pflux
+  static constexpr int sF2 = sF + C::NF * ES;                 // [NF][ES]  BB: L0 * pflux
+  static constexpr int sQuad = sF2 + (BB ? C::NF * ES : 0);   // [Nq][ES]  c2 * p at the cubature
+  __host__ __device__ static int work_size(int Nq) { return sQuad + round4(Nq * ES); }
 };
 
 // -------------------------------------------------------------- device code
-__device__ __forceinline__ void cp_async4(float *smem_dst, const float *gmem_src, bool valid) {
+__device__ __forceinline__ void cp_async4(void *smem_dst, const void *gmem_src, bool valid) {
   // 4-byte asynchronous copy; zero-fills the destination when !valid
   const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(gmem_src),
                "r"(valid ? 4 : 0)
                : "memory");
 }
-__device__ __forceinline__ void cp_async_commit_wait_all() {
-  asm volatile("cp.async.commit_group;\ncp.async.wait_all;\n" ::: "memory");
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
 // OPS_SMEM: the packed operators are staged in shared memory (every
 // operator read is a shared-memory broadcast); otherwise they are read
 // through the read-only data path (large N or large cubature rules).
-template <int N, bool BB, bool OPS_SMEM>
+// PIPE: two input-tile buffers (software pipelining across tiles).
+template <int N, bool BB, bool OPS_SMEM, bool PIPE>
 __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P) {
   using C = FusedCfg<N>;
   using L = FusedSmem<N, BB>;
   constexpr int Np = C::Np, Nfp = C::Nfp, NF = C::NF, W = C::W, T = C::T, R = C::R;
+  constexpr int FIT = cdiv(TILE_E * NF, T);        // flux items per thread
+  constexpr int QIT = cdiv(TILE_E * 4 * Np, T);    // state-tile floats per thread
   extern __shared__ __align__(16) float sm[];
   const int Nq = P.Nq, RQ = P.RQ, PRQ = P.PRQ;
-  float *sQ = sm + L::sQ, *sR = sm + L::sR, *sF = sm + L::sF, *sF2 = sm + L::sF2;
-  float *sGeo = sm + L::sGeo;
-  int *sNbr = (int *)(sm + L::sNbr);
-  float *sQuad = sm + L::sQuad;
-  float *sC2 = sQuad + round4(Nq * ES);
-  int *sTab = (int *)(sC2 + round4(Nq * ES));
+  const int inSize = L::in_size(Nq);
+  float *sIn = sm;                                   // [PIPE ? 2 : 1][inSize]
+  float *sW = sm + (PIPE ? 2 : 1) * inSize;          // work arrays
+  float *sR = sW + L::sR, *sF = sW + L::sF, *sF2 = sW + L::sF2, *sQuad = sW + L::sQuad;
+  int *sTab = (int *)(sW + L::work_size(Nq));
   float *sOps = (float *)(sTab + P.table_ints);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int r0 = warp * R;
@@ -142,59 +152,55 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
   const float *wLift = opBase + P.off_lift + warp * NF * C::PR;  // [W][NF][PR]
   const float *wPq = opBase + P.off_pq + warp * Nq * C::PR;      // [W][Nq][PR]
   const float *wVq = opBase + P.off_vq + warp * Np * PRQ;        // [W][Np][PRQ]
-  // BB tables: D ids int4 [4][Np], Dvals float4 [Np], L0 [Nfp][L0nnz]
-  // ids / vals, EEL rows bucketed by face (CSR)
+  // BB tables: D ids int4 [4][Np], Dvals float4 [Np], then the lift tables
   const int *bbTab = sTab + P.bb_off;
 
-  const int ntiles = cdiv(P.K, TILE_E);
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int k0 = tile * TILE_E;
-    const int ne = min(TILE_E, P.K - k0);
-    __syncthreads();  // previous tile fully consumed (and operators staged)
-
-    // ---- 1. per-element geometry and neighbour codes; state and c2 tiles
-    //         as asynchronous copies transposed to [row][element]
+  // asynchronous copies of one tile's inputs into buffer `buf`
+  auto issue_tile = [&](int tile, float *buf) {
+    const int k0 = tile * TILE_E, ne = min(TILE_E, P.K - k0);
+    float *bQ = buf + L::inQ, *bGeo = buf + L::inGeo, *bC2 = buf + L::inC2;
+    int *bNbr = (int *)(buf + L::inNbr);
     for (int i = tid; i < TILE_E * 9; i += T)
-      sGeo[(i / 9) * 25 + i % 9] = i < ne * 9 ? __ldg(P.vgeo + (size_t)k0 * 9 + i) : 0.f;
+      cp_async4(&bGeo[(i / 9) * 25 + i % 9], P.vgeo + (size_t)k0 * 9 + (i < ne * 9 ? i : 0), i < ne * 9);
     for (int i = tid; i < TILE_E * 16; i += T)
-      sGeo[(i / 16) * 25 + 9 + i % 16] = i < ne * 16 ? __ldg(P.fgeo + (size_t)k0 * 16 + i) : 0.f;
-    for (int i = tid; i < TILE_E * 4; i += T)
-      sNbr[i] = i < ne * 4 ? __ldg(P.nbr + (size_t)k0 * 4 + i) : 255;
-    {
-      const float *Qg = P.Qin + (size_t)k0 * 4 * Np;
-      constexpr int QIT = cdiv(TILE_E * 4 * Np, T);
+      cp_async4(&bGeo[(i / 16) * 25 + 9 + i % 16], P.fgeo + (size_t)k0 * 16 + (i < ne * 16 ? i : 0),
+                i < ne * 16);
+    for (int i = tid; i < TILE_E * 4; i += T)  // zero codes of absent elements: element 0, never used
+      cp_async4(&bNbr[i], P.nbr + (size_t)k0 * 4 + (i < ne * 4 ? i : 0), i < ne * 4);
+    const float *Qg = P.Qin + (size_t)k0 * 4 * Np;
 #pragma unroll 4
-      for (int j = 0; j < QIT; ++j) {
-        const int i = tid + j * T;
-        if (i < TILE_E * 4 * Np) {
-          const int e = i / (4 * Np), fn = i - e * (4 * Np);
-          const bool ok = e < ne;
-          cp_async4(&sQ[fn * ES + e], ok ? Qg + i : P.Qin, ok);
-        }
-      }
-      const float *cg = P.c2q + (size_t)k0 * Nq;
-      for (int i = tid; i < TILE_E * Nq; i += T) {
-        const int e = i / Nq, q = i - e * Nq;
+    for (int j = 0; j < QIT; ++j) {
+      const int i = tid + j * T;
+      if (i < TILE_E * 4 * Np) {
+        const int e = i / (4 * Np), fn = i - e * (4 * Np);
         const bool ok = e < ne;
-        cp_async4(&sC2[q * ES + e], ok ? cg + i : P.c2q, ok);
+        cp_async4(&bQ[fn * ES + e], ok ? Qg + i : P.Qin, ok);
       }
     }
-    __syncthreads();  // neighbour codes visible
-
-    // ---- 2. neighbour face traces into registers (in flight together with
-    //         the asynchronous tile copies)
-    constexpr int FIT = cdiv(TILE_E * NF, T);
-    float nb[FIT][4];
+    const float *cg = P.c2q + (size_t)k0 * Nq;
+    for (int i = tid; i < TILE_E * Nq; i += T) {
+      const int e = i / Nq, q = i - e * Nq;
+      const bool ok = e < ne;
+      cp_async4(&bC2[q * ES + e], ok ? cg + i : P.c2q, ok);
+    }
+    cp_async_commit();
+  };
+  // neighbour face traces of the tile in `buf` into registers
+  auto load_traces = [&](const float *buf, int tile_of_buf, float (&nb)[FIT][4]) {
+    const int ne_b = min(TILE_E, P.K - tile_of_buf * TILE_E);
+    const int *bNbr = (const int *)(buf + L::inNbr);
 #pragma unroll
     for (int j = 0; j < FIT; ++j) {
       const int i = tid + j * T;
       nb[j][0] = nb[j][1] = nb[j][2] = nb[j][3] = 0.f;
-      if (i < TILE_E * NF) {
+      if (i < TILE_E * NF && (i & 31) < ne_b) {  // absent elements have no codes
         const int e = i & 31, m = i >> 5, f = m / Nfp;
-        const int code = sNbr[e * 4 + f];
+        const int code = bNbr[e * 4 + f];
         const int pat = code & 255;
-        if (pat != 255) {
-          const float *q2 = P.Qin + (size_t)(code >> 8) * 4 * Np + sPat[pat * Nfp + (m - f * Nfp)];
+        const unsigned rel = (unsigned)((code >> 8) - tile_of_buf * TILE_E);
+        if (pat != 255 && rel >= (unsigned)ne_b) {  // neighbours inside the tile: from smem
+          const float *q2 =
+              P.Qin + (size_t)(code >> 8) * 4 * Np + sPat[pat * Nfp + (m - f * Nfp)];
           nb[j][0] = __ldg(q2);
           nb[j][1] = __ldg(q2 + Np);
           nb[j][2] = __ldg(q2 + 2 * Np);
@@ -202,16 +208,44 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
         }
       }
     }
-    cp_async_commit_wait_all();
-    __syncthreads();  // state and c2 tiles landed
+  };
 
-    // ---- 3. upwind flux at the 4Nfp face nodes (Uflux = -pflux)
+  const int ntiles = cdiv(P.K, TILE_E);
+  int tile = blockIdx.x, b = 0;
+  float nb[FIT][4];
+  __syncthreads();  // tables staged
+  if (tile < ntiles) {
+    issue_tile(tile, sIn);
+    cp_async_wait_all();
+    __syncthreads();
+    load_traces(sIn, tile, nb);
+  }
+  for (; tile < ntiles; tile += gridDim.x) {
+    const int k0 = tile * TILE_E;
+    const int ne = min(TILE_E, P.K - k0);
+    const int next = tile + gridDim.x;
+    float *cur = sIn + b * inSize;
+    const float *sQ = cur + L::inQ, *sGeo = cur + L::inGeo, *sC2 = cur + L::inC2;
+    const int *sNbr = (const int *)(cur + L::inNbr);
+    if (PIPE && next < ntiles) issue_tile(next, sIn + (b ^ 1) * inSize);
+
+    // ---- 1. upwind flux at the 4Nfp face nodes (Uflux = -pflux); traces of
+    //         neighbours inside the tile come from the state tile itself
 #pragma unroll
     for (int j = 0; j < FIT; ++j) {
       const int i = tid + j * T;
       if (i >= TILE_E * NF) continue;
       const int e = i & 31, m = i >> 5, f = m / Nfp;
-      const int pat = sNbr[e * 4 + f] & 255;
+      const int code = sNbr[e * 4 + f];
+      const int pat = code & 255;
+      const unsigned rel = (unsigned)((code >> 8) - k0);
+      if (pat != 255 && rel < (unsigned)ne) {
+        const int vP = sPat[pat * Nfp + (m - f * Nfp)];
+        nb[j][0] = sQ[vP * ES + rel];
+        nb[j][1] = sQ[(Np + vP) * ES + rel];
+        nb[j][2] = sQ[(2 * Np + vP) * ES + rel];
+        nb[j][3] = sQ[(3 * Np + vP) * ES + rel];
+      }
       const int vM = sFmask[m];
       const float pM = sQ[vM * ES + e], uM = sQ[(Np + vM) * ES + e],
                   vvM = sQ[(2 * Np + vM) * ES + e], wM = sQ[(3 * Np + vM) * ES + e];
@@ -233,7 +267,7 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
       sF[m * ES + e] = .5f * (pjump - Unjump) * Fscale;
     }
 
-    // ---- 3b. contravariant velocities Ur, Us, Ut into sR rows [Np, 4Np)
+    // ---- 2. contravariant velocities Ur, Us, Ut into sR rows [Np, 4Np)
     for (int i = tid; i < TILE_E * Np; i += T) {
       const int e = i & 31, n = i >> 5;
       const float *G = sGeo + e * 25;
@@ -245,7 +279,7 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
     }
     __syncthreads();
 
-    // ---- 4. volume term (registers: rows r0..r0+R of this warp, lane = element)
+    // ---- 3. volume term (registers: rows r0..r0+R of this warp, lane = element)
     float rp[R], ru[R], rv[R], rw[R];
     {
       const float *G = sGeo + lane * 25;
@@ -294,21 +328,21 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
           rp[i] = ru[i] = rv[i] = rw[i] = 0.f;
           if (n >= Np) continue;
           const float4 dv = Dv[n];
-          const int4 a = Dids[n], b = Dids[Np + n], c = Dids[2 * Np + n], d = Dids[3 * Np + n];
-          const float p1 = dv.x * p[a.x * ES] + dv.y * p[b.x * ES] + dv.z * p[c.x * ES] +
+          const int4 a = Dids[n], bq = Dids[Np + n], c = Dids[2 * Np + n], d = Dids[3 * Np + n];
+          const float p1 = dv.x * p[a.x * ES] + dv.y * p[bq.x * ES] + dv.z * p[c.x * ES] +
                            dv.w * p[d.x * ES];
-          const float p2 = dv.x * p[a.y * ES] + dv.y * p[b.y * ES] + dv.z * p[c.y * ES] +
+          const float p2 = dv.x * p[a.y * ES] + dv.y * p[bq.y * ES] + dv.z * p[c.y * ES] +
                            dv.w * p[d.y * ES];
-          const float p3 = dv.x * p[a.z * ES] + dv.y * p[b.z * ES] + dv.z * p[c.z * ES] +
+          const float p3 = dv.x * p[a.z * ES] + dv.y * p[bq.z * ES] + dv.z * p[c.z * ES] +
                            dv.w * p[d.z * ES];
-          const float p4 = dv.x * p[a.w * ES] + dv.y * p[b.w * ES] + dv.z * p[c.w * ES] +
+          const float p4 = dv.x * p[a.w * ES] + dv.y * p[bq.w * ES] + dv.z * p[c.w * ES] +
                            dv.w * p[d.w * ES];
           float dU1 = dv.x * (ur[a.y * ES] + us[a.z * ES] + ut[a.w * ES]);
-          dU1 += dv.y * (ur[b.y * ES] + us[b.z * ES] + ut[b.w * ES]);
+          dU1 += dv.y * (ur[bq.y * ES] + us[bq.z * ES] + ut[bq.w * ES]);
           dU1 += dv.z * (ur[c.y * ES] + us[c.z * ES] + ut[c.w * ES]);
           dU1 += dv.w * (ur[d.y * ES] + us[d.z * ES] + ut[d.w * ES]);
           float dU2 = dv.x * (ur[a.x * ES] + us[a.x * ES] + ut[a.x * ES]);
-          dU2 += dv.y * (ur[b.x * ES] + us[b.x * ES] + ut[b.x * ES]);
+          dU2 += dv.y * (ur[bq.x * ES] + us[bq.x * ES] + ut[bq.x * ES]);
           dU2 += dv.z * (ur[c.x * ES] + us[c.x * ES] + ut[c.x * ES]);
           dU2 += dv.w * (ur[d.x * ES] + us[d.x * ES] + ut[d.x * ES]);
           const float dpdr = .5f * (p2 - p1), dpds = .5f * (p3 - p1), dpdt = .5f * (p4 - p1);
@@ -320,7 +354,7 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
       }
     }
 
-    // ---- 5. lift of the face fluxes
+    // ---- 4. lift of the face fluxes
     {
       const float *fgl = sGeo + lane * 25 + 9;
       if constexpr (!BB) {
@@ -353,20 +387,29 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
           }
         }
       } else {
-        // BB lift: per face L0 (Nfp x Nfp sparse), then degree elevation EEL
-        // applied face by face (cpp/okl/WaveKernels.okl:576-644)
+        // BB lift: per face L0 (Nfp x Nfp sparse), then the degree elevation
+        // EEL face by face (cpp/okl/WaveKernels.okl:576-644).  Tables: header
+        // {L0nnz, EEL nnz}, L0 (offset, value) pairs [Nfp][L0nnz], EEL row
+        // pointers [Np][5], EEL (offset, value) pairs; offsets are
+        // pre-multiplied by the row stride.
+        __syncthreads();  // pflux complete (written in step 1 by other warps)
         const int L0nnz = bbTab[20 * Np];
-        const int *L0ids = bbTab + 20 * Np + 1;
-        const float *L0vals = reinterpret_cast<const float *>(L0ids + Nfp * L0nnz);
-        const int *eelPtr = reinterpret_cast<const int *>(L0vals + Nfp * L0nnz);  // [Np][5]
-        const int *eelCol = eelPtr + 5 * Np;
-        const float *eelVal = reinterpret_cast<const float *>(eelCol + eelPtr[5 * Np - 1]);
+        const int2 *L0p = reinterpret_cast<const int2 *>(bbTab + 20 * Np + 4);
+        const int *eelPtr = bbTab + 20 * Np + 4 + 2 * Nfp * L0nnz;
+        const int2 *eelP = reinterpret_cast<const int2 *>(eelPtr + ((5 * Np + 1) & ~1));
         for (int m = warp; m < NF; m += W) {
           const int f = m / Nfp, nt = m - f * Nfp;
-          float v = 0.f;
-          for (int j = 0; j < L0nnz; ++j)
-            v += L0vals[nt * L0nnz + j] * sF[(L0ids[nt * L0nnz + j] + f * Nfp) * ES + lane];
-          sF2[m * ES + lane] = v;
+          const float *src = sF + f * Nfp * ES + lane;
+          const int2 *row = L0p + nt * L0nnz;
+          float v0 = 0.f, v1 = 0.f;
+          int j = 0;
+          for (; j + 1 < L0nnz; j += 2) {
+            const int2 t0 = row[j], t1 = row[j + 1];
+            v0 += __int_as_float(t0.y) * src[t0.x];
+            v1 += __int_as_float(t1.y) * src[t1.x];
+          }
+          if (j < L0nnz) v0 += __int_as_float(row[j].y) * src[row[j].x];
+          sF2[m * ES + lane] = v0 + v1;
         }
         __syncthreads();
 #pragma unroll
@@ -376,8 +419,18 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
           const int *ptr = eelPtr + 5 * n;
 #pragma unroll 1
           for (int f = 0; f < 4; ++f) {
-            float acc = 0.f;
-            for (int j = ptr[f]; j < ptr[f + 1]; ++j) acc += eelVal[j] * sF2[eelCol[j] * ES + lane];
+            float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+            int j = ptr[f];
+            const int end = ptr[f + 1];
+            for (; j + 3 < end; j += 4) {
+              const int2 t0 = eelP[j], t1 = eelP[j + 1], t2 = eelP[j + 2], t3 = eelP[j + 3];
+              a0 += __int_as_float(t0.y) * sF2[t0.x + lane];
+              a1 += __int_as_float(t1.y) * sF2[t1.x + lane];
+              a2 += __int_as_float(t2.y) * sF2[t2.x + lane];
+              a3 += __int_as_float(t3.y) * sF2[t3.x + lane];
+            }
+            for (; j < end; ++j) a0 += __int_as_float(eelP[j].y) * sF2[eelP[j].x + lane];
+            const float acc = (a0 + a1) + (a2 + a3);
             rp[i] += acc;
             ru[i] -= fgl[4 * f + 1] * acc;
             rv[i] -= fgl[4 * f + 2] * acc;
@@ -397,9 +450,11 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
         sR[(3 * Np + n) * ES + lane] = rw[i];
       }
     }
+    if (PIPE) cp_async_wait_all();  // the next tile's inputs have landed
     __syncthreads();
+    if (PIPE && next < ntiles) load_traces(sIn + (b ^ 1) * inSize, next, nb);  // in flight from here
 
-    // ---- 6. WADG: p at the cubature points, times c2/J
+    // ---- 5. WADG: p at the cubature points, times c2/J
     {
       const int q0 = warp * RQ;
       for (int qb = 0; qb < RQ; qb += 4) {
@@ -423,15 +478,15 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
     }
     __syncthreads();
 
-    // ---- 7. project back: rhs_p = Pq * (c2 p_q); the residual tile is
-    //         fetched meanwhile for the stage update
-    constexpr int UIT = cdiv(TILE_E * Np, T);  // float4 per thread
-    const float4 *resg = reinterpret_cast<const float4 *>(P.res + (size_t)k0 * 4 * Np);
-    float4 rpre[UIT];
+    // ---- 6. project back: rhs_p = Pq * (c2 p_q); the residual tile is
+    //         fetched meanwhile for the stage update (scalar, coalesced)
+    constexpr int UIT = cdiv(TILE_E * 4 * Np, T);
+    const float *resg = P.res + (size_t)k0 * 4 * Np;
+    float rpre[UIT];
 #pragma unroll
     for (int j = 0; j < UIT; ++j) {
       const int i = tid + j * T;
-      rpre[j] = i < ne * Np ? resg[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+      rpre[j] = i < ne * 4 * Np ? resg[i] : 0.f;
     }
     {
       float acc[R];
@@ -450,50 +505,51 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
 #pragma unroll
         for (int i = 0; i < R; ++i) acc[i] += o[i] * x;
       }
-      __syncthreads();  // everyone has read sR rows [0, Np) in step 6
+      __syncthreads();  // everyone has read sR rows [0, Np) in step 5
 #pragma unroll
       for (int i = 0; i < R; ++i)
         if (r0 + i < Np) sR[(r0 + i) * ES + lane] = acc[i];
     }
     __syncthreads();
 
-    // ---- 8. LSRK stage update, coalesced: res = fa res + fdt rhs; Q += fb res
+    // ---- 7. LSRK stage update, coalesced and conflict-free:
+    //         res = fa res + fdt rhs; Q += fb res
     {
-      float4 *resw = reinterpret_cast<float4 *>(P.res + (size_t)k0 * 4 * Np);
-      float4 *qg = reinterpret_cast<float4 *>(P.Qout + (size_t)k0 * 4 * Np);
+      float *resw = P.res + (size_t)k0 * 4 * Np;
+      float *qg = P.Qout + (size_t)k0 * 4 * Np;
 #pragma unroll
       for (int j = 0; j < UIT; ++j) {
         const int i = tid + j * T;
-        if (i >= ne * Np) continue;
-        const int e = (4 * i) / (4 * Np), fn = (4 * i) % (4 * Np);
-        float4 r = rpre[j], q;
-        r.x = P.fa * r.x + P.fdt * sR[(fn + 0) * ES + e];
-        r.y = P.fa * r.y + P.fdt * sR[(fn + 1) * ES + e];
-        r.z = P.fa * r.z + P.fdt * sR[(fn + 2) * ES + e];
-        r.w = P.fa * r.w + P.fdt * sR[(fn + 3) * ES + e];
-        q.x = sQ[(fn + 0) * ES + e] + P.fb * r.x;
-        q.y = sQ[(fn + 1) * ES + e] + P.fb * r.y;
-        q.z = sQ[(fn + 2) * ES + e] + P.fb * r.z;
-        q.w = sQ[(fn + 3) * ES + e] + P.fb * r.w;
+        if (i >= ne * 4 * Np) continue;
+        const int e = i / (4 * Np), fn = i - e * (4 * Np);
+        const float r = P.fa * rpre[j] + P.fdt * sR[fn * ES + e];
         resw[i] = r;
-        qg[i] = q;
+        qg[i] = sQ[fn * ES + e] + P.fb * r;
       }
     }
+    __syncthreads();  // tile buffers and work arrays free for reuse
+    if (!PIPE && next < ntiles) {
+      issue_tile(next, sIn);
+      cp_async_wait_all();
+      __syncthreads();
+      load_traces(sIn, next, nb);
+    }
+    b ^= PIPE ? 1 : 0;
   }
 }
 
 // --------------------------------------------------------------- host side
 template <int N, bool BB>
-static size_t smem_bytes(int Nq, int ops_smem, int table_ints) {
+static size_t smem_bytes(int Nq, bool pipe, bool ops_smem, int ops_floats, int table_ints) {
   using L = FusedSmem<N, BB>;
-  return sizeof(float) * ((size_t)L::sQuad + 2 * (size_t)round4(Nq * ES) + ops_smem) +
+  return sizeof(float) * ((size_t)(pipe ? 2 : 1) * L::in_size(Nq) + L::work_size(Nq) +
+                          (ops_smem ? ops_floats : 0)) +
          sizeof(int) * (size_t)table_ints;
 }
 
 template <int N, bool BB>
 static bbw_status launch_fused(const FusedPlan &pl, const float *Qin, float *Qout, float *res,
                                float fa, float fb, float fdt, cudaStream_t st) {
-  const bool ops_smem = pl.ops_smem == pl.ops_floats;
   FusedParams P;
   P.K = pl.K, P.Nq = pl.Nq, P.RQ = pl.RQ, P.PRQ = pl.PRQ, P.bc = pl.bc, P.npat = pl.npat;
   P.pat_off = pl.pat_off, P.bb_off = pl.bb_off;
@@ -503,11 +559,13 @@ static bbw_status launch_fused(const FusedPlan &pl, const float *Qin, float *Qou
   P.ops = pl.ops;
   P.off_lift = pl.off_lift, P.off_pq = pl.off_pq, P.off_vq = pl.off_vq, P.off_end = pl.ops_floats;
   P.tables = pl.tables, P.table_ints = pl.table_ints;
-  const size_t sm = smem_bytes<N, BB>(pl.Nq, pl.ops_smem, pl.table_ints);
-  if (ops_smem)
-    k_fused_stage<N, BB, true><<<pl.grid, FusedCfg<N>::T, sm, st>>>(P);
-  else
-    k_fused_stage<N, BB, false><<<pl.grid, FusedCfg<N>::T, sm, st>>>(P);
+  const bool os = pl.ops_smem > 0;
+  const size_t sm = pl.smem;
+  const int T = FusedCfg<N>::T;
+  if (os && pl.pipe) k_fused_stage<N, BB, true, true><<<pl.grid, T, sm, st>>>(P);
+  else if (os) k_fused_stage<N, BB, true, false><<<pl.grid, T, sm, st>>>(P);
+  else if (pl.pipe) k_fused_stage<N, BB, false, true><<<pl.grid, T, sm, st>>>(P);
+  else k_fused_stage<N, BB, false, false><<<pl.grid, T, sm, st>>>(P);
   return check_launch("fused stage");
 }
 
@@ -517,23 +575,34 @@ static bbw_status prepare(FusedPlan &pl) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  // operators in shared memory when they fit, else through the read-only path
-  pl.ops_smem = smem_bytes<N, BB>(pl.Nq, pl.ops_floats, pl.table_ints) <= (size_t)maxsm
-                    ? pl.ops_floats
-                    : 0;
-  const size_t sm = smem_bytes<N, BB>(pl.Nq, pl.ops_smem, pl.table_ints);
-  if (sm > (size_t)maxsm)
+  // preference: operators in shared memory, then double-buffered input tiles
+  const bool cand[4][2] = {{true, true}, {true, false}, {false, true}, {false, false}};
+  int pick = -1;
+  for (int c = 0; c < 4 && pick < 0; ++c)
+    if (smem_bytes<N, BB>(pl.Nq, cand[c][1], cand[c][0], pl.ops_floats, pl.table_ints) <=
+        (size_t)maxsm)
+      pick = c;
+  if (pick < 0)
     return set_error(BBW_ERR_UNSUPPORTED, "fused stage: element tile does not fit in shared memory");
-  cudaError_t e = pl.ops_smem ? cudaFuncSetAttribute(k_fused_stage<N, BB, true>,
-                                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     (int)sm)
-                              : cudaFuncSetAttribute(k_fused_stage<N, BB, false>,
-                                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     (int)sm);
+  pl.ops_smem = cand[pick][0] ? pl.ops_floats : 0;
+  pl.pipe = cand[pick][1];
+  pl.smem = smem_bytes<N, BB>(pl.Nq, pl.pipe, pl.ops_smem > 0, pl.ops_floats, pl.table_ints);
+  cudaError_t e;
+  if (pl.ops_smem && pl.pipe)
+    e = cudaFuncSetAttribute(k_fused_stage<N, BB, true, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem);
+  else if (pl.ops_smem)
+    e = cudaFuncSetAttribute(k_fused_stage<N, BB, true, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem);
+  else if (pl.pipe)
+    e = cudaFuncSetAttribute(k_fused_stage<N, BB, false, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem);
+  else
+    e = cudaFuncSetAttribute(k_fused_stage<N, BB, false, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem);
   if (e != cudaSuccess) return set_cuda_error(e, "fused stage attribute");
   const int ntiles = cdiv(pl.K, TILE_E);
   pl.grid = std::min(ntiles, nsm > 0 ? nsm : 148);
-  pl.smem = sm;
   return BBW_OK;
 }
 
