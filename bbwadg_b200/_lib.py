@@ -60,6 +60,9 @@ SIGNATURES = {
                                     P, P, P, P]),
     "bbw_create": (c_int, [ctypes.POINTER(MeshDesc), ctypes.POINTER(OpsDesc), c_int, c_int,
                            ctypes.POINTER(c_void_p)]),
+    "bbw_create_ex": (c_int, [ctypes.POINTER(MeshDesc), ctypes.POINTER(OpsDesc), c_int, c_int,
+                              c_int, ctypes.POINTER(c_void_p)]),
+    "bbw_check": (c_int, [c_void_p]),
     "bbw_destroy": (c_int, [c_void_p]),
     "bbw_set_state": (c_int, [c_void_p, P]),
     "bbw_get_state": (c_int, [c_void_p, P]),

@@ -47,6 +47,11 @@ struct bbw_ctx {
   float *vgeo = nullptr, *fgeo = nullptr, *c2q = nullptr, *ops = nullptr;
   int *nbr = nullptr, *tables = nullptr;
   FusedPlan plan;
+  int precision = BBW_PREC_FP32;
+  TcPlan tc;
+  float *geo_tc = nullptr;
+  void *ops_tc = nullptr;
+  int *err = nullptr;
   // one graph per starting buffer parity, for one LSRK45 step of size dt
   cudaGraphExec_t step_graph[2] = {nullptr, nullptr};
   uint32_t graph_dt_bits[2] = {0, 0};
@@ -76,6 +81,9 @@ void release(bbw_ctx *c) {
   cudaFree(c->ops);
   cudaFree(c->nbr);
   cudaFree(c->tables);
+  cudaFree(c->geo_tc);
+  cudaFree(c->ops_tc);
+  cudaFree(c->err);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -126,10 +134,20 @@ bbw_status compress_connectivity(int N, int K, const int *Fmask, const int *vmap
 
 extern "C" bbw_status bbw_create(const bbw_mesh_desc *m, const bbw_ops_desc *o, int variant,
                                  int bc, bbw_ctx **out) {
+  return bbw_create_ex(m, o, variant, bc, BBW_PREC_FP32, out);
+}
+
+extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *o, int variant,
+                                    int bc, int precision, bbw_ctx **out) {
   if (!out) return set_error(BBW_ERR_ARG, "bbw_create: out is NULL");
   *out = nullptr;
-  if (!m || !o || (variant != BBW_NODAL && variant != BBW_BB) || (bc != 0 && bc != 1))
+  if (!m || !o || (variant != BBW_NODAL && variant != BBW_BB) || (bc != 0 && bc != 1) ||
+      (precision != BBW_PREC_FP32 && precision != BBW_PREC_F16X3))
     return set_error(BBW_ERR_ARG, "bbw_create: bad argument");
+  if (precision == BBW_PREC_F16X3 && (variant != BBW_NODAL || !tc_supported(m->N, m->Nq)))
+    return set_error(BBW_ERR_UNSUPPORTED,
+                     "bbw_create: the split-FP16 tensor-core stage supports the nodal variant "
+                     "with N in {3, 5} and Nq <= 128");
   const int N = m->N, K = m->K, Nq = m->Nq;
   if (N < 1 || N > BBW_MAX_N) return set_error(BBW_ERR_UNSUPPORTED, "bbw_create: N out of range");
   if (K <= 0 || K >= (1 << 23) || Nq <= 0)
@@ -297,8 +315,59 @@ extern "C" bbw_status bbw_create(const bbw_mesh_desc *m, const bbw_ops_desc *o, 
     release(c);
     return s;
   }
+  c->precision = precision;
+  if (precision == BBW_PREC_F16X3) {
+    // geometry records, split-FP16 operators in the canonical K-major layout
+    TcPlan &tp = c->tc;
+    tp.N = N, tp.K = K, tp.Nq = Nq, tp.bc = bc;
+    tp.table_ints = (int)tab.size(), tp.pat_off = pat_off;
+    tp.L = tc_layout(N, Nq, tp.table_ints);
+    const TcLayout &TL = tp.L;
+    std::vector<float> geo((size_t)K * TC_GEO, 0.f);
+    for (int k = 0; k < K; ++k) {
+      std::memcpy(&geo[(size_t)k * TC_GEO], m->vgeo + (size_t)k * 9, 9 * sizeof(float));
+      std::memcpy(&geo[(size_t)k * TC_GEO + 9], m->fgeo + (size_t)k * 16, 16 * sizeof(float));
+    }
+    std::vector<__half> h(TL.ops_halfs);
+    const float *Dd[3] = {o->Dr, o->Ds, o->Dt};
+    for (int d = 0; d < 3; ++d)
+      tc_pack_operator(Dd[d], Np, Np, 1, Np, 64, TL.KV, &h[TL.oD + 2 * d * 64 * TL.KV],
+                       &h[TL.oD + (2 * d + 1) * 64 * TL.KV]);
+    for (int f = 0; f < 4; ++f)
+      tc_pack_operator(o->LIFT + (size_t)f * Nfp * Np, Np, Nfp, 1, Np, 64, TL.KF,
+                       &h[TL.oL + 2 * f * 64 * TL.KF], &h[TL.oL + (2 * f + 1) * 64 * TL.KF]);
+    tc_pack_operator(o->Vq, Nq, Np, 1, Nq, TL.MQ, TL.KV, &h[TL.oVq], &h[TL.oVq + TL.MQ * TL.KV]);
+    tc_pack_operator(o->Pq, Np, Nq, 1, Np, 64, TL.KQ, &h[TL.oPq], &h[TL.oPq + 64 * TL.KQ]);
+    __half *dops = nullptr;
+    if ((s = upload(&c->geo_tc, geo.data(), geo.size(), "bbw_create: geometry")) != BBW_OK ||
+        (s = upload(&dops, h.data(), h.size(), "bbw_create: tensor-core operators")) != BBW_OK ||
+        (s = upload<int>(&c->err, nullptr, 1, "bbw_create: status")) != BBW_OK) {
+      c->ops_tc = dops;
+      release(c);
+      return s;
+    }
+    c->ops_tc = dops;
+    tp.geo = c->geo_tc, tp.c2q = c->c2q, tp.nbr = c->nbr, tp.tables = c->tables;
+    tp.ops = c->ops_tc, tp.err = c->err;
+    if ((s = tc_prepare(tp)) != BBW_OK) {
+      release(c);
+      return s;
+    }
+  }
   *out = c;
   return BBW_OK;
+}
+
+extern "C" bbw_status bbw_check(bbw_ctx *c) {
+  if (!c) return set_error(BBW_ERR_ARG, "bbw_check: ctx is NULL");
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return set_cuda_error(e, "bbw_check");
+  if (!c->err) return BBW_OK;
+  int h = 0;
+  e = cudaMemcpy(&h, c->err, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return set_cuda_error(e, "bbw_check");
+  return h ? set_error(BBW_ERR_TIMEOUT, "a bounded device wait gave up; state is invalid")
+           : BBW_OK;
 }
 
 extern "C" bbw_status bbw_destroy(bbw_ctx *c) {
@@ -337,8 +406,10 @@ extern "C" bbw_status bbw_get_residual(bbw_ctx *c, float *r) {
 
 extern "C" bbw_status bbw_stage(bbw_ctx *c, float fa, float fb, float fdt) {
   if (!c) return set_error(BBW_ERR_ARG, "bbw_stage: ctx is NULL");
-  bbw_status s = fused_launch(c->plan, c->Q[c->cur], c->Q[c->cur ^ 1], c->res, fa, fb, fdt,
-                              c->stream);
+  bbw_status s =
+      c->precision == BBW_PREC_F16X3
+          ? tc_launch(c->tc, c->Q[c->cur], c->Q[c->cur ^ 1], c->res, fa, fb, fdt, c->stream)
+          : fused_launch(c->plan, c->Q[c->cur], c->Q[c->cur ^ 1], c->res, fa, fb, fdt, c->stream);
   if (s == BBW_OK) c->cur ^= 1;
   return s;
 }

@@ -1,5 +1,6 @@
 // Host-visible description of a prepared fused-stage launch (kernels_fused.cu).
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cstddef>
@@ -26,6 +27,35 @@ struct FusedPlan {
 };
 
 int fused_warps(int N);
+
+// ---- tensor-core (tcgen05) stage, kernels_tc.cu
+constexpr int TC_GEO = 28;  // floats per element geometry record: vgeo 9 | fgeo 16 | pad 3
+
+struct TcLayout {
+  int KV = 0, KF = 0, KQ = 0, MQ = 0;         // padded K extents, Vq rows
+  int oD = 0, oL = 0, oVq = 0, oPq = 0;       // operator offsets (halves)
+  int ops_halfs = 0;
+  int ops = 0, Bp = 0, BU = 0, BF = 0, raw = 0, geo = 0, nbr = 0, tab = 0, misc = 0;  // bytes
+  int total = 0;
+};
+
+struct TcPlan {
+  int N = 0, K = 0, Nq = 0, bc = 0, grid = 0;
+  TcLayout L;
+  const float *geo = nullptr, *c2q = nullptr;
+  const int *nbr = nullptr, *tables = nullptr;
+  const void *ops = nullptr;
+  int table_ints = 0, pat_off = 0;
+  int *err = nullptr;
+};
+
+TcLayout tc_layout(int N, int Nq, int table_ints);
+bool tc_supported(int N, int Nq);
+bbw_status tc_prepare(TcPlan &pl);
+bbw_status tc_launch(const TcPlan &pl, const float *Qin, float *Qout, float *res, float fa,
+                     float fb, float fdt, cudaStream_t st);
+void tc_pack_operator(const float *A, int nrows, int ncols, int ld_row, int ld_col, int rows,
+                      int kp, __half *hi, __half *lo);
 bbw_status fused_prepare(FusedPlan &pl);
 bbw_status fused_launch(const FusedPlan &pl, const float *Qin, float *Qout, float *res, float fa,
                         float fb, float fdt, cudaStream_t st);

@@ -35,6 +35,7 @@ RK4C = (0.0,
         1.0)
 
 VARIANTS = {"nodal": 0, "bb": 1}
+PRECISIONS = {"fp32": 0, "f16x3": 1}
 BCS = {"pressure_release": 0, "rigid": 1}
 
 
@@ -50,7 +51,8 @@ class WaveSolver:
     """Fused-stage solver context for one mesh / operator set on the current GPU."""
 
     def __init__(self, problem=None, *, N=None, K=None, Nq=None, variant=None, ops=None,
-                 vgeo=None, fgeo=None, vmapP=None, c2q=None, Jq=None, bc="pressure_release"):
+                 vgeo=None, fgeo=None, vmapP=None, c2q=None, Jq=None, bc="pressure_release",
+                 precision="fp32"):
         if problem is not None:
             N, K, Nq = problem.N, problem.K, problem.Nq
             variant = variant or problem.variant
@@ -83,8 +85,9 @@ class WaveSolver:
             od.EEL_ids, od.EEL_vals = i(ops["EEL_ids"]), f(ops["EEL_vals"])
             od.L0_ids, od.L0_vals = i(ops["L0_ids"]), f(ops["L0_vals"])
         h = ctypes.c_void_p()
-        _lib.call("bbw_create", ctypes.byref(md), ctypes.byref(od), VARIANTS[variant], BCS[bc],
-                  ctypes.byref(h))
+        _lib.call("bbw_create_ex", ctypes.byref(md), ctypes.byref(od), VARIANTS[variant], BCS[bc],
+                  PRECISIONS[precision], ctypes.byref(h))
+        self.precision = precision
         self._h = h
         del keep
 
@@ -124,6 +127,10 @@ class WaveSolver:
 
     def sync(self):
         _lib.call("bbw_sync", self._h)
+
+    def check(self):
+        """Raise if a bounded device-side wait gave up (state invalid)."""
+        _lib.call("bbw_check", self._h)
 
     def device_state(self):
         q, r, s = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()

@@ -173,10 +173,21 @@ typedef struct bbw_ops_desc {
   const float *Vq, *Pq;
 } bbw_ops_desc;
 
+/* Arithmetic of the fused stage.  FP32: CUDA-core FP32 throughout.
+ * F16X3: the dense contractions (Dr/Ds/Dt, LIFT, Vq, Pq) on the tensor cores
+ * as three FP16 products per split pair (A_hi x_hi + A_hi x_lo + A_lo x_hi,
+ * per-tile power-of-two scaling, FP32 accumulation); state, fluxes and the
+ * update stay FP32.  F16X3 supports the nodal variant with N in {3, 5},
+ * Nq <= 128. */
+enum { BBW_PREC_FP32 = 0, BBW_PREC_F16X3 = 1 };
+
 /* Uploads mesh and operators (cpp/src/WaveOKL3d.cpp:1400-1615 and
- * :894-909) to the current CUDA device; state and residual start at zero. */
+ * :894-909) to the current CUDA device; state and residual start at zero.
+ * bbw_create is bbw_create_ex with BBW_PREC_FP32. */
 bbw_status bbw_create(const bbw_mesh_desc *mesh, const bbw_ops_desc *ops, int variant, int bc,
                       bbw_ctx **out);
+bbw_status bbw_create_ex(const bbw_mesh_desc *mesh, const bbw_ops_desc *ops, int variant, int bc,
+                         int precision, bbw_ctx **out);
 bbw_status bbw_destroy(bbw_ctx *ctx);
 
 /* WaveSetData3d / WaveGetData3d (cpp/src/WaveOKL3d.cpp:2527-2537): copy the
@@ -203,6 +214,10 @@ bbw_status bbw_run(bbw_ctx *ctx, double final_time, float dt);
 
 /* Waits for the context's stream. */
 bbw_status bbw_sync(bbw_ctx *ctx);
+
+/* Waits for the stream and reports BBW_ERR_TIMEOUT if a bounded device-side
+ * wait (tensor-core completion, bulk copies) gave up since creation. */
+bbw_status bbw_check(bbw_ctx *ctx);
 
 /* Device pointers of the current state and residual ([K][4][Np]) and the
  * context's cudaStream_t, for zero-copy interop.  Valid until the next

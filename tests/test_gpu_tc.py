@@ -1,0 +1,81 @@
+"""Tensor-core (tcgen05) stage, split-FP16 three-product form, against the
+reference's time loop (golden) and the FP32 C restatement.  Tolerance:
+1e-5 relative L2, the same bar as the FP32 path."""
+import numpy as np
+import pytest
+from conftest import golden, ref_ops, rel_l2
+
+from bbwadg_b200 import RK4A, RK4B, WaveSolver, make_problem
+from bbwadg_b200.mesh import kuhn_box
+from bbwadg_b200.problem import build_operators, connect_and_geometry
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def ref_rule(N):
+    g = golden("ops_N%d.npz" % N)
+    nfq = int(g["Nfq"][0])
+    return (g["rq"], g["sq"], g["tq"], g["wq"]), (g["rfq"][:nfq], g["sfq"][:nfq], g["wfqFace"])
+
+
+def test_tc_100_steps_match_reference(cuda):
+    r = golden("run_N3_box4.npz")
+    ops = ref_ops(3, "nodal")
+    m = connect_and_geometry(3, *kuhn_box(4), build_operators(3))
+    s = WaveSolver(N=3, K=384, Nq=int(ops["Nq"][0]), variant="nodal", ops=ops, vgeo=m["vgeo"],
+                   fgeo=m["fgeo"], vmapP=m["vmapP"], c2q=r["c2q"], precision="f16x3")
+    s.set_data(r["Q0_nodal"])
+    s.rk_step(np.float32(RK4A[0]), np.float32(RK4B[0]), float(r["dt"][0]))
+    assert rel_l2(s.get_data(), r["Q1stage_nodal"]) < TOL
+    s.close()
+    s = WaveSolver(N=3, K=384, Nq=int(ops["Nq"][0]), variant="nodal", ops=ops, vgeo=m["vgeo"],
+                   fgeo=m["fgeo"], vmapP=m["vmapP"], c2q=r["c2q"], precision="f16x3")
+    s.set_data(r["Q0_nodal"])
+    s.steps(float(r["dt"][0]), 100)
+    s.check()
+    assert rel_l2(s.get_data(), r["Q100_nodal"]) < TOL
+
+
+@pytest.mark.parametrize("bc", ["pressure_release", "rigid"])
+@pytest.mark.parametrize("n", [3, 4])
+def test_tc_n5_matches_oracle(cuda, bc, n):
+    """N=5 with the reference's 95-point rule; 4^3 x 6 (K=384, tiles full)
+    and 3^3 x 6 (K=162, a partial last tile)."""
+    from oracle import Oracle
+    cub, tri = ref_rule(5)
+    p = make_problem(5, n, variant="nodal", c2="sine", c2_jitter=0.5, seed=5, cubature=cub,
+                     tri_cubature=tri)
+    orc = Oracle(5, p.K, p.ops_dict(), p.geo_dict(), variant="nodal",
+                 bc=1 if bc == "rigid" else 0)
+    q_ref, r_ref = orc.run(p.Q0.copy(), p.dt, 25)
+    s = WaveSolver(p, bc=bc, precision="f16x3")
+    s.set_data(p.Q0)
+    s.steps(p.dt, 5)
+    s.check()
+    assert rel_l2(s.get_data(), q_ref) < TOL
+    assert rel_l2(s.get_residual(), r_ref) < 1e-4
+
+
+def test_tc_agrees_with_fp32_stage_over_many_steps(cuda):
+    cub, tri = ref_rule(5)
+    p = make_problem(5, 4, variant="nodal", c2="sine", c2_jitter=0.5, seed=9, cubature=cub,
+                     tri_cubature=tri, cfl=0.25)
+    a = WaveSolver(p, precision="fp32")
+    b = WaveSolver(p, precision="f16x3")
+    a.set_data(p.Q0)
+    b.set_data(p.Q0)
+    a.steps(p.dt, 50)
+    b.steps(p.dt, 50)
+    b.check()
+    assert rel_l2(b.get_data(), a.get_data()) < TOL
+
+
+def test_tc_rejects_unsupported(cuda):
+    from bbwadg_b200._lib import BBWError
+    p = make_problem(4, 2, variant="nodal")
+    with pytest.raises(BBWError):
+        WaveSolver(p, precision="f16x3")
+    p = make_problem(3, 2, variant="bb")
+    with pytest.raises(BBWError):
+        WaveSolver(p, precision="f16x3")
