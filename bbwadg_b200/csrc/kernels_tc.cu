@@ -216,16 +216,19 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
     tc::fence_after_sync();
   };
   // one operator/operand product chain: D (+)= A B^T over ksteps, 3 products
+  // descriptors of consecutive K steps differ only in the start-address field
+  // (+256 bytes = +16 in 16-byte units)
   auto chain = [&](uint32_t d, const __half *Ahi, const __half *Alo, int asbo, const __half *Bhi,
                    const __half *Blo, int bsbo, int ksteps, uint32_t idesc, bool acc) {
+    uint64_t ah = tc::smem_desc(tc::smem_u32(Ahi), 128, asbo);
+    uint64_t al = tc::smem_desc(tc::smem_u32(Alo), 128, asbo);
+    uint64_t bh = tc::smem_desc(tc::smem_u32(Bhi), 128, bsbo);
+    uint64_t bl = tc::smem_desc(tc::smem_u32(Blo), 128, bsbo);
     for (int s = 0; s < ksteps; ++s) {
-      const uint64_t ah = tc::smem_desc(tc::smem_u32(Ahi) + 256 * s, 128, asbo);
-      const uint64_t al = tc::smem_desc(tc::smem_u32(Alo) + 256 * s, 128, asbo);
-      const uint64_t bh = tc::smem_desc(tc::smem_u32(Bhi) + 256 * s, 128, bsbo);
-      const uint64_t bl = tc::smem_desc(tc::smem_u32(Blo) + 256 * s, 128, bsbo);
       tc::mma_f16(d, ah, bh, idesc, (acc || s > 0) ? 1u : 0u);
       tc::mma_f16(d, ah, bl, idesc, 1u);
       tc::mma_f16(d, al, bh, idesc, 1u);
+      ah += 16, al += 16, bh += 16, bl += 16;
     }
   };
 
@@ -243,7 +246,26 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
     if (tid < 8) sRed[tid] = 0;
     __syncthreads();
 
-    // ---- P1: neighbour traces, upwind flux (Uflux = -pflux), maxima
+    // ---- P1: neighbour traces (global ones issued first), upwind flux
+    //          (Uflux = -pflux), maxima
+    float nbv[FIT][4];
+#pragma unroll
+    for (int j = 0; j < FIT; ++j) {
+      nbv[j][0] = nbv[j][1] = nbv[j][2] = nbv[j][3] = 0.f;
+      const int i = tid + j * TC_T;
+      if (i >= TC_E * NF) continue;
+      const int e = i & 31, m = i >> 5, f = m / Nfp;
+      if (e >= ne) continue;
+      const int code = sNbr[e * 4 + f];
+      const int pat = code & 255;
+      if (pat == 255) continue;
+      const int vP = sPat[pat * Nfp + (m - f * Nfp)];
+      const unsigned rel = (unsigned)((code >> 8) - k0);
+      if (rel < (unsigned)ne) continue;  // inside the tile: read from shared memory below
+      const float *o = P.Qin + (size_t)(code >> 8) * 4 * Np + vP;
+      nbv[j][0] = __ldg(o), nbv[j][1] = __ldg(o + Np), nbv[j][2] = __ldg(o + 2 * Np),
+      nbv[j][3] = __ldg(o + 3 * Np);
+    }
     float pf[FIT];
     float mF = 0.f;
 #pragma unroll
@@ -270,15 +292,11 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
           Unjump = -2.f * (uM * nx + vvM * ny + wM * nz);
         }
       } else {
-        const int vP = sPat[pat * Nfp + (m - f * Nfp)];
         const unsigned rel = (unsigned)((code >> 8) - k0);
-        float pP, uP, vP_, wP;
+        float pP = nbv[j][0], uP = nbv[j][1], vP_ = nbv[j][2], wP = nbv[j][3];
         if (rel < (unsigned)ne) {  // neighbour inside the tile
-          const float *o = sRaw + rel * RS + vP;
+          const float *o = sRaw + rel * RS + sPat[pat * Nfp + (m - f * Nfp)];
           pP = o[0], uP = o[Np], vP_ = o[2 * Np], wP = o[3 * Np];
-        } else {
-          const float *o = P.Qin + (size_t)(code >> 8) * 4 * Np + vP;
-          pP = __ldg(o), uP = __ldg(o + Np), vP_ = __ldg(o + 2 * Np), wP = __ldg(o + 3 * Np);
         }
         pjump = pP - pM;
         Unjump = (uP - uM) * nx + (vP_ - vvM) * ny + (wP - wM) * nz;
@@ -373,6 +391,20 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
 #pragma unroll
       for (int f = 0; f < 4; ++f) tc::tmem_ld8(trow + 128 + 32 * f, lf[f]);
       const float isp = 1.f / sp, isU = 1.f / sU, isF = 1.f / sF;
+      // old residual and state of u, v, w for this row: all loads first
+      const bool rowok = lane < 16 && n < Np;
+      float ro[8][3], qo[8][3];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int e = 8 * g8 + j;
+        const size_t id = (size_t)(k0 + e) * 4 * Np + n;
+#pragma unroll
+        for (int fl = 1; fl < 4; ++fl) {
+          const bool ok = rowok && e < ne;
+          ro[j][fl - 1] = ok ? P.res[id + fl * Np] : 0.f;
+          qo[j][fl - 1] = ok ? __ldg(P.Qin + id + fl * Np) : 0.f;
+        }
+      }
       float mr = 0.f;
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
@@ -391,7 +423,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
           vv -= Ge[9 + 4 * f + 2] * a;
           vw -= Ge[9 + 4 * f + 3] * a;
         }
-        const bool ok = lane < 16 && n < Np && e < ne;
+        const bool ok = rowok && e < ne;
         rp[j] = ok ? vp : 0.f;
         mr = fmaxf(mr, fabsf(rp[j]));
         if (ok) {
@@ -399,9 +431,9 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
           const float rv3[3] = {vu, vv, vw};
 #pragma unroll
           for (int fl = 1; fl < 4; ++fl) {
-            const float r = P.fa * P.res[id + fl * Np] + P.fdt * rv3[fl - 1];
+            const float r = P.fa * ro[j][fl - 1] + P.fdt * rv3[fl - 1];
             P.res[id + fl * Np] = r;
-            P.Qout[id + fl * Np] = __ldg(P.Qin + id + fl * Np) + P.fb * r;
+            P.Qout[id + fl * Np] = qo[j][fl - 1] + P.fb * r;
           }
         }
       }
@@ -469,14 +501,22 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       tc::tmem_ld8(tbase + ((uint32_t)(32 * q4) << 16) + 32 + 8 * g8, w);
       const float isc = 1.f / sc;
       if (lane < 16 && n < Np) {
+        float ro[8], qo[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int e = 8 * g8 + j;
+          const size_t id = (size_t)(k0 + e) * 4 * Np + n;
+          ro[j] = e < ne ? P.res[id] : 0.f;
+          qo[j] = e < ne ? __ldg(P.Qin + id) : 0.f;
+        }
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
           const int e = 8 * g8 + j;
           if (e >= ne) continue;
           const size_t id = (size_t)(k0 + e) * 4 * Np + n;
-          const float r = P.fa * P.res[id] + P.fdt * (w[j] * isc);
+          const float r = P.fa * ro[j] + P.fdt * (w[j] * isc);
           P.res[id] = r;
-          P.Qout[id] = __ldg(P.Qin + id) + P.fb * r;
+          P.Qout[id] = qo[j] + P.fb * r;
         }
       }
     }

@@ -179,10 +179,11 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--variant", default="nodal", choices=["nodal", "bb"])
+    ap.add_argument("--variant", default="nodal", choices=["nodal", "bb", "nodal-f16x3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--hex", type=int, default=N_HEX, help="hexes per direction (profiling cases)")
-    ap.add_argument("--variants", default="nodal,bb", help="variants to run, comma separated")
+    ap.add_argument("--variants", default="nodal,bb,nodal-f16x3",
+                    help="variants to run, comma separated (nodal, bb, nodal-f16x3)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -204,10 +205,11 @@ def main():
     if args.variant not in variants:
         variants.insert(0, args.variant)
     for variant in variants:
-        prob = make_problem(N_ORDER, args.hex, variant=variant, c2="sine", c2_jitter=0.5,
+        basis, prec = (variant.split("-") + ["fp32"])[:2]
+        prob = make_problem(N_ORDER, args.hex, variant=basis, c2="sine", c2_jitter=0.5,
                             seed=1234 + rank, cubature=cub, tri_cubature=tri, cfl=0.25)
         K, Np, Nq = prob.K, prob.Np, prob.Nq
-        s = WaveSolver(prob)
+        s = WaveSolver(prob, precision=prec)
         s.set_data(prob.Q0)
         qptr, rptr, stream_ptr = s.device_state()
         stream = torch.cuda.ExternalStream(stream_ptr)
@@ -275,7 +277,8 @@ def main():
         "data": "synthetic", "config": workload_config(args, args.variant),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "kernel": "k_fused_stage<%d,%s>" % (N_ORDER, args.variant == "bb"),
+                     "kernel": ("k_tc_stage<%d>" % N_ORDER) if args.variant.endswith("f16x3")
+                     else "k_fused_stage<%d,%s>" % (N_ORDER, args.variant == "bb"),
                      "peak_kind": peak_kind},
         "e2e": {"value": world * head["dofs"] / head["e2e_s"], "unit": "DOF-stage/s",
                 "h2d_bytes_per_step": head["state_bytes"] / args.steps,
