@@ -50,6 +50,7 @@ SIGNATURES = {
     "bbw_ops_build": (c_int, [c_int, P, c_int, P, c_int, ctypes.POINTER(c_void_p)]),
     "bbw_ops_get": (c_int, [c_void_p, ctypes.c_char_p, c_int, P, ctypes.POINTER(ctypes.c_longlong)]),
     "bbw_ops_free": (None, [c_void_p]),
+    "bbw_basis_eval": (c_int, [c_int, c_int, c_int, P, P, P, P]),
     "bbw_rk_volume": (c_int, [c_int, c_int, P, P, P, P, P, P, P]),
     "bbw_rk_surface": (c_int, [c_int, c_int, c_int, P, P, P, P, P, P, P]),
     "bbw_rk_update": (c_int, [c_int, c_int, c_float, c_float, c_float, P, P, P, P]),
@@ -72,6 +73,13 @@ SIGNATURES = {
     "bbw_steps": (c_int, [c_void_p, c_float, c_int]),
     "bbw_run": (c_int, [c_void_p, c_double, c_float]),
     "bbw_sync": (c_int, [c_void_p]),
+    "bbw_stage_ex": (c_int, [c_void_p, c_float, c_float, c_float, c_float]),
+    "bbw_set_shots": (c_int, [c_void_p, c_int]),
+    "bbw_set_sources": (c_int, [c_void_p, c_int, P, P, P, c_float, c_float, c_float, c_int]),
+    "bbw_set_receivers": (c_int, [c_void_p, c_int, P, P, c_int]),
+    "bbw_get_traces": (c_int, [c_void_p, P, ctypes.POINTER(c_int)]),
+    "bbw_set_time": (c_int, [c_void_p, c_double]),
+    "bbw_get_time": (c_int, [c_void_p, ctypes.POINTER(c_double), ctypes.POINTER(c_int)]),
     "bbw_device_state": (c_int, [c_void_p, ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p),
                                  ctypes.POINTER(c_void_p)]),
 }

@@ -7,6 +7,7 @@
 // Wave_RK :2014-2081, WaveSetData3d / WaveGetData3d :2527-2558).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -30,6 +31,11 @@ static const double kRK4B[5] = {1432997174477.0 / 9575080441755.0,
                                 1720146321549.0 / 2090206949498.0,
                                 3134564353537.0 / 4481467310338.0,
                                 2277821191437.0 / 14882151754819.0};
+// stage times t + rk4c[s] dt, cpp/src/StartUp3d.cpp:531-537
+static const double kRK4C[5] = {0.0, 1432997174477.0 / 9575080441755.0,
+                                2526269341429.0 / 6820363962896.0,
+                                2006345519317.0 / 3224310063776.0,
+                                2802321613138.0 / 2924317926251.0};
 
 static int round4i(int x) { return (x + 3) & ~3; }
 static int cdivi(int a, int b) { return (a + b - 1) / b; }
@@ -48,6 +54,15 @@ struct bbw_ctx {
   int *nbr = nullptr, *tables = nullptr;
   FusedPlan plan;
   int precision = BBW_PREC_FP32;
+  int S = 1;  // shots
+  double *d_time = nullptr;
+  int *d_step = nullptr;
+  int *src_off = nullptr, *src_elem = nullptr;
+  float *src_vec = nullptr;
+  int src_stage_times = 0;
+  int R = 0, max_steps = 0;
+  int *rec_elem = nullptr;
+  float *rec_w = nullptr, *traces = nullptr;
   TcPlan tc;
   float *geo_tc = nullptr;
   void *ops_tc = nullptr;
@@ -81,6 +96,14 @@ void release(bbw_ctx *c) {
   cudaFree(c->ops);
   cudaFree(c->nbr);
   cudaFree(c->tables);
+  cudaFree(c->d_time);
+  cudaFree(c->d_step);
+  cudaFree(c->src_off);
+  cudaFree(c->src_elem);
+  cudaFree(c->src_vec);
+  cudaFree(c->rec_elem);
+  cudaFree(c->rec_w);
+  cudaFree(c->traces);
   cudaFree(c->geo_tc);
   cudaFree(c->ops_tc);
   cudaFree(c->err);
@@ -300,7 +323,9 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
       (s = upload(&c->c2q, c2J.data(), c2J.size(), "bbw_create: c2q")) != BBW_OK ||
       (s = upload(&c->nbr, nbr.data(), nbr.size(), "bbw_create: connectivity")) != BBW_OK ||
       (s = upload(&c->ops, ops.data(), ops.size(), "bbw_create: operators")) != BBW_OK ||
-      (s = upload(&c->tables, tab.data(), tab.size(), "bbw_create: tables")) != BBW_OK) {
+      (s = upload(&c->tables, tab.data(), tab.size(), "bbw_create: tables")) != BBW_OK ||
+      (s = upload<double>(&c->d_time, nullptr, 1, "bbw_create: clock")) != BBW_OK ||
+      (s = upload<int>(&c->d_step, nullptr, 1, "bbw_create: clock")) != BBW_OK) {
     release(c);
     return s;
   }
@@ -311,6 +336,7 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
   pl.ops = c->ops, pl.ops_floats = (int)ops.size();
   pl.off_lift = off_lift, pl.off_pq = off_pq, pl.off_vq = off_vq;
   pl.tables = c->tables, pl.table_ints = (int)tab.size(), pl.pat_off = pat_off, pl.bb_off = bb_off;
+  pl.S = 1, pl.time = c->d_time;
   if ((s = fused_prepare(pl)) != BBW_OK) {
     release(c);
     return s;
@@ -379,7 +405,7 @@ extern "C" bbw_status bbw_destroy(bbw_ctx *c) {
 
 static bbw_status copy_state(bbw_ctx *c, float *dev, const float *src, float *dst) {
   if (!c) return set_error(BBW_ERR_ARG, "bbw: ctx is NULL");
-  const size_t bytes = (size_t)c->K * 4 * c->Np * sizeof(float);
+  const size_t bytes = (size_t)c->S * c->K * 4 * c->Np * sizeof(float);
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return set_cuda_error(e, "bbw: sync");
   if (src) e = cudaMemcpy(dev, src, bytes, cudaMemcpyHostToDevice);
@@ -404,14 +430,38 @@ extern "C" bbw_status bbw_get_residual(bbw_ctx *c, float *r) {
   return copy_state(c, c->res, nullptr, r);
 }
 
-extern "C" bbw_status bbw_stage(bbw_ctx *c, float fa, float fb, float fdt) {
+static void drop_graphs(bbw_ctx *c) {
+  for (int i = 0; i < 2; ++i) {
+    if (c->step_graph[i]) cudaGraphExecDestroy(c->step_graph[i]);
+    c->step_graph[i] = nullptr;
+  }
+}
+
+extern "C" bbw_status bbw_stage_ex(bbw_ctx *c, float fa, float fb, float fdt, float cstage) {
   if (!c) return set_error(BBW_ERR_ARG, "bbw_stage: ctx is NULL");
   bbw_status s =
       c->precision == BBW_PREC_F16X3
           ? tc_launch(c->tc, c->Q[c->cur], c->Q[c->cur ^ 1], c->res, fa, fb, fdt, c->stream)
-          : fused_launch(c->plan, c->Q[c->cur], c->Q[c->cur ^ 1], c->res, fa, fb, fdt, c->stream);
+          : fused_launch(c->plan, c->Q[c->cur], c->Q[c->cur ^ 1], c->res, fa, fb, fdt, cstage,
+                         c->stream);
   if (s == BBW_OK) c->cur ^= 1;
   return s;
+}
+
+extern "C" bbw_status bbw_stage(bbw_ctx *c, float fa, float fb, float fdt) {
+  return bbw_stage_ex(c, fa, fb, fdt, 0.f);
+}
+
+// one LSRK45 step: five fused stages at times t + rk4c[s] dt, then the
+// receivers and the clock
+static bbw_status one_step(bbw_ctx *c, float dt) {
+  bbw_status s = BBW_OK;
+  for (int i = 0; i < 5 && s == BBW_OK; ++i)
+    s = bbw_stage_ex(c, (float)kRK4A[i], (float)kRK4B[i], dt,
+                     c->src_stage_times ? (float)kRK4C[i] : 0.f);
+  if (s != BBW_OK) return s;
+  return record_and_advance(c->N, c->K, c->S, c->Q[c->cur], c->R, c->rec_elem, c->rec_w,
+                            c->traces, c->max_steps, c->d_time, c->d_step, dt, c->stream);
 }
 
 extern "C" bbw_status bbw_steps(bbw_ctx *c, float dt, int nsteps) {
@@ -426,9 +476,7 @@ extern "C" bbw_status bbw_steps(bbw_ctx *c, float dt, int nsteps) {
       cudaGraph_t g;
       cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
       if (e != cudaSuccess) return set_cuda_error(e, "bbw_steps: capture");
-      bbw_status s = BBW_OK;
-      for (int i = 0; i < 5 && s == BBW_OK; ++i)
-        s = bbw_stage(c, (float)kRK4A[i], (float)kRK4B[i], dt);
+      bbw_status s = one_step(c, dt);
       e = cudaStreamEndCapture(c->stream, &g);
       c->cur = par;  // capture recorded the launches without running them
       if (s != BBW_OK) return s;
@@ -443,6 +491,139 @@ extern "C" bbw_status bbw_steps(bbw_ctx *c, float dt, int nsteps) {
     c->cur ^= 1;  // five stages swap the buffers an odd number of times
   }
   return BBW_OK;
+}
+
+extern "C" bbw_status bbw_set_shots(bbw_ctx *c, int S) {
+  if (!c || S < 1) return set_error(BBW_ERR_ARG, "bbw_set_shots: bad argument");
+  if (S > 1 && c->precision != BBW_PREC_FP32)
+    return set_error(BBW_ERR_UNSUPPORTED, "bbw_set_shots: batched shots need BBW_PREC_FP32");
+  cudaStreamSynchronize(c->stream);
+  const size_t n = (size_t)S * c->K * 4 * c->Np;
+  if ((size_t)S * c->K * 4 * c->Np > ((size_t)1 << 40))
+    return set_error(BBW_ERR_ARG, "bbw_set_shots: too large");
+  float *q0 = nullptr, *q1 = nullptr, *r = nullptr;
+  bbw_status s;
+  if ((s = upload<float>(&q0, nullptr, n, "bbw_set_shots")) != BBW_OK ||
+      (s = upload<float>(&q1, nullptr, n, "bbw_set_shots")) != BBW_OK ||
+      (s = upload<float>(&r, nullptr, n, "bbw_set_shots")) != BBW_OK) {
+    cudaFree(q0);
+    cudaFree(q1);
+    cudaFree(r);
+    return s;
+  }
+  cudaFree(c->Q[0]);
+  cudaFree(c->Q[1]);
+  cudaFree(c->res);
+  c->Q[0] = q0, c->Q[1] = q1, c->res = r, c->cur = 0;
+  c->S = S;
+  c->plan.S = S;
+  if (c->src_off) {  // source table is per shot: drop it
+    cudaFree(c->src_off), cudaFree(c->src_elem), cudaFree(c->src_vec);
+    c->src_off = c->src_elem = nullptr, c->src_vec = nullptr;
+    c->plan.src_off = c->plan.src_elem = nullptr, c->plan.src_vec = nullptr;
+  }
+  if (c->traces) {
+    cudaFree(c->traces);
+    c->traces = nullptr;
+    if (c->R > 0 &&
+        (s = upload<float>(&c->traces, nullptr, (size_t)S * c->R * c->max_steps,
+                           "bbw_set_shots: traces")) != BBW_OK)
+      return s;
+  }
+  drop_graphs(c);
+  return BBW_OK;
+}
+
+extern "C" bbw_status bbw_set_sources(bbw_ctx *c, int nent, const int *shot, const int *elem,
+                                      const float *vec, float f0, float t_delay, float amplitude,
+                                      int stage_times) {
+  if (!c || nent < 0 || (nent > 0 && (!shot || !elem || !vec)))
+    return set_error(BBW_ERR_ARG, "bbw_set_sources: bad argument");
+  if (nent > 0 && c->precision != BBW_PREC_FP32)
+    return set_error(BBW_ERR_UNSUPPORTED, "bbw_set_sources: sources need BBW_PREC_FP32");
+  cudaStreamSynchronize(c->stream);
+  cudaFree(c->src_off), cudaFree(c->src_elem), cudaFree(c->src_vec);
+  c->src_off = c->src_elem = nullptr, c->src_vec = nullptr;
+  c->plan.src_off = c->plan.src_elem = nullptr, c->plan.src_vec = nullptr;
+  drop_graphs(c);
+  if (nent == 0) return BBW_OK;
+  const int Np = c->Np;
+  std::vector<int> off(c->S + 1, 0), order(nent), el(nent);
+  for (int j = 0; j < nent; ++j) {
+    if (shot[j] < 0 || shot[j] >= c->S || elem[j] < 0 || elem[j] >= c->K)
+      return set_error(BBW_ERR_ARG, "bbw_set_sources: shot or element out of range");
+    off[shot[j] + 1] += 1;
+  }
+  for (int i = 0; i < c->S; ++i) off[i + 1] += off[i];
+  std::vector<int> fill(off.begin(), off.end() - 1);
+  std::vector<float> v((size_t)nent * Np);
+  for (int j = 0; j < nent; ++j) {
+    const int at = fill[shot[j]]++;
+    el[at] = elem[j];
+    std::memcpy(&v[(size_t)at * Np], vec + (size_t)j * Np, Np * sizeof(float));
+  }
+  bbw_status s;
+  if ((s = upload(&c->src_off, off.data(), off.size(), "bbw_set_sources")) != BBW_OK ||
+      (s = upload(&c->src_elem, el.data(), el.size(), "bbw_set_sources")) != BBW_OK ||
+      (s = upload(&c->src_vec, v.data(), v.size(), "bbw_set_sources")) != BBW_OK)
+    return s;
+  c->plan.src_off = c->src_off, c->plan.src_elem = c->src_elem, c->plan.src_vec = c->src_vec;
+  c->plan.f0 = f0, c->plan.tR = t_delay, c->plan.samp = amplitude;
+  c->src_stage_times = stage_times != 0;
+  return BBW_OK;
+}
+
+extern "C" bbw_status bbw_set_receivers(bbw_ctx *c, int R, const int *elem, const float *w,
+                                        int max_steps) {
+  if (!c || R < 0 || max_steps < 0 || (R > 0 && (!elem || !w)))
+    return set_error(BBW_ERR_ARG, "bbw_set_receivers: bad argument");
+  cudaStreamSynchronize(c->stream);
+  cudaFree(c->rec_elem), cudaFree(c->rec_w), cudaFree(c->traces);
+  c->rec_elem = nullptr, c->rec_w = nullptr, c->traces = nullptr;
+  c->R = 0, c->max_steps = 0;
+  drop_graphs(c);
+  if (R == 0) return BBW_OK;
+  for (int r = 0; r < R; ++r)
+    if (elem[r] < 0 || elem[r] >= c->K)
+      return set_error(BBW_ERR_ARG, "bbw_set_receivers: element out of range");
+  bbw_status s;
+  if ((s = upload(&c->rec_elem, elem, (size_t)R, "bbw_set_receivers")) != BBW_OK ||
+      (s = upload(&c->rec_w, w, (size_t)R * c->Np, "bbw_set_receivers")) != BBW_OK ||
+      (s = upload<float>(&c->traces, nullptr, (size_t)c->S * R * std::max(max_steps, 1),
+                         "bbw_set_receivers")) != BBW_OK)
+    return s;
+  c->R = R, c->max_steps = max_steps;
+  return BBW_OK;
+}
+
+extern "C" bbw_status bbw_get_traces(bbw_ctx *c, float *out, int *nsteps) {
+  if (!c || !out) return set_error(BBW_ERR_ARG, "bbw_get_traces: bad argument");
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return set_cuda_error(e, "bbw_get_traces");
+  int st = 0;
+  e = cudaMemcpy(&st, c->d_step, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return set_cuda_error(e, "bbw_get_traces");
+  if (nsteps) *nsteps = std::min(st, c->max_steps);
+  if (c->R == 0) return BBW_OK;
+  e = cudaMemcpy(out, c->traces, (size_t)c->S * c->R * c->max_steps * sizeof(float),
+                 cudaMemcpyDeviceToHost);
+  return set_cuda_error(e, "bbw_get_traces");
+}
+
+extern "C" bbw_status bbw_set_time(bbw_ctx *c, double t) {
+  if (!c) return set_error(BBW_ERR_ARG, "bbw_set_time: ctx is NULL");
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e == cudaSuccess) e = cudaMemcpy(c->d_time, &t, sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(c->d_step, 0, sizeof(int));
+  return set_cuda_error(e, "bbw_set_time");
+}
+
+extern "C" bbw_status bbw_get_time(bbw_ctx *c, double *t, int *step) {
+  if (!c) return set_error(BBW_ERR_ARG, "bbw_get_time: ctx is NULL");
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e == cudaSuccess && t) e = cudaMemcpy(t, c->d_time, sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && step) e = cudaMemcpy(step, c->d_step, sizeof(int), cudaMemcpyDeviceToHost);
+  return set_cuda_error(e, "bbw_get_time");
 }
 
 extern "C" bbw_status bbw_run(bbw_ctx *c, double final_time, float dt) {

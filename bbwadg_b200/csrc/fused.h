@@ -24,6 +24,11 @@ struct FusedPlan {
   int off_lift = 0, off_pq = 0, off_vq = 0;
   const int *tables = nullptr;
   int table_ints = 0, pat_off = 0, bb_off = 0;
+  int S = 1, nsm = 148;  // shots per launch, SM count
+  const int *src_off = nullptr, *src_elem = nullptr;  // sources (null: none)
+  const float *src_vec = nullptr;
+  float f0 = 0.f, tR = 0.f, samp = 0.f;
+  const double *time = nullptr;
 };
 
 int fused_warps(int N);
@@ -58,6 +63,10 @@ void tc_pack_operator(const float *A, int nrows, int ncols, int ld_row, int ld_c
                       int kp, __half *hi, __half *lo);
 bbw_status fused_prepare(FusedPlan &pl);
 bbw_status fused_launch(const FusedPlan &pl, const float *Qin, float *Qout, float *res, float fa,
-                        float fb, float fdt, cudaStream_t st);
+                        float fb, float fdt, float cstage, cudaStream_t st);
+// receivers of all shots after a step, then time += dt, step += 1
+bbw_status record_and_advance(int N, int K, int S, const float *Q, int R, const int *rec_elem,
+                              const float *rec_w, float *traces, int max_steps, double *time,
+                              int *step, float dt, cudaStream_t st);
 
 }  // namespace bbw

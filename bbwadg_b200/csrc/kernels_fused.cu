@@ -82,7 +82,23 @@ struct FusedParams {
   int off_lift, off_pq, off_vq, off_end;  // operator offsets in ops (floats)
   const int *__restrict__ tables;   // Fmask [NF] | patterns [npat][Nfp] | BB tables
   int table_ints;
+  // batched shots: state arrays hold S consecutive [K][4][Np] blocks
+  int S;
+  // sources: entries [src_off[s], src_off[s+1]) of shot s add
+  // ricker(t) * src_vec[j][:] to the projected rhs_p of element src_elem[j],
+  // t = *time + cstage * fdt
+  const int *__restrict__ src_off;
+  const int *__restrict__ src_elem;
+  const float *__restrict__ src_vec;
+  float f0, tR, samp, cstage;
+  const double *__restrict__ time;  // simulation time at the start of the step
 };
+
+// Ricker wavelet amp (1 - 2 a^2) exp(-a^2), a = pi f0 (t - tR)
+__device__ __forceinline__ float ricker(float t, float f0, float tR, float amp) {
+  const float a = 3.14159265358979f * f0 * (t - tR);
+  return amp * (1.f - 2.f * a * a) * expf(-a * a);
+}
 
 // Shared-memory map (floats, rows of stride ES).  Input tiles are double
 // buffered when they fit (PIPE): the next tile's copies are in flight while
@@ -156,7 +172,10 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
   const int *bbTab = sTab + P.bb_off;
 
   // asynchronous copies of one tile's inputs into buffer `buf`
-  auto issue_tile = [&](int tile, float *buf) {
+  const int ntiles = cdiv(P.K, TILE_E);
+  const size_t sstride = (size_t)P.K * 4 * Np;  // floats per shot
+  auto issue_tile = [&](int vt, float *buf) {
+    const int shot = vt / ntiles, tile = vt - shot * ntiles;
     const int k0 = tile * TILE_E, ne = min(TILE_E, P.K - k0);
     float *bQ = buf + L::inQ, *bGeo = buf + L::inGeo, *bC2 = buf + L::inC2;
     int *bNbr = (int *)(buf + L::inNbr);
@@ -167,7 +186,7 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
                 i < ne * 16);
     for (int i = tid; i < TILE_E * 4; i += T)  // zero codes of absent elements: element 0, never used
       cp_async4(&bNbr[i], P.nbr + (size_t)k0 * 4 + (i < ne * 4 ? i : 0), i < ne * 4);
-    const float *Qg = P.Qin + (size_t)k0 * 4 * Np;
+    const float *Qg = P.Qin + shot * sstride + (size_t)k0 * 4 * Np;
 #pragma unroll 4
     for (int j = 0; j < QIT; ++j) {
       const int i = tid + j * T;
@@ -186,7 +205,8 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
     cp_async_commit();
   };
   // neighbour face traces of the tile in `buf` into registers
-  auto load_traces = [&](const float *buf, int tile_of_buf, float (&nb)[FIT][4]) {
+  auto load_traces = [&](const float *buf, int vt, float (&nb)[FIT][4]) {
+    const int shot = vt / ntiles, tile_of_buf = vt - shot * ntiles;
     const int ne_b = min(TILE_E, P.K - tile_of_buf * TILE_E);
     const int *bNbr = (const int *)(buf + L::inNbr);
 #pragma unroll
@@ -199,8 +219,8 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
         const int pat = code & 255;
         const unsigned rel = (unsigned)((code >> 8) - tile_of_buf * TILE_E);
         if (pat != 255 && rel >= (unsigned)ne_b) {  // neighbours inside the tile: from smem
-          const float *q2 =
-              P.Qin + (size_t)(code >> 8) * 4 * Np + sPat[pat * Nfp + (m - f * Nfp)];
+          const float *q2 = P.Qin + shot * sstride + (size_t)(code >> 8) * 4 * Np +
+                            sPat[pat * Nfp + (m - f * Nfp)];
           nb[j][0] = __ldg(q2);
           nb[j][1] = __ldg(q2 + Np);
           nb[j][2] = __ldg(q2 + 2 * Np);
@@ -210,24 +230,26 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
     }
   };
 
-  const int ntiles = cdiv(P.K, TILE_E);
-  int tile = blockIdx.x, b = 0;
+  const int nvt = P.S * ntiles;  // (shot, tile) work items
+  int vt = blockIdx.x, b = 0;
   float nb[FIT][4];
   __syncthreads();  // tables staged
-  if (tile < ntiles) {
-    issue_tile(tile, sIn);
+  if (vt < nvt) {
+    issue_tile(vt, sIn);
     cp_async_wait_all();
     __syncthreads();
-    load_traces(sIn, tile, nb);
+    load_traces(sIn, vt, nb);
   }
-  for (; tile < ntiles; tile += gridDim.x) {
+  for (; vt < nvt; vt += gridDim.x) {
+    const int shot = vt / ntiles, tile = vt - shot * ntiles;
     const int k0 = tile * TILE_E;
     const int ne = min(TILE_E, P.K - k0);
-    const int next = tile + gridDim.x;
+    const int next = vt + gridDim.x;
+    const size_t sbase = shot * sstride;
     float *cur = sIn + b * inSize;
     const float *sQ = cur + L::inQ, *sGeo = cur + L::inGeo, *sC2 = cur + L::inC2;
     const int *sNbr = (const int *)(cur + L::inNbr);
-    if (PIPE && next < ntiles) issue_tile(next, sIn + (b ^ 1) * inSize);
+    if (PIPE && next < nvt) issue_tile(next, sIn + (b ^ 1) * inSize);
 
     // ---- 1. upwind flux at the 4Nfp face nodes (Uflux = -pflux); traces of
     //         neighbours inside the tile come from the state tile itself
@@ -452,7 +474,7 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
     }
     if (PIPE) cp_async_wait_all();  // the next tile's inputs have landed
     __syncthreads();
-    if (PIPE && next < ntiles) load_traces(sIn + (b ^ 1) * inSize, next, nb);  // in flight from here
+    if (PIPE && next < nvt) load_traces(sIn + (b ^ 1) * inSize, next, nb);  // in flight from here
 
     // ---- 5. WADG: p at the cubature points, times c2/J
     {
@@ -481,7 +503,7 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
     // ---- 6. project back: rhs_p = Pq * (c2 p_q); the residual tile is
     //         fetched meanwhile for the stage update (scalar, coalesced)
     constexpr int UIT = cdiv(TILE_E * 4 * Np, T);
-    const float *resg = P.res + (size_t)k0 * 4 * Np;
+    const float *resg = P.res + sbase + (size_t)k0 * 4 * Np;
     float rpre[UIT];
 #pragma unroll
     for (int j = 0; j < UIT; ++j) {
@@ -505,6 +527,22 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
 #pragma unroll
         for (int i = 0; i < R; ++i) acc[i] += o[i] * x;
       }
+      // source term of this shot, added to the projected rhs_p as
+      // rk_update_elas does (acous_elas_cpp/okl/ElasKernelsWADG.okl:400-403)
+      if (P.src_off) {
+        const int j0 = __ldg(P.src_off + shot), j1 = __ldg(P.src_off + shot + 1);
+        if (j1 > j0) {
+          const float amp = ricker((float)(*P.time) + P.cstage * P.fdt, P.f0, P.tR, P.samp);
+          for (int j = j0; j < j1; ++j) {
+            const unsigned rel = (unsigned)(__ldg(P.src_elem + j) - k0);
+            if (rel < (unsigned)ne && lane == (int)rel) {
+#pragma unroll
+              for (int i = 0; i < R; ++i)
+                if (r0 + i < Np) acc[i] += amp * __ldg(P.src_vec + (size_t)j * Np + r0 + i);
+            }
+          }
+        }
+      }
       __syncthreads();  // everyone has read sR rows [0, Np) in step 5
 #pragma unroll
       for (int i = 0; i < R; ++i)
@@ -515,8 +553,8 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
     // ---- 7. LSRK stage update, coalesced and conflict-free:
     //         res = fa res + fdt rhs; Q += fb res
     {
-      float *resw = P.res + (size_t)k0 * 4 * Np;
-      float *qg = P.Qout + (size_t)k0 * 4 * Np;
+      float *resw = P.res + sbase + (size_t)k0 * 4 * Np;
+      float *qg = P.Qout + sbase + (size_t)k0 * 4 * Np;
 #pragma unroll
       for (int j = 0; j < UIT; ++j) {
         const int i = tid + j * T;
@@ -528,7 +566,7 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
       }
     }
     __syncthreads();  // tile buffers and work arrays free for reuse
-    if (!PIPE && next < ntiles) {
+    if (!PIPE && next < nvt) {
       issue_tile(next, sIn);
       cp_async_wait_all();
       __syncthreads();
@@ -549,7 +587,7 @@ static size_t smem_bytes(int Nq, bool pipe, bool ops_smem, int ops_floats, int t
 
 template <int N, bool BB>
 static bbw_status launch_fused(const FusedPlan &pl, const float *Qin, float *Qout, float *res,
-                               float fa, float fb, float fdt, cudaStream_t st) {
+                               float fa, float fb, float fdt, float cstage, cudaStream_t st) {
   FusedParams P;
   P.K = pl.K, P.Nq = pl.Nq, P.RQ = pl.RQ, P.PRQ = pl.PRQ, P.bc = pl.bc, P.npat = pl.npat;
   P.pat_off = pl.pat_off, P.bb_off = pl.bb_off;
@@ -559,13 +597,18 @@ static bbw_status launch_fused(const FusedPlan &pl, const float *Qin, float *Qou
   P.ops = pl.ops;
   P.off_lift = pl.off_lift, P.off_pq = pl.off_pq, P.off_vq = pl.off_vq, P.off_end = pl.ops_floats;
   P.tables = pl.tables, P.table_ints = pl.table_ints;
+  P.S = pl.S;
+  P.src_off = pl.src_off, P.src_elem = pl.src_elem, P.src_vec = pl.src_vec;
+  P.f0 = pl.f0, P.tR = pl.tR, P.samp = pl.samp, P.cstage = cstage;
+  P.time = pl.time;
   const bool os = pl.ops_smem > 0;
   const size_t sm = pl.smem;
   const int T = FusedCfg<N>::T;
-  if (os && pl.pipe) k_fused_stage<N, BB, true, true><<<pl.grid, T, sm, st>>>(P);
-  else if (os) k_fused_stage<N, BB, true, false><<<pl.grid, T, sm, st>>>(P);
-  else if (pl.pipe) k_fused_stage<N, BB, false, true><<<pl.grid, T, sm, st>>>(P);
-  else k_fused_stage<N, BB, false, false><<<pl.grid, T, sm, st>>>(P);
+  const int grid = std::min(cdiv(pl.K, TILE_E) * std::max(pl.S, 1), pl.nsm);
+  if (os && pl.pipe) k_fused_stage<N, BB, true, true><<<grid, T, sm, st>>>(P);
+  else if (os) k_fused_stage<N, BB, true, false><<<grid, T, sm, st>>>(P);
+  else if (pl.pipe) k_fused_stage<N, BB, false, true><<<grid, T, sm, st>>>(P);
+  else k_fused_stage<N, BB, false, false><<<grid, T, sm, st>>>(P);
   return check_launch("fused stage");
 }
 
@@ -601,8 +644,8 @@ static bbw_status prepare(FusedPlan &pl) {
     e = cudaFuncSetAttribute(k_fused_stage<N, BB, false, false>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem);
   if (e != cudaSuccess) return set_cuda_error(e, "fused stage attribute");
-  const int ntiles = cdiv(pl.K, TILE_E);
-  pl.grid = std::min(ntiles, nsm > 0 ? nsm : 148);
+  pl.nsm = nsm > 0 ? nsm : 148;
+  pl.grid = std::min(cdiv(pl.K, TILE_E) * std::max(pl.S, 1), pl.nsm);
   return BBW_OK;
 }
 
@@ -644,8 +687,8 @@ int fused_warps(int N) {
 bbw_status fused_prepare(FusedPlan &pl) { FUSED_SWITCH(prepare, pl) }
 
 bbw_status fused_launch(const FusedPlan &pl, const float *Qin, float *Qout, float *res, float fa,
-                        float fb, float fdt, cudaStream_t st) {
-  FUSED_SWITCH(launch_fused, pl, Qin, Qout, res, fa, fb, fdt, st)
+                        float fb, float fdt, float cstage, cudaStream_t st) {
+  FUSED_SWITCH(launch_fused, pl, Qin, Qout, res, fa, fb, fdt, cstage, st)
 }
 
 }  // namespace bbw

@@ -817,3 +817,24 @@ extern "C" bbw_status bbw_ops_get(const bbw_ops *o, const char *name, int dtype,
 }
 
 extern "C" void bbw_ops_free(bbw_ops *o) { delete o; }
+
+extern "C" bbw_status bbw_basis_eval(int N, int variant, int npts, const double *r,
+                                     const double *s, const double *t, double *out) {
+  if (N < 1 || N > BBW_MAX_N || npts < 0 || (npts > 0 && (!r || !s || !t || !out)) ||
+      (variant != BBW_NODAL && variant != BBW_BB))
+    return BBW_ERR_ARG;
+  if (npts == 0) return BBW_OK;
+  bbw::Vec rr(r, r + npts), ss(s, s + npts), tt(t, t + npts);
+  bbw::Mat B;
+  if (variant == BBW_NODAL) {
+    bbw::Vec rn, sn, tn;
+    bbw::nodes3d(N, rn, sn, tn);
+    B = bbw::mrdivide(bbw::vandermonde3d(N, rr, ss, tt), bbw::vandermonde3d(N, rn, sn, tn));
+  } else {
+    B = bbw::bernTet(N, rr, ss, tt);
+  }
+  const int Np = (N + 1) * (N + 2) * (N + 3) / 6;
+  for (int i = 0; i < npts; ++i)
+    for (int n = 0; n < Np; ++n) out[(size_t)i * Np + n] = B(i, n);
+  return BBW_OK;
+}

@@ -188,6 +188,70 @@ class Problem:
         return err, err / nrm
 
 
+def gaussian_source(prob, x0, a=100.0):
+    """Smoothed point source of acous_elas_cpp/src/WaveOKL3d.cpp:176-186 and
+    :226-228: exp(-a^2 |x - x0|^2) at the cubature points, normalised to max 1
+    over the mesh, projected with Pq (L2 projection onto the element basis).
+    Returns the dense [K][Np] float32 array the reference uploads (c_fsrc)."""
+    xq, yq, zq = prob.cubature_xyz()
+    r2 = (xq - x0[0]) ** 2 + (yq - x0[1]) ** 2 + (zq - x0[2]) ** 2
+    f = np.exp(-a * a * r2)
+    f *= 1.0 / np.abs(f).max()
+    Pq = prob.ops["Pq_%s64" % prob.variant].reshape(prob.Nq, prob.Np).T  # [Np][Nq]
+    return np.ascontiguousarray(f @ Pq.T, np.float32)
+
+
+def source_entries(fsrc, shot=0, rtol=1e-9):
+    """Sparse (shot, elem, vec) entries of a dense [K][Np] source: the
+    elements whose coefficients reach rtol * max|fsrc| (the rest are below
+    FP32 resolution of the step and contribute nothing)."""
+    f = np.asarray(fsrc, np.float32)
+    m = np.abs(f).max(axis=1)
+    elem = np.nonzero(m >= rtol * m.max())[0].astype(np.int32)
+    return np.full(len(elem), shot, np.int32), elem, np.ascontiguousarray(f[elem])
+
+
+def locate_points(prob, pts):
+    """Element and reference coordinates (r, s, t) of each physical point
+    (first containing element; tolerance 1e-10 in barycentric coordinates).
+    The affine map is x = -(1+r+s+t)/2 v1 + (1+r)/2 v2 + (1+s)/2 v3 + (1+t)/2 v4
+    (cpp/src/StartUp3d.cpp:556-559, vertex order of EToV)."""
+    (VX, VY, VZ), EToV = prob.extra["VX"], np.asarray(prob.extra["EToV"])
+    V = np.stack([np.asarray(VX)[EToV], np.asarray(VY)[EToV], np.asarray(VZ)[EToV]], -1)
+    A = np.stack([V[:, 1] - V[:, 0], V[:, 2] - V[:, 0], V[:, 3] - V[:, 0]], -1)  # [K][3][3]
+    Ainv = np.linalg.inv(A)
+    pts = np.atleast_2d(np.asarray(pts, np.float64))
+    elem = np.empty(len(pts), np.int32)
+    rst = np.empty((len(pts), 3))
+    for i, x in enumerate(pts):
+        lam = np.einsum("kij,kj->ki", Ainv, x[None, :] - V[:, 0])  # barycentric 1..3
+        ok = (lam >= -1e-10).all(1) & (lam.sum(1) <= 1 + 1e-10)
+        hit = np.nonzero(ok)[0]
+        if len(hit) == 0:
+            raise ValueError("point %r is outside the mesh" % (tuple(x),))
+        k = hit[0]
+        elem[i] = k
+        rst[i] = 2.0 * lam[k] - 1.0
+    return elem, rst
+
+
+def basis_eval(N, variant, rst):
+    """phi_n at reference points: [npts][Np] FP64 (nodal Lagrange or Bernstein)."""
+    rst = np.ascontiguousarray(np.atleast_2d(rst), np.float64)
+    r, s, t = (np.ascontiguousarray(rst[:, i]) for i in range(3))
+    out = np.empty((len(rst), np_of(N)), np.float64)
+    _lib.call("bbw_basis_eval", N, 0 if variant == "nodal" else 1, len(rst), _lib.ptr(r),
+              _lib.ptr(s), _lib.ptr(t), _lib.ptr(out))
+    return out
+
+
+def receiver_weights(prob, pts):
+    """Receivers at physical points: (elem[R], w[R][Np]) with
+    p(x) = sum_n w[n] Q[elem][p][n] for the problem's basis."""
+    elem, rst = locate_points(prob, pts)
+    return elem, np.ascontiguousarray(basis_eval(prob.N, prob.variant, rst), np.float32)
+
+
 def _jacobians(VX, VY, VZ, EToV):
     x, y, z = VX[EToV], VY[EToV], VZ[EToV]
     d = [np.stack([x[:, m] - x[:, 0], y[:, m] - y[:, 0], z[:, m] - z[:, 0]], 1) / 2 for m in (1, 2, 3)]

@@ -88,28 +88,36 @@ class WaveSolver:
         _lib.call("bbw_create_ex", ctypes.byref(md), ctypes.byref(od), VARIANTS[variant], BCS[bc],
                   PRECISIONS[precision], ctypes.byref(h))
         self.precision = precision
+        self.S, self.R, self.max_steps = 1, 0, 0
         self._h = h
         del keep
 
     # ---- reference-named entry points
+    @property
+    def state_size(self):
+        return self.S * self.K * 4 * self.Np
+
     def set_data(self, Q):
-        """WaveSetData3d: host state [K][4][Np] -> device."""
+        """WaveSetData3d: host state [S][K][4][Np] -> device."""
         Q = _f32(Q)
-        assert Q.size == self.K * 4 * self.Np
+        if Q.size != self.state_size:
+            raise ValueError("state has %d values, expected %d" % (Q.size, self.state_size))
         _lib.call("bbw_set_state", self._h, Q.ctypes.data)
 
     def get_data(self):
         """WaveGetData3d (raw coefficients; BB -> nodal is Problem.to_nodal)."""
-        Q = np.empty(self.K * 4 * self.Np, np.float32)
+        Q = np.empty(self.state_size, np.float32)
         _lib.call("bbw_get_state", self._h, Q.ctypes.data)
         return Q
 
     def set_residual(self, r):
         r = _f32(r)
+        if r.size != self.state_size:
+            raise ValueError("residual has %d values, expected %d" % (r.size, self.state_size))
         _lib.call("bbw_set_residual", self._h, r.ctypes.data)
 
     def get_residual(self):
-        r = np.empty(self.K * 4 * self.Np, np.float32)
+        r = np.empty(self.state_size, np.float32)
         _lib.call("bbw_get_residual", self._h, r.ctypes.data)
         return r
 
@@ -124,6 +132,57 @@ class WaveSolver:
     def wave_rk(self, final_time, dt):
         """Wave_RK: steps of dt until final_time, last step shortened."""
         _lib.call("bbw_run", self._h, float(final_time), float(dt))
+
+    def rk_stage(self, rka, rkb, fdt, c):
+        """One fused stage with stage-time offset c (source time = clock + c fdt)."""
+        _lib.call("bbw_stage_ex", self._h, float(rka), float(rkb), float(fdt), float(c))
+
+    # ---- batched shots, sources, receivers
+    def set_shots(self, S):
+        """S independent shots per launch (state [S][K][4][Np], zeroed)."""
+        _lib.call("bbw_set_shots", self._h, int(S))
+        self.S = int(S)
+
+    def set_sources(self, shot, elem, vec, f0=10.0, t_delay=None, amplitude=1e4,
+                    stage_times=False):
+        """Ricker sources (acous_elas_cpp/src/WaveOKL3d.cpp:765-781): entry j adds
+        ricker(t) * vec[j] to the projected rhs_p of element elem[j] in shot
+        shot[j].  Defaults are the reference's f0 = 10, tR = 1/f0, 1e4."""
+        shot, elem = _i32(shot).ravel(), _i32(elem).ravel()
+        vec = _f32(vec)
+        if vec.size != len(elem) * self.Np or len(shot) != len(elem):
+            raise ValueError("source entries: shot, elem and vec[n][Np] disagree")
+        tR = 1.0 / f0 if t_delay is None else t_delay
+        _lib.call("bbw_set_sources", self._h, len(elem), shot.ctypes.data, elem.ctypes.data,
+                  vec.ctypes.data, float(f0), float(tR), float(amplitude), int(bool(stage_times)))
+
+    def clear_sources(self):
+        _lib.call("bbw_set_sources", self._h, 0, None, None, None, 0.0, 0.0, 0.0, 0)
+
+    def set_receivers(self, elem, w, max_steps):
+        """Receivers p(x_r) = w[r] . Q[elem[r]][p], recorded after every step."""
+        elem, w = _i32(elem).ravel(), _f32(w)
+        if w.size != len(elem) * self.Np:
+            raise ValueError("receiver weights must be [R][Np]")
+        _lib.call("bbw_set_receivers", self._h, len(elem), elem.ctypes.data, w.ctypes.data,
+                  int(max_steps))
+        self.R, self.max_steps = len(elem), int(max_steps)
+
+    def get_traces(self):
+        """Recorded traces [S][R][nsteps]."""
+        out = np.zeros((self.S, self.R, max(self.max_steps, 1)), np.float32)
+        n = ctypes.c_int(0)
+        _lib.call("bbw_get_traces", self._h, out.ctypes.data, ctypes.byref(n))
+        return out[:, :, :n.value]
+
+    def set_time(self, t=0.0):
+        """Device clock (time of the next step's start); resets the step count."""
+        _lib.call("bbw_set_time", self._h, float(t))
+
+    def get_time(self):
+        t, st = ctypes.c_double(0), ctypes.c_int(0)
+        _lib.call("bbw_get_time", self._h, ctypes.byref(t), ctypes.byref(st))
+        return t.value, st.value
 
     def sync(self):
         _lib.call("bbw_sync", self._h)

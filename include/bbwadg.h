@@ -104,6 +104,13 @@ bbw_status bbw_ops_get(const bbw_ops *ops, const char *name, int dtype, void *ds
                        long long *count);
 void bbw_ops_free(bbw_ops *ops);
 
+/* Basis functions of degree N at reference points (r, s, t):
+ * out[i][n] = phi_n(r_i, s_i, t_i), nodal Lagrange basis on the
+ * warp-and-blend nodes (Vandermonde3D(r,s,t) / V, cpp/src/Basis.cpp:286) or
+ * Bernstein basis (BernTet, cpp/src/Basis.cpp:539).  Used for receiver interpolation. */
+bbw_status bbw_basis_eval(int N, int variant, int npts, const double *r, const double *s,
+                          const double *t, double *out);
+
 /* ------------------------------------------------ kernel-level entry points
  * One-to-one replacements of the reference's OKL kernels; same argument
  * order and meaning, device pointers, N at run time. */
@@ -200,8 +207,11 @@ bbw_status bbw_get_residual(bbw_ctx *ctx, float *res_host);
 
 /* RK_step_WADG_subelem (cpp/src/WaveOKL3d.cpp:2084-2109): one LSRK stage
  * res = fa*res + fdt*P(c2 rhs), Q += fb*res, as one fused kernel.
- * Asynchronous on the context's stream. */
+ * Asynchronous on the context's stream.  bbw_stage_ex also takes the stage
+ * time offset c (stage time = clock + c*fdt) used by the sources;
+ * bbw_stage uses c = 0. */
 bbw_status bbw_stage(bbw_ctx *ctx, float fa, float fb, float fdt);
+bbw_status bbw_stage_ex(bbw_ctx *ctx, float fa, float fb, float fdt, float c);
 
 /* nsteps full LSRK45 steps of size dt (the time loop of Wave_RK,
  * cpp/src/WaveOKL3d.cpp:2030-2079, with coefficients cast to float as at
@@ -211,6 +221,37 @@ bbw_status bbw_steps(bbw_ctx *ctx, float dt, int nsteps);
 /* Wave_RK(mesh, FinalTime, dt) semantics: steps of dt until FinalTime with
  * the last step shortened to land on it (cpp/src/WaveOKL3d.cpp:2048). */
 bbw_status bbw_run(bbw_ctx *ctx, double final_time, float dt);
+
+/* ---- batched shots, sources, receivers (FP32 stage)
+ * S independent shots share mesh, medium and operators; the state, residual
+ * and traces hold S consecutive blocks and every stage launch advances all
+ * of them.  Resizing drops state (zeroed) and the source table. */
+bbw_status bbw_set_shots(bbw_ctx *ctx, int S);
+
+/* Source entries (acous_elas_cpp/src/WaveOKL3d.cpp:765-781 and
+ * acous_elas_cpp/okl/ElasKernelsWADG.okl:400-403): entry j adds
+ * ricker(t) * vec[j][0..Np) to the WADG-projected rhs_p of element elem[j]
+ * of shot shot[j], with ricker(t) = amplitude (1 - 2 a^2) exp(-a^2),
+ * a = pi f0 (t - t_delay).  vec is the L2 projection (Pq) of the spatial
+ * source profile.  stage_times = 0 evaluates ricker at the step's start time
+ * in all five stages, as the reference does; nonzero uses the stage times
+ * t + rk4c[s] dt.  nent = 0 clears. */
+bbw_status bbw_set_sources(bbw_ctx *ctx, int nent, const int *shot, const int *elem,
+                           const float *vec, float f0, float t_delay, float amplitude,
+                           int stage_times);
+
+/* Receivers: trace[s][r][step] = sum_n w[r][n] p_n of element elem[r] in
+ * shot s, recorded after every full step of bbw_steps / bbw_run (up to
+ * max_steps).  R = 0 clears. */
+bbw_status bbw_set_receivers(bbw_ctx *ctx, int R, const int *elem, const float *w,
+                             int max_steps);
+/* Copies traces [S][R][max_steps] and the number of recorded steps. */
+bbw_status bbw_get_traces(bbw_ctx *ctx, float *out, int *nsteps);
+
+/* Device clock read by the sources: time at the start of the next step;
+ * bbw_set_time also resets the recorded step count. */
+bbw_status bbw_set_time(bbw_ctx *ctx, double t);
+bbw_status bbw_get_time(bbw_ctx *ctx, double *t, int *step);
 
 /* Waits for the context's stream. */
 bbw_status bbw_sync(bbw_ctx *ctx);

@@ -25,6 +25,18 @@ RK4B = (1432997174477.0 / 9575080441755.0,
         1720146321549.0 / 2090206949498.0,
         3134564353537.0 / 4481467310338.0,
         2277821191437.0 / 14882151754819.0)
+RK4C = (0.0,
+        1432997174477.0 / 9575080441755.0,
+        2526269341429.0 / 6820363962896.0,
+        2006345519317.0 / 3224310063776.0,
+        2802321613138.0 / 2924317926251.0)
+
+
+def ricker(t, f0, tR, amp):
+    """acous_elas_cpp/src/WaveOKL3d.cpp:767-770: amp (1 - 2 a^2) exp(-a^2),
+    a = pi f0 (t - tR)."""
+    a = np.pi * f0 * (t - tR)
+    return amp * (1.0 - 2.0 * a * a) * np.exp(-a * a)
 
 
 def lib():
@@ -111,19 +123,34 @@ class Oracle:
             self.K, self.Np, self.Nq, _p(self.Vq), _p(self.Pq), _p(self.Jq), _p(self.c2q),
             _R(self.dtype, fa), _R(self.dtype, fb), _R(self.dtype, fdt), _p(rhs), _p(res), _p(Q))
 
+    def rk_update_wadg_src(self, fa, fb, fdt, ftime, fsrc, rhs, res, Q):
+        getattr(lib(), "ora_rk_update_wadg_src" + _sfx(self.dtype))(
+            self.K, self.Np, self.Nq, _p(self.Vq), _p(self.Pq), _p(self.Jq), _p(self.c2q),
+            _R(self.dtype, fa), _R(self.dtype, fb), _R(self.dtype, fdt), _R(self.dtype, ftime),
+            _p(fsrc), _p(rhs), _p(res), _p(Q))
+
     def rk_update(self, fa, fb, fdt, rhs, res, Q):
         getattr(lib(), "ora_rk_update" + _sfx(self.dtype))(
             self.K, self.Np, _R(self.dtype, fa), _R(self.dtype, fb), _R(self.dtype, fdt),
             _p(rhs), _p(res), _p(Q))
 
     # ---- stage / step driver: RK_step_WADG_subelem + Wave_RK ----
-    def run(self, Q, dt, nstages, res=None):
+    def run(self, Q, dt, nstages, res=None, source=None, receivers=None, t0=0.0):
         """Advance Q in place by ``nstages`` LSRK45 stages (stage s uses
         coefficient s % 5), as cpp/src/WaveOKL3d.cpp:2050-2106 does.  The
-        FP32 family casts the coefficients to float like the reference."""
+        FP32 family casts the coefficients to float like the reference.
+
+        source = dict(fsrc=[K][Np] array, f0, tR, amp, stage_times): the
+        acous_elas_cpp source term (WaveOKL3d.cpp:765-781), evaluated at the
+        step start time (stage_times False, as the reference) or at the stage
+        times.  receivers = (elem[R], w[R][Np]): p interpolated after every
+        full step; returned as traces [R][nsteps] when given."""
         Q = np.ascontiguousarray(Q, dtype=self.dtype)
         res = np.zeros_like(Q) if res is None else res
         rhs = np.zeros_like(Q)
+        fsrc = None if source is None else _c(source["fsrc"], self.dtype)
+        traces = []
+        t = t0
         for s in range(nstages):
             i = s % 5
             fa, fb = RK4A[i], RK4B[i]
@@ -133,5 +160,19 @@ class Oracle:
                 fdt = dt
             self.rk_volume(Q, rhs)
             self.rk_surface(Q, rhs)
-            self.rk_update_wadg(fa, fb, fdt, rhs, res, Q)
+            if fsrc is None:
+                self.rk_update_wadg(fa, fb, fdt, rhs, res, Q)
+            else:
+                ts = t + (RK4C[i] * dt if source.get("stage_times") else 0.0)
+                ftime = ricker(ts, source["f0"], source["tR"], source["amp"])
+                self.rk_update_wadg_src(fa, fb, fdt, ftime, fsrc, rhs, res, Q)
+            if i == 4:
+                t += float(dt)
+                if receivers is not None:
+                    el, w = receivers
+                    Qr = Q.reshape(self.K, 4, self.Np)
+                    traces.append(np.einsum("rn,rn->r", np.asarray(w, np.float64),
+                                            Qr[np.asarray(el), 0, :].astype(np.float64)))
+        if receivers is not None:
+            return Q, res, np.array(traces).T
         return Q, res

@@ -124,10 +124,14 @@ void FN(ora_rk_update)(int K, int Np, REAL fa, REAL fb, REAL fdt, const REAL *rh
   }
 }
 
-/* cpp/okl/WaveKernelsWADG.okl:1760-1887 (rk_update_WADG) */
-void FN(ora_rk_update_wadg)(int K, int Np, int Nq, const REAL *Vq, const REAL *Pq,
-                            const REAL *Jq, const REAL *c2q, REAL fa, REAL fb, REAL fdt,
-                            const REAL *rhsQ, REAL *resQ, REAL *Q) {
+/* cpp/okl/WaveKernelsWADG.okl:1760-1887 (rk_update_WADG), with the optional
+ * source term of
+ * acous_elas_cpp/okl/ElasKernelsWADG.okl:400-403: ftime * fsrc[k][n] is added
+ * to the projected rhs_p (fsrc NULL: no source). */
+void FN(ora_rk_update_wadg_src)(int K, int Np, int Nq, const REAL *Vq, const REAL *Pq,
+                                const REAL *Jq, const REAL *c2q, REAL fa, REAL fb, REAL fdt,
+                                REAL ftime, const REAL *fsrc, const REAL *rhsQ, REAL *resQ,
+                                REAL *Q) {
 #pragma omp parallel for schedule(static)
   for (int k = 0; k < K; ++k) {
     REAL s[4][MAXNQ], r[4][MAXNQ];
@@ -160,6 +164,7 @@ void FN(ora_rk_update_wadg)(int K, int Np, int Nq, const REAL *Vq, const REAL *P
         rp[2] += P * s[2][j];
         rp[3] += P * s[3][j];
       }
+      if (fsrc) rp[0] += ftime * fsrc[n + (long)k * Np];
       for (int f = 0; f < 4; ++f) {
         const long id = n + f * Np + (long)k * 4 * Np;
         REAL res = fa * resQ[id] + fdt * rp[f];
@@ -168,6 +173,12 @@ void FN(ora_rk_update_wadg)(int K, int Np, int Nq, const REAL *Vq, const REAL *P
       }
     }
   }
+}
+
+void FN(ora_rk_update_wadg)(int K, int Np, int Nq, const REAL *Vq, const REAL *Pq,
+                            const REAL *Jq, const REAL *c2q, REAL fa, REAL fb, REAL fdt,
+                            const REAL *rhsQ, REAL *resQ, REAL *Q) {
+  FN(ora_rk_update_wadg_src)(K, Np, Nq, Vq, Pq, Jq, c2q, fa, fb, fdt, 0, 0, rhsQ, resQ, Q);
 }
 
 /* cpp/okl/WaveKernels.okl:344-474 (rk_volume_bern).  D_idsj[4*i+m] holds
