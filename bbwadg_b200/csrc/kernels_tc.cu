@@ -114,11 +114,15 @@ struct TcParams {
 };
 
 __device__ __forceinline__ float pow2_scale(int bits_of_max) {
-  // s = 2^-E with max = m 2^E, m in [0.5, 1): max * s < 1
+  // s = 2^-E with max = m 2^E, m in [0.5, 1): max * s < 1.  E is clamped to
+  // [-100, 100] so that s and 1/s stay finite normal numbers (a tile whose
+  // values are all below 2^-100 keeps them below 1 after scaling; they are
+  // far below the FP32 resolution of any tile that carries the solution)
   const float mx = __int_as_float(bits_of_max);
   if (!(mx > 0.f) || !isfinite(mx)) return 1.f;
   int E;
   frexpf(mx, &E);
+  E = max(-100, min(100, E));
   return ldexpf(1.f, -E);
 }
 

@@ -71,6 +71,30 @@ def test_tc_agrees_with_fp32_stage_over_many_steps(cuda):
     assert rel_l2(b.get_data(), a.get_data()) < TOL
 
 
+def test_tc_many_tiles_per_cta_and_tiny_tiles(cuda):
+    """10^3 x 6 tets (K=6000, 188 tiles: CTAs loop over several tiles) with
+    one tile scaled to ~1e-39 (below 2^-127, where a per-tile power-of-two
+    scale must stay finite) and one tile exactly zero."""
+    from oracle import Oracle
+    cub, tri = ref_rule(5)
+    p = make_problem(5, 10, variant="nodal", c2="sine", c2_jitter=0.5, seed=11, cubature=cub,
+                     tri_cubature=tri, cfl=0.25)
+    Q0 = p.Q0.reshape(p.K, 4, p.Np).copy()
+    Q0[:, 0, :] += 0.1  # every tile carries signal
+    Q0[32 * 40:32 * 41] = 1e-39 * np.sign(Q0[32 * 40:32 * 41] + 0.5)
+    Q0[32 * 90:32 * 91] = 0.0
+    Q0 = Q0.ravel()
+    q_ref, _ = Oracle(5, p.K, p.ops_dict(), p.geo_dict(), variant="nodal").run(Q0.copy(), p.dt, 10)
+    s = WaveSolver(p, precision="f16x3")
+    s.set_data(Q0)
+    s.steps(p.dt, 2)
+    s.check()
+    q = s.get_data()
+    assert np.isfinite(q).all()
+    assert rel_l2(q, q_ref) < TOL
+    s.close()
+
+
 def test_tc_rejects_unsupported(cuda):
     from bbwadg_b200._lib import BBWError
     p = make_problem(4, 2, variant="nodal")
