@@ -80,6 +80,10 @@ SIGNATURES = {
     "bbw_get_traces": (c_int, [c_void_p, P, ctypes.POINTER(c_int)]),
     "bbw_set_time": (c_int, [c_void_p, c_double]),
     "bbw_get_time": (c_int, [c_void_p, ctypes.POINTER(c_double), ctypes.POINTER(c_int)]),
+    "bbw_set_c2q": (c_int, [c_void_p, P]),
+    "bbw_forward": (c_int, [c_void_p, c_float, c_int, c_int, ctypes.POINTER(c_void_p)]),
+    "bbw_backward": (c_int, [c_void_p, c_void_p, P, P, P]),
+    "bbw_tape_free": (c_int, [c_void_p]),
     "bbw_device_state": (c_int, [c_void_p, ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p),
                                  ctypes.POINTER(c_void_p)]),
 }

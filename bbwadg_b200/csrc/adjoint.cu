@@ -1,0 +1,298 @@
+// Forward / backward pair of the discrete adjoint (receiver-misfit
+// gradient with respect to c^2 at the cubature points).
+//
+// bbw_forward advances the context like bbw_steps (same fused stage, same
+// CUDA graph, traces recorded by the receivers) and keeps the state at
+// every `checkpoint_every`-th step start.  bbw_backward sweeps the steps in
+// reverse: each checkpoint segment is recomputed forward once (step-start
+// states kept), each step's five stage inputs are recomputed from its start
+// state with the same fused kernel, and the stages are reversed with the
+// adjoint kernels of kernels_adj.cu.  The c^2 gradient is accumulated in
+// FP64.  There is no reference counterpart; the forward operators are the
+// reference's rk_volume / rk_surface / rk_update_WADG
+// (cpp/okl/WaveKernels.okl:44-260, cpp/okl/WaveKernelsWADG.okl:1760-1887).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "bbwadg.h"
+#include "ctx.h"
+#include "internal.h"
+
+using namespace bbw;
+
+struct bbw_tape {
+  int nsteps = 0, every = 1, step0 = 0;
+  float dt = 0.f;
+  double t0 = 0.0;
+  size_t state = 0;           // floats per state (all shots)
+  std::vector<float *> ck;    // step-start states at steps 0, every, 2 every, ...
+};
+
+namespace bbw {
+
+void adj_release(bbw_ctx *c) {
+  AdjOps &a = c->adj;
+  for (int d = 0; d < 3; ++d) cudaFree(a.D[d]), cudaFree(a.DT[d]);
+  cudaFree(a.LIFT), cudaFree(a.Vq), cudaFree(a.Pq);
+  cudaFree(a.Fmask), cudaFree(a.vmapP), cudaFree(a.fidx), cudaFree(a.mapP);
+  a = AdjOps();
+}
+
+}  // namespace bbw
+
+namespace {
+
+// face-node pairing in face-node space from vmapP (vmapP is an involution on
+// the face nodes of a conforming mesh)
+bbw_status build_maps(const bbw_ctx *c, std::vector<int> &fidx, std::vector<int> &mapP) {
+  const int K = c->K, Np = c->Np, Nfp = c->Nfp, NF = 4 * Nfp;
+  const int *Fm = c->hFmask.data(), *vm = c->hvmapP.data();
+  fidx.assign((size_t)4 * Np, -1);
+  for (int f = 0; f < 4; ++f)
+    for (int i = 0; i < Nfp; ++i) fidx[(size_t)f * Np + Fm[f * Nfp + i]] = i;
+  mapP.assign((size_t)K * NF, -1);
+  std::vector<int> inv(Np);
+  for (int k = 0; k < K; ++k)
+    for (int f = 0; f < 4; ++f) {
+      const int *v = vm + (size_t)k * NF + f * Nfp;
+      const int k2 = v[0] / (4 * Np);
+      bool boundary = k2 == k;
+      for (int i = 0; i < Nfp && boundary; ++i) boundary = v[i] % (4 * Np) == Fm[f * Nfp + i];
+      if (boundary) continue;
+      // the face of k2 whose traces point back into k
+      int f2 = -1;
+      for (int g = 0; g < 4 && f2 < 0; ++g)
+        if (vm[(size_t)k2 * NF + g * Nfp] / (4 * Np) == k) f2 = g;
+      if (f2 < 0) return set_error(BBW_ERR_MESH, "adjoint: vmapP is not symmetric");
+      std::fill(inv.begin(), inv.end(), -1);
+      for (int j = 0; j < Nfp; ++j) inv[Fm[f2 * Nfp + j]] = j;
+      for (int i = 0; i < Nfp; ++i) {
+        const int j = inv[v[i] % (4 * Np)];
+        if (j < 0 || vm[(size_t)k2 * NF + f2 * Nfp + j] != k * 4 * Np + Fm[f * Nfp + i])
+          return set_error(BBW_ERR_MESH, "adjoint: vmapP is not symmetric");
+        mapP[(size_t)k * NF + f * Nfp + i] = k2 * NF + f2 * Nfp + j;
+      }
+    }
+  return BBW_OK;
+}
+
+bbw_status adj_setup(bbw_ctx *c) {
+  AdjOps &a = c->adj;
+  if (a.ready) return BBW_OK;
+  const int Np = c->Np, NF = 4 * c->Nfp;
+  std::vector<int> fidx, mapP;
+  bbw_status s = build_maps(c, fidx, mapP);
+  if (s != BBW_OK) return s;
+  for (int d = 0; d < 3; ++d) {
+    std::vector<float> t((size_t)Np * Np);
+    for (int n = 0; n < Np; ++n)
+      for (int m = 0; m < Np; ++m) t[n + (size_t)m * Np] = c->hD[d][m + (size_t)n * Np];
+    if ((s = upload(&a.D[d], c->hD[d].data(), c->hD[d].size(), "adjoint: D")) != BBW_OK ||
+        (s = upload(&a.DT[d], t.data(), t.size(), "adjoint: D^T")) != BBW_OK)
+      return s;
+  }
+  if ((s = upload(&a.LIFT, c->hLIFT.data(), c->hLIFT.size(), "adjoint: LIFT")) != BBW_OK ||
+      (s = upload(&a.Vq, c->hVq.data(), c->hVq.size(), "adjoint: Vq")) != BBW_OK ||
+      (s = upload(&a.Pq, c->hPq.data(), c->hPq.size(), "adjoint: Pq")) != BBW_OK ||
+      (s = upload(&a.Fmask, c->hFmask.data(), c->hFmask.size(), "adjoint: Fmask")) != BBW_OK ||
+      (s = upload(&a.vmapP, c->hvmapP.data(), c->hvmapP.size(), "adjoint: vmapP")) != BBW_OK ||
+      (s = upload(&a.fidx, fidx.data(), fidx.size(), "adjoint: face index")) != BBW_OK ||
+      (s = upload(&a.mapP, mapP.data(), mapP.size(), "adjoint: mapP")) != BBW_OK)
+    return s;
+  (void)NF;
+  a.ready = true;
+  return BBW_OK;
+}
+
+struct DevBuf {  // freed on scope exit
+  std::vector<void *> p;
+  ~DevBuf() {
+    for (void *x : p) cudaFree(x);
+  }
+  template <class T>
+  bbw_status get(T **out, size_t n, const char *what) {
+    bbw_status s = upload<T>(out, nullptr, n, what);
+    if (s == BBW_OK) p.push_back(*out);
+    return s;
+  }
+};
+
+}  // namespace
+
+extern "C" bbw_status bbw_set_c2q(bbw_ctx *c, const float *c2q) {
+  if (!c || !c2q) return set_error(BBW_ERR_ARG, "bbw_set_c2q: NULL");
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(c->c2q, c2q, (size_t)c->K * c->Nq * sizeof(float), cudaMemcpyHostToDevice);
+  return set_cuda_error(e, "bbw_set_c2q");
+}
+
+extern "C" bbw_status bbw_tape_free(bbw_tape *t) {
+  if (!t) return BBW_OK;
+  for (float *p : t->ck) cudaFree(p);
+  delete t;
+  return BBW_OK;
+}
+
+extern "C" bbw_status bbw_forward(bbw_ctx *c, float dt, int nsteps, int checkpoint_every,
+                                  bbw_tape **out) {
+  if (!c || !out || nsteps < 1 || checkpoint_every < 1 || !(dt > 0.f))
+    return set_error(BBW_ERR_ARG, "bbw_forward: bad argument");
+  *out = nullptr;
+  if (c->precision != BBW_PREC_FP32)
+    return set_error(BBW_ERR_UNSUPPORTED, "bbw_forward: the adjoint needs BBW_PREC_FP32");
+  if (c->R <= 0) return set_error(BBW_ERR_STATE, "bbw_forward: no receivers set");
+  bbw_status s = adj_setup(c);
+  if (s != BBW_OK) return s;
+  double t0 = 0;
+  int st0 = 0;
+  if ((s = bbw_get_time(c, &t0, &st0)) != BBW_OK) return s;
+  if (st0 + nsteps > c->max_steps)
+    return set_error(BBW_ERR_ARG, "bbw_forward: receiver capacity (max_steps) too small");
+  bbw_tape *t = new bbw_tape;
+  t->nsteps = nsteps, t->every = checkpoint_every, t->step0 = st0, t->dt = dt, t->t0 = t0;
+  t->state = (size_t)c->S * c->K * 4 * c->Np;
+  const int nck = (nsteps + checkpoint_every - 1) / checkpoint_every;
+  for (int i = 0; i < nck; ++i) {
+    float *p = nullptr;
+    if ((s = upload<float>(&p, nullptr, t->state, "bbw_forward: checkpoint")) != BBW_OK) {
+      bbw_tape_free(t);
+      return s;
+    }
+    t->ck.push_back(p);
+  }
+  for (int n = 0; n < nsteps; ++n) {
+    if (n % checkpoint_every == 0) {
+      float *Q = nullptr;
+      bbw_device_state(c, &Q, nullptr, nullptr);
+      cudaError_t e = cudaMemcpyAsync(t->ck[n / checkpoint_every], Q, t->state * sizeof(float),
+                                      cudaMemcpyDeviceToDevice, c->stream);
+      if (e != cudaSuccess) {
+        bbw_tape_free(t);
+        return set_cuda_error(e, "bbw_forward: checkpoint");
+      }
+    }
+    if ((s = bbw_steps(c, dt, 1)) != BBW_OK) {
+      bbw_tape_free(t);
+      return s;
+    }
+  }
+  *out = t;
+  return BBW_OK;
+}
+
+extern "C" bbw_status bbw_backward(bbw_ctx *c, bbw_tape *t, const float *dL_dtraces,
+                                   double *dL_dc2q, float *dL_dQ0) {
+  if (!c || !t || !dL_dtraces || !dL_dc2q) return set_error(BBW_ERR_ARG, "bbw_backward: NULL");
+  if (t->state != (size_t)c->S * c->K * 4 * c->Np)
+    return set_error(BBW_ERR_STATE, "bbw_backward: tape does not match the context");
+  bbw_status s = adj_setup(c);
+  if (s != BBW_OK) return s;
+  const int N = c->N, K = c->K, Np = c->Np, Nq = c->Nq, NF = 4 * c->Nfp, S = c->S, R = c->R;
+  const int nsteps = t->nsteps, every = t->every;
+  const size_t shot = (size_t)K * 4 * Np;
+  const float dt = t->dt;
+  cudaStream_t st = c->stream;
+  const AdjOps &a = c->adj;
+  DevBuf buf;
+  float *lamQ, *lamR, *z, *rhs, *sigma, *res, *g, *seg, *stq;
+  double *grad, *tdev;
+  const int seglen = std::min(every, nsteps);
+  if ((s = buf.get(&lamQ, t->state, "bbw_backward")) != BBW_OK ||
+      (s = buf.get(&lamR, t->state, "bbw_backward")) != BBW_OK ||
+      (s = buf.get(&z, t->state, "bbw_backward")) != BBW_OK ||
+      (s = buf.get(&rhs, shot, "bbw_backward")) != BBW_OK ||
+      (s = buf.get(&sigma, (size_t)K * NF, "bbw_backward")) != BBW_OK ||
+      (s = buf.get(&res, t->state, "bbw_backward")) != BBW_OK ||
+      (s = buf.get(&g, (size_t)S * R * nsteps, "bbw_backward")) != BBW_OK ||
+      (s = buf.get(&seg, (size_t)seglen * t->state, "bbw_backward: segment states")) != BBW_OK ||
+      (s = buf.get(&stq, (size_t)5 * t->state, "bbw_backward: stage states")) != BBW_OK ||
+      (s = buf.get(&grad, (size_t)K * Nq, "bbw_backward")) != BBW_OK ||
+      (s = buf.get(&tdev, 1, "bbw_backward")) != BBW_OK)
+    return s;
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(g, dL_dtraces, (size_t)S * R * nsteps * sizeof(float), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return set_cuda_error(e, "bbw_backward: upload");
+
+  FusedPlan pl = c->plan;
+  pl.time = tdev;
+  // step-start times exactly as the device clock accumulated them
+  std::vector<double> tn(nsteps + 1);
+  tn[0] = t->t0;
+  for (int n = 0; n < nsteps; ++n) tn[n + 1] = tn[n] + (double)dt;
+  auto stage = [&](int i, const float *in, float *outq) {
+    return fused_launch(pl, in, outq, res, (float)kRK4A[i], (float)kRK4B[i], dt,
+                        c->src_stage_times ? (float)kRK4C[i] : 0.f, st);
+  };
+  auto step_fwd = [&](int n, const float *in, float *outq) {  // stage outputs in stq[1..4]
+    bbw_status r = set_device_double(tdev, tn[n], st);
+    const float *q = in;
+    for (int i = 0; i < 5 && r == BBW_OK; ++i) {
+      float *o = i < 4 ? stq + (size_t)(i + 1) * t->state : outq;
+      r = stage(i, q, o);
+      q = o;
+    }
+    return r;
+  };
+
+  const int nseg = (nsteps + every - 1) / every;
+  for (int sg = nseg - 1; sg >= 0; --sg) {
+    const int n0 = sg * every, len = std::min(every, nsteps - n0);
+    e = cudaMemcpyAsync(seg, t->ck[sg], t->state * sizeof(float), cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return set_cuda_error(e, "bbw_backward: segment");
+    for (int j = 1; j < len; ++j)
+      if ((s = step_fwd(n0 + j - 1, seg + (size_t)(j - 1) * t->state,
+                        seg + (size_t)j * t->state)) != BBW_OK)
+        return s;
+    for (int j = len - 1; j >= 0; --j) {
+      const int n = n0 + j;
+      if ((s = adj_receivers(S, K, Np, R, c->rec_elem, c->rec_w, g, nsteps, n, lamQ, st)) !=
+          BBW_OK)
+        return s;
+      // stage inputs: stq[0] = step start, stq[1..4] recomputed (the step's
+      // output lands in stq[0]'s slot, which is not needed any more)
+      e = cudaMemcpyAsync(stq, seg + (size_t)j * t->state, t->state * sizeof(float),
+                          cudaMemcpyDeviceToDevice, st);
+      if (e != cudaSuccess) return set_cuda_error(e, "bbw_backward: stage state");
+      if ((s = set_device_double(tdev, tn[n], st)) != BBW_OK) return s;
+      {
+        const float *q = stq;
+        for (int i = 0; i < 4 && s == BBW_OK; ++i) {
+          float *o = stq + (size_t)(i + 1) * t->state;
+          s = stage(i, q, o);
+          q = o;
+        }
+        if (s != BBW_OK) return s;
+      }
+      for (int i = 4; i >= 0; --i) {
+        const float ai = (float)kRK4A[i], bi = (float)kRK4B[i];
+        for (int sh = 0; sh < S; ++sh) {
+          const size_t o = sh * shot;
+          const float *Qi = stq + (size_t)i * t->state + o;
+          if ((s = bbw_rk_volume(N, K, c->vgeo, a.D[0], a.D[1], a.D[2], Qi, rhs, st)) !=
+                  BBW_OK ||
+              (s = bbw_rk_surface(N, K, c->bc, c->fgeo, a.Fmask, a.vmapP, a.LIFT, Qi, rhs, st)) !=
+                  BBW_OK ||
+              (s = adj_wadg(N, K, Nq, a.Vq, a.Pq, pl.c2q, lamQ + o, lamR + o, ai, bi, dt, rhs,
+                            z + o, grad, st)) != BBW_OK ||
+              (s = bbw_rk_volume(N, K, c->vgeo, a.DT[0], a.DT[1], a.DT[2], z + o, rhs, st)) !=
+                  BBW_OK ||
+              (s = adj_sigma(N, K, c->fgeo, a.LIFT, z + o, sigma, st)) != BBW_OK ||
+              (s = adj_gather(N, K, c->bc, dt, c->fgeo, a.fidx, a.mapP, sigma, rhs, lamQ + o,
+                              st)) != BBW_OK)
+            return s;
+        }
+      }
+    }
+  }
+  e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(dL_dc2q, grad, (size_t)K * Nq * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && dL_dQ0)
+    e = cudaMemcpy(dL_dQ0, lamQ, t->state * sizeof(float), cudaMemcpyDeviceToHost);
+  return set_cuda_error(e, "bbw_backward: download");
+}

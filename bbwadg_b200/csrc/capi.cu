@@ -17,22 +17,23 @@
 #include "bbwadg.h"
 #include "device_common.cuh"
 #include "fused.h"
+#include "ctx.h"
 #include "internal.h"
 
 namespace bbw {
 
 // LSRK45 coefficients (Carpenter-Kennedy), cpp/src/StartUp3d.cpp:517-529
-static const double kRK4A[5] = {0.0, -567301805773.0 / 1357537059087.0,
+const double kRK4A[5] = {0.0, -567301805773.0 / 1357537059087.0,
                                 -2404267990393.0 / 2016746695238.0,
                                 -3550918686646.0 / 2091501179385.0,
                                 -1275806237668.0 / 842570457699.0};
-static const double kRK4B[5] = {1432997174477.0 / 9575080441755.0,
+const double kRK4B[5] = {1432997174477.0 / 9575080441755.0,
                                 5161836677717.0 / 13612068292357.0,
                                 1720146321549.0 / 2090206949498.0,
                                 3134564353537.0 / 4481467310338.0,
                                 2277821191437.0 / 14882151754819.0};
 // stage times t + rk4c[s] dt, cpp/src/StartUp3d.cpp:531-537
-static const double kRK4C[5] = {0.0, 1432997174477.0 / 9575080441755.0,
+const double kRK4C[5] = {0.0, 1432997174477.0 / 9575080441755.0,
                                 2526269341429.0 / 6820363962896.0,
                                 2006345519317.0 / 3224310063776.0,
                                 2802321613138.0 / 2924317926251.0};
@@ -44,44 +45,7 @@ static int cdivi(int a, int b) { return (a + b - 1) / b; }
 
 using namespace bbw;
 
-struct bbw_ctx {
-  int N = 0, K = 0, Nq = 0, Np = 0, Nfp = 0, variant = 0, bc = 0, device = 0;
-  cudaStream_t stream = nullptr;
-  float *Q[2] = {nullptr, nullptr};
-  int cur = 0;
-  float *res = nullptr;
-  float *vgeo = nullptr, *fgeo = nullptr, *c2q = nullptr, *ops = nullptr;
-  int *nbr = nullptr, *tables = nullptr;
-  FusedPlan plan;
-  int precision = BBW_PREC_FP32;
-  int S = 1;  // shots
-  double *d_time = nullptr;
-  int *d_step = nullptr;
-  int *src_off = nullptr, *src_elem = nullptr;
-  float *src_vec = nullptr;
-  int src_stage_times = 0;
-  int R = 0, max_steps = 0;
-  int *rec_elem = nullptr;
-  float *rec_w = nullptr, *traces = nullptr;
-  TcPlan tc;
-  float *geo_tc = nullptr;
-  void *ops_tc = nullptr;
-  int *err = nullptr;
-  // one graph per starting buffer parity, for one LSRK45 step of size dt
-  cudaGraphExec_t step_graph[2] = {nullptr, nullptr};
-  uint32_t graph_dt_bits[2] = {0, 0};
-};
-
 namespace {
-
-template <class T>
-bbw_status upload(T **dst, const T *src, size_t n, const char *what) {
-  cudaError_t e = cudaMalloc((void **)dst, n * sizeof(T) + 16);
-  if (e != cudaSuccess) return set_cuda_error(e, what);
-  if (src) e = cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice);
-  else e = cudaMemset(*dst, 0, n * sizeof(T));
-  return set_cuda_error(e, what);
-}
 
 void release(bbw_ctx *c) {
   if (!c) return;
@@ -107,8 +71,59 @@ void release(bbw_ctx *c) {
   cudaFree(c->geo_tc);
   cudaFree(c->ops_tc);
   cudaFree(c->err);
+  adj_release(c);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
+}
+
+// Dense operators of the context's basis, kept on the host for the adjoint.
+// Nodal: the given Dr, Ds, Dt, LIFT.  BB: the same linear maps assembled
+// from the sparse forms the BB kernels apply (cpp/okl/WaveKernels.okl:
+// 428-467 derivative, :576-644 L0 then EEL lift).
+void dense_operators(int N, int Nq, const bbw_ops_desc *o, bool bb, bbw_ctx *c) {
+  const int Np = np_of(N), Nfp = nfp_of(N), NF = 4 * Nfp;
+  for (int d = 0; d < 3; ++d) c->hD[d].assign((size_t)Np * Np, 0.f);
+  c->hLIFT.assign((size_t)Np * NF, 0.f);
+  c->hVq.assign(o->Vq, o->Vq + (size_t)Nq * Np);
+  c->hPq.assign(o->Pq, o->Pq + (size_t)Np * Nq);
+  if (!bb) {
+    const float *Dd[3] = {o->Dr, o->Ds, o->Dt};
+    for (int d = 0; d < 3; ++d) c->hD[d].assign(Dd[d], Dd[d] + (size_t)Np * Np);
+    c->hLIFT.assign(o->LIFT, o->LIFT + (size_t)Np * NF);
+    return;
+  }
+  // dpdr = .5 (p2 - p1), dpds = .5 (p3 - p1), dpdt = .5 (p4 - p1) with
+  // p_c = sum_j Dvals[n].j p[Dj_ids[n].c]; column-major D[n + col Np]
+  const int *Dp[4] = {o->D_ids1, o->D_ids2, o->D_ids3, o->D_ids4};
+  std::vector<double> acc[3];
+  for (int d = 0; d < 3; ++d) acc[d].assign((size_t)Np * Np, 0.0);
+  for (int n = 0; n < Np; ++n)
+    for (int j = 0; j < 4; ++j) {
+      const double v = o->Dvals4[4 * n + j];
+      const int *id = Dp[j] + 4 * n;
+      for (int d = 0; d < 3; ++d) {
+        acc[d][n + (size_t)id[d + 1] * Np] += .5 * v;
+        acc[d][n + (size_t)id[0] * Np] -= .5 * v;
+      }
+    }
+  for (int d = 0; d < 3; ++d)
+    for (size_t i = 0; i < acc[d].size(); ++i) c->hD[d][i] = (float)acc[d][i];
+  // LIFT[n][f Nfp + i] = sum over EEL entries (n, f Nfp + i') of EEL * L0[i'][i]
+  const int L0 = o->L0_nnz;
+  std::vector<double> lift((size_t)Np * NF, 0.0);
+  for (int n = 0; n < Np; ++n)
+    for (int j = 0; j < o->EEL_nnz; ++j) {
+      const int col = o->EEL_ids[n + j * Np];
+      const double ev = o->EEL_vals[n + j * Np];
+      if (ev == 0.0 || col < 0 || col >= NF) continue;
+      const int f = col / Nfp, ip = col - f * Nfp;
+      for (int l = 0; l < L0; ++l) {
+        const int i = o->L0_ids[ip + l * Nfp];
+        if (i < 0 || i >= Nfp) continue;
+        lift[n + (size_t)(f * Nfp + i) * Np] += ev * o->L0_vals[ip + l * Nfp];
+      }
+    }
+  for (size_t i = 0; i < lift.size(); ++i) c->hLIFT[i] = (float)lift[i];
 }
 
 // vmapP -> per face (neighbour << 8 | permutation id), permutation table
@@ -308,6 +323,9 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
 
   bbw_ctx *c = new bbw_ctx;
   c->N = N, c->K = K, c->Nq = Nq, c->Np = Np, c->Nfp = Nfp, c->variant = variant, c->bc = bc;
+  dense_operators(N, Nq, o, bb, c);
+  c->hFmask.assign(m->Fmask, m->Fmask + NF);
+  c->hvmapP.assign(m->vmapP, m->vmapP + (size_t)K * NF);
   cudaGetDevice(&c->device);
   const size_t nstate = (size_t)K * 4 * Np;
   cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);

@@ -1,0 +1,89 @@
+// Solver context shared by the runtime translation units (capi.cu,
+// adjoint.cu).  Internal: the public surface is include/bbwadg.h.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "bbwadg.h"
+#include "device_common.cuh"
+#include "fused.h"
+
+namespace bbw {
+
+// device operators and maps of the discrete adjoint (uploaded on first use)
+struct AdjOps {
+  bool ready = false;
+  float *D[3] = {nullptr, nullptr, nullptr};   // Dr, Ds, Dt
+  float *DT[3] = {nullptr, nullptr, nullptr};  // their transposes
+  float *LIFT = nullptr, *Vq = nullptr, *Pq = nullptr;
+  int *Fmask = nullptr, *vmapP = nullptr;
+  int *fidx = nullptr;  // [4][Np]: index of node n on face f, or -1
+  int *mapP = nullptr;  // [K][4Nfp]: matching face node k2*4Nfp + m2, -1 on the boundary
+};
+
+// LSRK45 coefficients (Carpenter-Kennedy), cpp/src/StartUp3d.cpp:517-537
+extern const double kRK4A[5], kRK4B[5], kRK4C[5];
+
+template <class T>
+bbw_status upload(T **dst, const T *src, size_t n, const char *what) {
+  cudaError_t e = cudaMalloc((void **)dst, n * sizeof(T) + 16);
+  if (e != cudaSuccess) return set_cuda_error(e, what);
+  if (src) e = cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice);
+  else e = cudaMemset(*dst, 0, n * sizeof(T));
+  return set_cuda_error(e, what);
+}
+
+// adjoint kernels (kernels_adj.cu)
+bbw_status adj_wadg(int N, int K, int Nq, const float *Vq, const float *Pq, const float *c2q,
+                    const float *lamQ, float *lamR, float a, float b, float dt, const float *rhs,
+                    float *z, double *grad, cudaStream_t st);
+bbw_status adj_sigma(int N, int K, const float *fgeo, const float *LIFT, const float *z,
+                     float *sigma, cudaStream_t st);
+bbw_status adj_gather(int N, int K, int bc, float dt, const float *fgeo, const int *fidx,
+                      const int *mapP, const float *sigma, const float *vol, float *lamQ,
+                      cudaStream_t st);
+bbw_status adj_receivers(int S, int K, int Np, int R, const int *rec_elem, const float *rec_w,
+                         const float *g, int nsteps, int n, float *lamQ, cudaStream_t st);
+bbw_status set_device_double(double *p, double v, cudaStream_t st);
+
+}  // namespace bbw
+
+struct bbw_ctx {
+  int N = 0, K = 0, Nq = 0, Np = 0, Nfp = 0, variant = 0, bc = 0, device = 0;
+  cudaStream_t stream = nullptr;
+  float *Q[2] = {nullptr, nullptr};
+  int cur = 0;
+  float *res = nullptr;
+  float *vgeo = nullptr, *fgeo = nullptr, *c2q = nullptr, *ops = nullptr;
+  int *nbr = nullptr, *tables = nullptr;
+  bbw::FusedPlan plan;
+  int precision = BBW_PREC_FP32;
+  int S = 1;  // shots
+  double *d_time = nullptr;
+  int *d_step = nullptr;
+  int *src_off = nullptr, *src_elem = nullptr;
+  float *src_vec = nullptr;
+  int src_stage_times = 0;
+  int R = 0, max_steps = 0;
+  int *rec_elem = nullptr;
+  float *rec_w = nullptr, *traces = nullptr;
+  bbw::TcPlan tc;
+  float *geo_tc = nullptr;
+  void *ops_tc = nullptr;
+  int *err = nullptr;
+  // one graph per starting buffer parity, for one LSRK45 step of size dt
+  cudaGraphExec_t step_graph[2] = {nullptr, nullptr};
+  uint32_t graph_dt_bits[2] = {0, 0};
+  // host copies for the adjoint: dense operators of the chosen basis
+  // (column-major Np x Np / Np x 4Nfp / Nq x Np / Np x Nq), Fmask, vmapP
+  std::vector<float> hD[3], hLIFT, hVq, hPq;
+  std::vector<int> hFmask, hvmapP;
+  bbw::AdjOps adj;
+};
+
+
+namespace bbw {
+void adj_release(bbw_ctx *c);
+}  // namespace bbw

@@ -1,0 +1,261 @@
+// Discrete-adjoint kernels of the LSRK45 WADG step (sm_100a).
+//
+// One forward stage maps (Q, res) -> (Q', res'):
+//     res' = a res + dt A(c2) Q,     Q' = Q + b res',
+// with A = W(c2) S: S the DG operator (volume + surface, rk_volume /
+// rk_surface, cpp/okl/WaveKernels.okl:44-260) and W the WADG projection of
+// the pressure row, Pq diag(c2/J) Vq (rk_update_WADG,
+// cpp/okl/WaveKernelsWADG.okl:1760-1887; J = 1, so the velocity rows are the
+// identity).  Given the adjoint state (lamQ, lamR) of (Q', res') the stage
+// is reversed as
+//     mu = lamR + b lamQ
+//     z  = W^T mu = (Vq^T diag(c2) Pq^T mu_p, mu_u, mu_v, mu_w)
+//     dL/dc2q[k][q] += dt (Pq^T mu_p)_q (Vq S(Q)_p)_q        (FP64)
+//     lamQ += dt S^T z,  lamR = a mu.
+// S^T z = volume^T z + surface^T z.  The volume part has the forward
+// volume's form with Dr, Ds, Dt replaced by their transposes (run through
+// the kernel-level volume kernel).  The surface part: with
+//     sigma[k][f][i] = .5 Fscale LIFT_f^T (z_p - n_f . z_U)   (per face node)
+// the pressure and velocity adjoints of each face node collect
+//     p: -sigma_k + sigma_k2,   U: n_k sigma_k - n_k2 sigma_k2
+// from the element's own face and the matching face node of the neighbour
+// k2, and -2 sigma (p = 0 wall) or 2 n sigma (rigid wall) on the boundary.
+#include <cuda_runtime.h>
+
+#include "bbwadg.h"
+#include "device_common.cuh"
+
+namespace bbw {
+
+// mu = lamR + b lamQ; lamR <- a mu; z <- W^T mu; grad += dt t (Vq r_p)
+template <int N>
+__global__ void __launch_bounds__(256) k_adj_wadg(int K, int Nq, const float *__restrict__ Vq,
+                                                  const float *__restrict__ Pq,
+                                                  const float *__restrict__ c2q,
+                                                  const float *__restrict__ lamQ,
+                                                  float *__restrict__ lamR, float a, float b,
+                                                  float dt, const float *__restrict__ rhs,
+                                                  float *__restrict__ z,
+                                                  double *__restrict__ grad) {
+  constexpr int Np = NP(N), EB = UPD_EB(N);
+  extern __shared__ float smem[];
+  float *s_mu = smem;                // [EB][Np]  mu_p
+  float *s_r = s_mu + EB * Np;       // [EB][Np]  forward raw rhs_p
+  float *s_t = s_r + EB * Np;        // [EB][Nq]  c2 * Pq^T mu_p
+  const int k0 = blockIdx.x * EB;
+  for (int i = threadIdx.x; i < EB * 4 * Np; i += blockDim.x) {
+    const int e = i / (4 * Np), fn = i - e * 4 * Np;
+    if (k0 + e >= K) continue;
+    const size_t id = (size_t)k0 * 4 * Np + i;
+    const float mu = lamR[id] + b * lamQ[id];
+    lamR[id] = a * mu;
+    if (fn < Np) {
+      s_mu[e * Np + fn] = mu;
+      s_r[e * Np + fn] = rhs ? rhs[id] : 0.f;
+    } else {
+      z[id] = mu;  // velocity rows: Pq Vq = I (J = 1)
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < EB * Nq; i += blockDim.x) {
+    const int e = i / Nq, q = i - e * Nq, k = k0 + e;
+    if (k >= K) continue;
+    const float *mu = s_mu + e * Np, *r = s_r + e * Np;
+    float t = 0.f, v = 0.f;
+    for (int n = 0; n < Np; ++n) {
+      t += __ldg(Pq + n + (size_t)q * Np) * mu[n];
+      v += __ldg(Vq + q + (size_t)n * Nq) * r[n];
+    }
+    if (rhs) grad[(size_t)k * Nq + q] += (double)dt * (double)t * (double)v;
+    s_t[e * Nq + q] = c2q[(size_t)k * Nq + q] * t;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < EB * Np; i += blockDim.x) {
+    const int e = i / Np, n = i - e * Np, k = k0 + e;
+    if (k >= K) continue;
+    const float *t = s_t + e * Nq;
+    float acc = 0.f;
+    for (int q = 0; q < Nq; ++q) acc += __ldg(Vq + q + (size_t)n * Nq) * t[q];
+    z[(size_t)k * 4 * Np + n] = acc;
+  }
+}
+
+// sigma[k][m] = .5 Fscale_f sum_n LIFT[n + m Np] (z_p[n] - n_f . z_U[n])
+template <int N>
+__global__ void __launch_bounds__(256) k_adj_sigma(int K, const float *__restrict__ fgeo,
+                                                   const float *__restrict__ LIFT,
+                                                   const float *__restrict__ z,
+                                                   float *__restrict__ sigma) {
+  constexpr int Np = NP(N), Nfp = NFP(N), NF = 4 * NFP(N), EB = SURF_EB(N);
+  __shared__ float sz[EB][4 * Np];
+  const int k0 = blockIdx.x * EB;
+  for (int i = threadIdx.x; i < EB * 4 * Np; i += blockDim.x) {
+    const int e = i / (4 * Np);
+    if (k0 + e < K) sz[e][i - e * 4 * Np] = z[(size_t)k0 * 4 * Np + i];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < EB * NF; i += blockDim.x) {
+    const int e = i / NF, m = i - e * NF, k = k0 + e;
+    if (k >= K) continue;
+    const int f = m / Nfp;
+    const float *fg = fgeo + (size_t)k * 16 + 4 * f;
+    const float Fscale = fg[0], nx = fg[1], ny = fg[2], nz = fg[3];
+    const float *w = sz[e];
+    float acc = 0.f;
+    for (int n = 0; n < Np; ++n)
+      acc += __ldg(LIFT + n + (size_t)m * Np) *
+             (w[n] - (nx * w[Np + n] + ny * w[2 * Np + n] + nz * w[3 * Np + n]));
+    sigma[(size_t)k * NF + m] = .5f * Fscale * acc;
+  }
+}
+
+// lamQ[k][.][n] += dt (vol[k][.][n] + surface adjoint at node n)
+template <int N>
+__global__ void __launch_bounds__(256) k_adj_gather(int K, int bc, float dt,
+                                                    const float *__restrict__ fgeo,
+                                                    const int *__restrict__ fidx,
+                                                    const int *__restrict__ mapP,
+                                                    const float *__restrict__ sigma,
+                                                    const float *__restrict__ vol,
+                                                    float *__restrict__ lamQ) {
+  constexpr int Np = NP(N), Nfp = NFP(N), NF = 4 * NFP(N);
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)K * Np) return;
+  const int k = (int)(i / Np), n = (int)(i - (long long)k * Np);
+  float dp = 0.f, du = 0.f, dv = 0.f, dw = 0.f;
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    const int fi = __ldg(fidx + f * Np + n);
+    if (fi < 0) continue;
+    const int m = f * Nfp + fi;
+    const float s = sigma[(size_t)k * NF + m];
+    const float *fg = fgeo + (size_t)k * 16 + 4 * f;
+    const float nx = fg[1], ny = fg[2], nz = fg[3];
+    const int code = __ldg(mapP + (size_t)k * NF + m);
+    if (code < 0) {
+      if (bc == BBW_BC_PRESSURE_RELEASE) {
+        dp -= 2.f * s;
+      } else {
+        du += 2.f * nx * s, dv += 2.f * ny * s, dw += 2.f * nz * s;
+      }
+    } else {
+      const int k2 = code / NF, f2 = (code - k2 * NF) / Nfp;
+      const float s2 = sigma[code];
+      const float *g2 = fgeo + (size_t)k2 * 16 + 4 * f2;
+      dp += s2 - s;
+      du += nx * s - g2[1] * s2;
+      dv += ny * s - g2[2] * s2;
+      dw += nz * s - g2[3] * s2;
+    }
+  }
+  const size_t id = (size_t)k * 4 * Np + n;
+  lamQ[id] += dt * (vol[id] + dp);
+  lamQ[id + Np] += dt * (vol[id + Np] + du);
+  lamQ[id + 2 * Np] += dt * (vol[id + 2 * Np] + dv);
+  lamQ[id + 3 * Np] += dt * (vol[id + 3 * Np] + dw);
+}
+
+// trace[s][r][n] = w_r . Q_p(elem_r) after step n  =>  lamQ_p(elem_r) += g w_r.
+// One warp per shot, receivers in order (deterministic when receivers share
+// an element).
+__global__ void k_adj_receivers(int S, int K, int Np, int R, const int *__restrict__ rec_elem,
+                                const float *__restrict__ rec_w, const float *__restrict__ g,
+                                int nsteps, int n, float *__restrict__ lamQ) {
+  const int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (s >= S) return;
+  for (int r = 0; r < R; ++r) {
+    const float gr = g[((size_t)s * R + r) * nsteps + n];
+    float *q = lamQ + ((size_t)s * K + rec_elem[r]) * 4 * Np;
+    for (int j = lane; j < Np; j += 32) q[j] += gr * rec_w[(size_t)r * Np + j];
+    __syncwarp();
+  }
+}
+
+__global__ void k_set_double(double *p, double v) { *p = v; }
+
+// ------------------------------------------------------------- host side
+template <int N>
+static bbw_status launch_adj_n(int K, int Nq, const float *Vq, const float *Pq, const float *c2q,
+                               const float *lamQ, float *lamR, float a, float b, float dt,
+                               const float *rhs, float *z, double *grad, cudaStream_t st) {
+  constexpr int Np = NP(N), EB = UPD_EB(N);
+  const size_t sm = (size_t)EB * (2 * Np + Nq) * sizeof(float);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_adj_wadg<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr = true;
+  }
+  k_adj_wadg<N><<<(K + EB - 1) / EB, 256, sm, st>>>(K, Nq, Vq, Pq, c2q, lamQ, lamR, a, b, dt,
+                                                     rhs, z, grad);
+  return check_launch("adjoint WADG");
+}
+
+template <int N>
+static bbw_status launch_sigma_n(int K, const float *fgeo, const float *LIFT, const float *z,
+                                 float *sigma, cudaStream_t st) {
+  constexpr int EB = SURF_EB(N);
+  k_adj_sigma<N><<<(K + EB - 1) / EB, 256, 0, st>>>(K, fgeo, LIFT, z, sigma);
+  return check_launch("adjoint lift");
+}
+
+template <int N>
+static bbw_status launch_gather_n(int K, int bc, float dt, const float *fgeo, const int *fidx,
+                                  const int *mapP, const float *sigma, const float *vol,
+                                  float *lamQ, cudaStream_t st) {
+  const long long n = (long long)K * NP(N);
+  k_adj_gather<N><<<(int)((n + 255) / 256), 256, 0, st>>>(K, bc, dt, fgeo, fidx, mapP, sigma,
+                                                           vol, lamQ);
+  return check_launch("adjoint face gather");
+}
+
+#define BBW_N_SWITCH(CALL)                    \
+  switch (N) {                                \
+    case 1: return CALL(1);                   \
+    case 2: return CALL(2);                   \
+    case 3: return CALL(3);                   \
+    case 4: return CALL(4);                   \
+    case 5: return CALL(5);                   \
+    case 6: return CALL(6);                   \
+    case 7: return CALL(7);                   \
+    case 8: return CALL(8);                   \
+  }                                           \
+  return set_error(BBW_ERR_UNSUPPORTED, "adjoint: N out of range");
+
+bbw_status adj_wadg(int N, int K, int Nq, const float *Vq, const float *Pq, const float *c2q,
+                    const float *lamQ, float *lamR, float a, float b, float dt, const float *rhs,
+                    float *z, double *grad, cudaStream_t st) {
+#define CALL(n) launch_adj_n<n>(K, Nq, Vq, Pq, c2q, lamQ, lamR, a, b, dt, rhs, z, grad, st)
+  BBW_N_SWITCH(CALL)
+#undef CALL
+}
+
+bbw_status adj_sigma(int N, int K, const float *fgeo, const float *LIFT, const float *z,
+                     float *sigma, cudaStream_t st) {
+#define CALL(n) launch_sigma_n<n>(K, fgeo, LIFT, z, sigma, st)
+  BBW_N_SWITCH(CALL)
+#undef CALL
+}
+
+bbw_status adj_gather(int N, int K, int bc, float dt, const float *fgeo, const int *fidx,
+                      const int *mapP, const float *sigma, const float *vol, float *lamQ,
+                      cudaStream_t st) {
+#define CALL(n) launch_gather_n<n>(K, bc, dt, fgeo, fidx, mapP, sigma, vol, lamQ, st)
+  BBW_N_SWITCH(CALL)
+#undef CALL
+}
+
+bbw_status adj_receivers(int S, int K, int Np, int R, const int *rec_elem, const float *rec_w,
+                         const float *g, int nsteps, int n, float *lamQ, cudaStream_t st) {
+  if (R <= 0) return BBW_OK;
+  const int wpb = 4;
+  k_adj_receivers<<<(S + wpb - 1) / wpb, 32 * wpb, 0, st>>>(S, K, Np, R, rec_elem, rec_w, g,
+                                                            nsteps, n, lamQ);
+  return check_launch("adjoint receivers");
+}
+
+bbw_status set_device_double(double *p, double v, cudaStream_t st) {
+  k_set_double<<<1, 1, 0, st>>>(p, v);
+  return check_launch("device clock");
+}
+
+}  // namespace bbw

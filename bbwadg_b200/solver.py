@@ -184,6 +184,33 @@ class WaveSolver:
         _lib.call("bbw_get_time", self._h, ctypes.byref(t), ctypes.byref(st))
         return t.value, st.value
 
+    # ---- discrete adjoint
+    def set_c2q(self, c2q):
+        """Replace c^2/J at the cubature points ([K][Nq])."""
+        c2q = _f32(c2q)
+        if c2q.size != self.K * self.Nq:
+            raise ValueError("c2q must have K*Nq values")
+        _lib.call("bbw_set_c2q", self._h, c2q.ctypes.data)
+
+    def forward(self, dt, nsteps, checkpoint_every=50):
+        """nsteps steps as steps() does, keeping checkpoints; returns a Tape."""
+        t = ctypes.c_void_p()
+        _lib.call("bbw_forward", self._h, float(dt), int(nsteps), int(checkpoint_every),
+                  ctypes.byref(t))
+        return Tape(t, int(nsteps))
+
+    def backward(self, tape, dL_dtraces, want_state=False):
+        """dL/dtraces [S][R][nsteps] -> dL/dc2q [K][Nq] (FP64, summed over
+        shots) and, with want_state, dL/d(initial state) [S*K*4*Np]."""
+        g = _f32(dL_dtraces)
+        if g.size != self.S * self.R * tape.nsteps:
+            raise ValueError("dL/dtraces must be [S][R][nsteps]")
+        grad = np.zeros((self.K, self.Nq), np.float64)
+        dq = np.zeros(self.state_size, np.float32) if want_state else None
+        _lib.call("bbw_backward", self._h, tape.handle, g.ctypes.data, grad.ctypes.data,
+                  dq.ctypes.data if want_state else None)
+        return (grad, dq) if want_state else grad
+
     def sync(self):
         _lib.call("bbw_sync", self._h)
 
@@ -212,3 +239,21 @@ class WaveSolver:
 
     def __exit__(self, *a):
         self.close()
+
+
+class Tape:
+    """Checkpoints of one bbw_forward call (freed with the object)."""
+
+    def __init__(self, handle, nsteps):
+        self.handle, self.nsteps = handle, nsteps
+
+    def free(self):
+        if getattr(self, "handle", None):
+            _lib.call("bbw_tape_free", self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

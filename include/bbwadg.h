@@ -253,6 +253,32 @@ bbw_status bbw_get_traces(bbw_ctx *ctx, float *out, int *nsteps);
 bbw_status bbw_set_time(bbw_ctx *ctx, double t);
 bbw_status bbw_get_time(bbw_ctx *ctx, double *t, int *step);
 
+/* ---- discrete adjoint: gradient of a receiver-trace loss with respect to
+ * c^2 at the cubature points.  No reference counterpart: the adjoint
+ * reverses the reference's stage (rk_volume + rk_surface + rk_update_WADG,
+ * cpp/okl/WaveKernels.okl:44-260, cpp/okl/WaveKernelsWADG.okl:1760-1887)
+ * and its LSRK45 loop (cpp/src/WaveOKL3d.cpp:2014-2109).  FP32 stage only;
+ * both bases; any number of shots. */
+typedef struct bbw_tape bbw_tape;
+
+/* Replaces c^2 / J at the cubature points ([K][Nq], host). */
+bbw_status bbw_set_c2q(bbw_ctx *ctx, const float *c2q);
+
+/* Advances nsteps steps of dt exactly as bbw_steps does (receivers must be
+ * set; traces land at the current step count onwards) and returns a tape
+ * holding the state at every checkpoint_every-th step start. */
+bbw_status bbw_forward(bbw_ctx *ctx, float dt, int nsteps, int checkpoint_every,
+                       bbw_tape **tape);
+
+/* Given dL/dtraces [S][R][nsteps] (host, for the tape's steps), writes
+ * dL/d(c2q) [K][Nq] (host, FP64, summed over shots) and, if dL_dQ0 is not
+ * NULL, dL/d(state at the tape's first step) [S][K][4][Np].  Recomputes the
+ * forward states from the checkpoints; the context's own state is left as
+ * bbw_forward left it. */
+bbw_status bbw_backward(bbw_ctx *ctx, bbw_tape *tape, const float *dL_dtraces, double *dL_dc2q,
+                        float *dL_dQ0);
+bbw_status bbw_tape_free(bbw_tape *tape);
+
 /* Waits for the context's stream. */
 bbw_status bbw_sync(bbw_ctx *ctx);
 

@@ -1,0 +1,140 @@
+"""GPU discrete adjoint (bbw_forward / bbw_backward) against the FP64
+restatement (oracle/adjoint.py) and FP64 central finite differences.
+
+Tolerances: gradient vs the FP64 discrete adjoint 1e-4 relative L2;
+directional derivatives vs finite differences 1e-4 relative (5 seeded
+directions)."""
+import numpy as np
+import pytest
+from conftest import rel_l2
+from test_adjoint_oracle import adjoint_oracle
+
+from bbwadg_b200 import WaveSolver, make_problem
+from bbwadg_b200._lib import BBWError
+from bbwadg_b200.problem import gaussian_source, receiver_weights, source_entries
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-4
+
+
+def setup(variant, bc, S=2, N=3, n=2, seed=0):
+    p = make_problem(N, n, variant=variant, c2="sine", c2_jitter=0.3, seed=seed)
+    pts = np.array([[0.1, 0.2, -0.3], [0.5, -0.5, 0.25], [-0.4, 0.0, 0.6], [0.0, 0.3, 0.0]])
+    rec = receiver_weights(p, pts)
+    centres = [(0.0, 0.0, 0.1), (0.3, -0.2, -0.1), (-0.3, 0.3, 0.2)][:S]
+    dense = [gaussian_source(p, x0, a=3.0) for x0 in centres]
+    return p, rec, dense
+
+
+def gpu_gradient(p, rec, dense, bc, nsteps, every, Q0, stage_times=True):
+    S = len(dense)
+    s = WaveSolver(p, bc="rigid" if bc else "pressure_release")
+    s.set_shots(S)
+    ent = [source_entries(f, shot=i, rtol=0.0) for i, f in enumerate(dense)]
+    s.set_sources(*(np.concatenate(x) for x in zip(*ent)), f0=10.0, amplitude=1e2,
+                  stage_times=stage_times)
+    s.set_receivers(*rec, nsteps)
+    s.set_data(np.tile(Q0, S))
+    s.set_time(0.0)
+    tape = s.forward(p.dt, nsteps, every)
+    tr = s.get_traces()
+    grad, dq = s.backward(tape, tr, want_state=True)
+    tape.free()
+    s.close()
+    return tr, grad, dq
+
+
+def oracle_gradient(p, rec, dense, bc, nsteps, Q0, stage_times=True):
+    ad = adjoint_oracle(p, bc)
+    dt = float(np.float32(p.dt))
+    total = np.zeros((p.K, p.Nq))
+    trs = []
+    for f in dense:
+        src = dict(fsrc=f.astype(np.float64), f0=10.0, tR=0.1, amp=1e2, stage_times=stage_times)
+        _, tr, states = ad.forward(Q0.astype(np.float64), dt, nsteps, rec, src)
+        g, _ = ad.backward(dt, nsteps, states, tr, rec, src)
+        total += g
+        trs.append(tr)
+    return np.array(trs), total, ad
+
+
+@pytest.mark.parametrize("variant", ["nodal", "bb"])
+@pytest.mark.parametrize("bc", [0, 1])
+def test_gradient_matches_fp64_adjoint(cuda, variant, bc):
+    p, rec, dense = setup(variant, bc)
+    nsteps = 12
+    tr, grad, _ = gpu_gradient(p, rec, dense, bc, nsteps, 5, p.Q0)
+    tr64, grad64, _ = oracle_gradient(p, rec, dense, bc, nsteps, p.Q0)
+    assert rel_l2(tr, tr64) < 1e-5
+    assert rel_l2(grad, grad64) < TOL
+
+
+def test_directional_derivatives_match_finite_differences(cuda):
+    p, rec, dense = setup("nodal", 0, S=1)
+    nsteps = 12
+    _, grad, _ = gpu_gradient(p, rec, dense, 0, nsteps, 4, p.Q0)
+    ad = adjoint_oracle(p, 0)
+    dt = float(np.float32(p.dt))
+    src = dict(fsrc=dense[0].astype(np.float64), f0=10.0, tR=0.1, amp=1e2, stage_times=True)
+    c2 = ad.c2q.copy()
+
+    def loss(c):
+        ad.c2q = c
+        return 0.5 * float((ad.forward(p.Q0.astype(np.float64), dt, nsteps, rec, src)[1] ** 2).sum())
+
+    rng = np.random.default_rng(11)
+    for _ in range(5):
+        d = rng.standard_normal(c2.shape)
+        eps = 1e-4
+        fd = (loss(c2 + eps * d) - loss(c2 - eps * d)) / (2 * eps)
+        assert abs(float((grad * d).sum()) - fd) <= TOL * abs(fd)
+
+
+def test_checkpoint_interval_does_not_change_the_gradient(cuda):
+    p, rec, dense = setup("nodal", 0, S=1)
+    ref = gpu_gradient(p, rec, dense, 0, 10, 1, p.Q0)[1]
+    for every in (3, 10, 64):
+        assert np.array_equal(gpu_gradient(p, rec, dense, 0, 10, every, p.Q0)[1], ref)
+
+
+def test_state_gradient_matches_fp64_adjoint(cuda):
+    p, rec, dense = setup("nodal", 0, S=1)
+    _, _, dq = gpu_gradient(p, rec, dense, 0, 8, 3, p.Q0)
+    ad = adjoint_oracle(p, 0)
+    dt = float(np.float32(p.dt))
+    src = dict(fsrc=dense[0].astype(np.float64), f0=10.0, tR=0.1, amp=1e2, stage_times=True)
+    _, tr, states = ad.forward(p.Q0.astype(np.float64), dt, 8, rec, src)
+    _, gQ = ad.backward(dt, 8, states, tr, rec, src)
+    assert rel_l2(dq, gQ.ravel()) < TOL
+
+
+def test_autograd_function(cuda):
+    import torch
+    from bbwadg_b200.autograd import receiver_traces
+    p, rec, dense = setup("nodal", 0, S=1)
+    s = WaveSolver(p)
+    s.set_sources(*source_entries(dense[0], rtol=0.0), f0=10.0, amplitude=1e2, stage_times=True)
+    s.set_receivers(*rec, 16)
+    c2 = torch.tensor(p.c2q, dtype=torch.float64, requires_grad=True)
+    tr = receiver_traces(c2, s, p.Q0, p.dt, 10, 4)
+    loss = 0.5 * (tr.double() ** 2).sum()
+    loss.backward()
+    _, g64, _ = oracle_gradient(p, rec, dense, 0, 10, p.Q0)
+    assert rel_l2(c2.grad.numpy(), g64) < TOL
+    s.close()
+
+
+def test_adjoint_errors(cuda):
+    p, rec, dense = setup("nodal", 0, S=1)
+    s = WaveSolver(p)
+    with pytest.raises(BBWError):  # no receivers
+        s.forward(p.dt, 4, 2)
+    s.set_receivers(*rec, 3)
+    with pytest.raises(BBWError):  # capacity
+        s.forward(p.dt, 4, 2)
+    s.close()
+    t = WaveSolver(make_problem(3, 2), precision="f16x3")
+    t.set_receivers(*rec, 8)
+    with pytest.raises(BBWError):
+        t.forward(p.dt, 4, 2)
+    t.close()
