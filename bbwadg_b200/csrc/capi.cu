@@ -573,10 +573,14 @@ extern "C" bbw_status bbw_set_sources(bbw_ctx *c, int nent, const int *shot, con
     off[shot[j] + 1] += 1;
   }
   for (int i = 0; i < c->S; ++i) off[i + 1] += off[i];
-  std::vector<int> fill(off.begin(), off.end() - 1);
+  // order by (shot, element); the kernel bisects a shot's entries by element
+  for (int j = 0; j < nent; ++j) order[j] = j;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return shot[a] != shot[b] ? shot[a] < shot[b] : elem[a] < elem[b];
+  });
   std::vector<float> v((size_t)nent * Np);
-  for (int j = 0; j < nent; ++j) {
-    const int at = fill[shot[j]]++;
+  for (int at = 0; at < nent; ++at) {
+    const int j = order[at];
     el[at] = elem[j];
     std::memcpy(&v[(size_t)at * Np], vec + (size_t)j * Np, Np * sizeof(float));
   }

@@ -530,15 +530,26 @@ __global__ void __launch_bounds__(FusedCfg<N>::T, 1) k_fused_stage(FusedParams P
       // source term of this shot, added to the projected rhs_p as
       // rk_update_elas does (acous_elas_cpp/okl/ElasKernelsWADG.okl:400-403)
       if (P.src_off) {
-        const int j0 = __ldg(P.src_off + shot), j1 = __ldg(P.src_off + shot + 1);
+        // entries of a shot are sorted by element: find the first one of
+        // this tile by bisection, then walk the tile's entries
+        int j0 = __ldg(P.src_off + shot), j1 = __ldg(P.src_off + shot + 1);
         if (j1 > j0) {
-          const float amp = ricker((float)(*P.time) + P.cstage * P.fdt, P.f0, P.tR, P.samp);
-          for (int j = j0; j < j1; ++j) {
-            const unsigned rel = (unsigned)(__ldg(P.src_elem + j) - k0);
-            if (rel < (unsigned)ne && lane == (int)rel) {
+          int lo = j0, hi = j1;
+          while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (__ldg(P.src_elem + mid) < k0) lo = mid + 1;
+            else hi = mid;
+          }
+          if (lo < j1 && __ldg(P.src_elem + lo) < k0 + ne) {
+            const float amp = ricker((float)(*P.time) + P.cstage * P.fdt, P.f0, P.tR, P.samp);
+            for (int j = lo; j < j1; ++j) {
+              const int rel = __ldg(P.src_elem + j) - k0;
+              if (rel >= ne) break;
+              if (lane == rel) {
 #pragma unroll
-              for (int i = 0; i < R; ++i)
-                if (r0 + i < Np) acc[i] += amp * __ldg(P.src_vec + (size_t)j * Np + r0 + i);
+                for (int i = 0; i < R; ++i)
+                  if (r0 + i < Np) acc[i] += amp * __ldg(P.src_vec + (size_t)j * Np + r0 + i);
+              }
             }
           }
         }

@@ -188,12 +188,12 @@ class Problem:
         return err, err / nrm
 
 
-def gaussian_source(prob, x0, a=100.0):
+def gaussian_source(prob, x0, a=100.0, xyz=None):
     """Smoothed point source of acous_elas_cpp/src/WaveOKL3d.cpp:176-186 and
     :226-228: exp(-a^2 |x - x0|^2) at the cubature points, normalised to max 1
     over the mesh, projected with Pq (L2 projection onto the element basis).
     Returns the dense [K][Np] float32 array the reference uploads (c_fsrc)."""
-    xq, yq, zq = prob.cubature_xyz()
+    xq, yq, zq = prob.cubature_xyz() if xyz is None else xyz
     r2 = (xq - x0[0]) ** 2 + (yq - x0[1]) ** 2 + (zq - x0[2]) ** 2
     f = np.exp(-a * a * r2)
     f *= 1.0 / np.abs(f).max()

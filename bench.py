@@ -173,6 +173,140 @@ def workload_config(args, variant):
             "l2_flush": "state 3x176 MB > L2", "bc": "pressure_release"}
 
 
+def c2_inclusions(seed, n=10, lo=-0.8, hi=0.8):
+    """c^2 in [1, 2): 1 + s/(1+s), s a sum of n seeded Gaussian inclusions."""
+    rng = np.random.default_rng(seed)
+    cen = rng.uniform(lo, hi, (n, 3))
+    rad = rng.uniform(0.1, 0.3, n)
+    amp = rng.uniform(0.5, 2.0, n)
+
+    def f(x, y, z):
+        s = np.zeros_like(x)
+        for c, r, a in zip(cen, rad, amp):
+            s += a * np.exp(-((x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2) / r ** 2)
+        return 1.0 + s / (1.0 + s)
+    return f
+
+
+def anomalies(base, seed, n=5, amp=0.3):
+    """base + n seeded Gaussian anomalies of amplitude +-amp."""
+    rng = np.random.default_rng(seed)
+    cen = rng.uniform(-0.6, 0.6, (n, 3))
+    rad = rng.uniform(0.15, 0.3, n)
+    sgn = rng.choice([-1.0, 1.0], n)
+
+    def f(x, y, z):
+        v = base(x, y, z)
+        for c, r, sg in zip(cen, rad, sgn):
+            v = v + sg * amp * np.exp(-((x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2) / r ** 2)
+        return v
+    return f
+
+
+def shot_sources(prob, S, seed, a=20.0):
+    """S seeded point-like sources in [-0.8, 0.8]^3: (shot, elem, vec) entries."""
+    from bbwadg_b200.problem import gaussian_source, source_entries
+    rng = np.random.default_rng(seed)
+    xyz = prob.cubature_xyz()
+    ent = [source_entries(gaussian_source(prob, rng.uniform(-0.8, 0.8, 3), a=a, xyz=xyz), shot=i)
+           for i in range(S)]
+    return [np.concatenate(x) for x in zip(*ent)]
+
+
+def shots_workload(args, torch, dist, world):
+    """Batched multi-shot: N=4, 24^3 x 6 tets (K=82944), 32 shots in one
+    launch per stage (graph-captured steps), Ricker f0 = 4 point sources at
+    seeded locations, c^2 in [1, 2] with 10 seeded Gaussian inclusions."""
+    from bbwadg_b200 import WaveSolver, make_problem
+    N, nh, S = 4, args.shots_hex, args.shots
+    cub, tri = reference_rule(N)
+    prob = make_problem(N, nh, c2=c2_inclusions(77), cubature=cub, tri_cubature=tri, cfl=0.25)
+    out = {"workload": "batched shots, N=4, %d^3x6 tets (K=%d), %d shots, Ricker f0=4, "
+                       "c2 in [1,2] with 10 inclusions" % (nh, prob.K, S),
+           "N": N, "K": prob.K, "shots": S}
+    for label, nshot in (("batched", S), ("one_shot", 1)):
+        s = WaveSolver(prob)
+        s.set_shots(nshot)
+        s.set_sources(*shot_sources(prob, nshot, 99), f0=4.0, amplitude=1e4, stage_times=True)
+        s.set_time(0.0)
+        _, _, sp = s.device_state()
+        stream = torch.cuda.ExternalStream(sp)
+        s.steps(prob.dt, args.warmup)
+        s.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        s.steps(prob.dt, args.shots_steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        dofs = prob.K * prob.Np * 4 * 5 * args.shots_steps * nshot
+        out[label] = {"value": world * dofs / (ms / 1e3), "unit": "DOF-stage/s",
+                      "ms_per_step": ms / args.shots_steps, "steps": args.shots_steps,
+                      "finite": bool(np.isfinite(s.get_data()).all())}
+        s.close()
+    return out
+
+
+def adjoint_workload(args):
+    """Forward + adjoint gradient: N=4, 16^3 x 6 tets (K=24576), 8 seeded
+    Ricker shots, 64 seeded receivers, 400 steps, checkpoints every 50, L2
+    trace misfit against a target with 5 seeded +-0.3 Gaussian anomalies."""
+    from bbwadg_b200 import WaveSolver, make_problem
+    from bbwadg_b200.problem import c2_sine, receiver_weights
+    N, nh, S, R, steps, every = 4, 16, 8, 64, args.adj_steps, 50
+    cub, tri = reference_rule(N)
+    base = c2_sine
+    prob = make_problem(N, nh, c2=anomalies(base, 5), cubature=cub, tri_cubature=tri, cfl=0.25)
+    xq, yq, zq = prob.cubature_xyz()
+    c2_target = prob.c2q.copy()
+    c2_back = np.ascontiguousarray(base(xq, yq, zq), np.float32)
+    rng = np.random.default_rng(64)
+    el, w = receiver_weights(prob, rng.uniform(-0.8, 0.8, (R, 3)))
+    s = WaveSolver(prob)
+    s.set_shots(S)
+    s.set_sources(*shot_sources(prob, S, 8), f0=4.0, amplitude=1e4, stage_times=True)
+    s.set_receivers(el, w, steps)
+    zero = np.zeros(s.state_size, np.float32)
+
+    def run(c2, tape):
+        s.set_c2q(c2)
+        s.set_data(zero)
+        s.set_residual(zero)
+        s.set_time(0.0)
+        if tape:
+            return s.forward(prob.dt, steps, every)
+        s.steps(prob.dt, steps)
+        s.sync()
+        return None
+
+    run(c2_target, False)
+    obs = s.get_traces().copy()
+    s.sync()
+    t0 = time.perf_counter()
+    tape = run(c2_back, True)
+    s.sync()
+    t1 = time.perf_counter()
+    tr = s.get_traces()
+    misfit = 0.5 * float(((tr - obs).astype(np.float64) ** 2).sum())
+    t2 = time.perf_counter()
+    grad = s.backward(tape, tr - obs)
+    t3 = time.perf_counter()
+    tape.free()
+    s.close()
+    return {"workload": "forward + adjoint c2 gradient, N=4, 16^3x6 tets (K=%d), %d shots, "
+                        "%d receivers, %d steps, checkpoints every %d" % (prob.K, S, R, steps, every),
+            "forward_s": t1 - t0, "backward_s": t3 - t2, "total_s": (t1 - t0) + (t3 - t2),
+            "misfit": misfit, "grad_norm": float(np.linalg.norm(grad)),
+            "grad_finite": bool(np.isfinite(grad).all())}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -184,6 +318,12 @@ def main():
     ap.add_argument("--hex", type=int, default=N_HEX, help="hexes per direction (profiling cases)")
     ap.add_argument("--variants", default="nodal,bb,nodal-f16x3",
                     help="variants to run, comma separated (nodal, bb, nodal-f16x3)")
+    ap.add_argument("--extra", default="shots,adjoint",
+                    help="extra workloads reported beside the headline: shots, adjoint")
+    ap.add_argument("--shots", type=int, default=32)
+    ap.add_argument("--shots-hex", type=int, default=24)
+    ap.add_argument("--shots-steps", type=int, default=10)
+    ap.add_argument("--adj-steps", type=int, default=400)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -252,6 +392,9 @@ def main():
                                 finite=bool(np.isfinite(out.numpy()).all()))
         s.close()
 
+    extra = [x for x in args.extra.split(",") if x]
+    shots = shots_workload(args, torch, dist, world) if "shots" in extra else None
+    adj = adjoint_workload(args) if "adjoint" in extra else None
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
@@ -301,6 +444,10 @@ def main():
                           "via oracle/_ref" % (SAMPLE_HEX, r["K"], r["steps"])}
         else:
             line["cpu_baseline"] = {"value": None, "unavailable": err}
+    if shots is not None:
+        line["shots"] = shots
+    if adj is not None:
+        line["adjoint"] = adj
     print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
