@@ -76,6 +76,66 @@ void release(bbw_ctx *c) {
   delete c;
 }
 
+}  // namespace
+
+namespace bbw {
+
+// Operators packed per warp for the fused kernel with W warps per CTA:
+//   vol  [W][Np(m)][P3R]  (Dr, Ds, Dt)[r0+i][m] at 3i + {0,1,2}   (nodal)
+//   lift [W][NF(m)][PR]   LIFT[r0+i][m]                           (nodal)
+//   pq   [W][Nq(q)][PR]   Pq[r0+i][q]
+//   vq   [W][Np(n)][PRQ]  Vq[q0+i][n]
+// rows r0 = w R, R = ceil(Np / W); cubature rows q0 = w RQ, RQ = ceil(Nq / W).
+void pack_fused_ops(int N, int Nq, int W, bool bb, const float *Dr, const float *Ds,
+                    const float *Dt, const float *LIFT, const float *Vq, const float *Pq,
+                    FusedOps &out) {
+  const int Np = np_of(N), NF = 4 * nfp_of(N);
+  const int R = cdivi(Np, W), PR = round4i(R), P3R = round4i(3 * R);
+  const int RQ = cdivi(Nq, W), PRQ = round4i(RQ);
+  std::vector<float> &ops = out.ops;
+  ops.clear();
+  if (!bb) {
+    std::vector<float> vol((size_t)W * Np * P3R, 0.f), lift((size_t)W * NF * PR, 0.f);
+    for (int w = 0; w < W; ++w)
+      for (int i = 0; i < R; ++i) {
+        const int r = w * R + i;
+        if (r >= Np) continue;
+        for (int mm = 0; mm < Np; ++mm) {
+          float *d = &vol[((size_t)w * Np + mm) * P3R + 3 * i];
+          d[0] = Dr[r + mm * Np], d[1] = Ds[r + mm * Np], d[2] = Dt[r + mm * Np];
+        }
+        for (int mm = 0; mm < NF; ++mm) lift[((size_t)w * NF + mm) * PR + i] = LIFT[r + mm * Np];
+      }
+    ops.insert(ops.end(), vol.begin(), vol.end());
+    out.off_lift = (int)ops.size();
+    ops.insert(ops.end(), lift.begin(), lift.end());
+  } else {
+    out.off_lift = 0;
+  }
+  out.off_pq = (int)ops.size();
+  std::vector<float> pq((size_t)W * Nq * PR, 0.f), vq((size_t)W * Np * PRQ, 0.f);
+  for (int w = 0; w < W; ++w) {
+    for (int i = 0; i < R; ++i) {
+      const int r = w * R + i;
+      if (r < Np)
+        for (int q = 0; q < Nq; ++q) pq[((size_t)w * Nq + q) * PR + i] = Pq[r + q * Np];
+    }
+    for (int i = 0; i < RQ; ++i) {
+      const int q = w * RQ + i;
+      if (q < Nq)
+        for (int n = 0; n < Np; ++n) vq[((size_t)w * Np + n) * PRQ + i] = Vq[q + n * Nq];
+    }
+  }
+  ops.insert(ops.end(), pq.begin(), pq.end());
+  out.off_vq = (int)ops.size();
+  ops.insert(ops.end(), vq.begin(), vq.end());
+  out.RQ = RQ, out.PRQ = PRQ;
+}
+
+}  // namespace bbw
+
+namespace {
+
 // Dense operators of the context's basis, kept on the host for the adjoint.
 // Nodal: the given Dr, Ds, Dt, LIFT.  BB: the same linear maps assembled
 // from the sparse forms the BB kernels apply (cpp/okl/WaveKernels.okl:
@@ -216,50 +276,16 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
   bbw_status s = compress_connectivity(N, K, m->Fmask, m->vmapP, nbr, pats, npat);
   if (s != BBW_OK) return s;
 
-  // ---- pack operators in the per-warp layouts of kernels_fused.cu
-  const int W = fused_warps(N), R = cdivi(Np, W), PR = round4i(R), P3R = round4i(3 * R);
-  const int RQ = cdivi(Nq, W), PRQ = round4i(RQ);
+  // ---- pack operators in the per-warp layouts of the fused kernel
   for (int i = 0; i < NF; ++i)
     if (m->Fmask[i] < 0 || m->Fmask[i] >= Np)
       return set_error(BBW_ERR_ARG, "bbw_create: Fmask entry out of range");
-  std::vector<float> ops;
-  int off_lift = 0, off_pq = 0, off_vq = 0;
-  if (!bb) {
-    std::vector<float> vol((size_t)W * Np * P3R, 0.f), lift((size_t)W * NF * PR, 0.f);
-    for (int w = 0; w < W; ++w)
-      for (int i = 0; i < R; ++i) {
-        const int r = w * R + i;
-        if (r >= Np) continue;
-        for (int mm = 0; mm < Np; ++mm) {
-          float *d = &vol[((size_t)w * Np + mm) * P3R + 3 * i];
-          d[0] = o->Dr[r + mm * Np], d[1] = o->Ds[r + mm * Np], d[2] = o->Dt[r + mm * Np];
-        }
-        for (int mm = 0; mm < NF; ++mm) lift[((size_t)w * NF + mm) * PR + i] = o->LIFT[r + mm * Np];
-      }
-    ops.insert(ops.end(), vol.begin(), vol.end());
-    off_lift = (int)ops.size();
-    ops.insert(ops.end(), lift.begin(), lift.end());
-  }
-  if (bb) off_lift = 0;
-  off_pq = (int)ops.size();
-  {
-    std::vector<float> pq((size_t)W * Nq * PR, 0.f), vq((size_t)W * Np * PRQ, 0.f);
-    for (int w = 0; w < W; ++w) {
-      for (int i = 0; i < R; ++i) {
-        const int r = w * R + i;
-        if (r < Np)
-          for (int q = 0; q < Nq; ++q) pq[((size_t)w * Nq + q) * PR + i] = o->Pq[r + q * Np];
-      }
-      for (int i = 0; i < RQ; ++i) {
-        const int q = w * RQ + i;
-        if (q < Nq)
-          for (int n = 0; n < Np; ++n) vq[((size_t)w * Np + n) * PRQ + i] = o->Vq[q + n * Nq];
-      }
-    }
-    ops.insert(ops.end(), pq.begin(), pq.end());
-    off_vq = (int)ops.size();
-    ops.insert(ops.end(), vq.begin(), vq.end());
-  }
+  const int W = fused_default_warps(N);
+  FusedOps fo;
+  pack_fused_ops(N, Nq, W, bb, o->Dr, o->Ds, o->Dt, o->LIFT, o->Vq, o->Pq, fo);
+  const std::vector<float> &ops = fo.ops;
+  const int off_lift = fo.off_lift, off_pq = fo.off_pq, off_vq = fo.off_vq;
+  const int RQ = fo.RQ, PRQ = fo.PRQ;
   // ---- integer tables: Fmask | patterns | BB tables
   std::vector<int> tab(m->Fmask, m->Fmask + NF);
   tab.resize(round4i((int)tab.size()), 0);
@@ -354,7 +380,7 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
   pl.ops = c->ops, pl.ops_floats = (int)ops.size();
   pl.off_lift = off_lift, pl.off_pq = off_pq, pl.off_vq = off_vq;
   pl.tables = c->tables, pl.table_ints = (int)tab.size(), pl.pat_off = pat_off, pl.bb_off = bb_off;
-  pl.S = 1, pl.time = c->d_time;
+  pl.S = 1, pl.time = c->d_time, pl.W = W;
   if ((s = fused_prepare(pl)) != BBW_OK) {
     release(c);
     return s;
@@ -508,6 +534,113 @@ extern "C" bbw_status bbw_steps(bbw_ctx *c, float dt, int nsteps) {
     if (e != cudaSuccess) return set_cuda_error(e, "bbw_steps: launch");
     c->cur ^= 1;  // five stages swap the buffers an odd number of times
   }
+  return BBW_OK;
+}
+
+// plan of the fused stage with W warps and the requested placement; the
+// packed operators are uploaded to *ops_buf (owned by the caller)
+static bbw_status make_variant(bbw_ctx *c, int W, int want_ops, int want_pipe, FusedPlan &p,
+                               float **ops_buf) {
+  FusedOps fo;
+  pack_fused_ops(c->N, c->Nq, W, c->variant == BBW_BB, c->hD[0].data(), c->hD[1].data(),
+                 c->hD[2].data(), c->hLIFT.data(), c->hVq.data(), c->hPq.data(), fo);
+  bbw_status s = upload(ops_buf, fo.ops.data(), fo.ops.size(), "fused stage: operators");
+  if (s != BBW_OK) return s;
+  p = c->plan;
+  p.W = W;
+  p.ops = *ops_buf, p.ops_floats = (int)fo.ops.size();
+  p.off_lift = fo.off_lift, p.off_pq = fo.off_pq, p.off_vq = fo.off_vq;
+  p.RQ = fo.RQ, p.PRQ = fo.PRQ;
+  p.want_ops = want_ops, p.want_pipe = want_pipe;
+  return fused_prepare(p);
+}
+
+static int config_code(const FusedPlan &p) {
+  return p.W | (p.ops_smem > 0 ? 1 << 8 : 0) | (p.pipe ? 1 << 9 : 0);
+}
+
+extern "C" bbw_status bbw_set_config(bbw_ctx *c, int config) {
+  if (!c) return set_error(BBW_ERR_ARG, "bbw_set_config: ctx is NULL");
+  const int W = config & 255;
+  if ((W != 8 && W != 16) || (config >> 10) != 0)
+    return set_error(BBW_ERR_ARG, "bbw_set_config: W must be 8 or 16, flags bits 8-9");
+  if (c->precision != BBW_PREC_FP32) return BBW_OK;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return set_cuda_error(e, "bbw_set_config");
+  FusedPlan p;
+  float *buf = nullptr;
+  bbw_status s = make_variant(c, W, config >> 8 & 1, config >> 9 & 1, p, &buf);
+  if (s != BBW_OK) {
+    cudaFree(buf);
+    return s;
+  }
+  cudaFree(c->ops);
+  c->ops = buf;
+  c->plan = p;
+  drop_graphs(c);
+  return BBW_OK;
+}
+
+extern "C" bbw_status bbw_autotune(bbw_ctx *c, float dt, int stages, int *config) {
+  if (!c || !(dt > 0.f) || stages < 1) return set_error(BBW_ERR_ARG, "bbw_autotune: bad argument");
+  if (c->precision != BBW_PREC_FP32) {  // nothing to choose for the tensor-core stage
+    if (config) *config = 0;
+    return BBW_OK;
+  }
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return set_cuda_error(e, "bbw_autotune");
+  const size_t n = (size_t)c->S * c->K * 4 * c->Np;
+  float *q[2] = {nullptr, nullptr}, *r = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  auto cleanup = [&]() {
+    cudaFree(q[0]), cudaFree(q[1]), cudaFree(r);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  };
+  bbw_status s;
+  if ((s = upload<float>(&q[0], nullptr, n, "bbw_autotune")) != BBW_OK ||
+      (s = upload<float>(&q[1], nullptr, n, "bbw_autotune")) != BBW_OK ||
+      (s = upload<float>(&r, nullptr, n, "bbw_autotune")) != BBW_OK) {
+    cleanup();
+    return s;
+  }
+  cudaMemcpy(q[0], c->Q[c->cur], n * sizeof(float), cudaMemcpyDeviceToDevice);
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int Ws[2] = {8, 16};
+  float best_ms = 0.f;
+  int best = -1;
+  for (int wi = 0; wi < 2; ++wi)
+    for (int v = 0; v < 4; ++v) {
+      FusedPlan p;
+      float *buf = nullptr;
+      if (make_variant(c, Ws[wi], v < 2 ? 1 : 0, v % 2 == 0 ? 1 : 0, p, &buf) != BBW_OK) {
+        cudaFree(buf);  // does not fit
+        continue;
+      }
+      int cur = 0;
+      for (int i = 0; i < 2; ++i, cur ^= 1)  // warm-up
+        fused_launch(p, q[cur], q[cur ^ 1], r, 0.f, (float)kRK4B[0], dt, 0.f, c->stream);
+      cudaEventRecord(e0, c->stream);
+      for (int i = 0; i < stages; ++i, cur ^= 1)
+        fused_launch(p, q[cur], q[cur ^ 1], r, (float)kRK4A[i % 5], (float)kRK4B[i % 5], dt, 0.f,
+                     c->stream);
+      cudaEventRecord(e1, c->stream);
+      e = cudaEventSynchronize(e1);
+      cudaFree(buf);
+      if (e != cudaSuccess) {
+        cleanup();
+        return set_cuda_error(e, "bbw_autotune: timing");
+      }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (best < 0 || ms < best_ms) best = config_code(p), best_ms = ms;
+    }
+  cleanup();
+  if (best < 0) return set_error(BBW_ERR_UNSUPPORTED, "bbw_autotune: no variant fits");
+  bbw_status s2 = bbw_set_config(c, best);
+  if (s2 != BBW_OK) return s2;
+  if (config) *config = config_code(c->plan);
   return BBW_OK;
 }
 

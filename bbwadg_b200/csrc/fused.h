@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstddef>
+#include <vector>
 
 #include "bbwadg.h"
 
@@ -14,6 +15,8 @@ constexpr int kFusedRowStride = 33;
 
 struct FusedPlan {
   int N = 0, K = 0, Nq = 0, RQ = 0, PRQ = 0, bc = 0, npat = 0;
+  int W = 0;                            // warps per CTA (8 or 16; 0 = default for N)
+  int want_ops = -1, want_pipe = -1;    // requested placement (-1: first that fits)
   bool bb = false, pipe = false;
   int grid = 0;
   size_t smem = 0;
@@ -31,7 +34,16 @@ struct FusedPlan {
   const double *time = nullptr;
 };
 
-int fused_warps(int N);
+int fused_default_warps(int N);
+
+// operators packed per warp for a W-warp fused kernel (capi.cu)
+struct FusedOps {
+  std::vector<float> ops;
+  int off_lift = 0, off_pq = 0, off_vq = 0, RQ = 0, PRQ = 0;
+};
+void pack_fused_ops(int N, int Nq, int W, bool bb, const float *Dr, const float *Ds,
+                    const float *Dt, const float *LIFT, const float *Vq, const float *Pq,
+                    FusedOps &out);
 
 // ---- tensor-core (tcgen05) stage, kernels_tc.cu
 constexpr int TC_GEO = 28;  // floats per element geometry record: vgeo 9 | fgeo 16 | pad 3

@@ -1,0 +1,686 @@
+#pragma once
+// Fused LSRK stage for the affine-tet acoustic WADG method (sm_100a):
+// kernel template and its host-side launch helpers, instantiated per order N
+// by kernels_fused_n<N>.cu.
+//
+// One kernel per stage replaces the reference's three launches
+// (rk_volume + rk_surface + rk_update_WADG, cpp/src/WaveOKL3d.cpp:2084-2106,
+// or their BB counterparts): per element it forms the volume term, the upwind
+// surface flux and lift, projects c^2 * rhs_p with the WADG operators and
+// applies the LSRK45 stage update, reading each element's state once from
+// HBM and writing the new state and residual once.
+//
+// Work decomposition: a persistent CTA owns a tile of E = 32 consecutive
+// elements at a time; lane l of every warp works on element l of the tile,
+// warp w owns a block of R output rows (nodes) or RQ cubature points.  The
+// reference-element operators are staged in shared memory once per CTA in a
+// per-warp packed layout, so every operator read is a warp-uniform broadcast
+// (float4) while the element data is read conflict-free with lane = element.
+// State tiles are moved between HBM and shared memory with coalesced float4
+// traffic and transposed to [row][element] (stride 33) on the way.
+//
+// Double-buffered state: the stage reads Qin (this element and its
+// neighbours' face traces) and writes Qout, so neighbour gathers never race
+// with updates.  res is updated in place.
+//
+// Connectivity: vmapP is compressed at context creation into, per element
+// face, the neighbour element and the index of its face-node permutation
+// (at most 24 distinct permutations exist: 4 faces x 6 orientations), the
+// permutations being kept in a small table; boundary faces are flagged.
+//
+// Simplifications that are exact in exact arithmetic and checked at
+// creation: Uflux = -pflux (both are formed from the same jump with opposite
+// sign, cpp/okl/WaveKernels.okl:215-216), so one lift of pflux per face
+// serves p and, scaled by -n_f, u,v,w; with Jq = 1 (affine tets,
+// cpp/src/WaveOKL3d.cpp:463) the velocity rows of the WADG update are
+// Pq*Vq = I and are skipped.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "bbwadg.h"
+#include "device_common.cuh"
+#include "fused.h"
+
+namespace bbw {
+
+constexpr int TILE_E = 32;
+constexpr int ES = kFusedRowStride;  // shared-memory row stride (floats), TILE_E + 1
+static_assert(ES == TILE_E + 1, "row stride");
+
+__host__ __device__ constexpr int round4(int x) { return (x + 3) & ~3; }
+__host__ __device__ constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }
+
+// warps per CTA: 8 or 16 (run-time choice, see fused_prepare / bbw_autotune)
+__host__ __device__ constexpr int fused_default_warps_c(int N) { return N <= 3 ? 8 : 16; }
+
+template <int N, int W_>
+struct FusedCfg {
+  static constexpr int Np = NP(N), Nfp = NFP(N), NF = 4 * NFP(N);
+  static constexpr int W = W_;  // warps per CTA
+  static constexpr int T = 32 * W;
+  static constexpr int R = cdiv(Np, W);     // node rows per warp
+  static constexpr int PR = round4(R);
+  static constexpr int P3R = round4(3 * R);
+};
+
+// ------------------------------------------------------------------ layouts
+// Operators, packed per warp so that warp w reads one contiguous, 16-byte
+// aligned block per reduction index:
+//   vol  [W][Np(m)][P3R]  (Dr, Ds, Dt)[r0+i][m] at 3i + {0,1,2}
+//   lift [W][NF(m)][PR]   LIFT[r0+i][m]
+//   pq   [W][Nq(q)][PR]   Pq[r0+i][q]
+//   vq   [W][Np(n)][PRQ]  Vq[q0+i][n]
+// plus, for BB, the sparse tables.  Built on the host (fused_host.cu).
+struct FusedParams {
+  int K, Nq, RQ, PRQ, bc, npat;
+  int pat_off, bb_off;              // int offsets of the tables (multiples of 4)
+  float fa, fb, fdt;
+  const float *__restrict__ Qin;
+  float *__restrict__ Qout;
+  float *__restrict__ res;
+  const float *__restrict__ vgeo;   // [K][9]
+  const float *__restrict__ fgeo;   // [K][16]
+  const int *__restrict__ nbr;      // [K][4]  (k2 << 8) | pattern, pattern 255 = boundary
+  const float *__restrict__ c2q;    // [K][Nq] c2/J at the cubature points
+  const float *__restrict__ ops;    // packed operators (global copy)
+  int off_lift, off_pq, off_vq, off_end;  // operator offsets in ops (floats)
+  const int *__restrict__ tables;   // Fmask [NF] | patterns [npat][Nfp] | BB tables
+  int table_ints;
+  // batched shots: state arrays hold S consecutive [K][4][Np] blocks
+  int S;
+  // sources: entries [src_off[s], src_off[s+1]) of shot s add
+  // ricker(t) * src_vec[j][:] to the projected rhs_p of element src_elem[j],
+  // t = *time + cstage * fdt
+  const int *__restrict__ src_off;
+  const int *__restrict__ src_elem;
+  const float *__restrict__ src_vec;
+  float f0, tR, samp, cstage;
+  const double *__restrict__ time;  // simulation time at the start of the step
+};
+
+// Ricker wavelet amp (1 - 2 a^2) exp(-a^2), a = pi f0 (t - tR)
+__device__ __forceinline__ float ricker(float t, float f0, float tR, float amp) {
+  const float a = 3.14159265358979f * f0 * (t - tR);
+  return amp * (1.f - 2.f * a * a) * expf(-a * a);
+}
+
+// Shared-memory map (floats, rows of stride ES).  Input tiles are double
+// buffered when they fit (PIPE): the next tile's copies are in flight while
+// the current one is computed.
+template <int N, bool BB>
+struct FusedSmem {
+  using C = FusedCfg<N, 8>;  // row counts only; independent of the warp count
+  static constexpr int inQ = 0;                               // [4Np][ES] state tile
+  static constexpr int inGeo = 4 * C::Np * ES;                // [E][25]  vgeo + fgeo
+  static constexpr int inNbr = inGeo + TILE_E * 25;           // [E][4]   neighbour codes
+  static constexpr int inC2 = inNbr + TILE_E * 4;             // [Nq][ES] c2 (runtime Nq)
+  __host__ __device__ static int in_size(int Nq) { return inC2 + round4(Nq * ES); }
+  static constexpr int sR = 0;                                // [4Np][ES] rhs / U scratch
+  static constexpr int sF = sR + 4 * C::Np * ES;              // [NF][ES]  pflux
+  static constexpr int sF2 = sF + C::NF * ES;                 // [NF][ES]  BB: L0 * pflux
+  static constexpr int sQuad = sF2 + (BB ? C::NF * ES : 0);   // [Nq][ES]  c2 * p at the cubature
+  __host__ __device__ static int work_size(int Nq) { return sQuad + round4(Nq * ES); }
+};
+
+// -------------------------------------------------------------- device code
+__device__ __forceinline__ void cp_async4(void *smem_dst, const void *gmem_src, bool valid) {
+  // 4-byte asynchronous copy; zero-fills the destination when !valid
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(gmem_src),
+               "r"(valid ? 4 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// OPS_SMEM: the packed operators are staged in shared memory (every
+// operator read is a shared-memory broadcast); otherwise they are read
+// through the read-only data path (large N or large cubature rules).
+// PIPE: two input-tile buffers (software pipelining across tiles).
+template <int N, bool BB, bool OPS_SMEM, bool PIPE, int W_>
+__global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedParams P) {
+  using C = FusedCfg<N, W_>;
+  using L = FusedSmem<N, BB>;
+  constexpr int Np = C::Np, Nfp = C::Nfp, NF = C::NF, W = C::W, T = C::T, R = C::R;
+  constexpr int FIT = cdiv(TILE_E * NF, T);        // flux items per thread
+  constexpr int QIT = cdiv(TILE_E * 4 * Np, T);    // state-tile floats per thread
+  extern __shared__ __align__(16) float sm[];
+  const int Nq = P.Nq, RQ = P.RQ, PRQ = P.PRQ;
+  const int inSize = L::in_size(Nq);
+  float *sIn = sm;                                   // [PIPE ? 2 : 1][inSize]
+  float *sW = sm + (PIPE ? 2 : 1) * inSize;          // work arrays
+  float *sR = sW + L::sR, *sF = sW + L::sF, *sF2 = sW + L::sF2, *sQuad = sW + L::sQuad;
+  int *sTab = (int *)(sW + L::work_size(Nq));
+  float *sOps = (float *)(sTab + P.table_ints);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int r0 = warp * R;
+
+  // stage operators (when they fit) and tables once per CTA
+  if (OPS_SMEM)
+    for (int i = tid; i < P.off_end / 4; i += T)
+      reinterpret_cast<float4 *>(sOps)[i] = __ldg(reinterpret_cast<const float4 *>(P.ops) + i);
+  for (int i = tid; i < P.table_ints; i += T) sTab[i] = __ldg(P.tables + i);
+  const int *sFmask = sTab;
+  const int *sPat = sTab + P.pat_off;
+
+  const float *opBase = OPS_SMEM ? (const float *)sOps : P.ops;
+  const float *wVol = opBase + warp * Np * C::P3R;              // [W][Np][P3R]
+  const float *wLift = opBase + P.off_lift + warp * NF * C::PR;  // [W][NF][PR]
+  const float *wPq = opBase + P.off_pq + warp * Nq * C::PR;      // [W][Nq][PR]
+  const float *wVq = opBase + P.off_vq + warp * Np * PRQ;        // [W][Np][PRQ]
+  // BB tables: D ids int4 [4][Np], Dvals float4 [Np], then the lift tables
+  const int *bbTab = sTab + P.bb_off;
+
+  // asynchronous copies of one tile's inputs into buffer `buf`
+  const int ntiles = cdiv(P.K, TILE_E);
+  const size_t sstride = (size_t)P.K * 4 * Np;  // floats per shot
+  auto issue_tile = [&](int vt, float *buf) {
+    const int shot = vt / ntiles, tile = vt - shot * ntiles;
+    const int k0 = tile * TILE_E, ne = min(TILE_E, P.K - k0);
+    float *bQ = buf + L::inQ, *bGeo = buf + L::inGeo, *bC2 = buf + L::inC2;
+    int *bNbr = (int *)(buf + L::inNbr);
+    for (int i = tid; i < TILE_E * 9; i += T)
+      cp_async4(&bGeo[(i / 9) * 25 + i % 9], P.vgeo + (size_t)k0 * 9 + (i < ne * 9 ? i : 0), i < ne * 9);
+    for (int i = tid; i < TILE_E * 16; i += T)
+      cp_async4(&bGeo[(i / 16) * 25 + 9 + i % 16], P.fgeo + (size_t)k0 * 16 + (i < ne * 16 ? i : 0),
+                i < ne * 16);
+    for (int i = tid; i < TILE_E * 4; i += T)  // zero codes of absent elements: element 0, never used
+      cp_async4(&bNbr[i], P.nbr + (size_t)k0 * 4 + (i < ne * 4 ? i : 0), i < ne * 4);
+    const float *Qg = P.Qin + shot * sstride + (size_t)k0 * 4 * Np;
+#pragma unroll 4
+    for (int j = 0; j < QIT; ++j) {
+      const int i = tid + j * T;
+      if (i < TILE_E * 4 * Np) {
+        const int e = i / (4 * Np), fn = i - e * (4 * Np);
+        const bool ok = e < ne;
+        cp_async4(&bQ[fn * ES + e], ok ? Qg + i : P.Qin, ok);
+      }
+    }
+    const float *cg = P.c2q + (size_t)k0 * Nq;
+    for (int i = tid; i < TILE_E * Nq; i += T) {
+      const int e = i / Nq, q = i - e * Nq;
+      const bool ok = e < ne;
+      cp_async4(&bC2[q * ES + e], ok ? cg + i : P.c2q, ok);
+    }
+    cp_async_commit();
+  };
+  // neighbour face traces of the tile in `buf` into registers
+  auto load_traces = [&](const float *buf, int vt, float (&nb)[FIT][4]) {
+    const int shot = vt / ntiles, tile_of_buf = vt - shot * ntiles;
+    const int ne_b = min(TILE_E, P.K - tile_of_buf * TILE_E);
+    const int *bNbr = (const int *)(buf + L::inNbr);
+#pragma unroll
+    for (int j = 0; j < FIT; ++j) {
+      const int i = tid + j * T;
+      nb[j][0] = nb[j][1] = nb[j][2] = nb[j][3] = 0.f;
+      if (i < TILE_E * NF && (i & 31) < ne_b) {  // absent elements have no codes
+        const int e = i & 31, m = i >> 5, f = m / Nfp;
+        const int code = bNbr[e * 4 + f];
+        const int pat = code & 255;
+        const unsigned rel = (unsigned)((code >> 8) - tile_of_buf * TILE_E);
+        if (pat != 255 && rel >= (unsigned)ne_b) {  // neighbours inside the tile: from smem
+          const float *q2 = P.Qin + shot * sstride + (size_t)(code >> 8) * 4 * Np +
+                            sPat[pat * Nfp + (m - f * Nfp)];
+          nb[j][0] = __ldg(q2);
+          nb[j][1] = __ldg(q2 + Np);
+          nb[j][2] = __ldg(q2 + 2 * Np);
+          nb[j][3] = __ldg(q2 + 3 * Np);
+        }
+      }
+    }
+  };
+
+  const int nvt = P.S * ntiles;  // (shot, tile) work items
+  int vt = blockIdx.x, b = 0;
+  float nb[FIT][4];
+  __syncthreads();  // tables staged
+  if (vt < nvt) {
+    issue_tile(vt, sIn);
+    cp_async_wait_all();
+    __syncthreads();
+    load_traces(sIn, vt, nb);
+  }
+  for (; vt < nvt; vt += gridDim.x) {
+    const int shot = vt / ntiles, tile = vt - shot * ntiles;
+    const int k0 = tile * TILE_E;
+    const int ne = min(TILE_E, P.K - k0);
+    const int next = vt + gridDim.x;
+    const size_t sbase = shot * sstride;
+    float *cur = sIn + b * inSize;
+    const float *sQ = cur + L::inQ, *sGeo = cur + L::inGeo, *sC2 = cur + L::inC2;
+    const int *sNbr = (const int *)(cur + L::inNbr);
+    if (PIPE && next < nvt) issue_tile(next, sIn + (b ^ 1) * inSize);
+
+    // ---- 1. upwind flux at the 4Nfp face nodes (Uflux = -pflux); traces of
+    //         neighbours inside the tile come from the state tile itself
+#pragma unroll
+    for (int j = 0; j < FIT; ++j) {
+      const int i = tid + j * T;
+      if (i >= TILE_E * NF) continue;
+      const int e = i & 31, m = i >> 5, f = m / Nfp;
+      const int code = sNbr[e * 4 + f];
+      const int pat = code & 255;
+      const unsigned rel = (unsigned)((code >> 8) - k0);
+      if (pat != 255 && rel < (unsigned)ne) {
+        const int vP = sPat[pat * Nfp + (m - f * Nfp)];
+        nb[j][0] = sQ[vP * ES + rel];
+        nb[j][1] = sQ[(Np + vP) * ES + rel];
+        nb[j][2] = sQ[(2 * Np + vP) * ES + rel];
+        nb[j][3] = sQ[(3 * Np + vP) * ES + rel];
+      }
+      const int vM = sFmask[m];
+      const float pM = sQ[vM * ES + e], uM = sQ[(Np + vM) * ES + e],
+                  vvM = sQ[(2 * Np + vM) * ES + e], wM = sQ[(3 * Np + vM) * ES + e];
+      const float *fg = sGeo + e * 25 + 9 + 4 * f;
+      const float Fscale = fg[0], nx = fg[1], ny = fg[2], nz = fg[3];
+      float pjump, Unjump;
+      if (pat == 255) {
+        if (P.bc == BBW_BC_PRESSURE_RELEASE) {
+          pjump = -2.f * pM;
+          Unjump = 0.f;
+        } else {
+          pjump = 0.f;
+          Unjump = -2.f * (uM * nx + vvM * ny + wM * nz);
+        }
+      } else {
+        pjump = nb[j][0] - pM;
+        Unjump = (nb[j][1] - uM) * nx + (nb[j][2] - vvM) * ny + (nb[j][3] - wM) * nz;
+      }
+      sF[m * ES + e] = .5f * (pjump - Unjump) * Fscale;
+    }
+
+    // ---- 2. contravariant velocities Ur, Us, Ut into sR rows [Np, 4Np)
+    for (int i = tid; i < TILE_E * Np; i += T) {
+      const int e = i & 31, n = i >> 5;
+      const float *G = sGeo + e * 25;
+      const float u = sQ[(Np + n) * ES + e], v = sQ[(2 * Np + n) * ES + e],
+                  w = sQ[(3 * Np + n) * ES + e];
+      sR[(Np + n) * ES + e] = u * G[0] + v * G[1] + w * G[2];
+      sR[(2 * Np + n) * ES + e] = u * G[3] + v * G[4] + w * G[5];
+      sR[(3 * Np + n) * ES + e] = u * G[6] + v * G[7] + w * G[8];
+    }
+    __syncthreads();
+
+    // ---- 3. volume term (registers: rows r0..r0+R of this warp, lane = element)
+    float rp[R], ru[R], rv[R], rw[R];
+    {
+      const float *G = sGeo + lane * 25;
+      if constexpr (!BB) {
+        float dr[R], ds[R], dt[R], dv[R];
+#pragma unroll
+        for (int i = 0; i < R; ++i) dr[i] = ds[i] = dt[i] = dv[i] = 0.f;
+#pragma unroll 2
+        for (int m = 0; m < Np; ++m) {
+          const float pm = sQ[m * ES + lane];
+          const float ur = sR[(Np + m) * ES + lane], us = sR[(2 * Np + m) * ES + lane],
+                      ut = sR[(3 * Np + m) * ES + lane];
+          const float4 *op = reinterpret_cast<const float4 *>(wVol + m * C::P3R);
+          float o[C::P3R];
+#pragma unroll
+          for (int j = 0; j < C::P3R / 4; ++j) {
+            const float4 t4 = op[j];
+            o[4 * j] = t4.x, o[4 * j + 1] = t4.y, o[4 * j + 2] = t4.z, o[4 * j + 3] = t4.w;
+          }
+#pragma unroll
+          for (int i = 0; i < R; ++i) {
+            dr[i] += o[3 * i] * pm;
+            ds[i] += o[3 * i + 1] * pm;
+            dt[i] += o[3 * i + 2] * pm;
+            dv[i] += o[3 * i] * ur;
+            dv[i] += o[3 * i + 1] * us;
+            dv[i] += o[3 * i + 2] * ut;
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+          rp[i] = -dv[i];
+          ru[i] = -(G[0] * dr[i] + G[3] * ds[i] + G[6] * dt[i]);
+          rv[i] = -(G[1] * dr[i] + G[4] * ds[i] + G[7] * dt[i]);
+          rw[i] = -(G[2] * dr[i] + G[5] * ds[i] + G[8] * dt[i]);
+        }
+      } else {
+        // sparse Bernstein derivative, cpp/okl/WaveKernels.okl:428-467
+        const int4 *Dids = reinterpret_cast<const int4 *>(bbTab);          // [4][Np]
+        const float4 *Dv = reinterpret_cast<const float4 *>(bbTab + 16 * Np);  // [Np]
+        const float *p = sQ + lane, *ur = sR + Np * ES + lane, *us = sR + 2 * Np * ES + lane,
+                    *ut = sR + 3 * Np * ES + lane;
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+          const int n = r0 + i;
+          rp[i] = ru[i] = rv[i] = rw[i] = 0.f;
+          if (n >= Np) continue;
+          const float4 dv = Dv[n];
+          const int4 a = Dids[n], bq = Dids[Np + n], c = Dids[2 * Np + n], d = Dids[3 * Np + n];
+          const float p1 = dv.x * p[a.x * ES] + dv.y * p[bq.x * ES] + dv.z * p[c.x * ES] +
+                           dv.w * p[d.x * ES];
+          const float p2 = dv.x * p[a.y * ES] + dv.y * p[bq.y * ES] + dv.z * p[c.y * ES] +
+                           dv.w * p[d.y * ES];
+          const float p3 = dv.x * p[a.z * ES] + dv.y * p[bq.z * ES] + dv.z * p[c.z * ES] +
+                           dv.w * p[d.z * ES];
+          const float p4 = dv.x * p[a.w * ES] + dv.y * p[bq.w * ES] + dv.z * p[c.w * ES] +
+                           dv.w * p[d.w * ES];
+          float dU1 = dv.x * (ur[a.y * ES] + us[a.z * ES] + ut[a.w * ES]);
+          dU1 += dv.y * (ur[bq.y * ES] + us[bq.z * ES] + ut[bq.w * ES]);
+          dU1 += dv.z * (ur[c.y * ES] + us[c.z * ES] + ut[c.w * ES]);
+          dU1 += dv.w * (ur[d.y * ES] + us[d.z * ES] + ut[d.w * ES]);
+          float dU2 = dv.x * (ur[a.x * ES] + us[a.x * ES] + ut[a.x * ES]);
+          dU2 += dv.y * (ur[bq.x * ES] + us[bq.x * ES] + ut[bq.x * ES]);
+          dU2 += dv.z * (ur[c.x * ES] + us[c.x * ES] + ut[c.x * ES]);
+          dU2 += dv.w * (ur[d.x * ES] + us[d.x * ES] + ut[d.x * ES]);
+          const float dpdr = .5f * (p2 - p1), dpds = .5f * (p3 - p1), dpdt = .5f * (p4 - p1);
+          rp[i] = -.5f * (dU1 - dU2);
+          ru[i] = -(G[0] * dpdr + G[3] * dpds + G[6] * dpdt);
+          rv[i] = -(G[1] * dpdr + G[4] * dpds + G[7] * dpdt);
+          rw[i] = -(G[2] * dpdr + G[5] * dpds + G[8] * dpdt);
+        }
+      }
+    }
+
+    // ---- 4. lift of the face fluxes
+    {
+      const float *fgl = sGeo + lane * 25 + 9;
+      if constexpr (!BB) {
+#pragma unroll 1
+        for (int f = 0; f < 4; ++f) {
+          float acc[R];
+#pragma unroll
+          for (int i = 0; i < R; ++i) acc[i] = 0.f;
+#pragma unroll 3
+          for (int j = 0; j < Nfp; ++j) {
+            const int m = f * Nfp + j;
+            const float pf = sF[m * ES + lane];
+            const float4 *op = reinterpret_cast<const float4 *>(wLift + m * C::PR);
+            float o[C::PR];
+#pragma unroll
+            for (int q = 0; q < C::PR / 4; ++q) {
+              const float4 t4 = op[q];
+              o[4 * q] = t4.x, o[4 * q + 1] = t4.y, o[4 * q + 2] = t4.z, o[4 * q + 3] = t4.w;
+            }
+#pragma unroll
+            for (int i = 0; i < R; ++i) acc[i] += o[i] * pf;
+          }
+          const float nx = fgl[4 * f + 1], ny = fgl[4 * f + 2], nz = fgl[4 * f + 3];
+#pragma unroll
+          for (int i = 0; i < R; ++i) {
+            rp[i] += acc[i];
+            ru[i] -= nx * acc[i];
+            rv[i] -= ny * acc[i];
+            rw[i] -= nz * acc[i];
+          }
+        }
+      } else {
+        // BB lift: per face L0 (Nfp x Nfp sparse), then the degree elevation
+        // EEL face by face (cpp/okl/WaveKernels.okl:576-644).  Tables: header
+        // {L0nnz, EEL nnz}, L0 (offset, value) pairs [Nfp][L0nnz], EEL row
+        // pointers [Np][5], EEL (offset, value) pairs; offsets are
+        // pre-multiplied by the row stride.
+        __syncthreads();  // pflux complete (written in step 1 by other warps)
+        const int L0nnz = bbTab[20 * Np];
+        const int2 *L0p = reinterpret_cast<const int2 *>(bbTab + 20 * Np + 4);
+        const int *eelPtr = bbTab + 20 * Np + 4 + 2 * Nfp * L0nnz;
+        const int2 *eelP = reinterpret_cast<const int2 *>(eelPtr + ((5 * Np + 1) & ~1));
+        for (int m = warp; m < NF; m += W) {
+          const int f = m / Nfp, nt = m - f * Nfp;
+          const float *src = sF + f * Nfp * ES + lane;
+          const int2 *row = L0p + nt * L0nnz;
+          float v0 = 0.f, v1 = 0.f;
+          int j = 0;
+          for (; j + 1 < L0nnz; j += 2) {
+            const int2 t0 = row[j], t1 = row[j + 1];
+            v0 += __int_as_float(t0.y) * src[t0.x];
+            v1 += __int_as_float(t1.y) * src[t1.x];
+          }
+          if (j < L0nnz) v0 += __int_as_float(row[j].y) * src[row[j].x];
+          sF2[m * ES + lane] = v0 + v1;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+          const int n = r0 + i;
+          if (n >= Np) continue;
+          const int *ptr = eelPtr + 5 * n;
+#pragma unroll 1
+          for (int f = 0; f < 4; ++f) {
+            float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+            int j = ptr[f];
+            const int end = ptr[f + 1];
+            for (; j + 3 < end; j += 4) {
+              const int2 t0 = eelP[j], t1 = eelP[j + 1], t2 = eelP[j + 2], t3 = eelP[j + 3];
+              a0 += __int_as_float(t0.y) * sF2[t0.x + lane];
+              a1 += __int_as_float(t1.y) * sF2[t1.x + lane];
+              a2 += __int_as_float(t2.y) * sF2[t2.x + lane];
+              a3 += __int_as_float(t3.y) * sF2[t3.x + lane];
+            }
+            for (; j < end; ++j) a0 += __int_as_float(eelP[j].y) * sF2[eelP[j].x + lane];
+            const float acc = (a0 + a1) + (a2 + a3);
+            rp[i] += acc;
+            ru[i] -= fgl[4 * f + 1] * acc;
+            rv[i] -= fgl[4 * f + 2] * acc;
+            rw[i] -= fgl[4 * f + 3] * acc;
+          }
+        }
+      }
+    }
+    __syncthreads();  // all warps done reading Ur/Us/Ut from sR
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int n = r0 + i;
+      if (n < Np) {
+        sR[n * ES + lane] = rp[i];
+        sR[(Np + n) * ES + lane] = ru[i];
+        sR[(2 * Np + n) * ES + lane] = rv[i];
+        sR[(3 * Np + n) * ES + lane] = rw[i];
+      }
+    }
+    if (PIPE) cp_async_wait_all();  // the next tile's inputs have landed
+    __syncthreads();
+    if (PIPE && next < nvt) load_traces(sIn + (b ^ 1) * inSize, next, nb);  // in flight from here
+
+    // ---- 5. WADG: p at the cubature points, times c2/J
+    {
+      const int q0 = warp * RQ;
+      for (int qb = 0; qb < RQ; qb += 4) {
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+#pragma unroll 4
+        for (int n = 0; n < Np; ++n) {
+          const float x = sR[n * ES + lane];
+          const float4 v = *reinterpret_cast<const float4 *>(wVq + n * PRQ + qb);
+          a0 += v.x * x;
+          a1 += v.y * x;
+          a2 += v.z * x;
+          a3 += v.w * x;
+        }
+        const float av[4] = {a0, a1, a2, a3};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int q = q0 + qb + j;
+          if (qb + j < RQ && q < Nq) sQuad[q * ES + lane] = av[j] * sC2[q * ES + lane];
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---- 6. project back: rhs_p = Pq * (c2 p_q); the residual tile is
+    //         fetched meanwhile for the stage update (scalar, coalesced)
+    constexpr int UIT = cdiv(TILE_E * 4 * Np, T);
+    const float *resg = P.res + sbase + (size_t)k0 * 4 * Np;
+    float rpre[UIT];
+#pragma unroll
+    for (int j = 0; j < UIT; ++j) {
+      const int i = tid + j * T;
+      rpre[j] = i < ne * 4 * Np ? resg[i] : 0.f;
+    }
+    {
+      float acc[R];
+#pragma unroll
+      for (int i = 0; i < R; ++i) acc[i] = 0.f;
+#pragma unroll 2
+      for (int q = 0; q < Nq; ++q) {
+        const float x = sQuad[q * ES + lane];
+        const float4 *op = reinterpret_cast<const float4 *>(wPq + q * C::PR);
+        float o[C::PR];
+#pragma unroll
+        for (int j = 0; j < C::PR / 4; ++j) {
+          const float4 t4 = op[j];
+          o[4 * j] = t4.x, o[4 * j + 1] = t4.y, o[4 * j + 2] = t4.z, o[4 * j + 3] = t4.w;
+        }
+#pragma unroll
+        for (int i = 0; i < R; ++i) acc[i] += o[i] * x;
+      }
+      // source term of this shot, added to the projected rhs_p as
+      // rk_update_elas does (acous_elas_cpp/okl/ElasKernelsWADG.okl:400-403)
+      if (P.src_off) {
+        // entries of a shot are sorted by element: find the first one of
+        // this tile by bisection, then walk the tile's entries
+        int j0 = __ldg(P.src_off + shot), j1 = __ldg(P.src_off + shot + 1);
+        if (j1 > j0) {
+          int lo = j0, hi = j1;
+          while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (__ldg(P.src_elem + mid) < k0) lo = mid + 1;
+            else hi = mid;
+          }
+          if (lo < j1 && __ldg(P.src_elem + lo) < k0 + ne) {
+            const float amp = ricker((float)(*P.time) + P.cstage * P.fdt, P.f0, P.tR, P.samp);
+            for (int j = lo; j < j1; ++j) {
+              const int rel = __ldg(P.src_elem + j) - k0;
+              if (rel >= ne) break;
+              if (lane == rel) {
+#pragma unroll
+                for (int i = 0; i < R; ++i)
+                  if (r0 + i < Np) acc[i] += amp * __ldg(P.src_vec + (size_t)j * Np + r0 + i);
+              }
+            }
+          }
+        }
+      }
+      __syncthreads();  // everyone has read sR rows [0, Np) in step 5
+#pragma unroll
+      for (int i = 0; i < R; ++i)
+        if (r0 + i < Np) sR[(r0 + i) * ES + lane] = acc[i];
+    }
+    __syncthreads();
+
+    // ---- 7. LSRK stage update, coalesced and conflict-free:
+    //         res = fa res + fdt rhs; Q += fb res
+    {
+      float *resw = P.res + sbase + (size_t)k0 * 4 * Np;
+      float *qg = P.Qout + sbase + (size_t)k0 * 4 * Np;
+#pragma unroll
+      for (int j = 0; j < UIT; ++j) {
+        const int i = tid + j * T;
+        if (i >= ne * 4 * Np) continue;
+        const int e = i / (4 * Np), fn = i - e * (4 * Np);
+        const float r = P.fa * rpre[j] + P.fdt * sR[fn * ES + e];
+        resw[i] = r;
+        qg[i] = sQ[fn * ES + e] + P.fb * r;
+      }
+    }
+    __syncthreads();  // tile buffers and work arrays free for reuse
+    if (!PIPE && next < nvt) {
+      issue_tile(next, sIn);
+      cp_async_wait_all();
+      __syncthreads();
+      load_traces(sIn, next, nb);
+    }
+    b ^= PIPE ? 1 : 0;
+  }
+}
+
+// --------------------------------------------------------------- host side
+template <int N, bool BB>
+static size_t smem_bytes(int Nq, bool pipe, bool ops_smem, int ops_floats, int table_ints) {
+  using L = FusedSmem<N, BB>;
+  return sizeof(float) * ((size_t)(pipe ? 2 : 1) * L::in_size(Nq) + L::work_size(Nq) +
+                          (ops_smem ? ops_floats : 0)) +
+         sizeof(int) * (size_t)table_ints;
+}
+
+template <int N, bool BB>
+static bbw_status launch_fused(const FusedPlan &pl, const float *Qin, float *Qout, float *res,
+                               float fa, float fb, float fdt, float cstage, cudaStream_t st) {
+  FusedParams P;
+  P.K = pl.K, P.Nq = pl.Nq, P.RQ = pl.RQ, P.PRQ = pl.PRQ, P.bc = pl.bc, P.npat = pl.npat;
+  P.pat_off = pl.pat_off, P.bb_off = pl.bb_off;
+  P.fa = fa, P.fb = fb, P.fdt = fdt;
+  P.Qin = Qin, P.Qout = Qout, P.res = res;
+  P.vgeo = pl.vgeo, P.fgeo = pl.fgeo, P.nbr = pl.nbr, P.c2q = pl.c2q;
+  P.ops = pl.ops;
+  P.off_lift = pl.off_lift, P.off_pq = pl.off_pq, P.off_vq = pl.off_vq, P.off_end = pl.ops_floats;
+  P.tables = pl.tables, P.table_ints = pl.table_ints;
+  P.S = pl.S;
+  P.src_off = pl.src_off, P.src_elem = pl.src_elem, P.src_vec = pl.src_vec;
+  P.f0 = pl.f0, P.tR = pl.tR, P.samp = pl.samp, P.cstage = cstage;
+  P.time = pl.time;
+  const bool os = pl.ops_smem > 0;
+  const size_t sm = pl.smem;
+  const int grid = std::min(cdiv(pl.K, TILE_E) * std::max(pl.S, 1), pl.nsm);
+  if (pl.W == 8) {
+    constexpr int T = 256;
+    if (os && pl.pipe) k_fused_stage<N, BB, true, true, 8><<<grid, T, sm, st>>>(P);
+    else if (os) k_fused_stage<N, BB, true, false, 8><<<grid, T, sm, st>>>(P);
+    else if (pl.pipe) k_fused_stage<N, BB, false, true, 8><<<grid, T, sm, st>>>(P);
+    else k_fused_stage<N, BB, false, false, 8><<<grid, T, sm, st>>>(P);
+  } else {
+    constexpr int T = 512;
+    if (os && pl.pipe) k_fused_stage<N, BB, true, true, 16><<<grid, T, sm, st>>>(P);
+    else if (os) k_fused_stage<N, BB, true, false, 16><<<grid, T, sm, st>>>(P);
+    else if (pl.pipe) k_fused_stage<N, BB, false, true, 16><<<grid, T, sm, st>>>(P);
+    else k_fused_stage<N, BB, false, false, 16><<<grid, T, sm, st>>>(P);
+  }
+  return check_launch("fused stage");
+}
+
+template <int N, bool BB, int W>
+static cudaError_t set_smem_attr(bool os, bool pipe, int bytes) {
+  if (os && pipe)
+    return cudaFuncSetAttribute(k_fused_stage<N, BB, true, true, W>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (os)
+    return cudaFuncSetAttribute(k_fused_stage<N, BB, true, false, W>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (pipe)
+    return cudaFuncSetAttribute(k_fused_stage<N, BB, false, true, W>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  return cudaFuncSetAttribute(k_fused_stage<N, BB, false, false, W>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+template <int N, bool BB>
+static bbw_status prepare(FusedPlan &pl) {
+  int dev = 0, maxsm = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (pl.W != 8 && pl.W != 16) return set_error(BBW_ERR_ARG, "fused stage: warps must be 8 or 16");
+  // requested placement (want_ops / want_pipe >= 0) or the first that fits of:
+  // operators in shared memory, then double-buffered input tiles
+  const bool cand[4][2] = {{true, true}, {true, false}, {false, true}, {false, false}};
+  int pick = -1;
+  for (int c = 0; c < 4 && pick < 0; ++c) {
+    if (pl.want_ops >= 0 && cand[c][0] != (pl.want_ops > 0)) continue;
+    if (pl.want_pipe >= 0 && cand[c][1] != (pl.want_pipe > 0)) continue;
+    if (smem_bytes<N, BB>(pl.Nq, cand[c][1], cand[c][0], pl.ops_floats, pl.table_ints) <=
+        (size_t)maxsm)
+      pick = c;
+  }
+  if (pick < 0)
+    return set_error(BBW_ERR_UNSUPPORTED, "fused stage: element tile does not fit in shared memory");
+  pl.ops_smem = cand[pick][0] ? pl.ops_floats : 0;
+  pl.pipe = cand[pick][1];
+  pl.smem = smem_bytes<N, BB>(pl.Nq, pl.pipe, pl.ops_smem > 0, pl.ops_floats, pl.table_ints);
+  cudaError_t e = pl.W == 8 ? set_smem_attr<N, BB, 8>(pl.ops_smem > 0, pl.pipe, (int)pl.smem)
+                            : set_smem_attr<N, BB, 16>(pl.ops_smem > 0, pl.pipe, (int)pl.smem);
+  if (e != cudaSuccess) return set_cuda_error(e, "fused stage attribute");
+  pl.nsm = nsm > 0 ? nsm : 148;
+  pl.grid = std::min(cdiv(pl.K, TILE_E) * std::max(pl.S, 1), pl.nsm);
+  return BBW_OK;
+}
+
+}  // namespace bbw

@@ -137,6 +137,20 @@ class WaveSolver:
         """One fused stage with stage-time offset c (source time = clock + c fdt)."""
         _lib.call("bbw_stage_ex", self._h, float(rka), float(rkb), float(fdt), float(c))
 
+    def autotune(self, dt, stages=10):
+        """Pick the fastest fused-stage variant for this mesh and batch;
+        returns dict(warps, ops_in_smem, pipelined)."""
+        cfg = ctypes.c_int(0)
+        _lib.call("bbw_autotune", self._h, float(dt), int(stages), ctypes.byref(cfg))
+        v = cfg.value
+        return dict(warps=v & 255, ops_in_smem=bool(v >> 8 & 1), pipelined=bool(v >> 9 & 1),
+                    code=v)
+
+    def set_config(self, warps, ops_in_smem, pipelined):
+        """Pin a fused-stage variant (as returned by autotune)."""
+        _lib.call("bbw_set_config", self._h,
+                  int(warps) | (int(bool(ops_in_smem)) << 8) | (int(bool(pipelined)) << 9))
+
     # ---- batched shots, sources, receivers
     def set_shots(self, S):
         """S independent shots per launch (state [S][K][4][Np], zeroed)."""

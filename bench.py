@@ -229,6 +229,7 @@ def shots_workload(args, torch, dist, world):
         s.set_shots(nshot)
         s.set_sources(*shot_sources(prob, nshot, 99), f0=4.0, amplitude=1e4, stage_times=True)
         s.set_time(0.0)
+        tuned = s.autotune(prob.dt, 5)
         _, _, sp = s.device_state()
         stream = torch.cuda.ExternalStream(sp)
         s.steps(prob.dt, args.warmup)
@@ -249,6 +250,7 @@ def shots_workload(args, torch, dist, world):
         dofs = prob.K * prob.Np * 4 * 5 * args.shots_steps * nshot
         out[label] = {"value": world * dofs / (ms / 1e3), "unit": "DOF-stage/s",
                       "ms_per_step": ms / args.shots_steps, "steps": args.shots_steps,
+                      "autotuned": tuned,
                       "finite": bool(np.isfinite(s.get_data()).all())}
         s.close()
     return out
@@ -310,7 +312,7 @@ def adjoint_workload(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--variant", default="nodal", choices=["nodal", "bb", "nodal-f16x3"])
@@ -351,6 +353,7 @@ def main():
         K, Np, Nq = prob.K, prob.Np, prob.Nq
         s = WaveSolver(prob, precision=prec)
         s.set_data(prob.Q0)
+        tuned = s.autotune(prob.dt, 10) if prec == "fp32" else None
         qptr, rptr, stream_ptr = s.device_state()
         stream = torch.cuda.ExternalStream(stream_ptr)
         s.steps(prob.dt, args.warmup)
@@ -387,7 +390,7 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             t_e2e = float(t.item())
         state_bytes = K * 4 * Np * 4
-        results[variant] = dict(ms=ms, K=K, Np=Np, Nq=Nq, dofs=dofs, launches=launches,
+        results[variant] = dict(ms=ms, K=K, Np=Np, Nq=Nq, dofs=dofs, launches=launches, tuned=tuned,
                                 clocks=clk.summary(), e2e_s=t_e2e, state_bytes=state_bytes,
                                 finite=bool(np.isfinite(out.numpy()).all()))
         s.close()
@@ -417,7 +420,8 @@ def main():
         "value": value, "unit": "DOF-stage/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": head["ms"] / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": workload_config(args, args.variant),
+        "data": "synthetic", "config": dict(workload_config(args, args.variant),
+                                            autotuned=head["tuned"]),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "kernel": ("k_tc_stage<%d>" % N_ORDER) if args.variant.endswith("f16x3")

@@ -222,6 +222,19 @@ bbw_status bbw_steps(bbw_ctx *ctx, float dt, int nsteps);
  * the last step shortened to land on it (cpp/src/WaveOKL3d.cpp:2048). */
 bbw_status bbw_run(bbw_ctx *ctx, double final_time, float dt);
 
+/* Times every variant of the FP32 fused stage on this context's mesh, shots
+ * and state (8 or 16 warps per CTA, i.e. rows per warp ceil(Np/W);
+ * operators in shared or global memory; single or double-buffered input
+ * tiles), `stages` launches each on scratch copies of the state, and keeps
+ * the fastest.  *config (may be NULL) = W | ops_in_smem << 8 | pipelined << 9.
+ * The state is not modified.  No-op for the tensor-core stage.  The
+ * reference's counterpart is its hand-swept KblkV/KblkS/KblkU block sizes
+ * (cpp/src/WaveOKL3d.cpp:1618-1650, cpp/profileKernels). */
+bbw_status bbw_autotune(bbw_ctx *ctx, float dt, int stages, int *config);
+/* Applies a configuration code as returned by bbw_autotune (for instance one
+ * cached from an earlier run); BBW_ERR_UNSUPPORTED if it does not fit. */
+bbw_status bbw_set_config(bbw_ctx *ctx, int config);
+
 /* ---- batched shots, sources, receivers (FP32 stage)
  * S independent shots share mesh, medium and operators; the state, residual
  * and traces hold S consecutive blocks and every stage launch advances all

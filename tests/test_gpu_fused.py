@@ -113,3 +113,39 @@ def test_nodal_and_bb_agree(cuda):
     sn.steps(pn.dt, 5)
     sb.steps(pb.dt, 5)
     assert rel_l2(pb.to_nodal(sb.get_data()), sn.get_data()) < 1e-4
+
+
+@pytest.mark.parametrize("N", [3, 5])
+@pytest.mark.parametrize("variant", ["nodal", "bb"])
+def test_every_stage_configuration_matches_oracle(cuda, N, variant):
+    """All warps-per-CTA / operator-placement / pipelining variants the
+    autotuner chooses from give the restatement's result; the autotuner
+    keeps one of them and leaves the state untouched."""
+    from oracle import Oracle
+    from bbwadg_b200._lib import BBWError
+    p = make_problem(N, 3, variant=variant, c2="sine", c2_jitter=0.5, seed=3)
+    q_ref, _ = Oracle(N, p.K, p.ops_dict(), p.geo_dict(), variant=variant).run(p.Q0.copy(), p.dt, 10)
+    ran = 0
+    for warps in (8, 16):
+        for ops in (True, False):
+            for pipe in (True, False):
+                s = WaveSolver(p)
+                try:
+                    s.set_config(warps, ops, pipe)
+                except BBWError:
+                    s.close()
+                    continue
+                s.set_data(p.Q0)
+                s.steps(p.dt, 2)
+                assert rel_l2(s.get_data(), q_ref) < TOL, (warps, ops, pipe)
+                s.close()
+                ran += 1
+    assert ran >= 4
+    s = WaveSolver(p)
+    s.set_data(p.Q0)
+    cfg = s.autotune(p.dt, 5)
+    assert cfg["warps"] in (8, 16)
+    assert np.array_equal(s.get_data(), p.Q0.astype(np.float32))
+    s.steps(p.dt, 2)
+    assert rel_l2(s.get_data(), q_ref) < TOL
+    s.close()
