@@ -151,6 +151,22 @@ bbw_status bbw_rk_surface_bern(int N, int K, int bc, const float *fgeo, const in
                                const int *L0_ids, const float *L0_vals, const float *cEL,
                                const float *Q, float *rhsQ, void *stream);
 
+/* One LSRK stage as the reference's three launches (rk_volume, rk_surface,
+ * rk_update_WADG; arguments as above) for callers that cannot allocate
+ * device memory: the rhs buffer is a 16 MiB scratch array inside the
+ * library (K * 4 * Np <= 4 Mi floats, else BBW_ERR_UNSUPPORTED).  No
+ * reference counterpart (the reference allocates rhsQ at setup).  Make the
+ * first call on each device outside stream capture (it looks the scratch
+ * address up); nothing in the scratch needs to start at zero; calls that
+ * overlap on the same device race on the one scratch; it makes no
+ * allocation. */
+bbw_status bbw_rk_stage_noalloc(int N, int K, int Nq, int bc, const float *vgeo, const float *Dr,
+                                const float *Ds, const float *Dt, const float *fgeo,
+                                const int *Fmask, const int *vmapP, const float *LIFT,
+                                const float *Vq, const float *Pq, const float *Jq,
+                                const float *c2q, float fa, float fb, float fdt, float *resQ,
+                                float *Q, void *stream);
+
 /* ---------------------------------------------------------- solver context
  * Owns device copies of the mesh arrays and operators, the state Q (double
  * buffered) and the LSRK residual res.  One stream per context; contexts
