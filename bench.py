@@ -203,13 +203,15 @@ def anomalies(base, seed, n=5, amp=0.3):
     return f
 
 
-def shot_sources(prob, S, seed, a=20.0):
-    """S seeded point-like sources in [-0.8, 0.8]^3: (shot, elem, vec) entries."""
+def shot_sources(prob, S, seed, a=20.0, first=0):
+    """Seeded point-like sources in [-0.8, 0.8]^3 for global shots
+    first..first+S-1 (local shots 0..S-1): (shot, elem, vec) entries."""
     from bbwadg_b200.problem import gaussian_source, source_entries
     rng = np.random.default_rng(seed)
+    centres = rng.uniform(-0.8, 0.8, (first + S, 3))[first:]
     xyz = prob.cubature_xyz()
-    ent = [source_entries(gaussian_source(prob, rng.uniform(-0.8, 0.8, 3), a=a, xyz=xyz), shot=i)
-           for i in range(S)]
+    ent = [source_entries(gaussian_source(prob, c, a=a, xyz=xyz), shot=i)
+           for i, c in enumerate(centres)]
     return [np.concatenate(x) for x in zip(*ent)]
 
 
@@ -256,13 +258,18 @@ def shots_workload(args, torch, dist, world):
     return out
 
 
-def adjoint_workload(args):
+def adjoint_workload(args, torch, dist, rank, world):
     """Forward + adjoint gradient: N=4, 16^3 x 6 tets (K=24576), 8 seeded
-    Ricker shots, 64 seeded receivers, 400 steps, checkpoints every 50, L2
-    trace misfit against a target with 5 seeded +-0.3 Gaussian anomalies."""
+    Ricker shots per GPU, 64 seeded receivers, 400 steps, checkpoints every
+    50, L2 trace misfit against a target with 5 seeded +-0.3 Gaussian
+    anomalies.  With several ranks the shots are sharded (8 per rank) and the
+    FP64 gradient is summed with one all-reduce, inside the timed region."""
     from bbwadg_b200 import WaveSolver, make_problem
     from bbwadg_b200.problem import c2_sine, receiver_weights
-    N, nh, S, R, steps, every = 4, 16, 8, 64, args.adj_steps, 50
+    from bbwadg_b200.shards import allreduce_gradient, shot_range
+    N, nh, R, steps, every = 4, 16, 64, args.adj_steps, 50
+    lo, hi = shot_range(8 * world, rank, world)
+    S = hi - lo
     cub, tri = reference_rule(N)
     base = c2_sine
     prob = make_problem(N, nh, c2=anomalies(base, 5), cubature=cub, tri_cubature=tri, cfl=0.25)
@@ -273,7 +280,7 @@ def adjoint_workload(args):
     el, w = receiver_weights(prob, rng.uniform(-0.8, 0.8, (R, 3)))
     s = WaveSolver(prob)
     s.set_shots(S)
-    s.set_sources(*shot_sources(prob, S, 8), f0=4.0, amplitude=1e4, stage_times=True)
+    s.set_sources(*shot_sources(prob, S, 8, first=lo), f0=4.0, amplitude=1e4, stage_times=True)
     s.set_receivers(el, w, steps)
     zero = np.zeros(s.state_size, np.float32)
 
@@ -299,12 +306,21 @@ def adjoint_workload(args):
     misfit = 0.5 * float(((tr - obs).astype(np.float64) ** 2).sum())
     t2 = time.perf_counter()
     grad = s.backward(tape, tr - obs)
+    if world > 1:
+        grad = allreduce_gradient(grad, device="cuda")
+        misfit = allreduce_gradient(np.array([misfit]), device="cuda")[0]
     t3 = time.perf_counter()
     tape.free()
     s.close()
-    return {"workload": "forward + adjoint c2 gradient, N=4, 16^3x6 tets (K=%d), %d shots, "
-                        "%d receivers, %d steps, checkpoints every %d" % (prob.K, S, R, steps, every),
-            "forward_s": t1 - t0, "backward_s": t3 - t2, "total_s": (t1 - t0) + (t3 - t2),
+    tf, tb = t1 - t0, t3 - t2
+    if world > 1:
+        t = torch.tensor([tf, tb], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tf, tb = float(t[0]), float(t[1])
+    return {"workload": "forward + adjoint c2 gradient, N=4, 16^3x6 tets (K=%d), %d shots per "
+                        "GPU, %d receivers, %d steps, checkpoints every %d" % (prob.K, S, R, steps,
+                                                                               every),
+            "forward_s": tf, "backward_s": tb, "total_s": tf + tb, "shots_total": 8 * world,
             "misfit": misfit, "grad_norm": float(np.linalg.norm(grad)),
             "grad_finite": bool(np.isfinite(grad).all())}
 
@@ -397,7 +413,7 @@ def main():
 
     extra = [x for x in args.extra.split(",") if x]
     shots = shots_workload(args, torch, dist, world) if "shots" in extra else None
-    adj = adjoint_workload(args) if "adjoint" in extra else None
+    adj = adjoint_workload(args, torch, dist, rank, world) if "adjoint" in extra else None
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
