@@ -91,7 +91,7 @@ void pack_fused_ops(int N, int Nq, int W, bool bb, const float *Dr, const float 
                     FusedOps &out) {
   const int Np = np_of(N), NF = 4 * nfp_of(N);
   const int R = cdivi(Np, W), PR = round4i(R), P3R = round4i(3 * R);
-  const int RQ = cdivi(Nq, W), PRQ = round4i(RQ);
+  const int RQ = cdivi(Nq, W), QB = fused_vq_block(W), PRQ = cdivi(RQ, QB) * QB;
   std::vector<float> &ops = out.ops;
   ops.clear();
   if (!bb) {

@@ -35,6 +35,8 @@ struct FusedPlan {
 };
 
 int fused_default_warps(int N);
+// cubature rows per accumulator block of the fused kernel's Vq product
+__host__ __device__ constexpr int fused_vq_block(int W) { return W == 8 ? 12 : 8; }
 
 // operators packed per warp for a W-warp fused kernel (capi.cu)
 struct FusedOps {

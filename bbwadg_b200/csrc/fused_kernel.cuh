@@ -156,8 +156,12 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
   float *sIn = sm;                                   // [PIPE ? 2 : 1][inSize]
   float *sW = sm + (PIPE ? 2 : 1) * inSize;          // work arrays
   float *sR = sW + L::sR, *sF = sW + L::sF, *sF2 = sW + L::sF2, *sQuad = sW + L::sQuad;
+  // tables staged in shared memory: all of them with the operators, else
+  // Fmask and the face permutations only (the BB tables are then read
+  // through the cache like the operators)
+  const int tabSmem = OPS_SMEM ? P.table_ints : P.bb_off;
   int *sTab = (int *)(sW + L::work_size(Nq));
-  float *sOps = (float *)(sTab + P.table_ints);
+  float *sOps = (float *)(sTab + tabSmem);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int r0 = warp * R;
 
@@ -165,7 +169,7 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
   if (OPS_SMEM)
     for (int i = tid; i < P.off_end / 4; i += T)
       reinterpret_cast<float4 *>(sOps)[i] = __ldg(reinterpret_cast<const float4 *>(P.ops) + i);
-  for (int i = tid; i < P.table_ints; i += T) sTab[i] = __ldg(P.tables + i);
+  for (int i = tid; i < tabSmem; i += T) sTab[i] = __ldg(P.tables + i);
   const int *sFmask = sTab;
   const int *sPat = sTab + P.pat_off;
 
@@ -175,16 +179,19 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
   const float *wPq = opBase + P.off_pq + warp * Nq * C::PR;      // [W][Nq][PR]
   const float *wVq = opBase + P.off_vq + warp * Np * PRQ;        // [W][Np][PRQ]
   // BB tables: D ids int4 [4][Np], Dvals float4 [Np], then the lift tables
-  const int *bbTab = sTab + P.bb_off;
+  const int *bbTab = OPS_SMEM ? sTab + P.bb_off : P.tables + P.bb_off;
 
   // asynchronous copies of one tile's inputs into buffer `buf`
   const int ntiles = cdiv(P.K, TILE_E);
   const size_t sstride = (size_t)P.K * 4 * Np;  // floats per shot
-  auto issue_tile = [&](int vt, float *buf) {
+  // parts of a tile's inputs: geometry + neighbour codes, state, c2
+  constexpr int IN_GEO = 1, IN_Q = 2, IN_C2 = 4, IN_ALL = 7;
+  auto issue_tile = [&](int vt, float *buf, int parts) {
     const int shot = vt / ntiles, tile = vt - shot * ntiles;
     const int k0 = tile * TILE_E, ne = min(TILE_E, P.K - k0);
     float *bQ = buf + L::inQ, *bGeo = buf + L::inGeo, *bC2 = buf + L::inC2;
     int *bNbr = (int *)(buf + L::inNbr);
+    if (parts & IN_GEO) {
     for (int i = tid; i < TILE_E * 9; i += T)
       cp_async4(&bGeo[(i / 9) * 25 + i % 9], P.vgeo + (size_t)k0 * 9 + (i < ne * 9 ? i : 0), i < ne * 9);
     for (int i = tid; i < TILE_E * 16; i += T)
@@ -192,6 +199,8 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
                 i < ne * 16);
     for (int i = tid; i < TILE_E * 4; i += T)  // zero codes of absent elements: element 0, never used
       cp_async4(&bNbr[i], P.nbr + (size_t)k0 * 4 + (i < ne * 4 ? i : 0), i < ne * 4);
+    }
+    if (parts & IN_Q) {
     const float *Qg = P.Qin + shot * sstride + (size_t)k0 * 4 * Np;
 #pragma unroll 4
     for (int j = 0; j < QIT; ++j) {
@@ -202,11 +211,14 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
         cp_async4(&bQ[fn * ES + e], ok ? Qg + i : P.Qin, ok);
       }
     }
+    }
+    if (parts & IN_C2) {
     const float *cg = P.c2q + (size_t)k0 * Nq;
     for (int i = tid; i < TILE_E * Nq; i += T) {
       const int e = i / Nq, q = i - e * Nq;
       const bool ok = e < ne;
       cp_async4(&bC2[q * ES + e], ok ? cg + i : P.c2q, ok);
+    }
     }
     cp_async_commit();
   };
@@ -241,7 +253,7 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
   float nb[FIT][4];
   __syncthreads();  // tables staged
   if (vt < nvt) {
-    issue_tile(vt, sIn);
+    issue_tile(vt, sIn, IN_ALL);
     cp_async_wait_all();
     __syncthreads();
     load_traces(sIn, vt, nb);
@@ -255,7 +267,11 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
     float *cur = sIn + b * inSize;
     const float *sQ = cur + L::inQ, *sGeo = cur + L::inGeo, *sC2 = cur + L::inC2;
     const int *sNbr = (const int *)(cur + L::inNbr);
-    if (PIPE && next < nvt) issue_tile(next, sIn + (b ^ 1) * inSize);
+    // inputs of the next tile: with two buffers all at once; with one
+    // buffer each part as soon as this tile is done with it (geometry and
+    // state after the lift, c2 after the cubature step), the update then
+    // reading the old state from global memory
+    if (PIPE && next < nvt) issue_tile(next, sIn + (b ^ 1) * inSize, IN_ALL);
 
     // ---- 1. upwind flux at the 4Nfp face nodes (Uflux = -pflux); traces of
     //         neighbours inside the tile come from the state tile itself
@@ -478,33 +494,43 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
         sR[(3 * Np + n) * ES + lane] = rw[i];
       }
     }
+    if (!PIPE && next < nvt) issue_tile(next, sIn, IN_GEO | IN_Q);  // sQ, sGeo, sNbr are dead
     if (PIPE) cp_async_wait_all();  // the next tile's inputs have landed
     __syncthreads();
     if (PIPE && next < nvt) load_traces(sIn + (b ^ 1) * inSize, next, nb);  // in flight from here
 
     // ---- 5. WADG: p at the cubature points, times c2/J
     {
+      // blocks of QB cubature rows: QB independent accumulators per thread,
+      // one state value and QB/4 operator broadcasts per node
+      constexpr int QB = fused_vq_block(W_);
       const int q0 = warp * RQ;
-      for (int qb = 0; qb < RQ; qb += 4) {
-        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-#pragma unroll 4
+      for (int qb = 0; qb < RQ; qb += QB) {
+        float acc[QB];
+#pragma unroll
+        for (int j = 0; j < QB; ++j) acc[j] = 0.f;
+#pragma unroll 2
         for (int n = 0; n < Np; ++n) {
           const float x = sR[n * ES + lane];
-          const float4 v = *reinterpret_cast<const float4 *>(wVq + n * PRQ + qb);
-          a0 += v.x * x;
-          a1 += v.y * x;
-          a2 += v.z * x;
-          a3 += v.w * x;
-        }
-        const float av[4] = {a0, a1, a2, a3};
+          const float4 *v = reinterpret_cast<const float4 *>(wVq + n * PRQ + qb);
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+          for (int j = 0; j < QB / 4; ++j) {
+            const float4 t4 = v[j];
+            acc[4 * j] += t4.x * x;
+            acc[4 * j + 1] += t4.y * x;
+            acc[4 * j + 2] += t4.z * x;
+            acc[4 * j + 3] += t4.w * x;
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < QB; ++j) {
           const int q = q0 + qb + j;
-          if (qb + j < RQ && q < Nq) sQuad[q * ES + lane] = av[j] * sC2[q * ES + lane];
+          if (qb + j < RQ && q < Nq) sQuad[q * ES + lane] = acc[j] * sC2[q * ES + lane];
         }
       }
     }
     __syncthreads();
+    if (!PIPE && next < nvt) issue_tile(next, sIn, IN_C2);  // sC2 is dead
 
     // ---- 6. project back: rhs_p = Pq * (c2 p_q); the residual tile is
     //         fetched meanwhile for the stage update (scalar, coalesced)
@@ -572,6 +598,15 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
     {
       float *resw = P.res + sbase + (size_t)k0 * 4 * Np;
       float *qg = P.Qout + sbase + (size_t)k0 * 4 * Np;
+      const float *qin = P.Qin + sbase + (size_t)k0 * 4 * Np;
+      float qold[PIPE ? 1 : UIT];  // one buffer: the state tile is being refilled
+      if (!PIPE) {
+#pragma unroll
+        for (int j = 0; j < UIT; ++j) {
+          const int i = tid + j * T;
+          qold[PIPE ? 0 : j] = i < ne * 4 * Np ? __ldg(qin + i) : 0.f;
+        }
+      }
 #pragma unroll
       for (int j = 0; j < UIT; ++j) {
         const int i = tid + j * T;
@@ -579,12 +614,11 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
         const int e = i / (4 * Np), fn = i - e * (4 * Np);
         const float r = P.fa * rpre[j] + P.fdt * sR[fn * ES + e];
         resw[i] = r;
-        qg[i] = sQ[fn * ES + e] + P.fb * r;
+        qg[i] = (PIPE ? sQ[fn * ES + e] : qold[PIPE ? 0 : j]) + P.fb * r;
       }
     }
     __syncthreads();  // tile buffers and work arrays free for reuse
     if (!PIPE && next < nvt) {
-      issue_tile(next, sIn);
       cp_async_wait_all();
       __syncthreads();
       load_traces(sIn, next, nb);
@@ -595,7 +629,9 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
 
 // --------------------------------------------------------------- host side
 template <int N, bool BB>
-static size_t smem_bytes(int Nq, bool pipe, bool ops_smem, int ops_floats, int table_ints) {
+static size_t smem_bytes(int Nq, bool pipe, bool ops_smem, int ops_floats, int table_ints,
+                         int bb_off) {
+  if (!ops_smem) table_ints = bb_off;
   using L = FusedSmem<N, BB>;
   return sizeof(float) * ((size_t)(pipe ? 2 : 1) * L::in_size(Nq) + L::work_size(Nq) +
                           (ops_smem ? ops_floats : 0)) +
@@ -666,7 +702,8 @@ static bbw_status prepare(FusedPlan &pl) {
   for (int c = 0; c < 4 && pick < 0; ++c) {
     if (pl.want_ops >= 0 && cand[c][0] != (pl.want_ops > 0)) continue;
     if (pl.want_pipe >= 0 && cand[c][1] != (pl.want_pipe > 0)) continue;
-    if (smem_bytes<N, BB>(pl.Nq, cand[c][1], cand[c][0], pl.ops_floats, pl.table_ints) <=
+    if (smem_bytes<N, BB>(pl.Nq, cand[c][1], cand[c][0], pl.ops_floats, pl.table_ints,
+                          pl.bb_off) <=
         (size_t)maxsm)
       pick = c;
   }
@@ -674,7 +711,8 @@ static bbw_status prepare(FusedPlan &pl) {
     return set_error(BBW_ERR_UNSUPPORTED, "fused stage: element tile does not fit in shared memory");
   pl.ops_smem = cand[pick][0] ? pl.ops_floats : 0;
   pl.pipe = cand[pick][1];
-  pl.smem = smem_bytes<N, BB>(pl.Nq, pl.pipe, pl.ops_smem > 0, pl.ops_floats, pl.table_ints);
+  pl.smem = smem_bytes<N, BB>(pl.Nq, pl.pipe, pl.ops_smem > 0, pl.ops_floats, pl.table_ints,
+                              pl.bb_off);
   cudaError_t e = pl.W == 8 ? set_smem_attr<N, BB, 8>(pl.ops_smem > 0, pl.pipe, (int)pl.smem)
                             : set_smem_attr<N, BB, 16>(pl.ops_smem > 0, pl.pipe, (int)pl.smem);
   if (e != cudaSuccess) return set_cuda_error(e, "fused stage attribute");

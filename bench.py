@@ -41,6 +41,7 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 N_ORDER, N_HEX = 5, 32
 SAMPLE_HEX = 16
@@ -325,6 +326,58 @@ def adjoint_workload(args, torch, dist, rank, world):
             "grad_finite": bool(np.isfinite(grad).all())}
 
 
+def precision_workload(args, torch):
+    """Error study on the standing mode p = cos(pi x)cos(pi y)cos(pi z)
+    cos(sqrt(3) pi t), c^2 = 1, p = 0 walls on [-1/2, 1/2]^3 (exact for the
+    reference's boundary condition), h-refinement 8/16/24: FP32 stage at
+    N = 7 (the tensor-core form needs Np <= 64, Nq <= 128: N in {3, 5}), and
+    FP32 against the split-FP16 tensor-core form at N = 5.  Errors: relative
+    L2 against the exact solution at T (FP64 quadrature), and against the
+    FP64 C restatement over the first 10 steps on the 8^3 mesh."""
+    import math
+    from oracle import Oracle
+    from bbwadg_b200 import WaveSolver, make_problem
+    from bbwadg_b200.problem import cavity_mode
+    T = args.prec_time
+    rows = []
+    for N, precs in ((7, ("fp32",)), (5, ("fp32", "f16x3"))):
+        cub, tri = reference_rule(N)
+        for nh in (8, 16, 24):
+            p = make_problem(N, nh, c2="one", ic="cavity", lo=-0.5, hi=0.5, cubature=cub,
+                             tri_cubature=tri, cfl=0.25)
+            nsteps = int(math.ceil(T / p.dt))
+            dt = float(np.float32(T / nsteps))
+            zero = np.zeros(p.K * 4 * p.Np, np.float32)
+            for prec in precs:
+                s = WaveSolver(p, precision=prec)
+                s.set_data(p.Q0)
+                s.steps(dt, 2)  # warm-up (graph capture)
+                s.set_data(p.Q0)
+                s.set_residual(zero)
+                s.sync()
+                t0 = time.perf_counter()
+                s.steps(dt, nsteps)
+                s.sync()
+                el = time.perf_counter() - t0
+                Q = s.get_data()
+                err, rel = p.l2_error(Q, nsteps * dt, cavity_mode)
+                row = {"N": N, "n": nh, "K": p.K, "precision": prec, "steps": nsteps,
+                       "rel_l2_vs_exact": rel, "ms_per_step": 1e3 * el / nsteps}
+                if nh == 8:
+                    s.set_data(p.Q0)
+                    s.set_residual(zero)
+                    s.steps(dt, 10)
+                    q10 = s.get_data()
+                    q64, _ = Oracle(N, p.K, p.ops_dict(), p.geo_dict(), dtype=np.float64).run(
+                        p.Q0.astype(np.float64), dt, 50)
+                    row["rel_l2_vs_fp64_10_steps"] = float(
+                        np.linalg.norm(q10 - q64) / np.linalg.norm(q64))
+                rows.append(row)
+                s.close()
+    return {"workload": "standing mode, c2=1, p=0 walls on [-1/2,1/2]^3, T=%g, CFL 0.25" % T,
+            "rows": rows}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -336,8 +389,9 @@ def main():
     ap.add_argument("--hex", type=int, default=N_HEX, help="hexes per direction (profiling cases)")
     ap.add_argument("--variants", default="nodal,bb,nodal-f16x3",
                     help="variants to run, comma separated (nodal, bb, nodal-f16x3)")
-    ap.add_argument("--extra", default="shots,adjoint",
-                    help="extra workloads reported beside the headline: shots, adjoint")
+    ap.add_argument("--extra", default="shots,adjoint,precision",
+                    help="extra workloads reported beside the headline: shots, adjoint, precision")
+    ap.add_argument("--prec-time", type=float, default=0.02)
     ap.add_argument("--shots", type=int, default=32)
     ap.add_argument("--shots-hex", type=int, default=24)
     ap.add_argument("--shots-steps", type=int, default=10)
@@ -414,6 +468,7 @@ def main():
     extra = [x for x in args.extra.split(",") if x]
     shots = shots_workload(args, torch, dist, world) if "shots" in extra else None
     adj = adjoint_workload(args, torch, dist, rank, world) if "adjoint" in extra else None
+    prec = precision_workload(args, torch) if ("precision" in extra and rank == 0) else None
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
@@ -468,6 +523,8 @@ def main():
         line["shots"] = shots
     if adj is not None:
         line["adjoint"] = adj
+    if prec is not None:
+        line["precision"] = prec
     print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()

@@ -149,3 +149,27 @@ def test_every_stage_configuration_matches_oracle(cuda, N, variant):
     s.steps(p.dt, 2)
     assert rel_l2(s.get_data(), q_ref) < TOL
     s.close()
+
+
+@pytest.mark.parametrize("variant", ["nodal", "bb"])
+def test_fused_n7_matches_oracle(cuda, variant):
+    """N = 7 (Np = 120, reference rule Nq = 214): operators, and for BB the
+    lift tables, read through the cache (they do not fit in shared memory
+    next to the tiles)."""
+    from oracle import Oracle
+    g = golden("ops_N7.npz")
+    nfq = int(g["Nfq"][0])
+    p = make_problem(7, 2, variant=variant, c2="sine", c2_jitter=0.5, seed=8,
+                     cubature=(g["rq"], g["sq"], g["tq"], g["wq"]),
+                     tri_cubature=(g["rfq"][:nfq], g["sfq"][:nfq], g["wfqFace"]))
+    q_ref, _ = Oracle(7, p.K, p.ops_dict(), p.geo_dict(), variant=variant).run(p.Q0.copy(), p.dt, 15)
+    s = WaveSolver(p)
+    s.set_data(p.Q0)
+    s.steps(p.dt, 3)
+    assert rel_l2(s.get_data(), q_ref) < TOL
+    cfg = s.autotune(p.dt, 3)
+    s.set_data(p.Q0)
+    s.set_residual(np.zeros(p.K * 4 * p.Np, np.float32))
+    s.steps(p.dt, 3)
+    assert rel_l2(s.get_data(), q_ref) < TOL, cfg
+    s.close()

@@ -82,3 +82,49 @@ def test_fp64_oracle_is_closer_to_truth():
     q32, _ = o32.run(Q0.copy(), float(geo["dt"][0]), 5)
     q64, _ = o64.run(Q0.astype(np.float64), float(np.float32(geo["dt"][0])), 5)
     assert rel_l2(q32, q64) < 1e-6
+
+
+def test_c1_restatement_matches_reference_cpu_path(tmp_path):
+    """N=3 at full workload size (8^3 x 6 tets, CFL 0.5, 100 steps): the C
+    restatement against the reference's own CPU path on the same mesh file,
+    c^2, initial state and dt."""
+    import os
+    import subprocess
+
+    import bbwa
+    from conftest import ROOT, golden
+    from bbwadg_b200 import make_problem
+    from bbwadg_b200.mesh import kuhn_box, write_gmsh22
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_N3_B0")
+    if not os.path.exists(exe):
+        pytest.skip("oracle/_ref not built")
+    msh = str(tmp_path / "box8.msh")
+    write_gmsh22(msh, *kuhn_box(8))
+    g = golden("ops_N3.npz")
+    nfq = int(g["Nfq"][0])
+    p = make_problem(3, mesh=msh, c2="sine", ic="gauss", cubature=(g["rq"], g["sq"], g["tq"], g["wq"]),
+                     tri_cubature=(g["rfq"][:nfq], g["sfq"][:nfq], g["wfqFace"]), cfl=0.5)
+    np.ascontiguousarray(p.Q0, np.float32).tofile(tmp_path / "q0")
+    np.ascontiguousarray(p.c2q, np.float32).tofile(tmp_path / "c2")
+    subprocess.run([exe, "run", msh, str(tmp_path / "out"), "--stages", "500", "--q0",
+                    str(tmp_path / "q0"), "--c2q", str(tmp_path / "c2"), "--dt",
+                    "%.9g" % np.float32(p.dt), "--c2", "sine"], check=True,
+                   stdout=subprocess.DEVNULL, timeout=600)
+    q_ref = bbwa.read(str(tmp_path / "out"))["Q"]
+    q, _ = Oracle(3, p.K, p.ops_dict(), p.geo_dict()).run(p.Q0.copy(), p.dt, 500)
+    assert np.linalg.norm(q - q_ref) <= 1e-6 * np.linalg.norm(q_ref)
+
+
+@pytest.mark.parametrize("N", [3, 5, 7])
+@pytest.mark.parametrize("variant", ["nodal", "bb"])
+def test_wadg_projection_is_identity_on_polynomials(N, variant):
+    """Pq Vq = I (cpp/src/WaveOKL3d.cpp:895-896) for the reference's FP32
+    operators: the degree-2N+1 rule integrates the mass matrix exactly, which
+    the fused stage relies on when it skips the velocity rows of the WADG
+    update (J = 1)."""
+    g = golden("ops_N%d.npz" % N)
+    Np = (N + 1) * (N + 2) * (N + 3) // 6
+    Nq = int(g["Nq"][0])
+    Vq = np.asarray(g["Vq_" + variant], np.float64).reshape(Np, Nq).T
+    Pq = np.asarray(g["Pq_" + variant], np.float64).reshape(Nq, Np).T
+    assert np.abs(Pq @ Vq - np.eye(Np)).max() < 1e-5
