@@ -81,7 +81,8 @@ void release(bbw_ctx *c) {
 namespace bbw {
 
 // Operators packed per warp for the fused kernel with W warps per CTA:
-//   vol  [W][Np(m)][P3R]  (Dr, Ds, Dt)[r0+i][m] at 3i + {0,1,2}   (nodal)
+//   vol  [W][Np(m)][P3R]  rows in pairs p = i/2: Dr, Ds, Dt of row r0+i at
+//                         6p + (i%2) + {0, 2, 4}                      (nodal)
 //   lift [W][NF(m)][PR]   LIFT[r0+i][m]                           (nodal)
 //   pq   [W][Nq(q)][PR]   Pq[r0+i][q]
 //   vq   [W][Np(n)][PRQ]  Vq[q0+i][n]
@@ -90,7 +91,7 @@ void pack_fused_ops(int N, int Nq, int W, bool bb, const float *Dr, const float 
                     const float *Dt, const float *LIFT, const float *Vq, const float *Pq,
                     FusedOps &out) {
   const int Np = np_of(N), NF = 4 * nfp_of(N);
-  const int R = cdivi(Np, W), PR = round4i(R), P3R = round4i(3 * R);
+  const int R = cdivi(Np, W), PR = round4i(R), P3R = round4i(6 * cdivi(R, 2));
   const int RQ = cdivi(Nq, W), QB = fused_vq_block(W), PRQ = cdivi(RQ, QB) * QB;
   std::vector<float> &ops = out.ops;
   ops.clear();
@@ -100,9 +101,9 @@ void pack_fused_ops(int N, int Nq, int W, bool bb, const float *Dr, const float 
       for (int i = 0; i < R; ++i) {
         const int r = w * R + i;
         if (r >= Np) continue;
-        for (int mm = 0; mm < Np; ++mm) {
-          float *d = &vol[((size_t)w * Np + mm) * P3R + 3 * i];
-          d[0] = Dr[r + mm * Np], d[1] = Ds[r + mm * Np], d[2] = Dt[r + mm * Np];
+        for (int mm = 0; mm < Np; ++mm) {  // row pairs: (Dr, Dr', Ds, Ds', Dt, Dt')
+          float *d = &vol[((size_t)w * Np + mm) * P3R + 6 * (i / 2) + (i % 2)];
+          d[0] = Dr[r + mm * Np], d[2] = Ds[r + mm * Np], d[4] = Dt[r + mm * Np];
         }
         for (int mm = 0; mm < NF; ++mm) lift[((size_t)w * NF + mm) * PR + i] = LIFT[r + mm * Np];
       }

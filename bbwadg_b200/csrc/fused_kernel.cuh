@@ -61,14 +61,22 @@ struct FusedCfg {
   static constexpr int W = W_;  // warps per CTA
   static constexpr int T = 32 * W;
   static constexpr int R = cdiv(Np, W);     // node rows per warp
+  static constexpr int R2 = cdiv(R, 2);     // row pairs (packed FP32 FMAs)
   static constexpr int PR = round4(R);
-  static constexpr int P3R = round4(3 * R);
+  static constexpr int P3R = round4(6 * R2);
 };
+
+// packed FP32 pair helpers (sm_100 FFMA2: two independent FMAs per
+// instruction, each rounded as a scalar FMA)
+__device__ __forceinline__ float2 pair(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 pair(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float pick(const float2 *v, int i) { return (i & 1) ? v[i >> 1].y : v[i >> 1].x; }
 
 // ------------------------------------------------------------------ layouts
 // Operators, packed per warp so that warp w reads one contiguous, 16-byte
 // aligned block per reduction index:
-//   vol  [W][Np(m)][P3R]  (Dr, Ds, Dt)[r0+i][m] at 3i + {0,1,2}
+//   vol  [W][Np(m)][P3R]  rows in pairs p = i/2: (Dr, Ds, Dt)[r0+i][m] at
+//                         6p + (i%2) + {0, 2, 4}
 //   lift [W][NF(m)][PR]   LIFT[r0+i][m]
 //   pq   [W][Nq(q)][PR]   Pq[r0+i][q]
 //   vq   [W][Np(n)][PRQ]  Vq[q0+i][n]
@@ -328,14 +336,17 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
     {
       const float *G = sGeo + lane * 25;
       if constexpr (!BB) {
-        float dr[R], ds[R], dt[R], dv[R];
+        // rows in pairs: per pair the operator block is
+        // (Dr, Dr', Ds, Ds', Dt, Dt') of rows (i, i+1)
+        constexpr int R2 = C::R2;
+        float2 dr[R2], ds[R2], dt[R2], dv[R2];
 #pragma unroll
-        for (int i = 0; i < R; ++i) dr[i] = ds[i] = dt[i] = dv[i] = 0.f;
+        for (int i = 0; i < R2; ++i) dr[i] = ds[i] = dt[i] = dv[i] = pair(0.f);
 #pragma unroll 2
         for (int m = 0; m < Np; ++m) {
-          const float pm = sQ[m * ES + lane];
-          const float ur = sR[(Np + m) * ES + lane], us = sR[(2 * Np + m) * ES + lane],
-                      ut = sR[(3 * Np + m) * ES + lane];
+          const float2 pm = pair(sQ[m * ES + lane]);
+          const float2 ur = pair(sR[(Np + m) * ES + lane]), us = pair(sR[(2 * Np + m) * ES + lane]),
+                       ut = pair(sR[(3 * Np + m) * ES + lane]);
           const float4 *op = reinterpret_cast<const float4 *>(wVol + m * C::P3R);
           float o[C::P3R];
 #pragma unroll
@@ -344,21 +355,24 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
             o[4 * j] = t4.x, o[4 * j + 1] = t4.y, o[4 * j + 2] = t4.z, o[4 * j + 3] = t4.w;
           }
 #pragma unroll
-          for (int i = 0; i < R; ++i) {
-            dr[i] += o[3 * i] * pm;
-            ds[i] += o[3 * i + 1] * pm;
-            dt[i] += o[3 * i + 2] * pm;
-            dv[i] += o[3 * i] * ur;
-            dv[i] += o[3 * i + 1] * us;
-            dv[i] += o[3 * i + 2] * ut;
+          for (int i = 0; i < R2; ++i) {
+            const float2 Dr = pair(o[6 * i], o[6 * i + 1]), Ds = pair(o[6 * i + 2], o[6 * i + 3]),
+                         Dt = pair(o[6 * i + 4], o[6 * i + 5]);
+            dr[i] = __ffma2_rn(Dr, pm, dr[i]);
+            ds[i] = __ffma2_rn(Ds, pm, ds[i]);
+            dt[i] = __ffma2_rn(Dt, pm, dt[i]);
+            dv[i] = __ffma2_rn(Dr, ur, dv[i]);
+            dv[i] = __ffma2_rn(Ds, us, dv[i]);
+            dv[i] = __ffma2_rn(Dt, ut, dv[i]);
           }
         }
 #pragma unroll
         for (int i = 0; i < R; ++i) {
-          rp[i] = -dv[i];
-          ru[i] = -(G[0] * dr[i] + G[3] * ds[i] + G[6] * dt[i]);
-          rv[i] = -(G[1] * dr[i] + G[4] * ds[i] + G[7] * dt[i]);
-          rw[i] = -(G[2] * dr[i] + G[5] * ds[i] + G[8] * dt[i]);
+          const float a = pick(dr, i), bs = pick(ds, i), c = pick(dt, i);
+          rp[i] = -pick(dv, i);
+          ru[i] = -(G[0] * a + G[3] * bs + G[6] * c);
+          rv[i] = -(G[1] * a + G[4] * bs + G[7] * c);
+          rw[i] = -(G[2] * a + G[5] * bs + G[8] * c);
         }
       } else {
         // sparse Bernstein derivative, cpp/okl/WaveKernels.okl:428-467
@@ -404,30 +418,29 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
       if constexpr (!BB) {
 #pragma unroll 1
         for (int f = 0; f < 4; ++f) {
-          float acc[R];
+          float2 acc[C::PR / 2];
 #pragma unroll
-          for (int i = 0; i < R; ++i) acc[i] = 0.f;
+          for (int i = 0; i < C::PR / 2; ++i) acc[i] = pair(0.f);
 #pragma unroll 3
           for (int j = 0; j < Nfp; ++j) {
             const int m = f * Nfp + j;
-            const float pf = sF[m * ES + lane];
+            const float2 pf = pair(sF[m * ES + lane]);
             const float4 *op = reinterpret_cast<const float4 *>(wLift + m * C::PR);
-            float o[C::PR];
 #pragma unroll
             for (int q = 0; q < C::PR / 4; ++q) {
               const float4 t4 = op[q];
-              o[4 * q] = t4.x, o[4 * q + 1] = t4.y, o[4 * q + 2] = t4.z, o[4 * q + 3] = t4.w;
+              acc[2 * q] = __ffma2_rn(pair(t4.x, t4.y), pf, acc[2 * q]);
+              acc[2 * q + 1] = __ffma2_rn(pair(t4.z, t4.w), pf, acc[2 * q + 1]);
             }
-#pragma unroll
-            for (int i = 0; i < R; ++i) acc[i] += o[i] * pf;
           }
           const float nx = fgl[4 * f + 1], ny = fgl[4 * f + 2], nz = fgl[4 * f + 3];
 #pragma unroll
           for (int i = 0; i < R; ++i) {
-            rp[i] += acc[i];
-            ru[i] -= nx * acc[i];
-            rv[i] -= ny * acc[i];
-            rw[i] -= nz * acc[i];
+            const float a = pick(acc, i);
+            rp[i] += a;
+            ru[i] -= nx * a;
+            rv[i] -= ny * a;
+            rw[i] -= nz * a;
           }
         }
       } else {
@@ -506,26 +519,24 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
       constexpr int QB = fused_vq_block(W_);
       const int q0 = warp * RQ;
       for (int qb = 0; qb < RQ; qb += QB) {
-        float acc[QB];
+        float2 acc[QB / 2];
 #pragma unroll
-        for (int j = 0; j < QB; ++j) acc[j] = 0.f;
+        for (int j = 0; j < QB / 2; ++j) acc[j] = pair(0.f);
 #pragma unroll 2
         for (int n = 0; n < Np; ++n) {
-          const float x = sR[n * ES + lane];
+          const float2 x = pair(sR[n * ES + lane]);
           const float4 *v = reinterpret_cast<const float4 *>(wVq + n * PRQ + qb);
 #pragma unroll
           for (int j = 0; j < QB / 4; ++j) {
             const float4 t4 = v[j];
-            acc[4 * j] += t4.x * x;
-            acc[4 * j + 1] += t4.y * x;
-            acc[4 * j + 2] += t4.z * x;
-            acc[4 * j + 3] += t4.w * x;
+            acc[2 * j] = __ffma2_rn(pair(t4.x, t4.y), x, acc[2 * j]);
+            acc[2 * j + 1] = __ffma2_rn(pair(t4.z, t4.w), x, acc[2 * j + 1]);
           }
         }
 #pragma unroll
         for (int j = 0; j < QB; ++j) {
           const int q = q0 + qb + j;
-          if (qb + j < RQ && q < Nq) sQuad[q * ES + lane] = acc[j] * sC2[q * ES + lane];
+          if (qb + j < RQ && q < Nq) sQuad[q * ES + lane] = pick(acc, j) * sC2[q * ES + lane];
         }
       }
     }
@@ -543,22 +554,23 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
       rpre[j] = i < ne * 4 * Np ? resg[i] : 0.f;
     }
     {
-      float acc[R];
+      float2 acc2[C::PR / 2];
 #pragma unroll
-      for (int i = 0; i < R; ++i) acc[i] = 0.f;
+      for (int i = 0; i < C::PR / 2; ++i) acc2[i] = pair(0.f);
 #pragma unroll 2
       for (int q = 0; q < Nq; ++q) {
-        const float x = sQuad[q * ES + lane];
+        const float2 x = pair(sQuad[q * ES + lane]);
         const float4 *op = reinterpret_cast<const float4 *>(wPq + q * C::PR);
-        float o[C::PR];
 #pragma unroll
         for (int j = 0; j < C::PR / 4; ++j) {
           const float4 t4 = op[j];
-          o[4 * j] = t4.x, o[4 * j + 1] = t4.y, o[4 * j + 2] = t4.z, o[4 * j + 3] = t4.w;
+          acc2[2 * j] = __ffma2_rn(pair(t4.x, t4.y), x, acc2[2 * j]);
+          acc2[2 * j + 1] = __ffma2_rn(pair(t4.z, t4.w), x, acc2[2 * j + 1]);
         }
-#pragma unroll
-        for (int i = 0; i < R; ++i) acc[i] += o[i] * x;
       }
+      float acc[R];
+#pragma unroll
+      for (int i = 0; i < R; ++i) acc[i] = pick(acc2, i);
       // source term of this shot, added to the projected rhs_p as
       // rk_update_elas does (acous_elas_cpp/okl/ElasKernelsWADG.okl:400-403)
       if (P.src_off) {

@@ -392,6 +392,8 @@ def main():
     ap.add_argument("--extra", default="shots,adjoint,precision",
                     help="extra workloads reported beside the headline: shots, adjoint, precision")
     ap.add_argument("--prec-time", type=float, default=0.02)
+    ap.add_argument("--config", type=int, default=0,
+                    help="pin the fused-stage configuration code instead of autotuning")
     ap.add_argument("--shots", type=int, default=32)
     ap.add_argument("--shots-hex", type=int, default=24)
     ap.add_argument("--shots-steps", type=int, default=10)
@@ -423,7 +425,14 @@ def main():
         K, Np, Nq = prob.K, prob.Np, prob.Nq
         s = WaveSolver(prob, precision=prec)
         s.set_data(prob.Q0)
-        tuned = s.autotune(prob.dt, 10) if prec == "fp32" else None
+        tuned = None
+        if prec == "fp32" and args.config:  # a pinned configuration (profiling runs)
+            c = args.config
+            s.set_config(c & 255, c >> 8 & 1, c >> 9 & 1)
+            tuned = {"warps": c & 255, "ops_in_smem": bool(c >> 8 & 1),
+                     "pipelined": bool(c >> 9 & 1), "code": c, "pinned": True}
+        elif prec == "fp32":
+            tuned = s.autotune(prob.dt, 10)
         qptr, rptr, stream_ptr = s.device_state()
         stream = torch.cuda.ExternalStream(stream_ptr)
         s.steps(prob.dt, args.warmup)
