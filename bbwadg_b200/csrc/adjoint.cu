@@ -145,6 +145,8 @@ extern "C" bbw_status bbw_forward(bbw_ctx *c, float dt, int nsteps, int checkpoi
   if (c->precision != BBW_PREC_FP32)
     return set_error(BBW_ERR_UNSUPPORTED, "bbw_forward: the adjoint needs BBW_PREC_FP32");
   if (c->R <= 0) return set_error(BBW_ERR_STATE, "bbw_forward: no receivers set");
+  if (c->plan.Kc > 0 && c->plan.Kc < c->K)
+    return set_error(BBW_ERR_UNSUPPORTED, "bbw_forward: the adjoint needs the whole mesh (no halo)");
   bbw_status s = adj_setup(c);
   if (s != BBW_OK) return s;
   double t0 = 0;

@@ -645,6 +645,35 @@ extern "C" bbw_status bbw_autotune(bbw_ctx *c, float dt, int stages, int *config
   return BBW_OK;
 }
 
+extern "C" bbw_status bbw_set_compute_range(bbw_ctx *c, int Kc) {
+  if (!c || Kc < 1 || Kc > c->K) return set_error(BBW_ERR_ARG, "bbw_set_compute_range: bad Kc");
+  if (Kc < c->K && c->precision != BBW_PREC_FP32)
+    return set_error(BBW_ERR_UNSUPPORTED, "bbw_set_compute_range: halo elements need BBW_PREC_FP32");
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return set_cuda_error(e, "bbw_set_compute_range");
+  c->plan.Kc = Kc;
+  drop_graphs(c);
+  return BBW_OK;
+}
+
+static bbw_status check_element_list(bbw_ctx *c, int n, const int *idx, const void *buf,
+                                     const char *who) {
+  if (!c || n < 0 || (n > 0 && (!idx || !buf))) return set_error(BBW_ERR_ARG, who);
+  return BBW_OK;
+}
+
+extern "C" bbw_status bbw_gather_elements(bbw_ctx *c, int n, const int *idx, float *buf) {
+  bbw_status s = check_element_list(c, n, idx, buf, "bbw_gather_elements: bad argument");
+  if (s != BBW_OK) return s;
+  return gather_elements(c->Np, c->K, c->S, c->Q[c->cur], n, idx, buf, c->stream);
+}
+
+extern "C" bbw_status bbw_scatter_elements(bbw_ctx *c, int n, const int *idx, const float *buf) {
+  bbw_status s = check_element_list(c, n, idx, buf, "bbw_scatter_elements: bad argument");
+  if (s != BBW_OK) return s;
+  return scatter_elements(c->Np, c->K, c->S, c->Q[c->cur], n, idx, buf, c->stream);
+}
+
 extern "C" bbw_status bbw_set_shots(bbw_ctx *c, int S) {
   if (!c || S < 1) return set_error(BBW_ERR_ARG, "bbw_set_shots: bad argument");
   if (S > 1 && c->precision != BBW_PREC_FP32)

@@ -16,6 +16,7 @@ constexpr int kFusedRowStride = 33;
 struct FusedPlan {
   int N = 0, K = 0, Nq = 0, RQ = 0, PRQ = 0, bc = 0, npat = 0;
   int W = 0;                            // warps per CTA (8 or 16; 0 = default for N)
+  int Kc = 0;                           // elements advanced (0 = all K; rest are halo copies)
   int want_ops = -1, want_pipe = -1;    // requested placement (-1: first that fits)
   bool bb = false, pipe = false;
   int grid = 0;
@@ -79,6 +80,11 @@ bbw_status fused_prepare(FusedPlan &pl);
 bbw_status fused_launch(const FusedPlan &pl, const float *Qin, float *Qout, float *res, float fa,
                         float fb, float fdt, float cstage, cudaStream_t st);
 // receivers of all shots after a step, then time += dt, step += 1
+// state copies of listed elements (all shots) to / from a packed buffer
+bbw_status gather_elements(int Np, int K, int S, const float *Q, int n, const int *idx,
+                           float *buf, cudaStream_t st);
+bbw_status scatter_elements(int Np, int K, int S, float *Q, int n, const int *idx,
+                            const float *buf, cudaStream_t st);
 bbw_status record_and_advance(int N, int K, int S, const float *Q, int R, const int *rec_elem,
                               const float *rec_w, float *traces, int max_steps, double *time,
                               int *step, float dt, cudaStream_t st);

@@ -83,6 +83,7 @@ __device__ __forceinline__ float pick(const float2 *v, int i) { return (i & 1) ?
 // plus, for BB, the sparse tables.  Built on the host (fused_host.cu).
 struct FusedParams {
   int K, Nq, RQ, PRQ, bc, npat;
+  int Kc;  // elements [0, Kc) are advanced; [Kc, K) are halo copies (neighbour traces only)
   int pat_off, bb_off;              // int offsets of the tables (multiples of 4)
   float fa, fb, fdt;
   const float *__restrict__ Qin;
@@ -190,13 +191,13 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
   const int *bbTab = OPS_SMEM ? sTab + P.bb_off : P.tables + P.bb_off;
 
   // asynchronous copies of one tile's inputs into buffer `buf`
-  const int ntiles = cdiv(P.K, TILE_E);
+  const int ntiles = cdiv(P.Kc, TILE_E);
   const size_t sstride = (size_t)P.K * 4 * Np;  // floats per shot
   // parts of a tile's inputs: geometry + neighbour codes, state, c2
   constexpr int IN_GEO = 1, IN_Q = 2, IN_C2 = 4, IN_ALL = 7;
   auto issue_tile = [&](int vt, float *buf, int parts) {
     const int shot = vt / ntiles, tile = vt - shot * ntiles;
-    const int k0 = tile * TILE_E, ne = min(TILE_E, P.K - k0);
+    const int k0 = tile * TILE_E, ne = min(TILE_E, P.Kc - k0);
     float *bQ = buf + L::inQ, *bGeo = buf + L::inGeo, *bC2 = buf + L::inC2;
     int *bNbr = (int *)(buf + L::inNbr);
     if (parts & IN_GEO) {
@@ -233,7 +234,7 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
   // neighbour face traces of the tile in `buf` into registers
   auto load_traces = [&](const float *buf, int vt, float (&nb)[FIT][4]) {
     const int shot = vt / ntiles, tile_of_buf = vt - shot * ntiles;
-    const int ne_b = min(TILE_E, P.K - tile_of_buf * TILE_E);
+    const int ne_b = min(TILE_E, P.Kc - tile_of_buf * TILE_E);
     const int *bNbr = (const int *)(buf + L::inNbr);
 #pragma unroll
     for (int j = 0; j < FIT; ++j) {
@@ -269,7 +270,7 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
   for (; vt < nvt; vt += gridDim.x) {
     const int shot = vt / ntiles, tile = vt - shot * ntiles;
     const int k0 = tile * TILE_E;
-    const int ne = min(TILE_E, P.K - k0);
+    const int ne = min(TILE_E, P.Kc - k0);
     const int next = vt + gridDim.x;
     const size_t sbase = shot * sstride;
     float *cur = sIn + b * inSize;
@@ -655,6 +656,7 @@ static bbw_status launch_fused(const FusedPlan &pl, const float *Qin, float *Qou
                                float fa, float fb, float fdt, float cstage, cudaStream_t st) {
   FusedParams P;
   P.K = pl.K, P.Nq = pl.Nq, P.RQ = pl.RQ, P.PRQ = pl.PRQ, P.bc = pl.bc, P.npat = pl.npat;
+  P.Kc = pl.Kc > 0 ? pl.Kc : pl.K;
   P.pat_off = pl.pat_off, P.bb_off = pl.bb_off;
   P.fa = fa, P.fb = fb, P.fdt = fdt;
   P.Qin = Qin, P.Qout = Qout, P.res = res;
@@ -668,7 +670,7 @@ static bbw_status launch_fused(const FusedPlan &pl, const float *Qin, float *Qou
   P.time = pl.time;
   const bool os = pl.ops_smem > 0;
   const size_t sm = pl.smem;
-  const int grid = std::min(cdiv(pl.K, TILE_E) * std::max(pl.S, 1), pl.nsm);
+  const int grid = std::min(cdiv(pl.Kc > 0 ? pl.Kc : pl.K, TILE_E) * std::max(pl.S, 1), pl.nsm);
   if (pl.W == 8) {
     constexpr int T = 256;
     if (os && pl.pipe) k_fused_stage<N, BB, true, true, 8><<<grid, T, sm, st>>>(P);
@@ -729,7 +731,7 @@ static bbw_status prepare(FusedPlan &pl) {
                             : set_smem_attr<N, BB, 16>(pl.ops_smem > 0, pl.pipe, (int)pl.smem);
   if (e != cudaSuccess) return set_cuda_error(e, "fused stage attribute");
   pl.nsm = nsm > 0 ? nsm : 148;
-  pl.grid = std::min(cdiv(pl.K, TILE_E) * std::max(pl.S, 1), pl.nsm);
+  pl.grid = std::min(cdiv(pl.Kc > 0 ? pl.Kc : pl.K, TILE_E) * std::max(pl.S, 1), pl.nsm);
   return BBW_OK;
 }
 

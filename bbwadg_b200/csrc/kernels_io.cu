@@ -35,6 +35,43 @@ __global__ void k_clock(double *time, int *step, float dt) {
   }
 }
 
+// buf[s][j][0..4Np) <-> Q[s][idx[j]][0..4Np); one warp per (shot, element)
+__global__ void k_move_elements(int Np4, int K, int S, float *Q, int n, const int *idx,
+                                float *buf, int to_buf) {
+  const long long w = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (w >= (long long)S * n) return;
+  const int s = (int)(w / n), j = (int)(w - (long long)s * n);
+  const int k = idx[j];
+  if (k < 0 || k >= K) return;  // indices outside the mesh are skipped
+  float *q = Q + ((size_t)s * K + k) * Np4;
+  float *b = buf + ((size_t)s * n + j) * Np4;
+  if (to_buf)
+    for (int i = lane; i < Np4; i += 32) b[i] = q[i];
+  else
+    for (int i = lane; i < Np4; i += 32) q[i] = b[i];
+}
+
+static bbw_status move_elements(int Np, int K, int S, float *Q, int n, const int *idx, float *buf,
+                                int to_buf, cudaStream_t st) {
+  if (n <= 0) return BBW_OK;
+  const long long warps = (long long)S * n;
+  const int wpb = 8;
+  k_move_elements<<<(int)((warps + wpb - 1) / wpb), 32 * wpb, 0, st>>>(4 * Np, K, S, Q, n, idx,
+                                                                        buf, to_buf);
+  return check_launch("element copy");
+}
+
+bbw_status gather_elements(int Np, int K, int S, const float *Q, int n, const int *idx,
+                           float *buf, cudaStream_t st) {
+  return move_elements(Np, K, S, const_cast<float *>(Q), n, idx, buf, 1, st);
+}
+
+bbw_status scatter_elements(int Np, int K, int S, float *Q, int n, const int *idx,
+                            const float *buf, cudaStream_t st) {
+  return move_elements(Np, K, S, Q, n, idx, const_cast<float *>(buf), 0, st);
+}
+
 bbw_status record_and_advance(int N, int K, int S, const float *Q, int R, const int *rec_elem,
                               const float *rec_w, float *traces, int max_steps, double *time,
                               int *step, float dt, cudaStream_t st) {

@@ -137,6 +137,20 @@ class WaveSolver:
         """One fused stage with stage-time offset c (source time = clock + c fdt)."""
         _lib.call("bbw_stage_ex", self._h, float(rka), float(rkb), float(fdt), float(c))
 
+    # ---- element decomposition (see decomp.py)
+    def set_compute_range(self, Kc):
+        """Advance elements [0, Kc) only; [Kc, K) are halo copies."""
+        _lib.call("bbw_set_compute_range", self._h, int(Kc))
+
+    def gather_elements(self, idx, buf):
+        """buf[s][j] = state of element idx[j] in shot s (device int32 idx,
+        device float32 buf of S * len(idx) * 4 * Np floats)."""
+        _lib.call("bbw_gather_elements", self._h, int(idx.numel()), _lib.ptr(idx), _lib.ptr(buf))
+
+    def scatter_elements(self, idx, buf):
+        """State of element idx[j] in shot s = buf[s][j]."""
+        _lib.call("bbw_scatter_elements", self._h, int(idx.numel()), _lib.ptr(idx), _lib.ptr(buf))
+
     def autotune(self, dt, stages=10):
         """Pick the fastest fused-stage variant for this mesh and batch;
         returns dict(warps, ops_in_smem, pipelined)."""

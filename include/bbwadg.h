@@ -251,6 +251,19 @@ bbw_status bbw_autotune(bbw_ctx *ctx, float dt, int stages, int *config);
  * cached from an earlier run); BBW_ERR_UNSUPPORTED if it does not fit. */
 bbw_status bbw_set_config(bbw_ctx *ctx, int config);
 
+/* ---- element (slab) decomposition across devices.  Elements [0, Kc) of
+ * the context are advanced by each stage; elements [Kc, K) are halo copies of
+ * neighbouring elements owned elsewhere, read only for their face traces
+ * (their faces that leave the local mesh are given as boundary faces in
+ * vmapP).  Between stages the caller refreshes the halo: bbw_gather_elements
+ * packs the current state of listed elements (all shots,
+ * [S][n][4][Np], device idx and buf) and bbw_scatter_elements writes a packed
+ * buffer back.  No reference counterpart (the reference runs one device,
+ * cpp/src/WaveOKL3d.cpp:1415).  FP32 stage only. */
+bbw_status bbw_set_compute_range(bbw_ctx *ctx, int Kc);
+bbw_status bbw_gather_elements(bbw_ctx *ctx, int n, const int *idx, float *buf);
+bbw_status bbw_scatter_elements(bbw_ctx *ctx, int n, const int *idx, const float *buf);
+
 /* ---- batched shots, sources, receivers (FP32 stage)
  * S independent shots share mesh, medium and operators; the state, residual
  * and traces hold S consecutive blocks and every stage launch advances all
