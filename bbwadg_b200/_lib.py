@@ -59,6 +59,8 @@ SIGNATURES = {
     "bbw_rk_volume_bern": (c_int, [c_int, c_int, P, P, P, P, P, P, P, P, P]),
     "bbw_rk_surface_bern": (c_int, [c_int, c_int, c_int, P, P, P, P, c_int, P, P, c_int, P, P,
                                     P, P, P, P]),
+    "bbw_rk_surface_bern_slice": (c_int, [c_int, c_int, c_int, P, P, P, P, P, P, c_int, P, P, P,
+                                          P, P, P]),
     "bbw_rk_stage_noalloc": (c_int, [c_int, c_int, c_int, c_int, P, P, P, P, P, P, P, P, P, P, P,
                                      P, c_float, c_float, c_float, P, P, P]),
     "bbw_create": (c_int, [ctypes.POINTER(MeshDesc), ctypes.POINTER(OpsDesc), c_int, c_int,

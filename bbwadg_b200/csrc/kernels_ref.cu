@@ -351,6 +351,89 @@ __global__ void __launch_bounds__(256) k_rk_surface_bern(
 }
 
 // ------------------------------------------------------------ host launchers
+
+// --------------------------------------------------- rk_surface_bern_slice
+// cpp/okl/WaveKernels.okl:652-939: the BB lift applied slice by slice.  After
+// L0, slice 0 adds the face polynomial itself to the volume rows of its
+// slice (slice_ids), each later slice reduces the previous slice's face
+// polynomial by one degree with three nonzeros per node (EEL_ids / EEL_vals
+// packed per slice, the reference's EEL_id_vec / EEL_val_vec) and adds it
+// scaled by cEL[slice].  One CTA per element; the faces of one slice are
+// applied in turn, so every accumulation into a volume row has a fixed order.
+template <int N>
+__global__ void __launch_bounds__(64) k_rk_surface_bern_slice(
+    int K, int bc, const float *__restrict__ fgeo, const int *__restrict__ Fmask,
+    const int *__restrict__ vmapP, const int4 *__restrict__ slice_ids,
+    const int *__restrict__ EEL_ids, const float *__restrict__ EEL_vals, int L0_nnz,
+    const int *__restrict__ L0_ids, const float *__restrict__ L0_vals,
+    const float *__restrict__ cEL, const float *__restrict__ Q, float *__restrict__ rhsQ) {
+  constexpr int Np = NP(N), Nfp = NFP(N), NF = 4 * NFP(N);
+  __shared__ float sp[2][NF], sU[2][NF], st[4][Np], sg[16], sc[N + 1];
+  const int k = blockIdx.x, tid = threadIdx.x, T = blockDim.x;
+  const size_t base = (size_t)k * 4 * Np;
+  for (int i = tid; i < 4 * Np; i += T) st[i / Np][i % Np] = rhsQ[base + i];
+  if (tid < 16) sg[tid] = fgeo[(size_t)k * 16 + tid];
+  if (tid <= N) sc[tid] = cEL[tid];
+  __syncthreads();
+  for (int m = tid; m < NF; m += T) {
+    const int f = m / Nfp;
+    upwind_flux(Q, Fmask[m] + k * Np * 4, vmapP[m + (size_t)k * NF], Np, sg[4 * f],
+                sg[4 * f + 1], sg[4 * f + 2], sg[4 * f + 3], bc, sp[0][m], sU[0][m]);
+  }
+  __syncthreads();
+  for (int n = tid; n < Nfp; n += T) {  // L0 on every face
+    float v1[4] = {0.f, 0.f, 0.f, 0.f}, v2[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int j = 0; j < L0_nnz; ++j) {
+      const float L = L0_vals[n + j * Nfp];
+      const int id = L0_ids[n + j * Nfp];
+#pragma unroll
+      for (int f = 0; f < 4; ++f) {
+        v1[f] += L * sp[0][id + f * Nfp];
+        v2[f] += L * sU[0][id + f * Nfp];
+      }
+    }
+#pragma unroll
+    for (int f = 0; f < 4; ++f) sp[1][n + f * Nfp] = v1[f], sU[1][n + f * Nfp] = v2[f];
+  }
+  __syncthreads();
+  int off1 = 0, off2 = 0;
+  for (int slice = 0; slice <= N; ++slice) {
+    const int Ns = N - slice, Nps = (Ns + 1) * (Ns + 2) / 2;
+    const int w = slice & 1, r = w ^ 1;
+    const float cs = sc[slice];
+    for (int f = 0; f < 4; ++f) {
+      for (int n = tid; n < Nps; n += T) {
+        const int4 v4 = slice_ids[n + off1];
+        const int vol = f == 0 ? v4.x : f == 1 ? v4.y : f == 2 ? v4.z : v4.w;
+        float rp, rU;
+        if (slice == 0) {
+          rp = sp[1][n + f * Nfp];
+          rU = sU[1][n + f * Nfp];
+        } else {
+          const int i0 = n + off2;
+          const float a = EEL_vals[i0], b = EEL_vals[i0 + Nps], c = EEL_vals[i0 + 2 * Nps];
+          const int j1 = EEL_ids[i0] + f * Nfp, j2 = EEL_ids[i0 + Nps] + f * Nfp,
+                    j3 = EEL_ids[i0 + 2 * Nps] + f * Nfp;
+          rp = a * sp[r][j1] + b * sp[r][j2] + c * sp[r][j3];
+          rU = a * sU[r][j1] + b * sU[r][j2] + c * sU[r][j3];
+        }
+        sp[w][n + f * Nfp] = rp;
+        sU[w][n + f * Nfp] = rU;
+        rp *= cs;
+        rU *= cs;
+        st[0][vol] += rp;
+        st[1][vol] += rU * sg[4 * f + 1];
+        st[2][vol] += rU * sg[4 * f + 2];
+        st[3][vol] += rU * sg[4 * f + 3];
+      }
+      __syncthreads();
+    }
+    off1 += Nps;
+    if (slice > 0) off2 += 3 * Nps;
+  }
+  for (int i = tid; i < 4 * Np; i += T) rhsQ[base + i] = st[i / Np][i % Np];
+}
+
 template <int N>
 static bbw_status launch_volume(int K, const float *vgeo, const float *Dr, const float *Ds,
                                 const float *Dt, const float *Q, float *rhsQ, cudaStream_t st) {
@@ -407,6 +490,20 @@ static bbw_status launch_surface_bern(int K, int bc, const float *fgeo, const in
   k_rk_surface_bern<N><<<(K + EB - 1) / EB, 256, 0, st>>>(
       K, bc, fgeo, Fmask, vmapP, EEL_nnz, EEL_ids, EEL_vals, L0_nnz, L0_ids, L0_vals, Q, rhsQ);
   return check_launch("rk_surface_bern");
+}
+
+
+template <int N>
+static bbw_status launch_surface_bern_slice(int K, int bc, const float *fgeo, const int *Fmask,
+                                            const int *vmapP, const int *slice_ids,
+                                            const int *EEL_ids, const float *EEL_vals,
+                                            int L0_nnz, const int *L0_ids, const float *L0_vals,
+                                            const float *cEL, const float *Q, float *rhsQ,
+                                            cudaStream_t st) {
+  k_rk_surface_bern_slice<N><<<K, 64, 0, st>>>(K, bc, fgeo, Fmask, vmapP,
+                                                (const int4 *)slice_ids, EEL_ids, EEL_vals,
+                                                L0_nnz, L0_ids, L0_vals, cEL, Q, rhsQ);
+  return check_launch("rk_surface_bern_slice");
 }
 
 }  // namespace bbw
@@ -546,4 +643,34 @@ extern "C" bbw_status bbw_rk_surface_bern(int N, int K, int bc, const float *fge
   }
 #undef CALL
   return set_error(BBW_ERR_UNSUPPORTED, "bbw_rk_surface_bern: N out of range");
+}
+
+extern "C" bbw_status bbw_rk_surface_bern_slice(int N, int K, int bc, const float *fgeo,
+                                                const int *Fmask, const int *vmapP,
+                                                const int *slice_ids, const int *EEL_ids,
+                                                const float *EEL_vals, int L0_nnz,
+                                                const int *L0_ids, const float *L0_vals,
+                                                const float *cEL, const float *Q, float *rhsQ,
+                                                void *stream) {
+  if (K < 0 || (bc != 0 && bc != 1) || L0_nnz < 1 ||
+      (K > 0 && (!fgeo || !Fmask || !vmapP || !slice_ids || !EEL_ids || !EEL_vals || !L0_ids ||
+                 !L0_vals || !cEL || !Q || !rhsQ)))
+    return set_error(BBW_ERR_ARG, "bbw_rk_surface_bern_slice: bad argument");
+  if (K == 0) return BBW_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+#define CALL(n)                                                                             \
+  launch_surface_bern_slice<n>(K, bc, fgeo, Fmask, vmapP, slice_ids, EEL_ids, EEL_vals, L0_nnz, \
+                               L0_ids, L0_vals, cEL, Q, rhsQ, st)
+  switch (N) {
+    case 1: return CALL(1);
+    case 2: return CALL(2);
+    case 3: return CALL(3);
+    case 4: return CALL(4);
+    case 5: return CALL(5);
+    case 6: return CALL(6);
+    case 7: return CALL(7);
+    case 8: return CALL(8);
+  }
+#undef CALL
+  return set_error(BBW_ERR_UNSUPPORTED, "bbw_rk_surface_bern_slice: N out of range");
 }

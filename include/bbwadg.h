@@ -151,6 +151,18 @@ bbw_status bbw_rk_surface_bern(int N, int K, int bc, const float *fgeo, const in
                                const int *L0_ids, const float *L0_vals, const float *cEL,
                                const float *Q, float *rhsQ, void *stream);
 
+/* cpp/okl/WaveKernels.okl:652-939  rk_surface_bern_slice(K, fgeo, Fmask,
+ * vmapP, slice_ids, EEL_ids, EEL_vals, L0_ids, L0_vals, cEL, Q, rhsQ): the BB
+ * lift slice by slice (the reference's choice for N > 6).  slice_ids is int4
+ * [Np]; EEL_ids / EEL_vals are the per-slice packed reduction arrays
+ * (EEL_id_vec / EEL_val_vec, 3 entries per node of slices 1..N).  rhsQ +=
+ * lift; bc as for bbw_rk_surface. */
+bbw_status bbw_rk_surface_bern_slice(int N, int K, int bc, const float *fgeo, const int *Fmask,
+                                     const int *vmapP, const int *slice_ids, const int *EEL_ids,
+                                     const float *EEL_vals, int L0_nnz, const int *L0_ids,
+                                     const float *L0_vals, const float *cEL, const float *Q,
+                                     float *rhsQ, void *stream);
+
 /* One LSRK stage as the reference's three launches (rk_volume, rk_surface,
  * rk_update_WADG; arguments as above) for callers that cannot allocate
  * device memory: the rhs buffer is a 16 MiB scratch array inside the

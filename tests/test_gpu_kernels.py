@@ -130,3 +130,41 @@ def test_empty_and_bad_arguments(cuda):
     assert _lib.lib().bbw_rk_volume(5, 0, None, None, None, None, None, None, None) == 0
     with pytest.raises(_lib.BBWError):
         _lib.call("bbw_rk_volume", 11, 4, 1, 1, 1, 1, 1, 1, None)
+
+
+def _slice_args(o, N):
+    Nfp = (N + 1) * (N + 2) // 2
+    return [P(dev(o["slice_ids"])), P(dev(np.asarray(o["EEL_id_vec"], np.int32))),
+            P(dev(np.asarray(o["EEL_val_vec"], np.float32))), o["L0_ids"].size // Nfp,
+            P(dev(o["L0_ids"])), P(dev(o["L0_vals"])), P(dev(o["cEL"]))]
+
+
+@pytest.mark.parametrize("N", [3, 5])
+def test_rk_surface_bern_slice_matches_reference(cuda, N):
+    """The slice-by-slice BB lift against the reference's own
+    rk_surface_bern_slice (cpp/okl/WaveKernels.okl:652-939) on the same inputs."""
+    o, g, k = ref_ops(N, "bb"), golden("mesh_box2_N%d.npz" % N), golden("kernels_N%d_box2.npz" % N)
+    Q, rhs = dev(k["Q_in"]), dev(k["rhs_in"])
+    _lib.call("bbw_rk_surface_bern_slice", N, 48, 0, P(dev(g["fgeo"])), P(dev(o["Fmask"])),
+              P(dev(g["vmapP"])), *_slice_args(o, N), P(Q), P(rhs), None)
+    assert rel_l2(host(rhs), k["rk_surface_bern_slice.rhsQ"]) < TOL
+
+
+@pytest.mark.parametrize("bc", [0, 1])
+def test_slice_lift_equals_sparse_lift_at_n7(cuda, bc):
+    """N = 7, where the reference switches to the slice lift: both BB lifts
+    agree (both boundary conditions)."""
+    N = 7
+    o, g = ref_ops(N, "bb"), golden("mesh_box2_N%d.npz" % N)
+    Np, Nfp = (N + 1) * (N + 2) * (N + 3) // 6, (N + 1) * (N + 2) // 2
+    rng = np.random.default_rng(3)
+    Qh = rng.standard_normal(48 * 4 * Np).astype(np.float32)
+    r0 = rng.standard_normal(48 * 4 * Np).astype(np.float32)
+    Q, a, b = dev(Qh), dev(r0), dev(r0)
+    common = [P(dev(g["fgeo"])), P(dev(o["Fmask"])), P(dev(g["vmapP"]))]
+    _lib.call("bbw_rk_surface_bern_slice", N, 48, bc, *common, *_slice_args(o, N), P(Q), P(a), None)
+    _lib.call("bbw_rk_surface_bern", N, 48, bc, *common, P(dev(o["slice_ids"])),
+              o["EEL_ids"].size // Np, P(dev(o["EEL_ids"])), P(dev(o["EEL_vals"])),
+              o["L0_ids"].size // Nfp, P(dev(o["L0_ids"])), P(dev(o["L0_vals"])),
+              P(dev(o["cEL"])), P(Q), P(b), None)
+    assert rel_l2(host(a) - r0, host(b) - r0) < 1e-5
