@@ -236,23 +236,11 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
     }
   };
 
-  if (blockIdx.x < ntiles && tid == 0) issue_tma(blockIdx.x, 0);
-  uint32_t tphase = 0, mphase = 0;
-  int it = 0;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
-    const int k0 = tile * TC_E, ne = min(TC_E, P.K - k0), gb = it & 1;
-    const float *sGeo = sGeoB + gb * TC_E * TC_GEO;
-    const int next = tile + gridDim.x;
-
-    // ---- P0: tile inputs
-    if (!tc::mbar_wait(mbarT, tphase, TC_WAIT)) fail = true;
-    tphase ^= 1u;
-    if (tid < 8) sRed[tid] = 0;
-    __syncthreads();
-
-    // ---- P1: neighbour traces (global ones issued first), upwind flux
-    //          (Uflux = -pflux), maxima
-    float nbv[FIT][4];
+  // face traces of neighbours outside tile `tile` (whose inputs have landed)
+  // into registers; traces inside the tile are read from shared memory in P1
+  float nbv[FIT][4];
+  auto load_traces = [&](int tile) {
+    const int k0 = tile * TC_E, ne = min(TC_E, P.K - k0);
 #pragma unroll
     for (int j = 0; j < FIT; ++j) {
       nbv[j][0] = nbv[j][1] = nbv[j][2] = nbv[j][3] = 0.f;
@@ -265,11 +253,57 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       if (pat == 255) continue;
       const int vP = sPat[pat * Nfp + (m - f * Nfp)];
       const unsigned rel = (unsigned)((code >> 8) - k0);
-      if (rel < (unsigned)ne) continue;  // inside the tile: read from shared memory below
+      if (rel < (unsigned)ne) continue;
       const float *o = P.Qin + (size_t)(code >> 8) * 4 * Np + vP;
       nbv[j][0] = __ldg(o), nbv[j][1] = __ldg(o + Np), nbv[j][2] = __ldg(o + 2 * Np),
       nbv[j][3] = __ldg(o + 3 * Np);
     }
+  };
+
+  uint32_t tphase = 0, mphase = 0;
+  if (blockIdx.x < ntiles && tid == 0) issue_tma(blockIdx.x, 0);
+  int it = 0;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+    const int k0 = tile * TC_E, ne = min(TC_E, P.K - k0), gb = it & 1;
+    const float *sGeo = sGeoB + gb * TC_E * TC_GEO;
+    const int next = tile + gridDim.x;
+
+    // ---- P0: tile inputs (issued during the previous tile's epilogues);
+    //          outside neighbour traces in flight through the first half of P1
+    if (!tc::mbar_wait(mbarT, tphase, TC_WAIT)) fail = true;
+    tphase ^= 1u;
+    load_traces(tile);
+    if (tid < 8) sRed[tid] = 0;
+    __syncthreads();
+
+    // ---- P1: p and contravariant velocities (4 nodes x 1 element per item),
+    //          then the upwind flux; maxima
+    constexpr int NC = KV / 4;  // node chunks incl. padding
+    const int ce = tid & 31, cc = tid >> 5;  // item (chunk cc, element ce); TC_T = 16 * 32
+    float G[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) G[i] = sGeo[ce * TC_GEO + i];
+    float4 p4 = make_float4(0.f, 0.f, 0.f, 0.f), U4[3];
+    U4[0] = U4[1] = U4[2] = p4;
+    float mp = 0.f, mU = 0.f;
+    if (cc < NC && 4 * cc < Np && ce < ne) {
+      const float *rr = sRaw + ce * RS + 4 * cc;
+      p4 = *reinterpret_cast<const float4 *>(rr);
+      const float4 u4 = *reinterpret_cast<const float4 *>(rr + Np);
+      const float4 v4 = *reinterpret_cast<const float4 *>(rr + 2 * Np);
+      const float4 w4 = *reinterpret_cast<const float4 *>(rr + 3 * Np);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        U4[d].x = u4.x * G[3 * d] + v4.x * G[3 * d + 1] + w4.x * G[3 * d + 2];
+        U4[d].y = u4.y * G[3 * d] + v4.y * G[3 * d + 1] + w4.y * G[3 * d + 2];
+        U4[d].z = u4.z * G[3 * d] + v4.z * G[3 * d + 1] + w4.z * G[3 * d + 2];
+        U4[d].w = u4.w * G[3 * d] + v4.w * G[3 * d + 1] + w4.w * G[3 * d + 2];
+        mU = fmaxf(mU, fmaxf(fmaxf(fabsf(U4[d].x), fabsf(U4[d].y)),
+                             fmaxf(fabsf(U4[d].z), fabsf(U4[d].w))));
+      }
+      mp = fmaxf(fmaxf(fabsf(p4.x), fabsf(p4.y)), fmaxf(fabsf(p4.z), fabsf(p4.w)));
+    }
+    // upwind flux (Uflux = -pflux): last, its outside traces have had longest
     float pf[FIT];
     float mF = 0.f;
 #pragma unroll
@@ -308,32 +342,6 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       pf[j] = .5f * (pjump - Unjump) * Fscale;
       mF = fmaxf(mF, fabsf(pf[j]));
     }
-    // p and contravariant velocities: 4 nodes x 1 element per item
-    constexpr int NC = KV / 4;  // node chunks incl. padding
-    const int ce = tid & 31, cc = tid >> 5;  // item (chunk cc, element ce); TC_T = 16 * 32
-    float G[9];
-#pragma unroll
-    for (int i = 0; i < 9; ++i) G[i] = sGeo[ce * TC_GEO + i];
-    float4 p4 = make_float4(0.f, 0.f, 0.f, 0.f), U4[3];
-    U4[0] = U4[1] = U4[2] = p4;
-    float mp = 0.f, mU = 0.f;
-    if (cc < NC && 4 * cc < Np && ce < ne) {
-      const float *rr = sRaw + ce * RS + 4 * cc;
-      p4 = *reinterpret_cast<const float4 *>(rr);
-      const float4 u4 = *reinterpret_cast<const float4 *>(rr + Np);
-      const float4 v4 = *reinterpret_cast<const float4 *>(rr + 2 * Np);
-      const float4 w4 = *reinterpret_cast<const float4 *>(rr + 3 * Np);
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        U4[d].x = u4.x * G[3 * d] + v4.x * G[3 * d + 1] + w4.x * G[3 * d + 2];
-        U4[d].y = u4.y * G[3 * d] + v4.y * G[3 * d + 1] + w4.y * G[3 * d + 2];
-        U4[d].z = u4.z * G[3 * d] + v4.z * G[3 * d + 1] + w4.z * G[3 * d + 2];
-        U4[d].w = u4.w * G[3 * d] + v4.w * G[3 * d + 1] + w4.w * G[3 * d + 2];
-        mU = fmaxf(mU, fmaxf(fmaxf(fabsf(U4[d].x), fabsf(U4[d].y)),
-                             fmaxf(fabsf(U4[d].z), fabsf(U4[d].w))));
-      }
-      mp = fmaxf(fmaxf(fabsf(p4.x), fabsf(p4.y)), fmaxf(fabsf(p4.z), fabsf(p4.w)));
-    }
     mp = warp_max(mp);
     mU = warp_max(mU);
     mF = warp_max(mF);
@@ -362,9 +370,11 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
     }
     sync_for_mma();
 
-    // ---- P2: state buffer free: next tile's copies; gradient, divergence, lift MMAs
+    // ---- P2: gradient, divergence, lift MMAs; meanwhile every thread fetches
+    //          the old residual of u, v, w for its rows of epilogue 1
+    const int n = 16 * q4 + lane;  // M = 64 layout: lanes 0..15 of each sub-partition
+    const bool rowok = lane < 16 && n < Np;
     if (tid == 0) {
-      if (next < ntiles) issue_tma(next, gb ^ 1);
       const uint32_t id64 = tc::idesc_f16(64, TC_E, 0);
       const int sboV = (KV / 8) * 128, sboF = (KF / 8) * 128;
       for (int d = 0; d < 3; ++d)
@@ -379,11 +389,19 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
               sBF + (2 * f + 1) * TC_E * KF, sboF, KF / 16, id64, false);
       tc::mma_commit(mbarM);
     }
+    float ro[8][3];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int e = 8 * g8 + j;
+      const size_t id = (size_t)(k0 + e) * 4 * Np + n;
+#pragma unroll
+      for (int fl = 1; fl < 4; ++fl) ro[j][fl - 1] = rowok && e < ne ? P.res[id + fl * Np] : 0.f;
+    }
     mma_wait(mphase);
 
     // ---- P3: epilogue 1 (thread = node row n, 8 elements): rhs of p, u, v, w;
-    //          LSRK update of u, v, w; rhs_p -> B operand of the Vq product
-    const int n = 16 * q4 + lane;  // M = 64 layout: lanes 0..15 of each sub-partition
+    //          LSRK update of u, v, w (old state from the tile in shared
+    //          memory); rhs_p -> B operand of the Vq product
     const uint32_t trow = tbase + ((uint32_t)(32 * q4) << 16) + 8 * g8;
     float rp[8];
     {
@@ -395,20 +413,6 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
 #pragma unroll
       for (int f = 0; f < 4; ++f) tc::tmem_ld8(trow + 128 + 32 * f, lf[f]);
       const float isp = 1.f / sp, isU = 1.f / sU, isF = 1.f / sF;
-      // old residual and state of u, v, w for this row: all loads first
-      const bool rowok = lane < 16 && n < Np;
-      float ro[8][3], qo[8][3];
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int e = 8 * g8 + j;
-        const size_t id = (size_t)(k0 + e) * 4 * Np + n;
-#pragma unroll
-        for (int fl = 1; fl < 4; ++fl) {
-          const bool ok = rowok && e < ne;
-          ro[j][fl - 1] = ok ? P.res[id + fl * Np] : 0.f;
-          qo[j][fl - 1] = ok ? __ldg(P.Qin + id + fl * Np) : 0.f;
-        }
-      }
       float mr = 0.f;
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
@@ -437,7 +441,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
           for (int fl = 1; fl < 4; ++fl) {
             const float r = P.fa * ro[j][fl - 1] + P.fdt * rv3[fl - 1];
             P.res[id + fl * Np] = r;
-            P.Qout[id + fl * Np] = qo[j][fl - 1] + P.fb * r;
+            P.Qout[id + fl * Np] = sRaw[e * RS + fl * Np + n] + P.fb * r;
           }
         }
       }
@@ -445,6 +449,8 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       if (lane == 0) atomicMax(&sRed[3], __float_as_int(mr));
     }
     __syncthreads();
+    // the state tile is dead: the next tile's copies overlap the rest
+    if (tid == 0 && next < ntiles) issue_tma(next, gb ^ 1);
     const float srp = pow2_scale(sRed[3]);
     if (lane < 16) {
 #pragma unroll
@@ -456,26 +462,30 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
     }
     sync_for_mma();
 
-    // ---- P4: Vq product
+    // ---- P4: Vq product; meanwhile c2/J of this thread's cubature row
     if (tid == 0) {
       chain(tbase + 0, sOps + L.oVq, sOps + L.oVq + MQ * KV, (KV / 8) * 128, sBp, sBp + TC_E * KV,
             (KV / 8) * 128, KV / 16, tc::idesc_f16(MQ, TC_E, 0), false);
       tc::mma_commit(mbarM);
     }
+    const int q = MQ == 128 ? 32 * q4 + lane : (lane < 16 ? 16 * q4 + lane : MQ);
+    float c2v[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int e = 8 * g8 + j;
+      c2v[j] = q < Nq && e < ne ? __ldg(P.c2q + (size_t)(k0 + e) * Nq + q) : 0.f;
+    }
     mma_wait(mphase);
 
     // ---- P5: epilogue 2 (thread = cubature row q): c2/J * p_q -> B operand
     {
-      const int q = MQ == 128 ? 32 * q4 + lane : (lane < 16 ? 16 * q4 + lane : MQ);
       float v[8];
       tc::tmem_ld8(tbase + ((uint32_t)(32 * q4) << 16) + 8 * g8, v);
       const float isr = 1.f / srp;
       float mc = 0.f;
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
-        const int e = 8 * g8 + j;
-        const bool ok = q < Nq && e < ne;
-        v[j] = ok ? v[j] * isr * __ldg(P.c2q + (size_t)(k0 + e) * Nq + q) : 0.f;
+        v[j] = v[j] * isr * c2v[j];
         mc = fmaxf(mc, fabsf(v[j]));
       }
       mc = warp_max(mc);
@@ -498,21 +508,22 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
               sBU + TC_E * KQ, (KQ / 8) * 128, KQ / 16, tc::idesc_f16(64, TC_E, 0), false);
         tc::mma_commit(mbarM);
       }
+      float r7[8], q7[8];  // old residual and state of p, fetched during the MMAs
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int e = 8 * g8 + j;
+        const size_t id = (size_t)(k0 + e) * 4 * Np + n;
+        r7[j] = rowok && e < ne ? P.res[id] : 0.f;
+        q7[j] = rowok && e < ne ? __ldg(P.Qin + id) : 0.f;
+      }
       mma_wait(mphase);
 
       // ---- P7: epilogue 3: rhs_p = Pq (c2 p_q); LSRK update of p
       float w[8];
       tc::tmem_ld8(tbase + ((uint32_t)(32 * q4) << 16) + 32 + 8 * g8, w);
       const float isc = 1.f / sc;
-      if (lane < 16 && n < Np) {
-        float ro[8], qo[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          const int e = 8 * g8 + j;
-          const size_t id = (size_t)(k0 + e) * 4 * Np + n;
-          ro[j] = e < ne ? P.res[id] : 0.f;
-          qo[j] = e < ne ? __ldg(P.Qin + id) : 0.f;
-        }
+      if (rowok) {
+        const float *ro = r7, *qo = q7;
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
           const int e = 8 * g8 + j;
