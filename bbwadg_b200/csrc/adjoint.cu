@@ -206,8 +206,8 @@ extern "C" bbw_status bbw_backward(bbw_ctx *c, bbw_tape *t, const float *dL_dtra
   if ((s = buf.get(&lamQ, t->state, "bbw_backward")) != BBW_OK ||
       (s = buf.get(&lamR, t->state, "bbw_backward")) != BBW_OK ||
       (s = buf.get(&z, t->state, "bbw_backward")) != BBW_OK ||
-      (s = buf.get(&rhs, shot, "bbw_backward")) != BBW_OK ||
-      (s = buf.get(&sigma, (size_t)K * NF, "bbw_backward")) != BBW_OK ||
+      (s = buf.get(&rhs, t->state, "bbw_backward")) != BBW_OK ||
+      (s = buf.get(&sigma, (size_t)S * K * NF, "bbw_backward")) != BBW_OK ||
       (s = buf.get(&res, t->state, "bbw_backward")) != BBW_OK ||
       (s = buf.get(&g, (size_t)S * R * nsteps, "bbw_backward")) != BBW_OK ||
       (s = buf.get(&seg, (size_t)seglen * t->state, "bbw_backward: segment states")) != BBW_OK ||
@@ -272,22 +272,19 @@ extern "C" bbw_status bbw_backward(bbw_ctx *c, bbw_tape *t, const float *dL_dtra
       }
       for (int i = 4; i >= 0; --i) {
         const float ai = (float)kRK4A[i], bi = (float)kRK4B[i];
-        for (int sh = 0; sh < S; ++sh) {
-          const size_t o = sh * shot;
-          const float *Qi = stq + (size_t)i * t->state + o;
-          if ((s = bbw_rk_volume(N, K, c->vgeo, a.D[0], a.D[1], a.D[2], Qi, rhs, st)) !=
-                  BBW_OK ||
-              (s = bbw_rk_surface(N, K, c->bc, c->fgeo, a.Fmask, a.vmapP, a.LIFT, Qi, rhs, st)) !=
-                  BBW_OK ||
-              (s = adj_wadg(N, K, Nq, a.Vq, a.Pq, pl.c2q, lamQ + o, lamR + o, ai, bi, dt, rhs,
-                            z + o, grad, st)) != BBW_OK ||
-              (s = bbw_rk_volume(N, K, c->vgeo, a.DT[0], a.DT[1], a.DT[2], z + o, rhs, st)) !=
-                  BBW_OK ||
-              (s = adj_sigma(N, K, c->fgeo, a.LIFT, z + o, sigma, st)) != BBW_OK ||
-              (s = adj_gather(N, K, c->bc, dt, c->fgeo, a.fidx, a.mapP, sigma, rhs, lamQ + o,
-                              st)) != BBW_OK)
-            return s;
-        }
+        const float *Qi = stq + (size_t)i * t->state;
+        if ((s = rk_volume_shots(N, S, K, c->vgeo, a.D[0], a.D[1], a.D[2], Qi, rhs, st)) !=
+                BBW_OK ||
+            (s = rk_surface_shots(N, S, K, c->bc, c->fgeo, a.Fmask, a.vmapP, a.LIFT, Qi, rhs,
+                                  st)) != BBW_OK ||
+            (s = adj_wadg(N, S, K, Nq, a.Vq, a.Pq, pl.c2q, lamQ, lamR, ai, bi, dt, rhs, z, grad,
+                          st)) != BBW_OK ||
+            (s = rk_volume_shots(N, S, K, c->vgeo, a.DT[0], a.DT[1], a.DT[2], z, rhs, st)) !=
+                BBW_OK ||
+            (s = adj_sigma(N, S, K, c->fgeo, a.LIFT, z, sigma, st)) != BBW_OK ||
+            (s = adj_gather(N, S, K, c->bc, dt, c->fgeo, a.fidx, a.mapP, sigma, rhs, lamQ, st)) !=
+                BBW_OK)
+          return s;
       }
     }
   }

@@ -36,17 +36,24 @@ bbw_status upload(T **dst, const T *src, size_t n, const char *what) {
 }
 
 // adjoint kernels (kernels_adj.cu)
-bbw_status adj_wadg(int N, int K, int Nq, const float *Vq, const float *Pq, const float *c2q,
+bbw_status adj_wadg(int N, int S, int K, int Nq, const float *Vq, const float *Pq, const float *c2q,
                     const float *lamQ, float *lamR, float a, float b, float dt, const float *rhs,
                     float *z, double *grad, cudaStream_t st);
-bbw_status adj_sigma(int N, int K, const float *fgeo, const float *LIFT, const float *z,
+bbw_status adj_sigma(int N, int S, int K, const float *fgeo, const float *LIFT, const float *z,
                      float *sigma, cudaStream_t st);
-bbw_status adj_gather(int N, int K, int bc, float dt, const float *fgeo, const int *fidx,
+bbw_status adj_gather(int N, int S, int K, int bc, float dt, const float *fgeo, const int *fidx,
                       const int *mapP, const float *sigma, const float *vol, float *lamQ,
                       cudaStream_t st);
 bbw_status adj_receivers(int S, int K, int Np, int R, const int *rec_elem, const float *rec_w,
                          const float *g, int nsteps, int n, float *lamQ, cudaStream_t st);
 bbw_status set_device_double(double *p, double v, cudaStream_t st);
+// kernel-level volume / surface over S shots of one K-element mesh (kernels_ref.cu)
+bbw_status rk_volume_shots(int N, int S, int K, const float *vgeo, const float *Dr,
+                           const float *Ds, const float *Dt, const float *Q, float *rhsQ,
+                           cudaStream_t st);
+bbw_status rk_surface_shots(int N, int S, int K, int bc, const float *fgeo, const int *Fmask,
+                            const int *vmapP, const float *LIFT, const float *Q, float *rhsQ,
+                            cudaStream_t st);
 
 }  // namespace bbw
 

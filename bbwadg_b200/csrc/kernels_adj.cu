@@ -29,7 +29,7 @@ namespace bbw {
 
 // mu = lamR + b lamQ; lamR <- a mu; z <- W^T mu; grad += dt t (Vq r_p)
 template <int N>
-__global__ void __launch_bounds__(256) k_adj_wadg(int K, int Nq, const float *__restrict__ Vq,
+__global__ void __launch_bounds__(256) k_adj_wadg(int S, int K, int Nq, const float *__restrict__ Vq,
                                                   const float *__restrict__ Pq,
                                                   const float *__restrict__ c2q,
                                                   const float *__restrict__ lamQ,
@@ -43,46 +43,52 @@ __global__ void __launch_bounds__(256) k_adj_wadg(int K, int Nq, const float *__
   float *s_r = s_mu + EB * Np;       // [EB][Np]  forward raw rhs_p
   float *s_t = s_r + EB * Np;        // [EB][Nq]  c2 * Pq^T mu_p
   const int k0 = blockIdx.x * EB;
-  for (int i = threadIdx.x; i < EB * 4 * Np; i += blockDim.x) {
-    const int e = i / (4 * Np), fn = i - e * 4 * Np;
-    if (k0 + e >= K) continue;
-    const size_t id = (size_t)k0 * 4 * Np + i;
-    const float mu = lamR[id] + b * lamQ[id];
-    lamR[id] = a * mu;
-    if (fn < Np) {
-      s_mu[e * Np + fn] = mu;
-      s_r[e * Np + fn] = rhs ? rhs[id] : 0.f;
-    } else {
-      z[id] = mu;  // velocity rows: Pq Vq = I (J = 1)
+  // the shots of one element block in turn: each (k, q) gradient entry is
+  // accumulated by one thread, in shot order
+  for (int sh = 0; sh < S; ++sh) {
+    const size_t so = (size_t)sh * K * 4 * Np;
+    if (sh > 0) __syncthreads();  // shared arrays free
+    for (int i = threadIdx.x; i < EB * 4 * Np; i += blockDim.x) {
+      const int e = i / (4 * Np), fn = i - e * 4 * Np;
+      if (k0 + e >= K) continue;
+      const size_t id = so + (size_t)k0 * 4 * Np + i;
+      const float mu = lamR[id] + b * lamQ[id];
+      lamR[id] = a * mu;
+      if (fn < Np) {
+        s_mu[e * Np + fn] = mu;
+        s_r[e * Np + fn] = rhs ? rhs[id] : 0.f;
+      } else {
+        z[id] = mu;  // velocity rows: Pq Vq = I (J = 1)
+      }
     }
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < EB * Nq; i += blockDim.x) {
-    const int e = i / Nq, q = i - e * Nq, k = k0 + e;
-    if (k >= K) continue;
-    const float *mu = s_mu + e * Np, *r = s_r + e * Np;
-    float t = 0.f, v = 0.f;
-    for (int n = 0; n < Np; ++n) {
-      t += __ldg(Pq + n + (size_t)q * Np) * mu[n];
-      v += __ldg(Vq + q + (size_t)n * Nq) * r[n];
+    __syncthreads();
+    for (int i = threadIdx.x; i < EB * Nq; i += blockDim.x) {
+      const int e = i / Nq, q = i - e * Nq, k = k0 + e;
+      if (k >= K) continue;
+      const float *mu = s_mu + e * Np, *r = s_r + e * Np;
+      float t = 0.f, v = 0.f;
+      for (int n = 0; n < Np; ++n) {
+        t += __ldg(Pq + n + (size_t)q * Np) * mu[n];
+        v += __ldg(Vq + q + (size_t)n * Nq) * r[n];
+      }
+      if (rhs) grad[(size_t)k * Nq + q] += (double)dt * (double)t * (double)v;
+      s_t[e * Nq + q] = c2q[(size_t)k * Nq + q] * t;
     }
-    if (rhs) grad[(size_t)k * Nq + q] += (double)dt * (double)t * (double)v;
-    s_t[e * Nq + q] = c2q[(size_t)k * Nq + q] * t;
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < EB * Np; i += blockDim.x) {
-    const int e = i / Np, n = i - e * Np, k = k0 + e;
-    if (k >= K) continue;
-    const float *t = s_t + e * Nq;
-    float acc = 0.f;
-    for (int q = 0; q < Nq; ++q) acc += __ldg(Vq + q + (size_t)n * Nq) * t[q];
-    z[(size_t)k * 4 * Np + n] = acc;
+    __syncthreads();
+    for (int i = threadIdx.x; i < EB * Np; i += blockDim.x) {
+      const int e = i / Np, n = i - e * Np, k = k0 + e;
+      if (k >= K) continue;
+      const float *t = s_t + e * Nq;
+      float acc = 0.f;
+      for (int q = 0; q < Nq; ++q) acc += __ldg(Vq + q + (size_t)n * Nq) * t[q];
+      z[so + (size_t)k * 4 * Np + n] = acc;
+    }
   }
 }
 
 // sigma[k][m] = .5 Fscale_f sum_n LIFT[n + m Np] (z_p[n] - n_f . z_U[n])
 template <int N>
-__global__ void __launch_bounds__(256) k_adj_sigma(int K, const float *__restrict__ fgeo,
+__global__ void __launch_bounds__(256) k_adj_sigma(int K, int Kg, const float *__restrict__ fgeo,
                                                    const float *__restrict__ LIFT,
                                                    const float *__restrict__ z,
                                                    float *__restrict__ sigma) {
@@ -98,7 +104,7 @@ __global__ void __launch_bounds__(256) k_adj_sigma(int K, const float *__restric
     const int e = i / NF, m = i - e * NF, k = k0 + e;
     if (k >= K) continue;
     const int f = m / Nfp;
-    const float *fg = fgeo + (size_t)k * 16 + 4 * f;
+    const float *fg = fgeo + (size_t)(k % Kg) * 16 + 4 * f;
     const float Fscale = fg[0], nx = fg[1], ny = fg[2], nz = fg[3];
     const float *w = sz[e];
     float acc = 0.f;
@@ -111,7 +117,7 @@ __global__ void __launch_bounds__(256) k_adj_sigma(int K, const float *__restric
 
 // lamQ[k][.][n] += dt (vol[k][.][n] + surface adjoint at node n)
 template <int N>
-__global__ void __launch_bounds__(256) k_adj_gather(int K, int bc, float dt,
+__global__ void __launch_bounds__(256) k_adj_gather(int K, int Kg, int bc, float dt,
                                                     const float *__restrict__ fgeo,
                                                     const int *__restrict__ fidx,
                                                     const int *__restrict__ mapP,
@@ -122,6 +128,8 @@ __global__ void __launch_bounds__(256) k_adj_gather(int K, int bc, float dt,
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (long long)K * Np) return;
   const int k = (int)(i / Np), n = (int)(i - (long long)k * Np);
+  const int kg = k % Kg;                    // mesh row (shots share the mesh)
+  const size_t sbase = (size_t)(k - kg) * NF;  // sigma offset of the shot
   float dp = 0.f, du = 0.f, dv = 0.f, dw = 0.f;
 #pragma unroll
   for (int f = 0; f < 4; ++f) {
@@ -129,9 +137,9 @@ __global__ void __launch_bounds__(256) k_adj_gather(int K, int bc, float dt,
     if (fi < 0) continue;
     const int m = f * Nfp + fi;
     const float s = sigma[(size_t)k * NF + m];
-    const float *fg = fgeo + (size_t)k * 16 + 4 * f;
+    const float *fg = fgeo + (size_t)kg * 16 + 4 * f;
     const float nx = fg[1], ny = fg[2], nz = fg[3];
-    const int code = __ldg(mapP + (size_t)k * NF + m);
+    const int code = __ldg(mapP + (size_t)kg * NF + m);
     if (code < 0) {
       if (bc == BBW_BC_PRESSURE_RELEASE) {
         dp -= 2.f * s;
@@ -140,7 +148,7 @@ __global__ void __launch_bounds__(256) k_adj_gather(int K, int bc, float dt,
       }
     } else {
       const int k2 = code / NF, f2 = (code - k2 * NF) / Nfp;
-      const float s2 = sigma[code];
+      const float s2 = sigma[sbase + code];
       const float *g2 = fgeo + (size_t)k2 * 16 + 4 * f2;
       dp += s2 - s;
       du += nx * s - g2[1] * s2;
@@ -175,7 +183,7 @@ __global__ void k_set_double(double *p, double v) { *p = v; }
 
 // ------------------------------------------------------------- host side
 template <int N>
-static bbw_status launch_adj_n(int K, int Nq, const float *Vq, const float *Pq, const float *c2q,
+static bbw_status launch_adj_n(int S, int K, int Nq, const float *Vq, const float *Pq, const float *c2q,
                                const float *lamQ, float *lamR, float a, float b, float dt,
                                const float *rhs, float *z, double *grad, cudaStream_t st) {
   constexpr int Np = NP(N), EB = UPD_EB(N);
@@ -185,26 +193,26 @@ static bbw_status launch_adj_n(int K, int Nq, const float *Vq, const float *Pq, 
     cudaFuncSetAttribute(k_adj_wadg<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr = true;
   }
-  k_adj_wadg<N><<<(K + EB - 1) / EB, 256, sm, st>>>(K, Nq, Vq, Pq, c2q, lamQ, lamR, a, b, dt,
-                                                     rhs, z, grad);
+  k_adj_wadg<N><<<(K + EB - 1) / EB, 256, sm, st>>>(S, K, Nq, Vq, Pq, c2q, lamQ, lamR, a, b,
+                                                     dt, rhs, z, grad);
   return check_launch("adjoint WADG");
 }
 
 template <int N>
-static bbw_status launch_sigma_n(int K, const float *fgeo, const float *LIFT, const float *z,
-                                 float *sigma, cudaStream_t st) {
+static bbw_status launch_sigma_n(int S, int K, const float *fgeo, const float *LIFT,
+                                 const float *z, float *sigma, cudaStream_t st) {
   constexpr int EB = SURF_EB(N);
-  k_adj_sigma<N><<<(K + EB - 1) / EB, 256, 0, st>>>(K, fgeo, LIFT, z, sigma);
+  k_adj_sigma<N><<<(S * K + EB - 1) / EB, 256, 0, st>>>(S * K, K, fgeo, LIFT, z, sigma);
   return check_launch("adjoint lift");
 }
 
 template <int N>
-static bbw_status launch_gather_n(int K, int bc, float dt, const float *fgeo, const int *fidx,
-                                  const int *mapP, const float *sigma, const float *vol,
-                                  float *lamQ, cudaStream_t st) {
-  const long long n = (long long)K * NP(N);
-  k_adj_gather<N><<<(int)((n + 255) / 256), 256, 0, st>>>(K, bc, dt, fgeo, fidx, mapP, sigma,
-                                                           vol, lamQ);
+static bbw_status launch_gather_n(int S, int K, int bc, float dt, const float *fgeo,
+                                  const int *fidx, const int *mapP, const float *sigma,
+                                  const float *vol, float *lamQ, cudaStream_t st) {
+  const long long n = (long long)S * K * NP(N);
+  k_adj_gather<N><<<(int)((n + 255) / 256), 256, 0, st>>>(S * K, K, bc, dt, fgeo, fidx, mapP,
+                                                           sigma, vol, lamQ);
   return check_launch("adjoint face gather");
 }
 
@@ -221,25 +229,25 @@ static bbw_status launch_gather_n(int K, int bc, float dt, const float *fgeo, co
   }                                           \
   return set_error(BBW_ERR_UNSUPPORTED, "adjoint: N out of range");
 
-bbw_status adj_wadg(int N, int K, int Nq, const float *Vq, const float *Pq, const float *c2q,
+bbw_status adj_wadg(int N, int S, int K, int Nq, const float *Vq, const float *Pq, const float *c2q,
                     const float *lamQ, float *lamR, float a, float b, float dt, const float *rhs,
                     float *z, double *grad, cudaStream_t st) {
-#define CALL(n) launch_adj_n<n>(K, Nq, Vq, Pq, c2q, lamQ, lamR, a, b, dt, rhs, z, grad, st)
+#define CALL(n) launch_adj_n<n>(S, K, Nq, Vq, Pq, c2q, lamQ, lamR, a, b, dt, rhs, z, grad, st)
   BBW_N_SWITCH(CALL)
 #undef CALL
 }
 
-bbw_status adj_sigma(int N, int K, const float *fgeo, const float *LIFT, const float *z,
+bbw_status adj_sigma(int N, int S, int K, const float *fgeo, const float *LIFT, const float *z,
                      float *sigma, cudaStream_t st) {
-#define CALL(n) launch_sigma_n<n>(K, fgeo, LIFT, z, sigma, st)
+#define CALL(n) launch_sigma_n<n>(S, K, fgeo, LIFT, z, sigma, st)
   BBW_N_SWITCH(CALL)
 #undef CALL
 }
 
-bbw_status adj_gather(int N, int K, int bc, float dt, const float *fgeo, const int *fidx,
+bbw_status adj_gather(int N, int S, int K, int bc, float dt, const float *fgeo, const int *fidx,
                       const int *mapP, const float *sigma, const float *vol, float *lamQ,
                       cudaStream_t st) {
-#define CALL(n) launch_gather_n<n>(K, bc, dt, fgeo, fidx, mapP, sigma, vol, lamQ, st)
+#define CALL(n) launch_gather_n<n>(S, K, bc, dt, fgeo, fidx, mapP, sigma, vol, lamQ, st)
   BBW_N_SWITCH(CALL)
 #undef CALL
 }

@@ -18,7 +18,7 @@ namespace bbw {
 // ---------------------------------------------------------------- rk_volume
 // cpp/okl/WaveKernels.okl:44-153
 template <int N>
-__global__ void __launch_bounds__(256) k_rk_volume(int K, const float *__restrict__ vgeo,
+__global__ void __launch_bounds__(256) k_rk_volume(int K, int Kg, const float *__restrict__ vgeo,
                                                     const float *__restrict__ Dr,
                                                     const float *__restrict__ Ds,
                                                     const float *__restrict__ Dt,
@@ -29,8 +29,8 @@ __global__ void __launch_bounds__(256) k_rk_volume(int K, const float *__restric
   __shared__ float sG[EB][9];
   const int k0 = blockIdx.x * EB;
   for (int i = threadIdx.x; i < EB * 9; i += blockDim.x) {
-    const int e = i / 9;
-    if (k0 + e < K) sG[e][i % 9] = vgeo[(size_t)(k0 + e) * 9 + i % 9];
+    const int e = i / 9;  // geometry of element k is row k % Kg (shots share the mesh)
+    if (k0 + e < K) sG[e][i % 9] = vgeo[(size_t)((k0 + e) % Kg) * 9 + i % 9];
   }
   __syncthreads();
   for (int i = threadIdx.x; i < EB * Np; i += blockDim.x) {
@@ -96,7 +96,8 @@ __device__ __forceinline__ void upwind_flux(const float *__restrict__ Q, int idM
 // --------------------------------------------------------------- rk_surface
 // cpp/okl/WaveKernels.okl:156-260
 template <int N>
-__global__ void __launch_bounds__(256) k_rk_surface(int K, int bc, const float *__restrict__ fgeo,
+__global__ void __launch_bounds__(256) k_rk_surface(int K, int Kg, int bc,
+                                                     const float *__restrict__ fgeo,
                                                      const int *__restrict__ Fmask,
                                                      const int *__restrict__ vmapP,
                                                      const float *__restrict__ LIFT,
@@ -108,14 +109,16 @@ __global__ void __launch_bounds__(256) k_rk_surface(int K, int bc, const float *
   for (int i = threadIdx.x; i < EB * NF; i += blockDim.x) {
     const int e = i / NF, n = i % NF, k = k0 + e;
     if (k >= K) continue;
+    // mesh row of element k and its shot's first element (shots share the mesh)
+    const int kg = k % Kg, kb = k - kg;
     const int f = n / Nfp;
-    const float *fg = fgeo + (size_t)k * 16 + 4 * f;
+    const float *fg = fgeo + (size_t)kg * 16 + 4 * f;
     const float Fscale = fg[0], nx = fg[1], ny = fg[2], nz = fg[3];
     if (n % Nfp == 0) {
       s_nxyz[e][3 * f] = nx, s_nxyz[e][3 * f + 1] = ny, s_nxyz[e][3 * f + 2] = nz;
     }
-    upwind_flux(Q, Fmask[n] + k * Np * 4, vmapP[n + (size_t)k * NF], Np, Fscale, nx, ny, nz, bc,
-                s_pflux[e][n], s_Uflux[e][n]);
+    upwind_flux(Q, Fmask[n] + k * Np * 4, vmapP[n + (size_t)kg * NF] + kb * Np * 4, Np, Fscale, nx,
+                ny, nz, bc, s_pflux[e][n], s_Uflux[e][n]);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < EB * Np; i += blockDim.x) {
@@ -435,19 +438,21 @@ __global__ void __launch_bounds__(64) k_rk_surface_bern_slice(
 }
 
 template <int N>
-static bbw_status launch_volume(int K, const float *vgeo, const float *Dr, const float *Ds,
-                                const float *Dt, const float *Q, float *rhsQ, cudaStream_t st) {
+static bbw_status launch_volume(int K, int Kg, const float *vgeo, const float *Dr,
+                                const float *Ds, const float *Dt, const float *Q, float *rhsQ,
+                                cudaStream_t st) {
   constexpr int EB = VOL_EB(N);
-  k_rk_volume<N><<<(K + EB - 1) / EB, 256, 0, st>>>(K, vgeo, Dr, Ds, Dt, Q, rhsQ);
+  k_rk_volume<N><<<(K + EB - 1) / EB, 256, 0, st>>>(K, Kg, vgeo, Dr, Ds, Dt, Q, rhsQ);
   return check_launch("rk_volume");
 }
 
 template <int N>
-static bbw_status launch_surface(int K, int bc, const float *fgeo, const int *Fmask,
+static bbw_status launch_surface(int K, int Kg, int bc, const float *fgeo, const int *Fmask,
                                  const int *vmapP, const float *LIFT, const float *Q, float *rhsQ,
                                  cudaStream_t st) {
   constexpr int EB = SURF_EB(N);
-  k_rk_surface<N><<<(K + EB - 1) / EB, 256, 0, st>>>(K, bc, fgeo, Fmask, vmapP, LIFT, Q, rhsQ);
+  k_rk_surface<N><<<(K + EB - 1) / EB, 256, 0, st>>>(K, Kg, bc, fgeo, Fmask, vmapP, LIFT, Q,
+                                                      rhsQ);
   return check_launch("rk_surface");
 }
 
@@ -517,7 +522,7 @@ extern "C" bbw_status bbw_rk_volume(int N, int K, const float *vgeo, const float
     return set_error(BBW_ERR_ARG, "bbw_rk_volume: bad argument");
   if (K == 0) return BBW_OK;
   cudaStream_t st = (cudaStream_t)stream;
-#define CALL(n) launch_volume<n>(K, vgeo, Dr, Ds, Dt, Q, rhsQ, st)
+#define CALL(n) launch_volume<n>(K, K, vgeo, Dr, Ds, Dt, Q, rhsQ, st)
   switch (N) {
     case 1: return CALL(1);
     case 2: return CALL(2);
@@ -540,7 +545,7 @@ extern "C" bbw_status bbw_rk_surface(int N, int K, int bc, const float *fgeo, co
     return set_error(BBW_ERR_ARG, "bbw_rk_surface: bad argument");
   if (K == 0) return BBW_OK;
   cudaStream_t st = (cudaStream_t)stream;
-#define CALL(n) launch_surface<n>(K, bc, fgeo, Fmask, vmapP, LIFT, Q, rhsQ, st)
+#define CALL(n) launch_surface<n>(K, K, bc, fgeo, Fmask, vmapP, LIFT, Q, rhsQ, st)
   switch (N) {
     case 1: return CALL(1);
     case 2: return CALL(2);
@@ -674,3 +679,44 @@ extern "C" bbw_status bbw_rk_surface_bern_slice(int N, int K, int bc, const floa
 #undef CALL
   return set_error(BBW_ERR_UNSUPPORTED, "bbw_rk_surface_bern_slice: N out of range");
 }
+
+namespace bbw {
+
+// S shots of one mesh of K elements in one launch (state [S][K][4][Np])
+bbw_status rk_volume_shots(int N, int S, int K, const float *vgeo, const float *Dr,
+                           const float *Ds, const float *Dt, const float *Q, float *rhsQ,
+                           cudaStream_t st) {
+#define CALL(n) launch_volume<n>(S * K, K, vgeo, Dr, Ds, Dt, Q, rhsQ, st)
+  switch (N) {
+    case 1: return CALL(1);
+    case 2: return CALL(2);
+    case 3: return CALL(3);
+    case 4: return CALL(4);
+    case 5: return CALL(5);
+    case 6: return CALL(6);
+    case 7: return CALL(7);
+    case 8: return CALL(8);
+  }
+#undef CALL
+  return set_error(BBW_ERR_UNSUPPORTED, "volume: N out of range");
+}
+
+bbw_status rk_surface_shots(int N, int S, int K, int bc, const float *fgeo, const int *Fmask,
+                            const int *vmapP, const float *LIFT, const float *Q, float *rhsQ,
+                            cudaStream_t st) {
+#define CALL(n) launch_surface<n>(S * K, K, bc, fgeo, Fmask, vmapP, LIFT, Q, rhsQ, st)
+  switch (N) {
+    case 1: return CALL(1);
+    case 2: return CALL(2);
+    case 3: return CALL(3);
+    case 4: return CALL(4);
+    case 5: return CALL(5);
+    case 6: return CALL(6);
+    case 7: return CALL(7);
+    case 8: return CALL(8);
+  }
+#undef CALL
+  return set_error(BBW_ERR_UNSUPPORTED, "surface: N out of range");
+}
+
+}  // namespace bbw
