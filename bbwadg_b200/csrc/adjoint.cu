@@ -195,12 +195,11 @@ extern "C" bbw_status bbw_backward(bbw_ctx *c, bbw_tape *t, const float *dL_dtra
   if (s != BBW_OK) return s;
   const int N = c->N, K = c->K, Np = c->Np, Nq = c->Nq, NF = 4 * c->Nfp, S = c->S, R = c->R;
   const int nsteps = t->nsteps, every = t->every;
-  const size_t shot = (size_t)K * 4 * Np;
   const float dt = t->dt;
   cudaStream_t st = c->stream;
   const AdjOps &a = c->adj;
   DevBuf buf;
-  float *lamQ, *lamR, *z, *rhs, *sigma, *res, *g, *seg, *stq;
+  float *lamQ, *lamR, *z, *rhs, *sigma, *res, *g, *seg, *stq, *vq;
   double *grad, *tdev;
   const int seglen = std::min(every, nsteps);
   if ((s = buf.get(&lamQ, t->state, "bbw_backward")) != BBW_OK ||
@@ -212,6 +211,7 @@ extern "C" bbw_status bbw_backward(bbw_ctx *c, bbw_tape *t, const float *dL_dtra
       (s = buf.get(&g, (size_t)S * R * nsteps, "bbw_backward")) != BBW_OK ||
       (s = buf.get(&seg, (size_t)seglen * t->state, "bbw_backward: segment states")) != BBW_OK ||
       (s = buf.get(&stq, (size_t)5 * t->state, "bbw_backward: stage states")) != BBW_OK ||
+      (s = buf.get(&vq, (size_t)5 * S * Nq * K, "bbw_backward: cubature values")) != BBW_OK ||
       (s = buf.get(&grad, (size_t)K * Nq, "bbw_backward")) != BBW_OK ||
       (s = buf.get(&tdev, 1, "bbw_backward")) != BBW_OK)
     return s;
@@ -226,8 +226,15 @@ extern "C" bbw_status bbw_backward(bbw_ctx *c, bbw_tape *t, const float *dL_dtra
   std::vector<double> tn(nsteps + 1);
   tn[0] = t->t0;
   for (int n = 0; n < nsteps; ++n) tn[n + 1] = tn[n] + (double)dt;
+  FusedPlan pv = pl;  // same stage, also storing Vq S(Q)_p at the cubature points
   auto stage = [&](int i, const float *in, float *outq) {
     return fused_launch(pl, in, outq, res, (float)kRK4A[i], (float)kRK4B[i], dt,
+                        c->src_stage_times ? (float)kRK4C[i] : 0.f, st);
+  };
+  const size_t vqn = (size_t)S * Nq * K;  // per stage
+  auto stage_v = [&](int i, const float *in, float *outq) {
+    pv.vq_out = vq + (size_t)i * vqn;
+    return fused_launch(pv, in, outq, res, (float)kRK4A[i], (float)kRK4B[i], dt,
                         c->src_stage_times ? (float)kRK4C[i] : 0.f, st);
   };
   auto step_fwd = [&](int n, const float *in, float *outq) {  // stage outputs in stq[1..4]
@@ -255,30 +262,24 @@ extern "C" bbw_status bbw_backward(bbw_ctx *c, bbw_tape *t, const float *dL_dtra
       if ((s = adj_receivers(S, K, Np, R, c->rec_elem, c->rec_w, g, nsteps, n, lamQ, st)) !=
           BBW_OK)
         return s;
-      // stage inputs: stq[0] = step start, stq[1..4] recomputed (the step's
-      // output lands in stq[0]'s slot, which is not needed any more)
-      e = cudaMemcpyAsync(stq, seg + (size_t)j * t->state, t->state * sizeof(float),
-                          cudaMemcpyDeviceToDevice, st);
-      if (e != cudaSuccess) return set_cuda_error(e, "bbw_backward: stage state");
+      // the step's five stages again from its start state (bit-identical to
+      // the forward), keeping each stage's Vq S(Q)_p; stage inputs in stq
+      // (stq[0] = step start), the step's output into z (scratch until the
+      // adjoint stages below overwrite it)
       if ((s = set_device_double(tdev, tn[n], st)) != BBW_OK) return s;
       {
-        const float *q = stq;
-        for (int i = 0; i < 4 && s == BBW_OK; ++i) {
-          float *o = stq + (size_t)(i + 1) * t->state;
-          s = stage(i, q, o);
+        const float *q = seg + (size_t)j * t->state;
+        for (int i = 0; i < 5 && s == BBW_OK; ++i) {
+          float *o = i < 4 ? stq + (size_t)(i + 1) * t->state : z;
+          s = stage_v(i, q, o);
           q = o;
         }
         if (s != BBW_OK) return s;
       }
       for (int i = 4; i >= 0; --i) {
         const float ai = (float)kRK4A[i], bi = (float)kRK4B[i];
-        const float *Qi = stq + (size_t)i * t->state;
-        if ((s = rk_volume_shots(N, S, K, c->vgeo, a.D[0], a.D[1], a.D[2], Qi, rhs, st)) !=
-                BBW_OK ||
-            (s = rk_surface_shots(N, S, K, c->bc, c->fgeo, a.Fmask, a.vmapP, a.LIFT, Qi, rhs,
-                                  st)) != BBW_OK ||
-            (s = adj_wadg(N, S, K, Nq, a.Vq, a.Pq, pl.c2q, lamQ, lamR, ai, bi, dt, rhs, z, grad,
-                          st)) != BBW_OK ||
+        if ((s = adj_wadg(N, S, K, Nq, a.Vq, a.Pq, pl.c2q, lamQ, lamR, ai, bi, dt,
+                          vq + (size_t)i * vqn, z, grad, st)) != BBW_OK ||
             (s = rk_volume_shots(N, S, K, c->vgeo, a.DT[0], a.DT[1], a.DT[2], z, rhs, st)) !=
                 BBW_OK ||
             (s = adj_sigma(N, S, K, c->fgeo, a.LIFT, z, sigma, st)) != BBW_OK ||
@@ -289,8 +290,12 @@ extern "C" bbw_status bbw_backward(bbw_ctx *c, bbw_tape *t, const float *dL_dtra
     }
   }
   e = cudaStreamSynchronize(st);
+  std::vector<double> gq((size_t)K * Nq);  // device layout [Nq][K]
   if (e == cudaSuccess)
-    e = cudaMemcpy(dL_dc2q, grad, (size_t)K * Nq * sizeof(double), cudaMemcpyDeviceToHost);
+    e = cudaMemcpy(gq.data(), grad, gq.size() * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess)
+    for (int k = 0; k < K; ++k)
+      for (int q = 0; q < Nq; ++q) dL_dc2q[(size_t)k * Nq + q] = gq[(size_t)q * K + k];
   if (e == cudaSuccess && dL_dQ0)
     e = cudaMemcpy(dL_dQ0, lamQ, t->state * sizeof(float), cudaMemcpyDeviceToHost);
   return set_cuda_error(e, "bbw_backward: download");

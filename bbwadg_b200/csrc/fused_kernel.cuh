@@ -107,6 +107,9 @@ struct FusedParams {
   const float *__restrict__ src_vec;
   float f0, tR, samp, cstage;
   const double *__restrict__ time;  // simulation time at the start of the step
+  // optional: Vq (raw rhs_p) at the cubature points, before c2/J, stored as
+  // [shot][Nq][K] (the c^2 gradient of the discrete adjoint needs it)
+  float *__restrict__ vq_out;
 };
 
 // Ricker wavelet amp (1 - 2 a^2) exp(-a^2), a = pi f0 (t - tR)
@@ -537,7 +540,11 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
 #pragma unroll
         for (int j = 0; j < QB; ++j) {
           const int q = q0 + qb + j;
-          if (qb + j < RQ && q < Nq) sQuad[q * ES + lane] = pick(acc, j) * sC2[q * ES + lane];
+          if (qb + j < RQ && q < Nq) {
+            sQuad[q * ES + lane] = pick(acc, j) * sC2[q * ES + lane];
+            if (P.vq_out && lane < ne)
+              P.vq_out[((size_t)shot * Nq + q) * P.K + k0 + lane] = pick(acc, j);
+          }
         }
       }
     }
@@ -668,6 +675,7 @@ static bbw_status launch_fused(const FusedPlan &pl, const float *Qin, float *Qou
   P.src_off = pl.src_off, P.src_elem = pl.src_elem, P.src_vec = pl.src_vec;
   P.f0 = pl.f0, P.tR = pl.tR, P.samp = pl.samp, P.cstage = cstage;
   P.time = pl.time;
+  P.vq_out = pl.vq_out;
   const bool os = pl.ops_smem > 0;
   const size_t sm = pl.smem;
   const int grid = std::min(cdiv(pl.Kc > 0 ? pl.Kc : pl.K, TILE_E) * std::max(pl.S, 1), pl.nsm);

@@ -27,92 +27,106 @@
 
 namespace bbw {
 
-// mu = lamR + b lamQ; lamR <- a mu; z <- W^T mu; grad += dt t (Vq r_p)
+constexpr int AE = 32;   // elements per CTA (lane = element)
+constexpr int AW = 8;    // warps per CTA
+constexpr int AS = AE + 1;  // shared row stride
+
+// mu = lamR + b lamQ; lamR <- a mu; z <- W^T mu; grad[q][k] += dt t_q v_q with
+// t = Pq^T mu_p and v = Vq S(Q)_p stored by the forward recomputation
+// ([shot][Nq][K]).  Lane = element, warps own rows; operator values are warp
+// broadcasts.  The shots of a tile are done in turn, so every gradient
+// entry is accumulated by one thread in shot order.
 template <int N>
-__global__ void __launch_bounds__(256) k_adj_wadg(int S, int K, int Nq, const float *__restrict__ Vq,
-                                                  const float *__restrict__ Pq,
-                                                  const float *__restrict__ c2q,
-                                                  const float *__restrict__ lamQ,
-                                                  float *__restrict__ lamR, float a, float b,
-                                                  float dt, const float *__restrict__ rhs,
-                                                  float *__restrict__ z,
-                                                  double *__restrict__ grad) {
-  constexpr int Np = NP(N), EB = UPD_EB(N);
+__global__ void __launch_bounds__(AE * AW) k_adj_wadg(int S, int K, int Nq,
+                                                     const float *__restrict__ Vq,
+                                                     const float *__restrict__ Pq,
+                                                     const float *__restrict__ c2q,
+                                                     const float *__restrict__ lamQ,
+                                                     float *__restrict__ lamR, float a, float b,
+                                                     float dt, const float *__restrict__ vq,
+                                                     float *__restrict__ z,
+                                                     double *__restrict__ grad) {
+  constexpr int Np = NP(N);
   extern __shared__ float smem[];
-  float *s_mu = smem;                // [EB][Np]  mu_p
-  float *s_r = s_mu + EB * Np;       // [EB][Np]  forward raw rhs_p
-  float *s_t = s_r + EB * Np;        // [EB][Nq]  c2 * Pq^T mu_p
-  const int k0 = blockIdx.x * EB;
-  // the shots of one element block in turn: each (k, q) gradient entry is
-  // accumulated by one thread, in shot order
+  float *sMu = smem;               // [Np][AS]
+  float *sZ = sMu + Np * AS;       // [Np][AS]
+  float *sT = sZ + Np * AS;        // [Nq][AS]
+  float *sC = sT + Nq * AS;        // [Nq][AS] c2/J
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int k0 = blockIdx.x * AE, ne = min(AE, K - k0);
+  for (int i = tid; i < ne * Nq; i += AE * AW) sC[(i % Nq) * AS + i / Nq] = c2q[(size_t)k0 * Nq + i];
   for (int sh = 0; sh < S; ++sh) {
-    const size_t so = (size_t)sh * K * 4 * Np;
-    if (sh > 0) __syncthreads();  // shared arrays free
-    for (int i = threadIdx.x; i < EB * 4 * Np; i += blockDim.x) {
+    const size_t so = (size_t)sh * K * 4 * Np + (size_t)k0 * 4 * Np;
+    __syncthreads();
+    for (int i = tid; i < ne * 4 * Np; i += AE * AW) {
       const int e = i / (4 * Np), fn = i - e * 4 * Np;
-      if (k0 + e >= K) continue;
-      const size_t id = so + (size_t)k0 * 4 * Np + i;
-      const float mu = lamR[id] + b * lamQ[id];
-      lamR[id] = a * mu;
-      if (fn < Np) {
-        s_mu[e * Np + fn] = mu;
-        s_r[e * Np + fn] = rhs ? rhs[id] : 0.f;
-      } else {
-        z[id] = mu;  // velocity rows: Pq Vq = I (J = 1)
+      const float mu = lamR[so + i] + b * lamQ[so + i];
+      lamR[so + i] = a * mu;
+      if (fn < Np) sMu[fn * AS + e] = mu;
+      else z[so + i] = mu;  // velocity rows: Pq Vq = I (J = 1)
+    }
+    __syncthreads();
+    for (int q = warp; q < Nq; q += AW) {
+      float t = 0.f;
+#pragma unroll 5
+      for (int n = 0; n < Np; ++n) t += __ldg(Pq + n + (size_t)q * Np) * sMu[n * AS + lane];
+      if (lane < ne) {
+        const size_t g = (size_t)q * K + k0 + lane;
+        if (vq) grad[g] += (double)dt * (double)t * (double)vq[((size_t)sh * Nq + q) * K + k0 + lane];
+        sT[q * AS + lane] = sC[q * AS + lane] * t;
       }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < EB * Nq; i += blockDim.x) {
-      const int e = i / Nq, q = i - e * Nq, k = k0 + e;
-      if (k >= K) continue;
-      const float *mu = s_mu + e * Np, *r = s_r + e * Np;
-      float t = 0.f, v = 0.f;
-      for (int n = 0; n < Np; ++n) {
-        t += __ldg(Pq + n + (size_t)q * Np) * mu[n];
-        v += __ldg(Vq + q + (size_t)n * Nq) * r[n];
-      }
-      if (rhs) grad[(size_t)k * Nq + q] += (double)dt * (double)t * (double)v;
-      s_t[e * Nq + q] = c2q[(size_t)k * Nq + q] * t;
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < EB * Np; i += blockDim.x) {
-      const int e = i / Np, n = i - e * Np, k = k0 + e;
-      if (k >= K) continue;
-      const float *t = s_t + e * Nq;
+    for (int n = warp; n < Np; n += AW) {
       float acc = 0.f;
-      for (int q = 0; q < Nq; ++q) acc += __ldg(Vq + q + (size_t)n * Nq) * t[q];
-      z[so + (size_t)k * 4 * Np + n] = acc;
+      for (int q = 0; q < Nq; ++q) acc += __ldg(Vq + q + (size_t)n * Nq) * sT[q * AS + lane];
+      sZ[n * AS + lane] = acc;
+    }
+    __syncthreads();
+    for (int i = tid; i < ne * Np; i += AE * AW) {
+      const int e = i / Np, n = i - e * Np;
+      z[so + (size_t)e * 4 * Np + n] = sZ[n * AS + e];
     }
   }
 }
 
-// sigma[k][m] = .5 Fscale_f sum_n LIFT[n + m Np] (z_p[n] - n_f . z_U[n])
+// sigma[k][m] = .5 Fscale_f sum_n LIFT[n + m Np] (z_p[n] - n_f . z_U[n]) for the
+// S*K elements of all shots (geometry row k % Kg); lane = element
 template <int N>
-__global__ void __launch_bounds__(256) k_adj_sigma(int K, int Kg, const float *__restrict__ fgeo,
-                                                   const float *__restrict__ LIFT,
-                                                   const float *__restrict__ z,
-                                                   float *__restrict__ sigma) {
-  constexpr int Np = NP(N), Nfp = NFP(N), NF = 4 * NFP(N), EB = SURF_EB(N);
-  __shared__ float sz[EB][4 * Np];
-  const int k0 = blockIdx.x * EB;
-  for (int i = threadIdx.x; i < EB * 4 * Np; i += blockDim.x) {
-    const int e = i / (4 * Np);
-    if (k0 + e < K) sz[e][i - e * 4 * Np] = z[(size_t)k0 * 4 * Np + i];
+__global__ void __launch_bounds__(AE * AW) k_adj_sigma(int K, int Kg,
+                                                      const float *__restrict__ fgeo,
+                                                      const float *__restrict__ LIFT,
+                                                      const float *__restrict__ z,
+                                                      float *__restrict__ sigma) {
+  constexpr int Np = NP(N), Nfp = NFP(N), NF = 4 * NFP(N);
+  extern __shared__ float smem[];
+  float *sZ = smem;                 // [4Np][AS]
+  float *sO = sZ + 4 * Np * AS;     // [NF][AS]
+  float *sG = sO + NF * AS;         // [AE][16]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int k0 = blockIdx.x * AE, ne = min(AE, K - k0);
+  for (int i = tid; i < ne * 4 * Np; i += AE * AW)
+    sZ[(i % (4 * Np)) * AS + i / (4 * Np)] = z[(size_t)k0 * 4 * Np + i];
+  for (int i = tid; i < ne * 16; i += AE * AW)
+    sG[i] = fgeo[(size_t)((k0 + i / 16) % Kg) * 16 + i % 16];
+  __syncthreads();
+  for (int m = warp; m < NF; m += AW) {
+    const int f = m / Nfp;
+    const int e = lane < ne ? lane : 0;
+    const float Fs = sG[e * 16 + 4 * f], nx = sG[e * 16 + 4 * f + 1], ny = sG[e * 16 + 4 * f + 2],
+                nz = sG[e * 16 + 4 * f + 3];
+    float acc = 0.f;
+#pragma unroll 5
+    for (int n = 0; n < Np; ++n) {
+      const float w = sZ[n * AS + lane] - (nx * sZ[(Np + n) * AS + lane] +
+                                           ny * sZ[(2 * Np + n) * AS + lane] +
+                                           nz * sZ[(3 * Np + n) * AS + lane]);
+      acc += __ldg(LIFT + n + (size_t)m * Np) * w;
+    }
+    sO[m * AS + lane] = .5f * Fs * acc;
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < EB * NF; i += blockDim.x) {
-    const int e = i / NF, m = i - e * NF, k = k0 + e;
-    if (k >= K) continue;
-    const int f = m / Nfp;
-    const float *fg = fgeo + (size_t)(k % Kg) * 16 + 4 * f;
-    const float Fscale = fg[0], nx = fg[1], ny = fg[2], nz = fg[3];
-    const float *w = sz[e];
-    float acc = 0.f;
-    for (int n = 0; n < Np; ++n)
-      acc += __ldg(LIFT + n + (size_t)m * Np) *
-             (w[n] - (nx * w[Np + n] + ny * w[2 * Np + n] + nz * w[3 * Np + n]));
-    sigma[(size_t)k * NF + m] = .5f * Fscale * acc;
-  }
+  for (int i = tid; i < ne * NF; i += AE * AW) sigma[(size_t)k0 * NF + i] = sO[(i % NF) * AS + i / NF];
 }
 
 // lamQ[k][.][n] += dt (vol[k][.][n] + surface adjoint at node n)
@@ -183,26 +197,34 @@ __global__ void k_set_double(double *p, double v) { *p = v; }
 
 // ------------------------------------------------------------- host side
 template <int N>
-static bbw_status launch_adj_n(int S, int K, int Nq, const float *Vq, const float *Pq, const float *c2q,
-                               const float *lamQ, float *lamR, float a, float b, float dt,
-                               const float *rhs, float *z, double *grad, cudaStream_t st) {
-  constexpr int Np = NP(N), EB = UPD_EB(N);
-  const size_t sm = (size_t)EB * (2 * Np + Nq) * sizeof(float);
+static bbw_status launch_adj_n(int S, int K, int Nq, const float *Vq, const float *Pq,
+                               const float *c2q, const float *lamQ, float *lamR, float a, float b,
+                               float dt, const float *vq, float *z, double *grad,
+                               cudaStream_t st) {
+  constexpr int Np = NP(N);
+  const size_t sm = sizeof(float) * (size_t)AS * (2 * Np + 2 * Nq);
+  if (sm > 200 * 1024) return set_error(BBW_ERR_UNSUPPORTED, "adjoint WADG: Nq too large");
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_adj_wadg<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr = true;
   }
-  k_adj_wadg<N><<<(K + EB - 1) / EB, 256, sm, st>>>(S, K, Nq, Vq, Pq, c2q, lamQ, lamR, a, b,
-                                                     dt, rhs, z, grad);
+  k_adj_wadg<N><<<(K + AE - 1) / AE, AE * AW, sm, st>>>(S, K, Nq, Vq, Pq, c2q, lamQ, lamR, a, b,
+                                                        dt, vq, z, grad);
   return check_launch("adjoint WADG");
 }
 
 template <int N>
 static bbw_status launch_sigma_n(int S, int K, const float *fgeo, const float *LIFT,
                                  const float *z, float *sigma, cudaStream_t st) {
-  constexpr int EB = SURF_EB(N);
-  k_adj_sigma<N><<<(S * K + EB - 1) / EB, 256, 0, st>>>(S * K, K, fgeo, LIFT, z, sigma);
+  constexpr int Np = NP(N), NF = 4 * NFP(N);
+  const size_t sm = sizeof(float) * ((size_t)AS * (4 * Np + NF) + AE * 16);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_adj_sigma<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr = true;
+  }
+  k_adj_sigma<N><<<(S * K + AE - 1) / AE, AE * AW, sm, st>>>(S * K, K, fgeo, LIFT, z, sigma);
   return check_launch("adjoint lift");
 }
 
@@ -230,9 +252,9 @@ static bbw_status launch_gather_n(int S, int K, int bc, float dt, const float *f
   return set_error(BBW_ERR_UNSUPPORTED, "adjoint: N out of range");
 
 bbw_status adj_wadg(int N, int S, int K, int Nq, const float *Vq, const float *Pq, const float *c2q,
-                    const float *lamQ, float *lamR, float a, float b, float dt, const float *rhs,
+                    const float *lamQ, float *lamR, float a, float b, float dt, const float *vq,
                     float *z, double *grad, cudaStream_t st) {
-#define CALL(n) launch_adj_n<n>(S, K, Nq, Vq, Pq, c2q, lamQ, lamR, a, b, dt, rhs, z, grad, st)
+#define CALL(n) launch_adj_n<n>(S, K, Nq, Vq, Pq, c2q, lamQ, lamR, a, b, dt, vq, z, grad, st)
   BBW_N_SWITCH(CALL)
 #undef CALL
 }
