@@ -248,26 +248,60 @@ extern "C" bbw_status bbw_backward(bbw_ctx *c, bbw_tape *t, const float *dL_dtra
     return r;
   };
 
+  // Segment store: when the device has room, one forward pass per segment
+  // keeps the cubature values of every stage of the segment (vq_all), so the
+  // reverse sweep needs no second recomputation (the adjoint stages need only
+  // those values, not the forward states).
+  float *vq_all = nullptr;
+  {
+    size_t fr = 0, tot = 0;
+    const size_t need = (size_t)seglen * 5 * vqn * sizeof(float);
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && need + ((size_t)2 << 30) < fr &&
+        buf.get(&vq_all, (size_t)seglen * 5 * vqn, "bbw_backward") != BBW_OK)
+      vq_all = nullptr;  // fall back to recomputing each step again in the sweep
+  }
   const int nseg = (nsteps + every - 1) / every;
   for (int sg = nseg - 1; sg >= 0; --sg) {
     const int n0 = sg * every, len = std::min(every, nsteps - n0);
-    e = cudaMemcpyAsync(seg, t->ck[sg], t->state * sizeof(float), cudaMemcpyDeviceToDevice, st);
-    if (e != cudaSuccess) return set_cuda_error(e, "bbw_backward: segment");
-    for (int j = 1; j < len; ++j)
-      if ((s = step_fwd(n0 + j - 1, seg + (size_t)(j - 1) * t->state,
-                        seg + (size_t)j * t->state)) != BBW_OK)
-        return s;
+    if (vq_all) {
+      // forward over the segment; stage outputs chain through stq[1..4] and
+      // the step outputs alternate between z and seg
+      const float *q = t->ck[sg];
+      for (int j = 0; j < len; ++j) {
+        if ((s = set_device_double(tdev, tn[n0 + j], st)) != BBW_OK) return s;
+        float *out = (j & 1) ? seg : z;
+        const float *qi = q;
+        for (int i = 0; i < 5; ++i) {
+          float *o = i < 4 ? stq + (size_t)(i + 1) * t->state : out;
+          pv.vq_out = vq_all + ((size_t)j * 5 + i) * vqn;
+          if ((s = fused_launch(pv, qi, o, res, (float)kRK4A[i], (float)kRK4B[i], dt,
+                                c->src_stage_times ? (float)kRK4C[i] : 0.f, st)) != BBW_OK)
+            return s;
+          qi = o;
+        }
+        q = out;
+      }
+    } else {
+      e = cudaMemcpyAsync(seg, t->ck[sg], t->state * sizeof(float), cudaMemcpyDeviceToDevice, st);
+      if (e != cudaSuccess) return set_cuda_error(e, "bbw_backward: segment");
+      for (int j = 1; j < len; ++j)
+        if ((s = step_fwd(n0 + j - 1, seg + (size_t)(j - 1) * t->state,
+                          seg + (size_t)j * t->state)) != BBW_OK)
+          return s;
+    }
     for (int j = len - 1; j >= 0; --j) {
       const int n = n0 + j;
       if ((s = adj_receivers(S, K, Np, R, c->rec_elem, c->rec_w, g, nsteps, n, lamQ, st)) !=
           BBW_OK)
         return s;
-      // the step's five stages again from its start state (bit-identical to
-      // the forward), keeping each stage's Vq S(Q)_p; stage inputs in stq
-      // (stq[0] = step start), the step's output into z (scratch until the
-      // adjoint stages below overwrite it)
-      if ((s = set_device_double(tdev, tn[n], st)) != BBW_OK) return s;
-      {
+      const float *vqs = vq;
+      if (vq_all) {
+        vqs = vq_all + (size_t)j * 5 * vqn;
+      } else {
+        // the step's five stages again from its start state (bit-identical
+        // to the forward), keeping each stage's Vq S(Q)_p; the step's output
+        // goes to z (scratch until the adjoint stages below overwrite it)
+        if ((s = set_device_double(tdev, tn[n], st)) != BBW_OK) return s;
         const float *q = seg + (size_t)j * t->state;
         for (int i = 0; i < 5 && s == BBW_OK; ++i) {
           float *o = i < 4 ? stq + (size_t)(i + 1) * t->state : z;
@@ -279,7 +313,7 @@ extern "C" bbw_status bbw_backward(bbw_ctx *c, bbw_tape *t, const float *dL_dtra
       for (int i = 4; i >= 0; --i) {
         const float ai = (float)kRK4A[i], bi = (float)kRK4B[i];
         if ((s = adj_wadg(N, S, K, Nq, a.Vq, a.Pq, pl.c2q, lamQ, lamR, ai, bi, dt,
-                          vq + (size_t)i * vqn, z, grad, st)) != BBW_OK ||
+                          vqs + (size_t)i * vqn, z, grad, st)) != BBW_OK ||
             (s = rk_volume_shots(N, S, K, c->vgeo, a.DT[0], a.DT[1], a.DT[2], z, rhs, st)) !=
                 BBW_OK ||
             (s = adj_sigma(N, S, K, c->fgeo, a.LIFT, z, sigma, st)) != BBW_OK ||
