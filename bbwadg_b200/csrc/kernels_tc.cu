@@ -54,7 +54,10 @@ struct TcCfg {
   static constexpr int KV = r16(Np), KF = r16(Nfp);
   // raw state row stride (floats): multiple of 4 with RS/4 odd
   static constexpr int RS = (Np % 2) ? 4 * Np : 4 * Np + 4;
-  static constexpr int FIT = cdv(TC_E * NF, TC_T);
+  // flux items with lane = face node: (element, face) pairs per warp
+  static constexpr int FPW = (4 * TC_E) / (TC_T / 32);
+  static_assert((4 * TC_E) % (TC_T / 32) == 0, "face pairs per warp");
+  static_assert(NFP(N) <= 32, "one face per warp pass");
   static_assert(Np <= 64 && Np % 4 == 0, "tensor-core stage: Np <= 64, Np % 4 == 0");
 };
 
@@ -154,7 +157,7 @@ template <int N>
 __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
   using C = TcCfg<N>;
   constexpr int Np = C::Np, Nfp = C::Nfp, NF = C::NF, KV = C::KV, KF = C::KF, RS = C::RS;
-  constexpr int FIT = C::FIT;
+  constexpr int FPW = C::FPW;
   extern __shared__ __align__(1024) unsigned char smem[];
   const TcLayout &L = P.L;
   const int KQ = L.KQ, MQ = L.MQ, Nq = P.Nq;
@@ -237,24 +240,24 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
   };
 
   // face traces of neighbours outside tile `tile` (whose inputs have landed)
-  // into registers; traces inside the tile are read from shared memory in P1
-  float nbv[FIT][4];
+  // into registers.  Lane = face node, warp = (element, face) pairs: one load
+  // instruction reads the face of a single neighbour (a few sectors) instead
+  // of one node of 32 neighbours.  Traces inside the tile are read from
+  // shared memory in P1.
+  float nbv[FPW][4];
   auto load_traces = [&](int tile) {
     const int k0 = tile * TC_E, ne = min(TC_E, P.K - k0);
 #pragma unroll
-    for (int j = 0; j < FIT; ++j) {
+    for (int j = 0; j < FPW; ++j) {
       nbv[j][0] = nbv[j][1] = nbv[j][2] = nbv[j][3] = 0.f;
-      const int i = tid + j * TC_T;
-      if (i >= TC_E * NF) continue;
-      const int e = i & 31, m = i >> 5, f = m / Nfp;
-      if (e >= ne) continue;
+      const int pp = warp * FPW + j, e = pp >> 2, f = pp & 3;
+      if (lane >= Nfp || e >= ne) continue;
       const int code = sNbr[e * 4 + f];
       const int pat = code & 255;
       if (pat == 255) continue;
-      const int vP = sPat[pat * Nfp + (m - f * Nfp)];
       const unsigned rel = (unsigned)((code >> 8) - k0);
       if (rel < (unsigned)ne) continue;
-      const float *o = P.Qin + (size_t)(code >> 8) * 4 * Np + vP;
+      const float *o = P.Qin + (size_t)(code >> 8) * 4 * Np + sPat[pat * Nfp + lane];
       nbv[j][0] = __ldg(o), nbv[j][1] = __ldg(o + Np), nbv[j][2] = __ldg(o + 2 * Np),
       nbv[j][3] = __ldg(o + 3 * Np);
     }
@@ -303,16 +306,16 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       }
       mp = fmaxf(fmaxf(fabsf(p4.x), fabsf(p4.y)), fmaxf(fabsf(p4.z), fabsf(p4.w)));
     }
-    // upwind flux (Uflux = -pflux): last, its outside traces have had longest
-    float pf[FIT];
+    // upwind flux (Uflux = -pflux), lane = face node: last, its outside
+    // traces have had longest
+    float pf[FPW];
     float mF = 0.f;
 #pragma unroll
-    for (int j = 0; j < FIT; ++j) {
+    for (int j = 0; j < FPW; ++j) {
       pf[j] = 0.f;
-      const int i = tid + j * TC_T;
-      if (i >= TC_E * NF) continue;
-      const int e = i & 31, m = i >> 5, f = m / Nfp;
-      if (e >= ne) continue;
+      const int pp = warp * FPW + j, e = pp >> 2, f = pp & 3;
+      if (lane >= Nfp || e >= ne) continue;
+      const int m = f * Nfp + lane;
       const int code = sNbr[e * 4 + f];
       const int pat = code & 255;
       const int vM = sFmask[m];
@@ -333,7 +336,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
         const unsigned rel = (unsigned)((code >> 8) - k0);
         float pP = nbv[j][0], uP = nbv[j][1], vP_ = nbv[j][2], wP = nbv[j][3];
         if (rel < (unsigned)ne) {  // neighbour inside the tile
-          const float *o = sRaw + rel * RS + sPat[pat * Nfp + (m - f * Nfp)];
+          const float *o = sRaw + rel * RS + sPat[pat * Nfp + lane];
           pP = o[0], uP = o[Np], vP_ = o[2 * Np], wP = o[3 * Np];
         }
         pjump = pP - pM;
@@ -361,11 +364,10 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
         split_store4(sBU + 2 * d * TC_E * KV + o, sBU + (2 * d + 1) * TC_E * KV + o, U4[d], sU);
     }
 #pragma unroll
-    for (int j = 0; j < FIT; ++j) {
-      const int i = tid + j * TC_T;
-      if (i >= TC_E * NF) continue;
-      const int e = i & 31, m = i >> 5, f = m / Nfp;
-      const int o = tc::kmajor_offset_f16(e, m - f * Nfp, KF);
+    for (int j = 0; j < FPW; ++j) {
+      const int pp = warp * FPW + j, e = pp >> 2, f = pp & 3;
+      if (lane >= Nfp) continue;  // absent elements store zeros (pf = 0)
+      const int o = tc::kmajor_offset_f16(e, lane, KF);
       split_store1(sBF + 2 * f * TC_E * KF + o, sBF + (2 * f + 1) * TC_E * KF + o, pf[j] * sF);
     }
     sync_for_mma();
