@@ -408,12 +408,8 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
     float rp[8];
     {
       float gr[8], gs[8], gt[8], dv[8], lf[4][8];
-      tc::tmem_ld8(trow + 0, gr);
-      tc::tmem_ld8(trow + 32, gs);
-      tc::tmem_ld8(trow + 64, gt);
-      tc::tmem_ld8(trow + 96, dv);
-#pragma unroll
-      for (int f = 0; f < 4; ++f) tc::tmem_ld8(trow + 128 + 32 * f, lf[f]);
+      tc::tmem_ld8x4(trow + 0, trow + 32, trow + 64, trow + 96, gr, gs, gt, dv);
+      tc::tmem_ld8x4(trow + 128, trow + 160, trow + 192, trow + 224, lf[0], lf[1], lf[2], lf[3]);
       const float isp = 1.f / sp, isU = 1.f / sU, isF = 1.f / sF;
       float mr = 0.f;
 #pragma unroll
