@@ -39,6 +39,16 @@ class OpsDesc(ctypes.Structure):
                 ("EEL_vals", P), ("L0_vals", P), ("Vq", P), ("Pq", P)]
 
 
+class CurvedDesc(ctypes.Structure):
+    _fields_ = [("N", c_int), ("K", c_int), ("Nq", c_int), ("Nfq", c_int), ("Nq_reduced", c_int),
+                ("KCurved", c_int), ("KPlanar", c_int), ("KlistCurved", P), ("KlistPlanar", P),
+                ("vgeo", P), ("fgeo", P), ("Jplanar", P), ("Fmask", P), ("vmapP", P),
+                ("vgeoq", P), ("Jq", P), ("fgeoq", P), ("Jq_reduced", P), ("c2q", P),
+                ("Dr", P), ("Ds", P), ("Dt", P), ("LIFT", P), ("Vq", P), ("Vrq", P), ("Vsq", P),
+                ("Vtq", P), ("Pq", P), ("Prq", P), ("Psq", P), ("Ptq", P), ("VfqFace", P),
+                ("Pfq", P), ("Vq_reduced", P), ("Pq_reduced", P)]
+
+
 # name -> (restype, argtypes); every function returns bbw_status unless noted
 SIGNATURES = {
     "bbw_status_string": (ctypes.c_char_p, [c_int]),
@@ -95,6 +105,21 @@ SIGNATURES = {
     "bbw_tape_free": (c_int, [c_void_p]),
     "bbw_device_state": (c_int, [c_void_p, ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p),
                                  ctypes.POINTER(c_void_p)]),
+    "bbw_gordon_hall_sphere": (c_int, [c_int, c_int, P, P, P, P, P]),
+    "bbw_curved_geometry": (c_int, [c_int, c_int, P, P, P, c_int, P, c_int, P, P, P, P]),
+    "bbw_rk_volume_wadg_skew_combine": (c_int, [c_int, c_int, c_int] + [P] * 15 + [P]),
+    "bbw_rk_surface_wadg_skew_combine": (c_int, [c_int, c_int, c_int] + [P] * 9 + [P]),
+    "bbw_rk_volume_planar": (c_int, [c_int, c_int] + [P] * 8 + [P]),
+    "bbw_rk_surface_planar": (c_int, [c_int, c_int] + [P] * 8 + [P]),
+    "bbw_curved_create": (c_int, [ctypes.POINTER(CurvedDesc), c_int, ctypes.POINTER(c_void_p)]),
+    "bbw_curved_destroy": (c_int, [c_void_p]),
+    "bbw_curved_set_state": (c_int, [c_void_p, P]),
+    "bbw_curved_get_state": (c_int, [c_void_p, P]),
+    "bbw_curved_get_residual": (c_int, [c_void_p, P]),
+    "bbw_curved_stage": (c_int, [c_void_p, c_float, c_float, c_float]),
+    "bbw_curved_steps": (c_int, [c_void_p, c_float, c_int]),
+    "bbw_curved_sync": (c_int, [c_void_p]),
+    "bbw_curved_stream": (c_void_p, [c_void_p]),
 }
 
 _lib = None

@@ -26,4 +26,15 @@ Mat mldivide(const Mat &A, const Mat &B);  // A\B: square solve or least squares
 Mat mrdivide(const Mat &A, const Mat &B);  // A/B = (B'\A')'
 double maxabs(const Mat &A);
 
+typedef std::vector<double> Vec;
+// orthonormal Jacobi polynomial of degree d for weight (1-x)^a (1+x)^b
+Vec jacobiP(const Vec &x, double a, double b, int d);
+// Warp & Blend nodes of the reference tetrahedron (vertices (-1,-1,-1),
+// (1,-1,-1), (-1,1,-1), (-1,-1,1)) in the reference's node order
+void nodes3d(int N, Vec &r, Vec &s, Vec &t);
+// orthonormal simplex bases at the given points (rows) and their gradients
+Mat vandermonde3d(int N, const Vec &r, const Vec &s, const Vec &t);
+void gradVandermonde3d(int N, const Vec &r, const Vec &s, const Vec &t, Mat &Vr, Mat &Vs, Mat &Vt);
+Mat vandermonde2d(int N, const Vec &r, const Vec &s);
+
 }  // namespace bbw

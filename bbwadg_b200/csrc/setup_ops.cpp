@@ -11,6 +11,8 @@
 //   nodal Dr/Ds/Dt, Fmask, LIFT, Vq    cpp/src/StartUp3d.cpp:25-226
 //   BB D, LIFT pieces (L0, EEL), slices cpp/src/StartUp3d.cpp:228-510
 //   WADG Vq/Pq (nodal and BB)          cpp/src/WaveOKL3d.cpp:459-483, 894-897
+//   curvilinear Vrq.., Prq.., Vfq, Pfq,  cpp/src/StartUp3d.cpp:98-156, 848-856,
+//   VfqFace                            cpp/src/WaveOKL3d.cpp:238-242
 //   sparse packing                     cpp/src/Basis.cpp:980-1007,
 //                                      cpp/src/WaveOKL3d.cpp:1427-1526
 // The volume and face cubature rules are inputs; when none is given a
@@ -151,7 +153,6 @@ Mat mldivide(const Mat &A, const Mat &B) {
 Mat mrdivide(const Mat &A, const Mat &B) { return transpose(mldivide(transpose(B), transpose(A))); }
 
 // ------------------------------------------------------------ polynomials
-typedef std::vector<double> Vec;
 
 static double factorial(int n) {
   double f = 1;
@@ -160,7 +161,7 @@ static double factorial(int n) {
 }
 
 // orthonormal Jacobi polynomial of degree d w.r.t. (1-x)^a (1+x)^b on [-1,1]
-static Vec jacobiP(const Vec &x, double a, double b, int d) {
+Vec jacobiP(const Vec &x, double a, double b, int d) {
   const size_t nx = x.size();
   const double g0 = std::pow(2.0, a + b + 1) / (a + b + 1) * std::tgamma(a + 1) *
                     std::tgamma(b + 1) / std::tgamma(a + b + 1);
@@ -280,7 +281,7 @@ static void evalshift(int p, double pval, const Vec &L1, const Vec &L2, const Ve
 }
 
 // Warp & Blend nodes on the reference tetrahedron (Warburton 2006)
-static void nodes3d(int N, Vec &r, Vec &s, Vec &t) {
+void nodes3d(int N, Vec &r, Vec &s, Vec &t) {
   static const double alpopt[15] = {0, 0, 0, 0.1002, 1.1332, 1.5608, 1.3413, 1.2577,
                                     1.1603, 1.10153, 0.6080, 0.4523, 0.8856, 0.8717, 0.9655};
   const double alpha = N <= 15 ? alpopt[N - 1] : 1.0;
@@ -360,7 +361,7 @@ static void rsttoabc(const Vec &r, const Vec &s, const Vec &t, Vec &a, Vec &b, V
   }
 }
 
-static Mat vandermonde3d(int N, const Vec &r, const Vec &s, const Vec &t) {
+Mat vandermonde3d(int N, const Vec &r, const Vec &s, const Vec &t) {
   Vec a, b, c;
   rsttoabc(r, s, t, a, b, c);
   Mat V((int)r.size(), np_of(N));
@@ -377,7 +378,7 @@ static Mat vandermonde3d(int N, const Vec &r, const Vec &s, const Vec &t) {
   return V;
 }
 
-static void gradVandermonde3d(int N, const Vec &r, const Vec &s, const Vec &t, Mat &Vr, Mat &Vs,
+void gradVandermonde3d(int N, const Vec &r, const Vec &s, const Vec &t, Mat &Vr, Mat &Vs,
                               Mat &Vt) {
   Vec a, b, c;
   rsttoabc(r, s, t, a, b, c);
@@ -413,7 +414,7 @@ static void gradVandermonde3d(int N, const Vec &r, const Vec &s, const Vec &t, M
       }
 }
 
-static Mat vandermonde2d(int N, const Vec &r, const Vec &s) {
+Mat vandermonde2d(int N, const Vec &r, const Vec &s) {
   const size_t n = r.size();
   Vec a(n), b(n);
   for (size_t i = 0; i < n; ++i) {
@@ -613,6 +614,40 @@ static int build(int N, const double *cub, int Nq_in, const double *tri, int Nfq
   Mat MB = matmul(VBqtW, VBq);
   Mat PqB = mldivide(MB, VBqtW);
 
+  // curvilinear WADG operators (cpp/src/StartUp3d.cpp:98-156, 848-856;
+  // cpp/src/WaveOKL3d.cpp:238-242): derivative interpolants at the volume
+  // cubature, their weighted projections, interpolation to the face
+  // cubature of all four faces and the face-node -> face-cubature map
+  Mat Vrq, Vsq, Vtq;
+  {
+    Mat a, b, c;
+    gradVandermonde3d(N, rq, sq, tq, a, b, c);
+    Vrq = mrdivide(a, V), Vsq = mrdivide(b, V), Vtq = mrdivide(c, V);
+  }
+  auto weighted_proj = [&](const Mat &A, const Vec &w) {
+    Mat T = transpose(A);
+    for (int i = 0; i < T.m; ++i)
+      for (int q = 0; q < T.n; ++q) T(i, q) *= w[q];
+    return matmul(invM, T);
+  };
+  Mat Prq = weighted_proj(Vrq, wq), Psq = weighted_proj(Vsq, wq), Ptq = weighted_proj(Vtq, wq);
+  Vec rfa(4 * Nfq), sfa(4 * Nfq), tfa(4 * Nfq), wfa(4 * Nfq);
+  for (int q = 0; q < Nfq; ++q) {
+    const double a = rt[q], b = st[q];
+    const double pts[4][3] = {{a, b, -1.0}, {a, -1.0, b}, {-(1 + a + b), a, b}, {-1.0, a, b}};
+    for (int f = 0; f < 4; ++f)
+      rfa[f * Nfq + q] = pts[f][0], sfa[f * Nfq + q] = pts[f][1], tfa[f * Nfq + q] = pts[f][2],
+                    wfa[f * Nfq + q] = wt[q];
+  }
+  Mat Vfq = mrdivide(vandermonde3d(N, rfa, sfa, tfa), V);
+  Mat Pfq = weighted_proj(Vfq, wfa);
+  Mat VfqFace;
+  {
+    Vec rf0(Nfp), sf0(Nfp);
+    for (int i = 0; i < Nfp; ++i) rf0[i] = r[Fmask[i]], sf0[i] = s[Fmask[i]];
+    VfqFace = mrdivide(vandermonde2d(N, rt, st), vandermonde2d(N, rf0, sf0));
+  }
+
   // Bernstein derivative operators (cpp/src/StartUp3d.cpp:228-282)
   Mat G[4];
   Mat VB = bernTet(N, r, s, t, G);
@@ -723,7 +758,11 @@ static int build(int N, const double *cub, int Nq_in, const double *tri, int Nfq
   o.f64["LIFTB"] = colmajor(LIFTB), o.f64["EEL"] = colmajor(EEL);
   o.f64["cEL"] = cEL;
   o.f64["EEL_val_vec"] = eel_val_vec;
-  for (const char *k : {"Dr", "Ds", "Dt", "LIFT", "Vq_nodal", "Pq_nodal", "Vq_bb", "Pq_bb", "cEL"})
+  o.f64["Vrq"] = colmajor(Vrq), o.f64["Vsq"] = colmajor(Vsq), o.f64["Vtq"] = colmajor(Vtq);
+  o.f64["Prq"] = colmajor(Prq), o.f64["Psq"] = colmajor(Psq), o.f64["Ptq"] = colmajor(Ptq);
+  o.f64["Vfq"] = colmajor(Vfq), o.f64["Pfq"] = colmajor(Pfq), o.f64["VfqFace"] = colmajor(VfqFace);
+  for (const char *k : {"Dr", "Ds", "Dt", "LIFT", "Vq_nodal", "Pq_nodal", "Vq_bb", "Pq_bb", "cEL",
+                        "Vrq", "Vsq", "Vtq", "Prq", "Psq", "Ptq", "Vfq", "Pfq", "VfqFace"})
     o.f32[k] = to_f32(o.f64[k]);
   o.i32["Fmask"] = Fmask;
   o.i32["slice_ids"] = slice_ids;

@@ -74,6 +74,55 @@ def kuhn_box(n, lo=-1.0, hi=1.0):
     return VX, VY, VZ, EToV.astype(np.int32)
 
 
+def kuhn_ball(n):
+    """Return (VX, VY, VZ, EToV) for the unit ball, n even.
+
+    The box [-1,1]^3 is cut into n^3 hexahedra and each into 6 Kuhn
+    tetrahedra around the hexahedron's diagonal that points away from the
+    centre (the Kuhn pattern mirrored into each octant, which keeps shared
+    faces conforming).  Every vertex then moves radially, x -> x |x|_inf /
+    |x|_2, so the cube surface lands on the unit sphere.  With the diagonal
+    pointing outward, two vertices of one tetrahedron that both lie on the
+    sphere always share a boundary face, so no chord through the interior
+    has both ends on the sphere: the Gordon-Hall curving, which snaps every
+    edge whose end points lie on the sphere (cpp/src/WaveOKL3d.cpp:1071-1100),
+    only moves true boundary edges.  Stands in for the reference's Gmsh
+    sphere meshes (cpp/meshes/sphere*.msh)."""
+    n = int(n)
+    if n < 2 or n % 2:
+        raise ValueError("kuhn_ball: n must be even and >= 2")
+    VX, VY, VZ, _ = kuhn_box(n)
+    # vertex id of grid point (i,j,k), from the coordinates kuhn_box assigned
+    idx = np.rint((np.stack([VX, VY, VZ], 1) + 1.0) * n / 2.0).astype(np.int64)
+    vid = np.empty((n + 1) ** 3, np.int64)
+    vid[idx[:, 0] + (n + 1) * (idx[:, 1] + (n + 1) * idx[:, 2])] = np.arange(len(VX))
+    hk, hj, hi_ = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    h = np.stack([hi_.ravel(), hj.ravel(), hk.ravel()], 1)          # hex lower corner
+    sgn = np.where(h >= n // 2, 1, -1)                                # outward per axis
+    start = np.where(sgn > 0, h, h + 1)                               # corner nearest the centre
+    EToV = np.empty((len(h), 6, 4), np.int64)
+    for t, perm in enumerate(itertools.permutations(range(3))):
+        cur = start.copy()
+        for v in range(4):
+            if v:
+                ax = perm[v - 1]
+                cur[:, ax] += sgn[:, ax]
+            EToV[:, t, v] = vid[cur[:, 0] + (n + 1) * (cur[:, 1] + (n + 1) * cur[:, 2])]
+    EToV = EToV.reshape(-1, 4)
+    X = np.stack([VX, VY, VZ], 1)
+    n2 = np.linalg.norm(X, axis=1)
+    s = np.where(n2 > 0, np.abs(X).max(1) / np.where(n2 > 0, n2, 1.0), 1.0)
+    X = X * s[:, None]
+    v = X[EToV]
+    d = v[:, 1:] - v[:, :1]
+    J = np.einsum("ij,ij->i", d[:, 0], np.cross(d[:, 1], d[:, 2]))
+    neg = J < 0
+    EToV[neg, 2], EToV[neg, 3] = EToV[neg, 3].copy(), EToV[neg, 2].copy()
+    if (np.abs(J) <= 1e-14).any():
+        raise RuntimeError("kuhn_ball: degenerate element")
+    return X[:, 0].copy(), X[:, 1].copy(), X[:, 2].copy(), EToV.astype(np.int32)
+
+
 def write_gmsh22(path, VX, VY, VZ, EToV):
     """Write a Gmsh 2.2 ASCII file with coordinates in round-trip precision."""
     Nv = len(VX)

@@ -16,11 +16,12 @@ from . import _lib
 from .mesh import kuhn_box, read_gmsh22
 
 _F32, _F64, _I32 = 0, 1, 2
+_CURVED_OPS = ["Vrq", "Vsq", "Vtq", "Prq", "Psq", "Ptq", "Vfq", "Pfq", "VfqFace"]
 _OPS_F32 = ["Dr", "Ds", "Dt", "LIFT", "Vq_nodal", "Pq_nodal", "Vq_bb", "Pq_bb", "cEL", "Dvals4",
-            "EEL_vals", "L0_vals"]
+            "EEL_vals", "L0_vals"] + _CURVED_OPS
 _OPS_F64 = ["V", "VB", "invVB", "LIFTB", "EEL", "r", "s", "t", "rq", "sq", "tq", "wq", "rfq", "sfq",
             "wfq", "EEL_val_vec", "Dr", "Ds", "Dt", "LIFT", "Vq_nodal", "Pq_nodal", "Vq_bb",
-            "Pq_bb", "cEL", "Dvals4", "EEL_vals", "L0_vals"]
+            "Pq_bb", "cEL", "Dvals4", "EEL_vals", "L0_vals"] + _CURVED_OPS
 _OPS_I32 = ["Fmask", "D_ids1", "D_ids2", "D_ids3", "D_ids4", "EEL_ids", "L0_ids", "slice_ids",
             "EEL_id_vec", "faceVolPerm", "sizes"]
 

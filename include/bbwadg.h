@@ -80,6 +80,29 @@ bbw_status bbw_mesh_geometry(int N, int K, const double *VX, const double *VY,
                              const double *s, const double *t, float *vgeo, float *fgeo,
                              double *x, double *y, double *z, float *dt_out);
 
+/* Gordon-Hall curving of the elements that touch the unit sphere
+ * (GordonHallSphere, cpp/src/WaveOKL3d.cpp:929-1231): nodes of every edge
+ * whose end points lie on the sphere, and of every boundary face whose three
+ * vertices do, are projected onto it and the displacements blended into the
+ * element.  x, y, z [K][Np] FP64 node coordinates (bbw_mesh_geometry),
+ * updated in place; EToF from bbw_mesh_connect; curved[k] = 1 for a curved
+ * element, else 0.  Matches the reference for N <= 3; for N >= 4 the
+ * reference's face blend reads past a 2-vector (cpp/src/Basis.cpp:353-354)
+ * and this function uses the face coordinates it evidently intends. */
+bbw_status bbw_gordon_hall_sphere(int N, int K, const int *EToF, double *x, double *y, double *z,
+                                  int *curved);
+
+/* Geometric factors at the cubature points of curved elements
+ * (InitQuadratureArrays + the packing of InitWADG_curved,
+ * cpp/src/StartUp3d.cpp:829-909, cpp/src/WaveOKL3d.cpp:211-233).
+ * cub = {rq[Nq], sq, tq}, tri = {rfq[Nfq], sfq} (face-1 coordinates).
+ * Writes (FP64) vgeoq [K][9][Nq] (rx sx tx ry sy ty rz sz tz), Jq [K][Nq]
+ * and fgeoq [K][4 faces][nx ny nz sJ][Nfq] with sJ the surface Jacobian
+ * times J. */
+bbw_status bbw_curved_geometry(int N, int K, const double *x, const double *y, const double *z,
+                               int Nq, const double *cub, int Nfq, const double *tri,
+                               double *vgeoq, double *Jq, double *fgeoq);
+
 /* Trace map vmapP [K][4Nfp] in state indexing (cpp/src/StartUp3d.cpp:643-741
  * followed by the remap of cpp/src/WaveOKL3d.cpp:1590-1603). */
 bbw_status bbw_mesh_vmapP(int N, int K, const int *EToE, const int *EToF, const int *Fmask,
@@ -92,7 +115,10 @@ bbw_status bbw_mesh_vmapP(int N, int K, const int *EToE, const int *EToF, const 
  * name with bbw_ops_get (dtype 0 = FP32 kernel layout, 1 = FP64 column-major,
  * 2 = int32).  Names: Dr Ds Dt LIFT Vq_nodal Pq_nodal Vq_bb Pq_bb cEL
  * Dvals4 EEL_vals L0_vals (FP32 and FP64), V VB invVB LIFTB EEL r s t rq sq tq
- * wq rfq sfq wfq EEL_val_vec (FP64), Fmask D_ids1..4 EEL_ids L0_ids slice_ids
+ * wq rfq sfq wfq EEL_val_vec (FP64), the curvilinear-path operators Vrq Vsq
+ * Vtq [Nq x Np], Prq Psq Ptq [Np x Nq], Vfq [4Nfq x Np], Pfq [Np x 4Nfq],
+ * VfqFace [Nfq x Nfp] (FP32 and FP64; cpp/src/StartUp3d.cpp:98-156, 848-856,
+ * cpp/src/WaveOKL3d.cpp:238-242), Fmask D_ids1..4 EEL_ids L0_ids slice_ids
  * EEL_id_vec faceVolPerm sizes (int32; sizes = {N,Np,Nfp,Nq,Nfq,EEL_nnz,
  * L0_nnz,EEL_width,L0_width}). */
 typedef struct bbw_ops bbw_ops;
@@ -313,6 +339,90 @@ bbw_status bbw_get_time(bbw_ctx *ctx, double *t, int *step);
  * cpp/okl/WaveKernels.okl:44-260, cpp/okl/WaveKernelsWADG.okl:1760-1887)
  * and its LSRK45 loop (cpp/src/WaveOKL3d.cpp:2014-2109).  FP32 stage only;
  * both bases; any number of shots. */
+/* ------------------------------------------------------------------
+ * Curvilinear WADG path (cpp/src/WaveOKL3d.cpp:164-417 InitWADG_curved,
+ * :2111-2185 RK_step_WADG).  Kernel-level entry points take device
+ * pointers in the reference's layouts; N, Nq and Nfq are the reference's
+ * compile-time p_N, p_Nq, p_Nfq.  A stream of NULL is the legacy stream.
+ * ------------------------------------------------------------------ */
+
+/* rk_volume_WADG_skew_combine (cpp/okl/WaveKernelsWADG.okl:514-682): for the
+ * K elements Klist[0..K): interpolates u,v,w and grad_rst p to the Nq
+ * cubature points, forms J grad p and -J (rst-contravariant U), projects
+ * with Pq and Prq/Psq/Ptq and writes rhsQ.  vgeoq [K][9][Nq] (rx sx tx ry
+ * sy ty rz sz tz), Jq [K][Nq], Vq/Vrq/Vsq/Vtq [Nq x Np] and
+ * Pq/Prq/Psq/Ptq [Np x Nq] column-major.  Vskew/Pskew are accepted and not
+ * read, as in the reference kernel (may be NULL). */
+bbw_status bbw_rk_volume_wadg_skew_combine(int N, int Nq, int K, const int *Klist,
+                                           const float *vgeoq, const float *Jq, const float *Vq,
+                                           const float *Vrq, const float *Vsq, const float *Vtq,
+                                           const float *Pq, const float *Prq, const float *Psq,
+                                           const float *Ptq, const float *Vskew,
+                                           const float *Pskew, const float *Q, float *rhsQ,
+                                           void *stream);
+
+/* rk_surface_WADG_skew_combine (cpp/okl/WaveKernelsWADG.okl:3024-3195):
+ * jumps and averages at the face nodes (pressure-release wall), VfqFace
+ * [Nfq x Nfp] to the face cubature, upwind fluxes with fgeoq
+ * [K][4][nx ny nz sJ][Nfq], lifted with Pfq [Np x 4Nfq] and ADDED to rhsQ.
+ * fgeo is accepted and not read, as in the reference kernel. */
+bbw_status bbw_rk_surface_wadg_skew_combine(int N, int Nfq, int K, const int *Klist,
+                                            const float *fgeo, const float *fgeoq,
+                                            const float *VfqFace, const float *Pfq,
+                                            const int *Fmask, const int *vmapP, const float *Q,
+                                            float *rhsQ, void *stream);
+
+/* rk_volume_planar (cpp/okl/WaveKernelsWADG.okl:2203-2318): rk_volume on the
+ * listed affine elements with the output scaled by J[k]. */
+bbw_status bbw_rk_volume_planar(int N, int K, const int *Klist, const float *vgeo,
+                                const float *J, const float *Dr, const float *Ds,
+                                const float *Dt, const float *Q, float *rhsQ, void *stream);
+
+/* rk_surface_planar (cpp/okl/WaveKernelsWADG.okl:2320-2441): rk_surface
+ * (pressure-release wall) on the listed affine elements with Fscale scaled
+ * by J[k]; adds to rhsQ. */
+bbw_status bbw_rk_surface_planar(int N, int K, const int *Klist, const float *fgeo,
+                                 const float *J, const int *Fmask, const int *vmapP,
+                                 const float *LIFT, const float *Q, float *rhsQ, void *stream);
+
+/* Arrays InitWADG_curved uploads (host, FP32, reference layouts).  The
+ * element lists must partition 0..K-1; the curved-element arrays may be
+ * NULL when KCurved == 0.  Vq_reduced/Pq_reduced/Jq_reduced/c2q use the
+ * update's cubature of Nq_reduced points (the reference uses the same rule
+ * as the volume cubature). */
+typedef struct bbw_curved_desc {
+  int N, K, Nq, Nfq, Nq_reduced;
+  int KCurved, KPlanar;
+  const int *KlistCurved, *KlistPlanar;
+  const float *vgeo, *fgeo;     /* [K][9], [K][4][4] affine factors */
+  const float *Jplanar;         /* [K] J of the planar elements */
+  const int *Fmask, *vmapP;     /* [4Nfp], [K][4Nfp] */
+  const float *vgeoq, *Jq;      /* [K][9][Nq], [K][Nq] */
+  const float *fgeoq;           /* [K][4][4][Nfq] */
+  const float *Jq_reduced, *c2q;/* [K][Nq_reduced] */
+  const float *Dr, *Ds, *Dt, *LIFT;
+  const float *Vq, *Vrq, *Vsq, *Vtq, *Pq, *Prq, *Psq, *Ptq, *VfqFace, *Pfq;
+  const float *Vq_reduced, *Pq_reduced;
+} bbw_curved_desc;
+
+typedef struct bbw_curved bbw_curved;
+
+/* Uploads the arrays to `device`; state and residual start at zero. */
+bbw_status bbw_curved_create(const bbw_curved_desc *desc, int device, bbw_curved **out);
+bbw_status bbw_curved_destroy(bbw_curved *h);
+/* Host copies of the state [K][4][Np]; set_state also zeroes the residual. */
+bbw_status bbw_curved_set_state(bbw_curved *h, const float *Q);
+bbw_status bbw_curved_get_state(bbw_curved *h, float *Q);
+bbw_status bbw_curved_get_residual(bbw_curved *h, float *res);
+/* One stage: RK_step_WADG(mesh, fa, fb, fdt). */
+bbw_status bbw_curved_stage(bbw_curved *h, float fa, float fb, float fdt);
+/* nsteps LSRK45 steps of size dt (five stages with fa = (float)rk4a[s],
+ * fb = (float)rk4b[s]), one CUDA graph launch per step; asynchronous. */
+bbw_status bbw_curved_steps(bbw_curved *h, float dt, int nsteps);
+bbw_status bbw_curved_sync(bbw_curved *h);
+/* The handle's CUDA stream (cudaStream_t). */
+void *bbw_curved_stream(bbw_curved *h);
+
 typedef struct bbw_tape bbw_tape;
 
 /* Replaces c^2 / J at the cubature points ([K][Nq], host). */

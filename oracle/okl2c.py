@@ -26,7 +26,10 @@ no reference source is stored in this repository.
 Two defects of the shipped sources are handled by extracting kernels one by
 one instead of compiling whole files: ``matvec_example``
 (cpp/okl/WaveKernels.okl:15-41) is never closed, and a stray ``#endif``
-(cpp/okl/WaveKernelsWADG.okl:2439) sits inside an unused kernel.
+(cpp/okl/WaveKernelsWADG.okl:2439) closes nothing at the end of
+rk_surface_planar.  OCCA's own preprocessor accepted that kernel (the
+reference launches it every curvilinear stage); an unmatched ``#endif`` in
+an extracted kernel body is dropped here.
 
 Usage: okl2c.py SRC.okl OUT.cpp kernel_name [kernel_name ...]
 """
@@ -172,8 +175,12 @@ def rewrite_exclusive(body):
         toks = split_top(typ_and_names, ",")
         first = toks[0].split()
         typ, rest = " ".join(first[:-1]), [first[-1]] + [t.strip() for t in toks[1:]]
-        names.extend(rest)
-        return " ".join("%s %s[%d];" % (typ, nm, EXCL_SLOTS) for nm in rest)
+        out = []
+        for nm in rest:  # a name may carry array dimensions: one copy per slot
+            base, dims = (nm[:nm.index("[")], nm[nm.index("["):]) if "[" in nm else (nm, "")
+            names.append(base.strip())
+            out.append("%s %s[%d]%s;" % (typ, base.strip(), EXCL_SLOTS, dims))
+        return " ".join(out)
 
     body = re.sub(r"\bexclusive\s+([^;]+);", decl, body)
     if not names:
@@ -195,6 +202,21 @@ def rewrite_exclusive(body):
     return "\n".join(out)
 
 
+def drop_unmatched_endif(body):
+    """Remove #endif lines that close no #if inside the kernel body."""
+    out, depth = [], 0
+    for ln in body.split("\n"):
+        d = ln.strip()
+        if re.match(r"#\s*if", d):
+            depth += 1
+        elif re.match(r"#\s*endif", d):
+            if depth == 0:
+                continue
+            depth -= 1
+        out.append(ln)
+    return "\n".join(out)
+
+
 def translate(src_path, out_path, names):
     src = strip_comments(open(src_path).read())
     chunks = [
@@ -204,6 +226,7 @@ def translate(src_path, out_path, names):
     for name in names:
         params, body = extract_kernel(src, name)
         plist = parse_params(params)
+        body = drop_unmatched_endif(body)
         body = rewrite_exclusive(body)
         body = rewrite_loops(body)
         body = re.sub(r"\bshared\s+", "", body)
