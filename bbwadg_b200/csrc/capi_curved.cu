@@ -1,89 +1,103 @@
-// Curvilinear WADG solver handle: device copies of the curved path's arrays
-// and the reference's stage RK_step_WADG (cpp/src/WaveOKL3d.cpp:2111-2185):
-//   skew-form volume + surface kernels on the curved elements,
-//   J-weighted volume + surface kernels on the planar elements,
-//   rk_update_WADG (all four fields weighted by 1/J, c^2 on p) on all.
-// bbw_curved_steps runs the LSRK45 loop of Wave_RK (useWADG = 2,
-// cpp/src/WaveOKL3d.cpp:2014-2079) as one CUDA graph per step.
+// Curvilinear WADG solver handle: the reference's stage RK_step_WADG
+// (cpp/src/WaveOKL3d.cpp:2111-2185) and its LSRK45 loop (Wave_RK with
+// useWADG = 2, cpp/src/WaveOKL3d.cpp:2014-2079), B200 layout:
+//
+// * elements are renumbered planar first, curved last (host permutation on
+//   set/get; the kernel-level entry points keep the reference's numbering);
+// * the planar elements [0, KP) advance with the fused affine stage kernel
+//   (one pass: volume, surface, WADG projection of p with c^2, LSRK update).
+//   For an affine element J is constant, so the reference's J-weighted
+//   planar kernels followed by the 1/J update reduce to the unweighted
+//   stage with Pq diag(c^2) Vq on p and the identity on u, v, w (Pq Vq = I);
+// * the curved elements [KP, K) advance with one fused kernel
+//   (k_curved_stage: skew volume + skew surface + 1/J, c^2 WADG update +
+//   LSRK update), reading the same old state and writing the same new
+//   state buffer, so one stage is two launches and no rhs array exists.
+// bbw_curved_steps captures one LSRK45 step per buffer parity in a CUDA graph.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <vector>
 
 #include "bbwadg.h"
 #include "ctx.h"
+#include "curved.h"
 #include "device_common.cuh"
 
-namespace bbw {
-bbw_status curved_volume(int N, int K, const int *Klist, int Nq, const float *vgeoq,
-                         const float *Jq, const float *Vq, const float *Vrq, const float *Vsq,
-                         const float *Vtq, const float *Pq, const float *Prq, const float *Psq,
-                         const float *Ptq, const float *Q, float *rhsQ, cudaStream_t st);
-bbw_status curved_surface(int N, int K, const int *Klist, int Nfq, const float *fgeoq,
-                          const float *VfqFace, const float *Pfq, const int *Fmask,
-                          const int *vmapP, const float *Q, float *rhsQ, cudaStream_t st);
-bbw_status planar_volume(int N, int K, const int *Klist, const float *vgeo, const float *J,
-                         const float *Dr, const float *Ds, const float *Dt, const float *Q,
-                         float *rhsQ, cudaStream_t st);
-bbw_status planar_surface(int N, int K, const int *Klist, const float *fgeo, const float *J,
-                          const int *Fmask, const int *vmapP, const float *LIFT, const float *Q,
-                          float *rhsQ, cudaStream_t st);
-}  // namespace bbw
 
 using namespace bbw;
 
 struct bbw_curved {
-  int N = 0, K = 0, Nq = 0, Nfq = 0, Nq_red = 0, KC = 0, KP = 0, Np = 0, device = 0;
+  int N = 0, K = 0, Np = 0, KC = 0, KP = 0, device = 0;
   cudaStream_t stream = nullptr;
-  float *Q = nullptr, *res = nullptr, *rhs = nullptr;
-  int *KlistC = nullptr, *KlistP = nullptr, *Fmask = nullptr, *vmapP = nullptr;
-  float *vgeo = nullptr, *fgeo = nullptr, *Jplanar = nullptr, *vgeoq = nullptr, *Jq = nullptr,
-        *fgeoq = nullptr, *Jq_red = nullptr, *c2q = nullptr;
-  float *op[16] = {};  // Dr Ds Dt LIFT Vq Vrq Vsq Vtq Pq Prq Psq Ptq VfqFace Pfq Vq_red Pq_red
-  cudaGraphExec_t graph = nullptr;
-  uint32_t graph_dt_bits = 0;
+  bbw_ctx *aff = nullptr;             // fused affine stage of the planar elements
+  float *Q[2] = {nullptr, nullptr};   // state buffers (the affine context's when it exists)
+  float *res = nullptr;
+  int cur = 0;
+  std::vector<int> perm;              // new element index -> reference index
+  CurvedStageArgs args{};
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  uint32_t graph_dt_bits[2] = {0, 0};
   std::vector<void *> owned;
+  std::vector<float> host;            // permutation scratch
 };
 
 namespace {
 
-enum { kDr, kDs, kDt, kLIFT, kVq, kVrq, kVsq, kVtq, kPq, kPrq, kPsq, kPtq, kVfqFace, kPfq,
-       kVqRed, kPqRed };
-
 template <class T>
 bbw_status own_upload(bbw_curved *h, T **dst, const T *src, size_t n, const char *what) {
   bbw_status s = upload(dst, src, n, what);
-  if (s == BBW_OK) h->owned.push_back(*dst);
+  if (s == BBW_OK) h->owned.push_back((void *)*dst);
   return s;
 }
 
+template <class T>
+const T *own_upload_c(bbw_curved *h, const T *src, size_t n, bbw_status &s) {
+  T *d = nullptr;
+  if (s == BBW_OK) s = own_upload(h, &d, src, n, "bbw_curved_create: upload");
+  return d;
+}
+
 void release(bbw_curved *h) {
-  if (h->graph) cudaGraphExecDestroy(h->graph);
+  for (auto &g : h->graph)
+    if (g) cudaGraphExecDestroy(g);
+  if (h->aff) bbw_destroy(h->aff);
   for (void *p : h->owned) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
 
+// rows of a [K][w] array in the new element order (from position `from`)
+template <class T>
+std::vector<T> rows(const T *a, const std::vector<int> &perm, size_t w, int from = 0) {
+  std::vector<T> out((perm.size() - from) * w);
+  for (size_t i = from; i < perm.size(); ++i)
+    std::memcpy(&out[(i - from) * w], a + (size_t)perm[i] * w, w * sizeof(T));
+  return out;
+}
+
 bbw_status stage(bbw_curved *h, float fa, float fb, float fdt) {
-  const int N = h->N;
-  float **o = h->op;
-  bbw_status s = curved_volume(N, h->KC, h->KlistC, h->Nq, h->vgeoq, h->Jq, o[kVq], o[kVrq],
-                               o[kVsq], o[kVtq], o[kPq], o[kPrq], o[kPsq], o[kPtq], h->Q, h->rhs,
-                               h->stream);
-  if (s == BBW_OK)
-    s = curved_surface(N, h->KC, h->KlistC, h->Nfq, h->fgeoq, o[kVfqFace], o[kPfq], h->Fmask,
-                       h->vmapP, h->Q, h->rhs, h->stream);
-  if (s == BBW_OK)
-    s = planar_volume(N, h->KP, h->KlistP, h->vgeo, h->Jplanar, o[kDr], o[kDs], o[kDt], h->Q,
-                      h->rhs, h->stream);
-  if (s == BBW_OK)
-    s = planar_surface(N, h->KP, h->KlistP, h->fgeo, h->Jplanar, h->Fmask, h->vmapP, o[kLIFT],
-                       h->Q, h->rhs, h->stream);
-  if (s == BBW_OK)
-    s = bbw_rk_update_wadg(N, h->K, h->Nq_red, o[kVqRed], o[kPqRed], h->Jq_red, h->c2q, fa, fb,
-                           fdt, h->rhs, h->res, h->Q, h->stream);
+  const float *Qin = h->Q[h->cur];
+  float *Qout = h->Q[h->cur ^ 1];
+  bbw_status s = BBW_OK;
+  if (h->KP > 0)
+    s = fused_launch(h->aff->plan, Qin, Qout, h->res, fa, fb, fdt, 0.f, h->stream);
+  if (s == BBW_OK && h->KC > 0) {
+    CurvedStageArgs A = h->args;
+    A.fa = fa, A.fb = fb, A.fdt = fdt;
+    s = curved_stage(h->N, A, Qin, Qout, h->res, h->stream);
+  }
+  if (s == BBW_OK) h->cur ^= 1;
   return s;
+}
+
+void drop_graphs(bbw_curved *h) {
+  for (int i = 0; i < 2; ++i) {
+    if (h->graph[i]) cudaGraphExecDestroy(h->graph[i]);
+    h->graph[i] = nullptr;
+  }
 }
 
 }  // namespace
@@ -93,10 +107,9 @@ extern "C" bbw_status bbw_curved_create(const bbw_curved_desc *d, int device, bb
   *out = nullptr;
   const int N = d->N, K = d->K;
   if (N < 1 || N > BBW_MAX_N) return set_error(BBW_ERR_UNSUPPORTED, "bbw_curved_create: N");
-  const int Np = NP(N), NF = 4 * NFP(N);
+  const int Np = NP(N), Nfp = NFP(N), NF = 4 * Nfp;
   if (K < 1 || d->Nq < Np || d->Nfq < 1 || d->Nq_reduced < 1 || d->KCurved < 0 ||
-      d->KPlanar < 0 || d->KCurved + d->KPlanar != K ||
-      (long long)K * 4 * Np >= (1LL << 31))
+      d->KPlanar < 0 || d->KCurved + d->KPlanar != K || (long long)K * 4 * Np >= (1LL << 31))
     return set_error(BBW_ERR_ARG, "bbw_curved_create: bad sizes");
   const void *req[] = {d->vgeo, d->fgeo, d->Jplanar, d->Fmask, d->vmapP, d->Jq_reduced, d->c2q,
                        d->Dr, d->Ds, d->Dt, d->LIFT, d->Vq_reduced, d->Pq_reduced};
@@ -110,69 +123,79 @@ extern "C" bbw_status bbw_curved_create(const bbw_curved_desc *d, int device, bb
   }
   if (d->KPlanar > 0 && !d->KlistPlanar)
     return set_error(BBW_ERR_ARG, "bbw_curved_create: missing planar list");
-  // every element in exactly one list; traces inside the mesh
-  std::vector<char> seen(K, 0);
+  // every element in exactly one list: planar first, then curved
+  std::vector<int> perm, inv(K, -1);
   for (int pass = 0; pass < 2; ++pass) {
-    const int n = pass ? d->KPlanar : d->KCurved;
-    const int *L = pass ? d->KlistPlanar : d->KlistCurved;
+    const int n = pass ? d->KCurved : d->KPlanar;
+    const int *L = pass ? d->KlistCurved : d->KlistPlanar;
     for (int i = 0; i < n; ++i) {
-      if (L[i] < 0 || L[i] >= K || seen[L[i]])
+      if (L[i] < 0 || L[i] >= K || inv[L[i]] >= 0)
         return set_error(BBW_ERR_ARG, "bbw_curved_create: element lists must partition 0..K-1");
-      seen[L[i]] = 1;
+      inv[L[i]] = (int)perm.size();
+      perm.push_back(L[i]);
     }
   }
   for (int i = 0; i < NF; ++i)
     if (d->Fmask[i] < 0 || d->Fmask[i] >= Np)
       return set_error(BBW_ERR_ARG, "bbw_curved_create: Fmask entry out of range");
-  for (size_t i = 0; i < (size_t)K * NF; ++i) {
-    const int v = d->vmapP[i];
-    if (v < 0 || v >= K * 4 * Np || v % (4 * Np) >= Np)
-      return set_error(BBW_ERR_ARG, "bbw_curved_create: vmapP entry out of range");
-  }
+  std::vector<int> vmapP((size_t)K * NF);
+  for (int i = 0; i < K; ++i)
+    for (int m = 0; m < NF; ++m) {
+      const int v = d->vmapP[(size_t)perm[i] * NF + m];
+      if (v < 0 || v >= K * 4 * Np || v % (4 * Np) >= Np)
+        return set_error(BBW_ERR_ARG, "bbw_curved_create: vmapP entry out of range");
+      vmapP[(size_t)i * NF + m] = inv[v / (4 * Np)] * 4 * Np + v % (4 * Np);
+    }
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) return set_cuda_error(e, "bbw_curved_create: device");
   bbw_curved *h = new bbw_curved;
-  h->N = N, h->K = K, h->Nq = d->Nq, h->Nfq = d->Nfq, h->Nq_red = d->Nq_reduced;
-  h->KC = d->KCurved, h->KP = d->KPlanar, h->Np = Np, h->device = device;
+  h->N = N, h->K = K, h->Np = Np, h->KC = d->KCurved, h->KP = d->KPlanar, h->device = device;
+  h->perm = perm;
   e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     release(h);
     return set_cuda_error(e, "bbw_curved_create: stream");
   }
-  const size_t ns = (size_t)K * 4 * Np, Nq = d->Nq, Nfq = d->Nfq, Nr = d->Nq_reduced;
-  const int KC = std::max(d->KCurved, 1), KP = std::max(d->KPlanar, 1);
-  std::vector<int> zeros(1, 0);
-  struct OpSpec { const float *src; size_t n; };
-  const OpSpec ops[16] = {
-      {d->Dr, (size_t)Np * Np}, {d->Ds, (size_t)Np * Np}, {d->Dt, (size_t)Np * Np},
-      {d->LIFT, (size_t)Np * NF}, {d->Vq, Nq * Np}, {d->Vrq, Nq * Np}, {d->Vsq, Nq * Np},
-      {d->Vtq, Nq * Np}, {d->Pq, Np * Nq}, {d->Prq, Np * Nq}, {d->Psq, Np * Nq},
-      {d->Ptq, Np * Nq}, {d->VfqFace, Nfq * NFP(N)}, {d->Pfq, Np * 4 * Nfq},
-      {d->Vq_reduced, Nr * Np}, {d->Pq_reduced, Np * Nr}};
+  const size_t ns = (size_t)K * 4 * Np;
+  const int Nq = d->Nq, Nfq = d->Nfq, Nr = d->Nq_reduced, KP = d->KPlanar;
   bbw_status s = BBW_OK;
-  const bool curved = d->KCurved > 0;
-#define UP(dst, src, n) \
-  if (s == BBW_OK) s = own_upload(h, dst, src, n, "bbw_curved_create: upload")
-  UP(&h->Q, (const float *)nullptr, ns);
-  UP(&h->res, (const float *)nullptr, ns);
-  UP(&h->rhs, (const float *)nullptr, ns);
-  UP(&h->KlistC, curved ? d->KlistCurved : zeros.data(), (size_t)KC);
-  UP(&h->KlistP, d->KPlanar ? d->KlistPlanar : zeros.data(), (size_t)KP);
-  UP(&h->Fmask, d->Fmask, (size_t)NF);
-  UP(&h->vmapP, d->vmapP, (size_t)K * NF);
-  UP(&h->vgeo, d->vgeo, (size_t)K * 9);
-  UP(&h->fgeo, d->fgeo, (size_t)K * 16);
-  UP(&h->Jplanar, d->Jplanar, (size_t)K);
-  UP(&h->Jq_red, d->Jq_reduced, (size_t)K * Nr);
-  UP(&h->c2q, d->c2q, (size_t)K * Nr);
-  if (curved) {
-    UP(&h->vgeoq, d->vgeoq, (size_t)K * 9 * Nq);
-    UP(&h->Jq, d->Jq, (size_t)K * Nq);
-    UP(&h->fgeoq, d->fgeoq, (size_t)K * 16 * Nfq);
+  std::vector<float> c2 = rows(d->c2q, perm, Nr);
+  if (KP > 0) {  // fused affine stage over the planar prefix
+    std::vector<float> vgeo = rows(d->vgeo, perm, 9), fgeo = rows(d->fgeo, perm, 16);
+    bbw_mesh_desc md{N, K, Nr, vgeo.data(), fgeo.data(), d->Fmask, vmapP.data(), c2.data(),
+                     nullptr};
+    bbw_ops_desc od{};
+    od.Dr = d->Dr, od.Ds = d->Ds, od.Dt = d->Dt, od.LIFT = d->LIFT;
+    od.Vq = d->Vq_reduced, od.Pq = d->Pq_reduced;
+    s = bbw_create(&md, &od, BBW_NODAL, BBW_BC_PRESSURE_RELEASE, &h->aff);
+    if (s == BBW_OK && KP < K) s = bbw_set_compute_range(h->aff, KP);
+    if (s == BBW_OK) h->Q[0] = h->aff->Q[0], h->Q[1] = h->aff->Q[1], h->res = h->aff->res;
+  } else {
+    if (s == BBW_OK) s = own_upload(h, &h->Q[0], (const float *)nullptr, ns, "bbw_curved_create");
+    if (s == BBW_OK) s = own_upload(h, &h->Q[1], (const float *)nullptr, ns, "bbw_curved_create");
+    if (s == BBW_OK) s = own_upload(h, &h->res, (const float *)nullptr, ns, "bbw_curved_create");
   }
-  for (int i = 0; i < 16; ++i)
-    if (ops[i].src) UP(&h->op[i], ops[i].src, ops[i].n);
-#undef UP
+  if (d->KCurved > 0) {  // compact rows of the curved tail
+    CurvedStageArgs &A = h->args;
+    A.KC = d->KCurved, A.k_off = KP, A.Nq = Nq, A.Nfq = Nfq, A.Nr = Nr;
+    const size_t nq = Nq, nr = Nr, nf = Nfq;
+    std::vector<float> t;
+    t = rows(d->vgeoq, perm, 9 * nq, KP), A.vgeoq = own_upload_c(h, t.data(), t.size(), s);
+    t = rows(d->Jq, perm, nq, KP), A.Jq = own_upload_c(h, t.data(), t.size(), s);
+    t = rows(d->fgeoq, perm, 16 * nf, KP), A.fgeoq = own_upload_c(h, t.data(), t.size(), s);
+    t = rows(d->Jq_reduced, perm, nr, KP), A.Jr = own_upload_c(h, t.data(), t.size(), s);
+    A.c2q = own_upload_c(h, c2.data() + (size_t)KP * Nr, (size_t)d->KCurved * Nr, s);
+    const size_t mq = nq * Np, mr = nr * Np;
+    A.Vq = own_upload_c(h, d->Vq, mq, s), A.Vrq = own_upload_c(h, d->Vrq, mq, s);
+    A.Vsq = own_upload_c(h, d->Vsq, mq, s), A.Vtq = own_upload_c(h, d->Vtq, mq, s);
+    A.Pq = own_upload_c(h, d->Pq, mq, s), A.Prq = own_upload_c(h, d->Prq, mq, s);
+    A.Psq = own_upload_c(h, d->Psq, mq, s), A.Ptq = own_upload_c(h, d->Ptq, mq, s);
+    A.VfqFace = own_upload_c(h, d->VfqFace, nf * Nfp, s);
+    A.Pfq = own_upload_c(h, d->Pfq, (size_t)Np * 4 * nf, s);
+    A.Vqr = own_upload_c(h, d->Vq_reduced, mr, s), A.Pqr = own_upload_c(h, d->Pq_reduced, mr, s);
+    A.Fmask = own_upload_c(h, d->Fmask, (size_t)NF, s);
+    A.vmapP = own_upload_c(h, vmapP.data(), vmapP.size(), s);
+  }
   // one stage on the zero state (it stays zero) sets the kernels' launch
   // attributes outside any later graph capture
   if (s == BBW_OK) s = stage(h, 0.f, 0.f, 0.f);
@@ -181,6 +204,7 @@ extern "C" bbw_status bbw_curved_create(const bbw_curved_desc *d, int device, bb
     release(h);
     return s;
   }
+  h->cur = 0;
   *out = h;
   return BBW_OK;
 }
@@ -189,29 +213,46 @@ extern "C" bbw_status bbw_curved_destroy(bbw_curved *h) {
   if (!h) return BBW_OK;
   cudaSetDevice(h->device);
   cudaStreamSynchronize(h->stream);
+  drop_graphs(h);
   release(h);
   return BBW_OK;
 }
 
+// host [K][4][Np] in the reference's element order <-> device buffer
 static bbw_status copy_state(bbw_curved *h, float *dev, const float *src, float *dst,
                              const char *what) {
   if (!h || (!src && !dst)) return set_error(BBW_ERR_ARG, what);
-  const size_t n = (size_t)h->K * 4 * h->Np * sizeof(float);
-  cudaError_t e = src ? cudaMemcpyAsync(dev, src, n, cudaMemcpyHostToDevice, h->stream)
-                      : cudaMemcpyAsync(dst, dev, n, cudaMemcpyDeviceToHost, h->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  const size_t w = (size_t)4 * h->Np, n = (size_t)h->K * w;
+  h->host.resize(n);
+  cudaError_t e;
+  if (src) {
+    for (int i = 0; i < h->K; ++i)
+      std::memcpy(&h->host[i * w], src + (size_t)h->perm[i] * w, w * sizeof(float));
+    e = cudaMemcpyAsync(dev, h->host.data(), n * sizeof(float), cudaMemcpyHostToDevice,
+                        h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  } else {
+    e = cudaMemcpyAsync(h->host.data(), dev, n * sizeof(float), cudaMemcpyDeviceToHost,
+                        h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e == cudaSuccess)
+      for (int i = 0; i < h->K; ++i)
+        std::memcpy(dst + (size_t)h->perm[i] * w, &h->host[i * w], w * sizeof(float));
+  }
   return set_cuda_error(e, what);
 }
 
 extern "C" bbw_status bbw_curved_set_state(bbw_curved *h, const float *Q) {
-  bbw_status s = copy_state(h, h ? h->Q : nullptr, Q, nullptr, "bbw_curved_set_state");
+  bbw_status s = copy_state(h, h ? h->Q[h->cur] : nullptr, Q, nullptr, "bbw_curved_set_state");
   if (s != BBW_OK) return s;
   const size_t n = (size_t)h->K * 4 * h->Np * sizeof(float);
-  return set_cuda_error(cudaMemsetAsync(h->res, 0, n, h->stream), "bbw_curved_set_state");
+  cudaError_t e = cudaMemsetAsync(h->res, 0, n, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  return set_cuda_error(e, "bbw_curved_set_state");
 }
 
 extern "C" bbw_status bbw_curved_get_state(bbw_curved *h, float *Q) {
-  return copy_state(h, h ? h->Q : nullptr, nullptr, Q, "bbw_curved_get_state");
+  return copy_state(h, h ? h->Q[h->cur] : nullptr, nullptr, Q, "bbw_curved_get_state");
 }
 
 extern "C" bbw_status bbw_curved_get_residual(bbw_curved *h, float *r) {
@@ -227,29 +268,32 @@ extern "C" bbw_status bbw_curved_steps(bbw_curved *h, float dt, int nsteps) {
   if (!h || nsteps < 0) return set_error(BBW_ERR_ARG, "bbw_curved_steps: bad argument");
   uint32_t bits;
   std::memcpy(&bits, &dt, 4);
-  if (!h->graph || h->graph_dt_bits != bits) {
-    if (h->graph) cudaGraphExecDestroy(h->graph);
-    h->graph = nullptr;
-    cudaGraph_t g;
-    cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
-    if (e != cudaSuccess) return set_cuda_error(e, "bbw_curved_steps: capture");
-    bbw_status s = BBW_OK;
-    for (int i = 0; i < 5 && s == BBW_OK; ++i)
-      s = stage(h, (float)kRK4A[i], (float)kRK4B[i], dt);
-    e = cudaStreamEndCapture(h->stream, &g);
-    if (s != BBW_OK) {
-      if (e == cudaSuccess) cudaGraphDestroy(g);
-      return s;
-    }
-    if (e != cudaSuccess) return set_cuda_error(e, "bbw_curved_steps: end capture");
-    e = cudaGraphInstantiate(&h->graph, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) return set_cuda_error(e, "bbw_curved_steps: instantiate");
-    h->graph_dt_bits = bits;
-  }
   for (int step = 0; step < nsteps; ++step) {
-    cudaError_t e = cudaGraphLaunch(h->graph, h->stream);
+    const int par = h->cur;
+    if (!h->graph[par] || h->graph_dt_bits[par] != bits) {
+      if (h->graph[par]) cudaGraphExecDestroy(h->graph[par]);
+      h->graph[par] = nullptr;
+      cudaGraph_t g;
+      cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) return set_cuda_error(e, "bbw_curved_steps: capture");
+      bbw_status s = BBW_OK;
+      for (int i = 0; i < 5 && s == BBW_OK; ++i)
+        s = stage(h, (float)kRK4A[i], (float)kRK4B[i], dt);
+      e = cudaStreamEndCapture(h->stream, &g);
+      h->cur = par;  // capture recorded the launches without running them
+      if (s != BBW_OK) {
+        if (e == cudaSuccess) cudaGraphDestroy(g);
+        return s;
+      }
+      if (e != cudaSuccess) return set_cuda_error(e, "bbw_curved_steps: end capture");
+      e = cudaGraphInstantiate(&h->graph[par], g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return set_cuda_error(e, "bbw_curved_steps: instantiate");
+      h->graph_dt_bits[par] = bits;
+    }
+    cudaError_t e = cudaGraphLaunch(h->graph[par], h->stream);
     if (e != cudaSuccess) return set_cuda_error(e, "bbw_curved_steps: launch");
+    h->cur ^= 1;  // five stages swap the buffers an odd number of times
   }
   return BBW_OK;
 }

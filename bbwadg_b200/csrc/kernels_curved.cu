@@ -14,6 +14,7 @@
 #include <algorithm>
 
 #include "bbwadg.h"
+#include "curved.h"
 #include "device_common.cuh"
 
 namespace bbw {
@@ -279,6 +280,200 @@ __global__ void __launch_bounds__(kCurvedThreads) k_surface_planar(
   }
 }
 
+// -------------------------------------------------- fused curved-element stage
+// One LSRK stage of the curved elements k = k_off + i, i < KC, in one pass:
+// the skew volume terms, the skew surface terms (added in the order of
+// rk_surface_WADG_skew_combine), rk_update_WADG's projection with 1/J and c^2
+// on p, and the LSRK update.  Reads the old state Qold (own element and
+// neighbour traces), writes Qnew and res of these elements only, so it runs
+// beside the planar elements' stage on the same double-buffered state.
+// Geometry rows are compact: row i of vgeoq / Jq / fgeoq / Jr / c2q
+// (CurvedStageArgs, curved.h).
+
+template <int N>
+__global__ void __launch_bounds__(kCurvedThreads) k_curved_stage(CurvedStageArgs A,
+                                                                 const float *__restrict__ Qold,
+                                                                 float *__restrict__ Qnew,
+                                                                 float *__restrict__ res) {
+  constexpr int Np = NP(N), Nfp = NFP(N), NF = 4 * NFP(N);
+  extern __shared__ float smem[];
+  const int Nq = A.Nq, Nfq = A.Nfq, Nr = A.Nr;
+  // per element: q[4Np] | t[6Nq] | s[7NF] | fl[16Nfq] | r[4Np] | u[4Nr]
+  const int o_t = 4 * Np, o_s = o_t + 6 * Nq, o_f = o_s + 7 * NF, o_r = o_f + 16 * Nfq,
+            o_u = o_r + 4 * Np, per = o_u + 4 * Nr;
+  const int i0 = blockIdx.x * A.EB;
+  const int ne = min(A.EB, A.KC - i0);
+  const int T = blockDim.x;
+  for (int i = threadIdx.x; i < ne * 4 * Np; i += T) {
+    const int e = i / (4 * Np), j = i % (4 * Np);
+    smem[e * per + j] = Qold[(size_t)(A.k_off + i0 + e) * 4 * Np + j];
+  }
+  __syncthreads();
+  // volume: u, v, w and grad_rst p at the cubature (rk_volume_WADG_skew_combine)
+  for (int i = threadIdx.x; i < ne * Nq; i += T) {
+    const int e = i / Nq, n = i % Nq, row = i0 + e;
+    const float *sq = smem + e * per;
+    float dpdr = 0.f, dpds = 0.f, dpdt = 0.f, uq = 0.f, vq = 0.f, wq = 0.f;
+    for (int m = 0; m < Np; ++m) {
+      const float pm = sq[m], um = sq[Np + m], vm = sq[2 * Np + m], wm = sq[3 * Np + m];
+      const float V = __ldg(A.Vq + n + m * Nq);
+      uq += V * um;
+      vq += V * vm;
+      wq += V * wm;
+      dpdr += __ldg(A.Vrq + n + m * Nq) * pm;
+      dpds += __ldg(A.Vsq + n + m * Nq) * pm;
+      dpdt += __ldg(A.Vtq + n + m * Nq) * pm;
+    }
+    const float *g = A.vgeoq + (size_t)row * 9 * Nq + n;
+    const float rx = g[0], sx = g[Nq], tx = g[2 * Nq], ry = g[3 * Nq], sy = g[4 * Nq],
+                ty = g[5 * Nq], rz = g[6 * Nq], sz = g[7 * Nq], tz = g[8 * Nq];
+    const float J = A.Jq[n + (size_t)row * Nq];
+    float *t = smem + e * per + o_t;
+    t[n] = (rx * dpdr + sx * dpds + tx * dpdt) * J;
+    t[Nq + n] = (ry * dpdr + sy * dpds + ty * dpdt) * J;
+    t[2 * Nq + n] = (rz * dpdr + sz * dpds + tz * dpdt) * J;
+    t[3 * Nq + n] = -((uq * rx + vq * ry + wq * rz) * J);
+    t[4 * Nq + n] = -((uq * sx + vq * sy + wq * sz) * J);
+    t[5 * Nq + n] = -((uq * tx + vq * ty + wq * tz) * J);
+  }
+  // surface: jumps and averages at the face nodes (rk_surface_WADG_skew_combine)
+  for (int i = threadIdx.x; i < ne * NF; i += T) {
+    const int e = i / NF, m = i % NF, k = A.k_off + i0 + e;
+    const int idM = A.Fmask[m] + k * Np * 4, idP = A.vmapP[m + (size_t)k * NF];
+    const bool bnd = idM == idP;
+    const float pM = Qold[idM], uM = Qold[idM + Np], vM = Qold[idM + 2 * Np],
+                wM = Qold[idM + 3 * Np];
+    const float pP = Qold[idP], uP = Qold[idP + Np], vP = Qold[idP + 2 * Np],
+                wP = Qold[idP + 3 * Np];
+    float *sv = smem + e * per + o_s;
+    sv[m] = bnd ? -2.f * pM : pP - pM;
+    sv[NF + m] = bnd ? 0.f : uP - uM;
+    sv[2 * NF + m] = bnd ? 0.f : vP - vM;
+    sv[3 * NF + m] = bnd ? 0.f : wP - wM;
+    sv[4 * NF + m] = bnd ? uM : .5f * (uP + uM);
+    sv[5 * NF + m] = bnd ? vM : .5f * (vP + vM);
+    sv[6 * NF + m] = bnd ? wP : .5f * (wP + wM);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < ne * 4 * Nfq; i += T) {
+    const int e = i / (4 * Nfq), fq = i % (4 * Nfq), f = fq / Nfq, n = fq % Nfq, row = i0 + e;
+    const float *sv = smem + e * per + o_s + f * Nfp;
+    float dp = 0.f, du = 0.f, dv = 0.f, dw = 0.f, au = 0.f, av = 0.f, aw = 0.f;
+    for (int j = 0; j < Nfp; ++j) {
+      const float V = __ldg(A.VfqFace + n + j * Nfq);
+      dp += V * sv[j];
+      du += V * sv[NF + j];
+      dv += V * sv[2 * NF + j];
+      dw += V * sv[3 * NF + j];
+      au += V * sv[4 * NF + j];
+      av += V * sv[5 * NF + j];
+      aw += V * sv[6 * NF + j];
+    }
+    const float *g = A.fgeoq + ((size_t)row * 4 + f) * 4 * Nfq + n;
+    const float nx = g[0], ny = g[Nfq], nz = g[2 * Nfq], sJ = g[3 * Nfq];
+    const float Unjump = du * nx + dv * ny + dw * nz;
+    const float Unavg = au * nx + av * ny + aw * nz;
+    const float pflux = -(Unavg - .5f * dp) * sJ;
+    const float Uflux = -.5f * (dp - Unjump) * sJ;
+    float *fl = smem + e * per + o_f;
+    fl[fq] = pflux;
+    fl[4 * Nfq + fq] = Uflux * nx;
+    fl[8 * Nfq + fq] = Uflux * ny;
+    fl[12 * Nfq + fq] = Uflux * nz;
+  }
+  __syncthreads();
+  // rhs = volume projection, then the lifted fluxes added face by face
+  for (int i = threadIdx.x; i < ne * Np; i += T) {
+    const int e = i / Np, n = i % Np;
+    const float *t = smem + e * per + o_t;
+    const float *fl = smem + e * per + o_f;
+    float divU = 0.f, dpdx = 0.f, dpdy = 0.f, dpdz = 0.f;
+    for (int m = 0; m < Nq; ++m) {
+      const float P = __ldg(A.Pq + n + m * Np);
+      dpdx += P * t[m];
+      dpdy += P * t[Nq + m];
+      dpdz += P * t[2 * Nq + m];
+      divU += __ldg(A.Prq + n + m * Np) * t[3 * Nq + m];
+      divU += __ldg(A.Psq + n + m * Np) * t[4 * Nq + m];
+      divU += __ldg(A.Ptq + n + m * Np) * t[5 * Nq + m];
+    }
+    float rp = -divU, ru = -dpdx, rv = -dpdy, rw = -dpdz;
+    for (int m = 0; m < 4 * Nfq; ++m) {
+      const float P = __ldg(A.Pfq + n + (size_t)m * Np);
+      rp += P * fl[m];
+      ru += P * fl[4 * Nfq + m];
+      rv += P * fl[8 * Nfq + m];
+      rw += P * fl[12 * Nfq + m];
+    }
+    float *r = smem + e * per + o_r;
+    r[n] = rp, r[Np + n] = ru, r[2 * Np + n] = rv, r[3 * Np + n] = rw;
+  }
+  __syncthreads();
+  // rk_update_WADG: interpolate, weight with 1/J (and c^2 on p), project
+  for (int i = threadIdx.x; i < ne * Nr; i += T) {
+    const int e = i / Nr, n = i % Nr, row = i0 + e;
+    const float *r = smem + e * per + o_r;
+    float a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    for (int j = 0; j < Np; ++j) {
+      const float V = __ldg(A.Vqr + n + j * Nr);
+      a0 += V * r[j];
+      a1 += V * r[j + Np];
+      a2 += V * r[j + 2 * Np];
+      a3 += V * r[j + 3 * Np];
+    }
+    const float c2 = A.c2q[n + (size_t)row * Nr];
+    const float invJ = 1.f / A.Jr[n + (size_t)row * Nr];
+    float *u = smem + e * per + o_u;
+    u[n] = a0 * invJ * c2;
+    u[n + Nr] = a1 * invJ;
+    u[n + 2 * Nr] = a2 * invJ;
+    u[n + 3 * Nr] = a3 * invJ;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < ne * Np; i += T) {
+    const int e = i / Np, n = i % Np, k = A.k_off + i0 + e;
+    const float *u = smem + e * per + o_u;
+    const float *q = smem + e * per;
+    float rp = 0, ru = 0, rv = 0, rw = 0;
+    for (int j = 0; j < Nr; ++j) {
+      const float P = __ldg(A.Pqr + n + j * Np);
+      rp += P * u[j];
+      ru += P * u[j + Nr];
+      rv += P * u[j + 2 * Nr];
+      rw += P * u[j + 3 * Nr];
+    }
+    const float rr[4] = {rp, ru, rv, rw};
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      const size_t id = n + f * Np + (size_t)k * 4 * Np;
+      const float rs = A.fa * res[id] + A.fdt * rr[f];
+      res[id] = rs;
+      Qnew[id] = q[f * Np + n] + A.fb * rs;
+    }
+  }
+}
+
+template <int N>
+bbw_status launch_curved_stage(CurvedStageArgs A, const float *Qold, float *Qnew, float *res,
+                               cudaStream_t st) {
+  constexpr int Np = NP(N), NF = 4 * NFP(N);
+  const size_t per =
+      sizeof(float) * (8 * Np + 6 * (size_t)A.Nq + 7 * NF + 16 * (size_t)A.Nfq + 4 * (size_t)A.Nr);
+  const int width = std::max(std::max(A.Nq, A.Nr), std::max(4 * A.Nfq, NF));
+  A.EB = curved_eb(width, per);
+  if (A.EB * per > kCurvedSmemMax)
+    return set_error(BBW_ERR_UNSUPPORTED, "curved stage: cubature too large for shared memory");
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_curved_stage<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kCurvedSmemMax);
+    attr = true;
+  }
+  k_curved_stage<N><<<(A.KC + A.EB - 1) / A.EB, kCurvedThreads, A.EB * per, st>>>(A, Qold, Qnew,
+                                                                                   res);
+  return check_launch("curved stage");
+}
+
 // ----------------------------------------------------------------- launches
 template <int N>
 bbw_status launch_volume_skew(int K, const int *Klist, int Nq, const float *vgeoq,
@@ -390,6 +585,14 @@ bbw_status planar_surface(int N, int K, const int *Klist, const float *fgeo, con
   if (K == 0) return BBW_OK;
 #define CALL(n) launch_surface_planar<n>(K, Klist, fgeo, J, Fmask, vmapP, LIFT, Q, rhsQ, st)
   BBW_CURVED_DISPATCH(CALL, "rk_surface_planar")
+#undef CALL
+}
+
+bbw_status curved_stage(int N, const CurvedStageArgs &A, const float *Qold, float *Qnew,
+                        float *res, cudaStream_t st) {
+  if (A.KC == 0) return BBW_OK;
+#define CALL(n) launch_curved_stage<n>(A, Qold, Qnew, res, st)
+  BBW_CURVED_DISPATCH(CALL, "curved stage")
 #undef CALL
 }
 

@@ -378,6 +378,83 @@ def precision_workload(args, torch):
             "rows": rows}
 
 
+def curved_bytes_per_element(Np, Nq, Nfq, Nfp, curved):
+    """Algorithmic bytes of one curvilinear stage per element: state and
+    residual read + write (4 fields, FP32), J and c^2 at the update's
+    cubature, the trace map; curved elements add vgeoq + Jq at the volume
+    cubature and nx ny nz sJ at the face cubature, planar ones vgeo, fgeo, J."""
+    base = 64 * Np + 8 * Nq + 16 * Nfp
+    return base + (40 * Nq + 64 * Nfq if curved else 4 * (9 + 16 + 1))
+
+
+def reference_curved_cpu(steps, warmup, nhex, timeout=900):
+    """The reference's curvilinear path on the host cores (oracle/_ref/ref_curved_N3)."""
+    from bbwadg_b200.mesh import kuhn_ball, write_gmsh22
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_curved_N3")
+    if not os.path.exists(exe):
+        return None, "oracle/_ref/ref_curved_N3 not built"
+    d = tempfile.mkdtemp()
+    msh = os.path.join(d, "ball.msh")
+    write_gmsh22(msh, *kuhn_ball(nhex))
+    cores = os.cpu_count() or 1
+    env = dict(os.environ, OMP_NUM_THREADS=str(cores))
+    p = subprocess.run([exe, "bench", msh, "--steps", str(steps), "--warmup", str(warmup)],
+                       capture_output=True, text=True, env=env, timeout=timeout)
+    if p.returncode != 0:
+        return None, "reference run failed: " + p.stderr[-200:]
+    r = json.loads(p.stdout.strip().splitlines()[-1])
+    r["cores"] = cores
+    return r, None
+
+
+def curved_workload(args, torch):
+    """Curvilinear WADG step (RK_step_WADG) on the Gordon-Hall curved unit
+    ball kuhn_ball(n), N = 3 (the reference's tabulated degree-7 rules),
+    c^2 = 1 as InitWADG_curved sets, Bessel initial state: device-timed
+    DOF-stage/s, HBM fraction of the whole stage, and the reference's curved
+    path on the host cores on kuhn_ball(16)."""
+    from bbwadg_b200.curved import CurvedSolver, make_curved_problem
+    N, nh = 3, args.curved_hex
+    cub, tri = reference_rule(N)
+    p = make_curved_problem(N, nh, cubature=cub, tri_cubature=tri)
+    s = CurvedSolver(p)
+    s.set_data(p.Q0)
+    stream = torch.cuda.ExternalStream(s.stream)
+    s.steps(p.dt, 3)
+    s.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    steps = args.curved_steps
+    torch.cuda.synchronize()
+    e0.record(stream)
+    s.steps(p.dt, steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    Q = s.get_data()
+    s.close()
+    KC, KP = len(p.KlistCurved), len(p.KlistPlanar)
+    nfp = (N + 1) * (N + 2) // 2
+    alg = (KC * curved_bytes_per_element(p.Np, p.Nq, p.Nfq, nfp, True) +
+           KP * curved_bytes_per_element(p.Np, p.Nq, p.Nfq, nfp, False))
+    stage_s = ms / 1e3 / (5 * steps)
+    peak, kind = measured_peak()
+    dofs = p.K * p.Np * 4 * 5 * steps
+    out = {"workload": "curvilinear WADG step (RK_step_WADG), N=3, kuhn_ball(%d): K=%d, %d curved"
+                       % (nh, p.K, KC),
+           "value": dofs / (ms / 1e3), "unit": "DOF-stage/s", "ms_per_step": ms / steps,
+           "steps": steps, "hbm_frac_of_stage": alg / stage_s / 1e9 / peak, "peak_kind": kind,
+           "alg_bytes_per_stage": alg, "gpu_launches": 5 * 5 * steps,
+           "finite": bool(np.isfinite(Q).all())}
+    if not args.no_cpu_baseline:
+        r, err = reference_curved_cpu(5, 1, 16)
+        out["cpu_baseline"] = ({"value": r["dof_stage_per_s"], "unit": "DOF-stage/s",
+                                "cores": r["cores"], "kind": "reference",
+                                "sample": "N=3, kuhn_ball(16) (K=%d, %d curved), 5 LSRK45 steps, "
+                                          "reference kernels via oracle/_ref" % (r["K"], r["KCurved"])}
+                               if r else {"value": None, "unavailable": err})
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -389,8 +466,9 @@ def main():
     ap.add_argument("--hex", type=int, default=N_HEX, help="hexes per direction (profiling cases)")
     ap.add_argument("--variants", default="nodal,bb,nodal-f16x3",
                     help="variants to run, comma separated (nodal, bb, nodal-f16x3)")
-    ap.add_argument("--extra", default="shots,adjoint,precision",
-                    help="extra workloads reported beside the headline: shots, adjoint, precision")
+    ap.add_argument("--extra", default="shots,adjoint,precision,curved",
+                    help="extra workloads reported beside the headline: shots, adjoint, "
+                         "precision, curved")
     ap.add_argument("--prec-time", type=float, default=0.02)
     ap.add_argument("--config", type=int, default=0,
                     help="pin the fused-stage configuration code instead of autotuning")
@@ -398,6 +476,8 @@ def main():
     ap.add_argument("--shots-hex", type=int, default=24)
     ap.add_argument("--shots-steps", type=int, default=10)
     ap.add_argument("--adj-steps", type=int, default=400)
+    ap.add_argument("--curved-hex", type=int, default=24)
+    ap.add_argument("--curved-steps", type=int, default=50)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -478,6 +558,7 @@ def main():
     shots = shots_workload(args, torch, dist, world) if "shots" in extra else None
     adj = adjoint_workload(args, torch, dist, rank, world) if "adjoint" in extra else None
     prec = precision_workload(args, torch) if ("precision" in extra and rank == 0) else None
+    curv = curved_workload(args, torch) if ("curved" in extra and rank == 0) else None
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
@@ -534,6 +615,8 @@ def main():
         line["adjoint"] = adj
     if prec is not None:
         line["precision"] = prec
+    if curv is not None:
+        line["curved"] = curv
     print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
