@@ -443,7 +443,8 @@ def curved_workload(args, torch):
                        % (nh, p.K, KC),
            "value": dofs / (ms / 1e3), "unit": "DOF-stage/s", "ms_per_step": ms / steps,
            "steps": steps, "hbm_frac_of_stage": alg / stage_s / 1e9 / peak, "peak_kind": kind,
-           "alg_bytes_per_stage": alg, "gpu_launches": 5 * 5 * steps,
+           "alg_bytes_per_stage": alg,
+           "gpu_launches": 5 * steps * ((KP > 0) + (KC > 0)),  # planar + curved stage kernels
            "finite": bool(np.isfinite(Q).all())}
     if not args.no_cpu_baseline:
         r, err = reference_curved_cpu(5, 1, 16)

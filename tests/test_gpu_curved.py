@@ -8,7 +8,7 @@ import ctypes
 
 import numpy as np
 import pytest
-from conftest import rel_l2
+from conftest import golden, rel_l2
 from test_curved import oracle_of, problem_like_reference
 
 from bbwadg_b200 import _lib
@@ -90,9 +90,24 @@ def test_graph_steps_equal_stage_loop(cuda):
     assert np.array_equal(out[0], out[1])
 
 
+def reference_rules(N):
+    """The reference's tabulated degree-2N+1 rules where a fixture holds them
+    (the fused planar stage keeps a 32-element tile of Nq points in shared
+    memory: N = 7 needs the reference's 214-point rule, not the 512-point
+    Stroud rule)."""
+    import os
+    from conftest import GOLDEN
+    if not os.path.exists(os.path.join(GOLDEN, "ops_N%d.npz" % N)):
+        return None, None
+    g = golden("ops_N%d.npz" % N)
+    nfq = int(np.asarray(g["Nfq"]).ravel()[0])
+    return (g["rq"], g["sq"], g["tq"], g["wq"]), (g["rfq"][:nfq], g["sfq"][:nfq], g["wfqFace"])
+
+
 @pytest.mark.parametrize("N", [1, 4, 5, 7])
 def test_matches_oracle_at_higher_orders(cuda, N):
-    p = make_curved_problem(N, 4, c2=c2_sine)
+    cub, tri = reference_rules(N)
+    p = make_curved_problem(N, 4, c2=c2_sine, cubature=cub, tri_cubature=tri)
     s = CurvedSolver(p)
     s.set_data(p.Q0)
     stages(s, p.dt, 10)
