@@ -420,7 +420,7 @@ def curved_workload(args, torch):
     s = CurvedSolver(p)
     s.set_data(p.Q0)
     stream = torch.cuda.ExternalStream(s.stream)
-    s.steps(p.dt, 3)
+    s.steps(p.dt, args.warmup)
     s.sync()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     steps = args.curved_steps
@@ -479,10 +479,17 @@ def main():
     ap.add_argument("--adj-steps", type=int, default=400)
     ap.add_argument("--curved-hex", type=int, default=24)
     ap.add_argument("--curved-steps", type=int, default=50)
+    ap.add_argument("--curved-only", action="store_true",
+                    help="run only the curvilinear workload and print its object")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
     args.warmup = max(args.warmup, 3)
+    if args.curved_only:  # the curvilinear workload alone (profiling runs)
+        import torch
+        torch.cuda.set_device(dist_env()[2])
+        print(json.dumps({"curved": curved_workload(args, torch)}))
+        return 0
 
     import torch
     import torch.distributed as dist
