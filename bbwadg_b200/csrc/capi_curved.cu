@@ -13,6 +13,10 @@
 //   (k_curved_stage: skew volume + skew surface + 1/J, c^2 WADG update +
 //   LSRK update), reading the same old state and writing the same new
 //   state buffer, so one stage is two launches and no rhs array exists.
+//   The two write disjoint elements, so the curved kernel runs on a second
+//   stream beside the planar one (fork / join by events each stage): the
+//   planar kernel is bound by its shared-memory pipe, the curved one by
+//   latency, and their CTAs share the SMs.
 // bbw_curved_steps captures one LSRK45 step per buffer parity in a CUDA graph.
 #include <cuda_runtime.h>
 
@@ -31,7 +35,8 @@ using namespace bbw;
 
 struct bbw_curved {
   int N = 0, K = 0, Np = 0, KC = 0, KP = 0, device = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr, side = nullptr;  // main stream; the curved kernel's
+  cudaEvent_t fork = nullptr, join = nullptr;
   bbw_ctx *aff = nullptr;             // fused affine stage of the planar elements
   float *Q[2] = {nullptr, nullptr};   // state buffers (the affine context's when it exists)
   float *res = nullptr;
@@ -65,6 +70,9 @@ void release(bbw_curved *h) {
     if (g) cudaGraphExecDestroy(g);
   if (h->aff) bbw_destroy(h->aff);
   for (void *p : h->owned) cudaFree(p);
+  if (h->fork) cudaEventDestroy(h->fork);
+  if (h->join) cudaEventDestroy(h->join);
+  if (h->side) cudaStreamDestroy(h->side);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -81,13 +89,25 @@ std::vector<T> rows(const T *a, const std::vector<int> &perm, size_t w, int from
 bbw_status stage(bbw_curved *h, float fa, float fb, float fdt) {
   const float *Qin = h->Q[h->cur];
   float *Qout = h->Q[h->cur ^ 1];
+  const bool both = h->KP > 0 && h->KC > 0;
+  cudaStream_t cst = both ? h->side : h->stream;
   bbw_status s = BBW_OK;
-  if (h->KP > 0)
+  if (both) {  // fork: the curved kernel waits for everything before this stage
+    cudaError_t e = cudaEventRecord(h->fork, h->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(h->side, h->fork, 0);
+    s = set_cuda_error(e, "curved stage: fork");
+  }
+  if (s == BBW_OK && h->KP > 0)
     s = fused_launch(h->aff->plan, Qin, Qout, h->res, fa, fb, fdt, 0.f, h->stream);
   if (s == BBW_OK && h->KC > 0) {
     CurvedStageArgs A = h->args;
     A.fa = fa, A.fb = fb, A.fdt = fdt;
-    s = curved_stage(h->N, A, Qin, Qout, h->res, h->stream);
+    s = curved_stage(h->N, A, Qin, Qout, h->res, cst);
+  }
+  if (both) {  // join: the next stage reads what both wrote (always joined)
+    cudaError_t e = cudaEventRecord(h->join, h->side);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(h->stream, h->join, 0);
+    if (s == BBW_OK) s = set_cuda_error(e, "curved stage: join");
   }
   if (s == BBW_OK) h->cur ^= 1;
   return s;
@@ -152,6 +172,9 @@ extern "C" bbw_status bbw_curved_create(const bbw_curved_desc *d, int device, bb
   h->N = N, h->K = K, h->Np = Np, h->KC = d->KCurved, h->KP = d->KPlanar, h->device = device;
   h->perm = perm;
   e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming);
   if (e != cudaSuccess) {
     release(h);
     return set_cuda_error(e, "bbw_curved_create: stream");

@@ -289,7 +289,12 @@ __global__ void __launch_bounds__(kCurvedThreads) k_surface_planar(
 // beside the planar elements' stage on the same double-buffered state.
 // Geometry rows are compact: row i of vgeoq / Jq / fgeoq / Jr / c2q
 // (CurvedStageArgs, curved.h).
-
+//
+// The kernel is latency-bound (dependent operator loads, barriers between
+// phases), so every contraction is split into one work item per element x
+// output field x point: 6 Nq items for the volume interpolation, 4 Np for
+// the rhs, 4 Nr and 4 Np for the update, each a single dot product.  Per
+// field the summation order is the one of the reference's kernels.
 template <int N>
 __global__ void __launch_bounds__(kCurvedThreads) k_curved_stage(CurvedStageArgs A,
                                                                  const float *__restrict__ Qold,
@@ -298,9 +303,9 @@ __global__ void __launch_bounds__(kCurvedThreads) k_curved_stage(CurvedStageArgs
   constexpr int Np = NP(N), Nfp = NFP(N), NF = 4 * NFP(N);
   extern __shared__ float smem[];
   const int Nq = A.Nq, Nfq = A.Nfq, Nr = A.Nr;
-  // per element: q[4Np] | t[6Nq] | s[7NF] | fl[16Nfq] | r[4Np] | u[4Nr]
-  const int o_t = 4 * Np, o_s = o_t + 6 * Nq, o_f = o_s + 7 * NF, o_r = o_f + 16 * Nfq,
-            o_u = o_r + 4 * Np, per = o_u + 4 * Nr;
+  // per element: q[4Np] | raw[6Nq] | t[6Nq] | s[7NF] | fl[16Nfq] | r[4Np] | u[4Nr]
+  const int o_raw = 4 * Np, o_t = o_raw + 6 * Nq, o_s = o_t + 6 * Nq, o_f = o_s + 7 * NF,
+            o_r = o_f + 16 * Nfq, o_u = o_r + 4 * Np, per = o_u + 4 * Nr;
   const int i0 = blockIdx.x * A.EB;
   const int ne = min(A.EB, A.KC - i0);
   const int T = blockDim.x;
@@ -309,32 +314,15 @@ __global__ void __launch_bounds__(kCurvedThreads) k_curved_stage(CurvedStageArgs
     smem[e * per + j] = Qold[(size_t)(A.k_off + i0 + e) * 4 * Np + j];
   }
   __syncthreads();
-  // volume: u, v, w and grad_rst p at the cubature (rk_volume_WADG_skew_combine)
-  for (int i = threadIdx.x; i < ne * Nq; i += T) {
-    const int e = i / Nq, n = i % Nq, row = i0 + e;
-    const float *sq = smem + e * per;
-    float dpdr = 0.f, dpds = 0.f, dpdt = 0.f, uq = 0.f, vq = 0.f, wq = 0.f;
-    for (int m = 0; m < Np; ++m) {
-      const float pm = sq[m], um = sq[Np + m], vm = sq[2 * Np + m], wm = sq[3 * Np + m];
-      const float V = __ldg(A.Vq + n + m * Nq);
-      uq += V * um;
-      vq += V * vm;
-      wq += V * wm;
-      dpdr += __ldg(A.Vrq + n + m * Nq) * pm;
-      dpds += __ldg(A.Vsq + n + m * Nq) * pm;
-      dpdt += __ldg(A.Vtq + n + m * Nq) * pm;
-    }
-    const float *g = A.vgeoq + (size_t)row * 9 * Nq + n;
-    const float rx = g[0], sx = g[Nq], tx = g[2 * Nq], ry = g[3 * Nq], sy = g[4 * Nq],
-                ty = g[5 * Nq], rz = g[6 * Nq], sz = g[7 * Nq], tz = g[8 * Nq];
-    const float J = A.Jq[n + (size_t)row * Nq];
-    float *t = smem + e * per + o_t;
-    t[n] = (rx * dpdr + sx * dpds + tx * dpdt) * J;
-    t[Nq + n] = (ry * dpdr + sy * dpds + ty * dpdt) * J;
-    t[2 * Nq + n] = (rz * dpdr + sz * dpds + tz * dpdt) * J;
-    t[3 * Nq + n] = -((uq * rx + vq * ry + wq * rz) * J);
-    t[4 * Nq + n] = -((uq * sx + vq * sy + wq * sz) * J);
-    t[5 * Nq + n] = -((uq * tx + vq * ty + wq * tz) * J);
+  // volume interpolation (rk_volume_WADG_skew_combine): c = 0..2 u v w with
+  // Vq, c = 3..5 dp/dr, dp/ds, dp/dt with Vrq / Vsq / Vtq
+  for (int i = threadIdx.x; i < ne * 6 * Nq; i += T) {
+    const int n = i % Nq, c = (i / Nq) % 6, e = i / (6 * Nq);
+    const float *op = c < 3 ? A.Vq : c == 3 ? A.Vrq : c == 4 ? A.Vsq : A.Vtq;
+    const float *x = smem + e * per + (c < 3 ? (c + 1) * Np : 0);
+    float acc = 0.f;
+    for (int m = 0; m < Np; ++m) acc += __ldg(op + n + m * Nq) * x[m];
+    smem[e * per + o_raw + c * Nq + n] = acc;
   }
   // surface: jumps and averages at the face nodes (rk_surface_WADG_skew_combine)
   for (int i = threadIdx.x; i < ne * NF; i += T) {
@@ -355,6 +343,25 @@ __global__ void __launch_bounds__(kCurvedThreads) k_curved_stage(CurvedStageArgs
     sv[6 * NF + m] = bnd ? wP : .5f * (wP + wM);
   }
   __syncthreads();
+  // geometric factors at the cubature: J grad p and -J (rst-contravariant U)
+  for (int i = threadIdx.x; i < ne * Nq; i += T) {
+    const int e = i / Nq, n = i % Nq, row = i0 + e;
+    const float *raw = smem + e * per + o_raw;
+    const float uq = raw[n], vq = raw[Nq + n], wq = raw[2 * Nq + n];
+    const float dpdr = raw[3 * Nq + n], dpds = raw[4 * Nq + n], dpdt = raw[5 * Nq + n];
+    const float *g = A.vgeoq + (size_t)row * 9 * Nq + n;
+    const float rx = g[0], sx = g[Nq], tx = g[2 * Nq], ry = g[3 * Nq], sy = g[4 * Nq],
+                ty = g[5 * Nq], rz = g[6 * Nq], sz = g[7 * Nq], tz = g[8 * Nq];
+    const float J = A.Jq[n + (size_t)row * Nq];
+    float *t = smem + e * per + o_t;
+    t[n] = (rx * dpdr + sx * dpds + tx * dpdt) * J;
+    t[Nq + n] = (ry * dpdr + sy * dpds + ty * dpdt) * J;
+    t[2 * Nq + n] = (rz * dpdr + sz * dpds + tz * dpdt) * J;
+    t[3 * Nq + n] = -((uq * rx + vq * ry + wq * rz) * J);
+    t[4 * Nq + n] = -((uq * sx + vq * sy + wq * sz) * J);
+    t[5 * Nq + n] = -((uq * tx + vq * ty + wq * tz) * J);
+  }
+  // face cubature: interpolate jumps / averages, upwind fluxes
   for (int i = threadIdx.x; i < ne * 4 * Nfq; i += T) {
     const int e = i / (4 * Nfq), fq = i % (4 * Nfq), f = fq / Nfq, n = fq % Nfq, row = i0 + e;
     const float *sv = smem + e * per + o_s + f * Nfp;
@@ -382,74 +389,50 @@ __global__ void __launch_bounds__(kCurvedThreads) k_curved_stage(CurvedStageArgs
     fl[12 * Nfq + fq] = Uflux * nz;
   }
   __syncthreads();
-  // rhs = volume projection, then the lifted fluxes added face by face
-  for (int i = threadIdx.x; i < ne * Np; i += T) {
-    const int e = i / Np, n = i % Np;
+  // rhs of field c: volume projection (div U weakly for p, Pq grad p for
+  // u, v, w), then the lifted fluxes
+  for (int i = threadIdx.x; i < ne * 4 * Np; i += T) {
+    const int n = i % Np, c = (i / Np) % 4, e = i / (4 * Np);
     const float *t = smem + e * per + o_t;
-    const float *fl = smem + e * per + o_f;
-    float divU = 0.f, dpdx = 0.f, dpdy = 0.f, dpdz = 0.f;
-    for (int m = 0; m < Nq; ++m) {
-      const float P = __ldg(A.Pq + n + m * Np);
-      dpdx += P * t[m];
-      dpdy += P * t[Nq + m];
-      dpdz += P * t[2 * Nq + m];
-      divU += __ldg(A.Prq + n + m * Np) * t[3 * Nq + m];
-      divU += __ldg(A.Psq + n + m * Np) * t[4 * Nq + m];
-      divU += __ldg(A.Ptq + n + m * Np) * t[5 * Nq + m];
+    const float *fl = smem + e * per + o_f + c * 4 * Nfq;
+    float acc = 0.f;
+    if (c == 0) {
+      for (int m = 0; m < Nq; ++m) {
+        acc += __ldg(A.Prq + n + m * Np) * t[3 * Nq + m];
+        acc += __ldg(A.Psq + n + m * Np) * t[4 * Nq + m];
+        acc += __ldg(A.Ptq + n + m * Np) * t[5 * Nq + m];
+      }
+    } else {
+      const float *tc = t + (c - 1) * Nq;
+      for (int m = 0; m < Nq; ++m) acc += __ldg(A.Pq + n + m * Np) * tc[m];
     }
-    float rp = -divU, ru = -dpdx, rv = -dpdy, rw = -dpdz;
-    for (int m = 0; m < 4 * Nfq; ++m) {
-      const float P = __ldg(A.Pfq + n + (size_t)m * Np);
-      rp += P * fl[m];
-      ru += P * fl[4 * Nfq + m];
-      rv += P * fl[8 * Nfq + m];
-      rw += P * fl[12 * Nfq + m];
-    }
-    float *r = smem + e * per + o_r;
-    r[n] = rp, r[Np + n] = ru, r[2 * Np + n] = rv, r[3 * Np + n] = rw;
+    float r = -acc;
+    for (int m = 0; m < 4 * Nfq; ++m) r += __ldg(A.Pfq + n + (size_t)m * Np) * fl[m];
+    smem[e * per + o_r + c * Np + n] = r;
   }
   __syncthreads();
-  // rk_update_WADG: interpolate, weight with 1/J (and c^2 on p), project
-  for (int i = threadIdx.x; i < ne * Nr; i += T) {
-    const int e = i / Nr, n = i % Nr, row = i0 + e;
-    const float *r = smem + e * per + o_r;
-    float a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-    for (int j = 0; j < Np; ++j) {
-      const float V = __ldg(A.Vqr + n + j * Nr);
-      a0 += V * r[j];
-      a1 += V * r[j + Np];
-      a2 += V * r[j + 2 * Np];
-      a3 += V * r[j + 3 * Np];
-    }
-    const float c2 = A.c2q[n + (size_t)row * Nr];
+  // rk_update_WADG: interpolate field c, weight with 1/J (and c^2 on p)
+  for (int i = threadIdx.x; i < ne * 4 * Nr; i += T) {
+    const int n = i % Nr, c = (i / Nr) % 4, e = i / (4 * Nr), row = i0 + e;
+    const float *r = smem + e * per + o_r + c * Np;
+    float a = 0.f;
+    for (int j = 0; j < Np; ++j) a += __ldg(A.Vqr + n + j * Nr) * r[j];
     const float invJ = 1.f / A.Jr[n + (size_t)row * Nr];
-    float *u = smem + e * per + o_u;
-    u[n] = a0 * invJ * c2;
-    u[n + Nr] = a1 * invJ;
-    u[n + 2 * Nr] = a2 * invJ;
-    u[n + 3 * Nr] = a3 * invJ;
+    a *= invJ;
+    if (c == 0) a *= A.c2q[n + (size_t)row * Nr];
+    smem[e * per + o_u + c * Nr + n] = a;
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < ne * Np; i += T) {
-    const int e = i / Np, n = i % Np, k = A.k_off + i0 + e;
-    const float *u = smem + e * per + o_u;
-    const float *q = smem + e * per;
-    float rp = 0, ru = 0, rv = 0, rw = 0;
-    for (int j = 0; j < Nr; ++j) {
-      const float P = __ldg(A.Pqr + n + j * Np);
-      rp += P * u[j];
-      ru += P * u[j + Nr];
-      rv += P * u[j + 2 * Nr];
-      rw += P * u[j + 3 * Nr];
-    }
-    const float rr[4] = {rp, ru, rv, rw};
-#pragma unroll
-    for (int f = 0; f < 4; ++f) {
-      const size_t id = n + f * Np + (size_t)k * 4 * Np;
-      const float rs = A.fa * res[id] + A.fdt * rr[f];
-      res[id] = rs;
-      Qnew[id] = q[f * Np + n] + A.fb * rs;
-    }
+  // project and advance: res = fa res + dt r, Q = Q + fb res
+  for (int i = threadIdx.x; i < ne * 4 * Np; i += T) {
+    const int n = i % Np, c = (i / Np) % 4, e = i / (4 * Np), k = A.k_off + i0 + e;
+    const float *u = smem + e * per + o_u + c * Nr;
+    float acc = 0.f;
+    for (int j = 0; j < Nr; ++j) acc += __ldg(A.Pqr + n + j * Np) * u[j];
+    const size_t id = n + c * Np + (size_t)k * 4 * Np;
+    const float rs = A.fa * res[id] + A.fdt * acc;
+    res[id] = rs;
+    Qnew[id] = smem[e * per + c * Np + n] + A.fb * rs;
   }
 }
 
@@ -457,9 +440,10 @@ template <int N>
 bbw_status launch_curved_stage(CurvedStageArgs A, const float *Qold, float *Qnew, float *res,
                                cudaStream_t st) {
   constexpr int Np = NP(N), NF = 4 * NFP(N);
-  const size_t per =
-      sizeof(float) * (8 * Np + 6 * (size_t)A.Nq + 7 * NF + 16 * (size_t)A.Nfq + 4 * (size_t)A.Nr);
-  const int width = std::max(std::max(A.Nq, A.Nr), std::max(4 * A.Nfq, NF));
+  const size_t per = sizeof(float) * (8 * Np + 12 * (size_t)A.Nq + 7 * NF +
+                                      16 * (size_t)A.Nfq + 4 * (size_t)A.Nr);
+  // a few work items per thread in the widest phase, shared memory bounded
+  const int width = std::max(std::max(A.Nq, A.Nr), std::max(4 * A.Nfq, 4 * Np));
   A.EB = curved_eb(width, per);
   if (A.EB * per > kCurvedSmemMax)
     return set_error(BBW_ERR_UNSUPPORTED, "curved stage: cubature too large for shared memory");
