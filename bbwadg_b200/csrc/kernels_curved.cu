@@ -321,6 +321,7 @@ __global__ void __launch_bounds__(kCurvedThreads) k_curved_stage(CurvedStageArgs
     const float *op = c < 3 ? A.Vq : c == 3 ? A.Vrq : c == 4 ? A.Vsq : A.Vtq;
     const float *x = smem + e * per + (c < 3 ? (c + 1) * Np : 0);
     float acc = 0.f;
+#pragma unroll
     for (int m = 0; m < Np; ++m) acc += __ldg(op + n + m * Nq) * x[m];
     smem[e * per + o_raw + c * Nq + n] = acc;
   }
@@ -366,6 +367,7 @@ __global__ void __launch_bounds__(kCurvedThreads) k_curved_stage(CurvedStageArgs
     const int e = i / (4 * Nfq), fq = i % (4 * Nfq), f = fq / Nfq, n = fq % Nfq, row = i0 + e;
     const float *sv = smem + e * per + o_s + f * Nfp;
     float dp = 0.f, du = 0.f, dv = 0.f, dw = 0.f, au = 0.f, av = 0.f, aw = 0.f;
+#pragma unroll
     for (int j = 0; j < Nfp; ++j) {
       const float V = __ldg(A.VfqFace + n + j * Nfq);
       dp += V * sv[j];
@@ -397,6 +399,7 @@ __global__ void __launch_bounds__(kCurvedThreads) k_curved_stage(CurvedStageArgs
     const float *fl = smem + e * per + o_f + c * 4 * Nfq;
     float acc = 0.f;
     if (c == 0) {
+#pragma unroll 4
       for (int m = 0; m < Nq; ++m) {
         acc += __ldg(A.Prq + n + m * Np) * t[3 * Nq + m];
         acc += __ldg(A.Psq + n + m * Np) * t[4 * Nq + m];
@@ -404,9 +407,11 @@ __global__ void __launch_bounds__(kCurvedThreads) k_curved_stage(CurvedStageArgs
       }
     } else {
       const float *tc = t + (c - 1) * Nq;
+#pragma unroll 8
       for (int m = 0; m < Nq; ++m) acc += __ldg(A.Pq + n + m * Np) * tc[m];
     }
     float r = -acc;
+#pragma unroll 8
     for (int m = 0; m < 4 * Nfq; ++m) r += __ldg(A.Pfq + n + (size_t)m * Np) * fl[m];
     smem[e * per + o_r + c * Np + n] = r;
   }
@@ -416,6 +421,7 @@ __global__ void __launch_bounds__(kCurvedThreads) k_curved_stage(CurvedStageArgs
     const int n = i % Nr, c = (i / Nr) % 4, e = i / (4 * Nr), row = i0 + e;
     const float *r = smem + e * per + o_r + c * Np;
     float a = 0.f;
+#pragma unroll
     for (int j = 0; j < Np; ++j) a += __ldg(A.Vqr + n + j * Nr) * r[j];
     const float invJ = 1.f / A.Jr[n + (size_t)row * Nr];
     a *= invJ;
@@ -428,6 +434,7 @@ __global__ void __launch_bounds__(kCurvedThreads) k_curved_stage(CurvedStageArgs
     const int n = i % Np, c = (i / Np) % 4, e = i / (4 * Np), k = A.k_off + i0 + e;
     const float *u = smem + e * per + o_u + c * Nr;
     float acc = 0.f;
+#pragma unroll 8
     for (int j = 0; j < Nr; ++j) acc += __ldg(A.Pqr + n + j * Np) * u[j];
     const size_t id = n + c * Np + (size_t)k * 4 * Np;
     const float rs = A.fa * res[id] + A.fdt * acc;
