@@ -104,11 +104,18 @@ class WaveSolver:
             raise ValueError("state has %d values, expected %d" % (Q.size, self.state_size))
         _lib.call("bbw_set_state", self._h, Q.ctypes.data)
 
-    def get_data(self):
-        """WaveGetData3d (raw coefficients; BB -> nodal is Problem.to_nodal)."""
-        Q = np.empty(self.state_size, np.float32)
-        _lib.call("bbw_get_state", self._h, Q.ctypes.data)
-        return Q
+    def get_data(self, out=None):
+        """WaveGetData3d (raw coefficients; BB -> nodal is Problem.to_nodal).
+        ``out``: a contiguous float32 host array of the state's size to copy
+        into (pinned memory makes the device-to-host copy direct)."""
+        if out is None:
+            out = np.empty(self.state_size, np.float32)
+        elif (out.dtype != np.float32 or out.size != self.state_size
+              or not out.flags["C_CONTIGUOUS"]):
+            raise ValueError("out must be a contiguous float32 array of %d values"
+                             % self.state_size)
+        _lib.call("bbw_get_state", self._h, out.ctypes.data)
+        return out
 
     def set_residual(self, r):
         r = _f32(r)

@@ -550,7 +550,7 @@ def main():
         t0 = time.perf_counter()
         s.set_data(pinned.numpy())
         s.steps(prob.dt, args.steps)
-        out.copy_(torch.from_numpy(s.get_data()))
+        s.get_data(out=out.numpy())
         t_e2e = time.perf_counter() - t0
         if world > 1:
             t = torch.tensor([t_e2e], device="cuda")
