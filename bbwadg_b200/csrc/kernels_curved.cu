@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(kCurvedThreads) k_surface_planar(
 // the rhs, 4 Nr and 4 Np for the update, each a single dot product.  Per
 // field the summation order is the one of the reference's kernels.
 template <int N>
-__global__ void __launch_bounds__(kCurvedThreads) k_curved_stage(CurvedStageArgs A,
+__global__ void __launch_bounds__(kCurvedThreads, 6) k_curved_stage(CurvedStageArgs A,
                                                                  const float *__restrict__ Qold,
                                                                  float *__restrict__ Qnew,
                                                                  float *__restrict__ res) {
