@@ -314,7 +314,7 @@ extern "C" bbw_status bbw_backward(bbw_ctx *c, bbw_tape *t, const float *dL_dtra
         const float ai = (float)kRK4A[i], bi = (float)kRK4B[i];
         if ((s = adj_wadg(N, S, K, Nq, a.Vq, a.Pq, pl.c2q, lamQ, lamR, ai, bi, dt,
                           vqs + (size_t)i * vqn, z, grad, st)) != BBW_OK ||
-            (s = rk_volume_shots(N, S, K, c->vgeo, a.DT[0], a.DT[1], a.DT[2], z, rhs, st)) !=
+            (s = adj_volume(N, S, K, c->vgeo, a.DT[0], a.DT[1], a.DT[2], z, rhs, st)) !=
                 BBW_OK ||
             (s = adj_sigma(N, S, K, c->fgeo, a.LIFT, z, sigma, st)) != BBW_OK ||
             (s = adj_gather(N, S, K, c->bc, dt, c->fgeo, a.fidx, a.mapP, sigma, rhs, lamQ, st)) !=

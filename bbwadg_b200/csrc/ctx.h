@@ -41,6 +41,8 @@ bbw_status adj_wadg(int N, int S, int K, int Nq, const float *Vq, const float *P
                     float *z, double *grad, cudaStream_t st);
 bbw_status adj_sigma(int N, int S, int K, const float *fgeo, const float *LIFT, const float *z,
                      float *sigma, cudaStream_t st);
+bbw_status adj_volume(int N, int S, int K, const float *vgeo, const float *Dr, const float *Ds,
+                      const float *Dt, const float *z, float *vol, cudaStream_t st);
 bbw_status adj_gather(int N, int S, int K, int bc, float dt, const float *fgeo, const int *fidx,
                       const int *mapP, const float *sigma, const float *vol, float *lamQ,
                       cudaStream_t st);

@@ -13,8 +13,7 @@
 //     dL/dc2q[k][q] += dt (Pq^T mu_p)_q (Vq S(Q)_p)_q        (FP64)
 //     lamQ += dt S^T z,  lamR = a mu.
 // S^T z = volume^T z + surface^T z.  The volume part has the forward
-// volume's form with Dr, Ds, Dt replaced by their transposes (run through
-// the kernel-level volume kernel).  The surface part: with
+// volume's form with Dr, Ds, Dt replaced by their transposes (k_adj_volume).  The surface part: with
 //     sigma[k][f][i] = .5 Fscale LIFT_f^T (z_p - n_f . z_U)   (per face node)
 // the pressure and velocity adjoints of each face node collect
 //     p: -sigma_k + sigma_k2,   U: n_k sigma_k - n_k2 sigma_k2
@@ -31,11 +30,24 @@ constexpr int AE = 32;   // elements per CTA (lane = element)
 constexpr int AW = 8;    // warps per CTA
 constexpr int AS = AE + 1;  // shared row stride
 
+// Operators are staged per CTA in shared memory with the contraction index
+// outer and four consecutive output rows contiguous (row stride padded to 4):
+// one warp-uniform 16-byte shared load then feeds four rows of the warp's
+// register block, each applied to the element values of the 32 lanes.
+__device__ __forceinline__ int pad4(int x) { return (x + 3) & ~3; }
+
+__device__ __forceinline__ void fma4(float (&acc)[4], const float4 a, float x) {
+  acc[0] = fmaf(a.x, x, acc[0]);
+  acc[1] = fmaf(a.y, x, acc[1]);
+  acc[2] = fmaf(a.z, x, acc[2]);
+  acc[3] = fmaf(a.w, x, acc[3]);
+}
+
 // mu = lamR + b lamQ; lamR <- a mu; z <- W^T mu; grad[q][k] += dt t_q v_q with
 // t = Pq^T mu_p and v = Vq S(Q)_p stored by the forward recomputation
-// ([shot][Nq][K]).  Lane = element, warps own rows; operator values are warp
-// broadcasts.  The shots of a tile are done in turn, so every gradient
-// entry is accumulated by one thread in shot order.
+// ([shot][Nq][K]).  Lane = element, warps own quads of rows.  The shots of a
+// tile are done in turn, so every gradient entry is accumulated by one
+// thread in shot order.
 template <int N>
 __global__ void __launch_bounds__(AE * AW) k_adj_wadg(int S, int K, int Nq,
                                                      const float *__restrict__ Vq,
@@ -46,15 +58,26 @@ __global__ void __launch_bounds__(AE * AW) k_adj_wadg(int S, int K, int Nq,
                                                      float dt, const float *__restrict__ vq,
                                                      float *__restrict__ z,
                                                      double *__restrict__ grad) {
-  constexpr int Np = NP(N);
+  constexpr int Np = NP(N), ldp = (NP(N) + 3) & ~3;
   extern __shared__ float smem[];
-  float *sMu = smem;               // [Np][AS]
-  float *sZ = sMu + Np * AS;       // [Np][AS]
-  float *sT = sZ + Np * AS;        // [Nq][AS]
-  float *sC = sT + Nq * AS;        // [Nq][AS] c2/J
+  const int ldq = pad4(Nq);
+  float *sPt = smem;                // [Np][ldq]: Pq^T, row q of column n at n*ldq + q
+  float *sVt = sPt + Np * ldq;      // [Nq][ldp]: Vq^T, row n of column q at q*ldp + n
+  float *sMu = sVt + Nq * ldp;      // [Np][AS]
+  float *sT = sMu + Np * AS;        // [Nq][AS]
+  float *sC = sT + Nq * AS;         // [Nq][AS] c2/J
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int k0 = blockIdx.x * AE, ne = min(AE, K - k0);
+  for (int i = tid; i < Np * ldq; i += AE * AW) {
+    const int n = i / ldq, q = i - n * ldq;
+    sPt[i] = q < Nq ? __ldg(Pq + n + (size_t)q * Np) : 0.f;
+  }
+  for (int i = tid; i < Nq * ldp; i += AE * AW) {
+    const int q = i / ldp, n = i - q * ldp;
+    sVt[i] = n < Np ? __ldg(Vq + q + (size_t)n * Nq) : 0.f;
+  }
   for (int i = tid; i < ne * Nq; i += AE * AW) sC[(i % Nq) * AS + i / Nq] = c2q[(size_t)k0 * Nq + i];
+  const int nqq = (Nq + 3) >> 2, npq = (Np + 3) >> 2;
   for (int sh = 0; sh < S; ++sh) {
     const size_t so = (size_t)sh * K * 4 * Np + (size_t)k0 * 4 * Np;
     __syncthreads();
@@ -65,68 +88,182 @@ __global__ void __launch_bounds__(AE * AW) k_adj_wadg(int S, int K, int Nq,
       if (fn < Np) sMu[fn * AS + e] = mu;
       else z[so + i] = mu;  // velocity rows: Pq Vq = I (J = 1)
     }
+    for (int i = tid; i < (AE - ne) * Np; i += AE * AW)  // idle lanes of a partial tile
+      sMu[(i % Np) * AS + ne + i / Np] = 0.f;
     __syncthreads();
-    for (int q = warp; q < Nq; q += AW) {
-      float t = 0.f;
+    for (int qq = warp; qq < nqq; qq += AW) {  // t = Pq^T mu_p, rows 4qq..4qq+3
+      float t[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll 5
-      for (int n = 0; n < Np; ++n) t += __ldg(Pq + n + (size_t)q * Np) * sMu[n * AS + lane];
-      if (lane < ne) {
-        const size_t g = (size_t)q * K + k0 + lane;
-        if (vq) grad[g] += (double)dt * (double)t * (double)vq[((size_t)sh * Nq + q) * K + k0 + lane];
-        sT[q * AS + lane] = sC[q * AS + lane] * t;
+      for (int n = 0; n < Np; ++n)
+        fma4(t, reinterpret_cast<const float4 *>(sPt + n * ldq)[qq], sMu[n * AS + lane]);
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int q = 4 * qq + r;
+        if (q < Nq && lane < ne) {
+          const size_t g = (size_t)q * K + k0 + lane;
+          if (vq)
+            grad[g] += (double)dt * (double)t[r] *
+                       (double)vq[((size_t)sh * Nq + q) * K + k0 + lane];
+          sT[q * AS + lane] = sC[q * AS + lane] * t[r];
+        } else if (q < Nq) {
+          sT[q * AS + lane] = 0.f;
+        }
       }
     }
     __syncthreads();
-    for (int n = warp; n < Np; n += AW) {
-      float acc = 0.f;
-      for (int q = 0; q < Nq; ++q) acc += __ldg(Vq + q + (size_t)n * Nq) * sT[q * AS + lane];
-      sZ[n * AS + lane] = acc;
+    for (int nq = warp; nq < npq; nq += AW) {  // z_p = Vq^T (c2 t), rows 4nq..4nq+3
+      float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 4
+      for (int q = 0; q < Nq; ++q)
+        fma4(acc, reinterpret_cast<const float4 *>(sVt + q * ldp)[nq], sT[q * AS + lane]);
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {  // mu_p is dead: its rows take z_p
+        const int n = 4 * nq + r;
+        if (n < Np) sMu[n * AS + lane] = acc[r];
+      }
     }
     __syncthreads();
     for (int i = tid; i < ne * Np; i += AE * AW) {
       const int e = i / Np, n = i - e * Np;
-      z[so + (size_t)e * 4 * Np + n] = sZ[n * AS + e];
+      z[so + (size_t)e * 4 * Np + n] = sMu[n * AS + e];
     }
   }
 }
 
 // sigma[k][m] = .5 Fscale_f sum_n LIFT[n + m Np] (z_p[n] - n_f . z_U[n]) for the
-// S*K elements of all shots (geometry row k % Kg); lane = element
+// S*K elements of all shots (geometry row k % Kg); lane = element.  The face
+// combinations w_f = z_p - n_f . z_U are formed once per face, then each warp
+// takes quads of one face's rows.
 template <int N>
 __global__ void __launch_bounds__(AE * AW) k_adj_sigma(int K, int Kg,
                                                       const float *__restrict__ fgeo,
                                                       const float *__restrict__ LIFT,
                                                       const float *__restrict__ z,
                                                       float *__restrict__ sigma) {
-  constexpr int Np = NP(N), Nfp = NFP(N), NF = 4 * NFP(N);
+  constexpr int Np = NP(N), Nfp = NFP(N), NF = 4 * NFP(N), ldf = (NFP(N) + 3) & ~3;
   extern __shared__ float smem[];
-  float *sZ = smem;                 // [4Np][AS]
-  float *sO = sZ + 4 * Np * AS;     // [NF][AS]
+  float *sL = smem;                 // [4][Np][ldf]: LIFT^T per face
+  float *sZ = sL + 4 * Np * ldf;    // [4Np][AS]
+  float *sW = sZ + 4 * Np * AS;     // [4][Np][AS]
+  float *sO = sW + 4 * Np * AS;     // [NF][AS]
   float *sG = sO + NF * AS;         // [AE][16]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int k0 = blockIdx.x * AE, ne = min(AE, K - k0);
+  for (int i = tid; i < 4 * Np * ldf; i += AE * AW) {
+    const int f = i / (Np * ldf), r = i - f * Np * ldf, n = r / ldf, j = r - n * ldf;
+    sL[i] = j < Nfp ? __ldg(LIFT + n + (size_t)(f * Nfp + j) * Np) : 0.f;
+  }
   for (int i = tid; i < ne * 4 * Np; i += AE * AW)
     sZ[(i % (4 * Np)) * AS + i / (4 * Np)] = z[(size_t)k0 * 4 * Np + i];
   for (int i = tid; i < ne * 16; i += AE * AW)
     sG[i] = fgeo[(size_t)((k0 + i / 16) % Kg) * 16 + i % 16];
   __syncthreads();
-  for (int m = warp; m < NF; m += AW) {
-    const int f = m / Nfp;
-    const int e = lane < ne ? lane : 0;
-    const float Fs = sG[e * 16 + 4 * f], nx = sG[e * 16 + 4 * f + 1], ny = sG[e * 16 + 4 * f + 2],
+  const int e = lane < ne ? lane : 0;
+  for (int i = warp; i < 4 * Np; i += AW) {  // w_f[n] per lane
+    const int f = i / Np, n = i - f * Np;
+    const float nx = sG[e * 16 + 4 * f + 1], ny = sG[e * 16 + 4 * f + 2],
                 nz = sG[e * 16 + 4 * f + 3];
-    float acc = 0.f;
+    sW[i * AS + lane] = lane < ne ? sZ[n * AS + lane] - (nx * sZ[(Np + n) * AS + lane] +
+                                                         ny * sZ[(2 * Np + n) * AS + lane] +
+                                                         nz * sZ[(3 * Np + n) * AS + lane])
+                                  : 0.f;
+  }
+  __syncthreads();
+  constexpr int nfq = (Nfp + 3) >> 2;
+  for (int u = warp; u < 4 * nfq; u += AW) {
+    const int f = u / nfq, jq = u - f * nfq;
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    const float *L = sL + f * Np * ldf;
+    const float *w = sW + f * Np * AS;
 #pragma unroll 5
-    for (int n = 0; n < Np; ++n) {
-      const float w = sZ[n * AS + lane] - (nx * sZ[(Np + n) * AS + lane] +
-                                           ny * sZ[(2 * Np + n) * AS + lane] +
-                                           nz * sZ[(3 * Np + n) * AS + lane]);
-      acc += __ldg(LIFT + n + (size_t)m * Np) * w;
+    for (int n = 0; n < Np; ++n)
+      fma4(acc, reinterpret_cast<const float4 *>(L + n * ldf)[jq], w[n * AS + lane]);
+    const float Fs = sG[e * 16 + 4 * f];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int j = 4 * jq + r;
+      if (j < Nfp) sO[(f * Nfp + j) * AS + lane] = .5f * Fs * acc[r];
     }
-    sO[m * AS + lane] = .5f * Fs * acc;
   }
   __syncthreads();
   for (int i = tid; i < ne * NF; i += AE * AW) sigma[(size_t)k0 * NF + i] = sO[(i % NF) * AS + i / NF];
+}
+
+// Volume part of S^T z: the forward volume form (rk_volume,
+// cpp/okl/WaveKernels.okl:44-153) with the given derivative operators (the
+// transposes of Dr, Ds, Dt), for the S*K elements of all shots (geometry row
+// k % Kg).  Lane = element; each warp takes quads of output rows with the
+// four gradient / divergence sums in registers; per-output summation order
+// as in the forward kernel.
+template <int N>
+__global__ void __launch_bounds__(AE * AW) k_adj_volume(int K, int Kg,
+                                                       const float *__restrict__ vgeo,
+                                                       const float *__restrict__ Dr,
+                                                       const float *__restrict__ Ds,
+                                                       const float *__restrict__ Dt,
+                                                       const float *__restrict__ z,
+                                                       float *__restrict__ vol) {
+  constexpr int Np = NP(N), ldp = (NP(N) + 3) & ~3, npq = (NP(N) + 3) >> 2;
+  extern __shared__ float smem[];
+  float *sD = smem;                   // [3][Np][ldp]: column m of D_d at (d*Np + m)*ldp
+  float *sX = sD + 3 * Np * ldp;      // [4Np][AS]: p, then U in the rst directions
+  float *sO = sX + 4 * Np * AS;       // [4Np][AS]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int k0 = blockIdx.x * AE, ne = min(AE, K - k0);
+  for (int i = tid; i < 3 * Np * ldp; i += AE * AW) {
+    const int d = i / (Np * ldp), r = i - d * Np * ldp, m = r / ldp, n = r - m * ldp;
+    const float *D = d == 0 ? Dr : d == 1 ? Ds : Dt;
+    sD[i] = n < Np ? __ldg(D + n + (size_t)m * Np) : 0.f;
+  }
+  for (int i = tid; i < AE * 4 * Np; i += AE * AW) {
+    const int e = i / (4 * Np), j = i - e * 4 * Np;
+    sX[j * AS + e] = e < ne ? z[(size_t)k0 * 4 * Np + i] : 0.f;
+  }
+  float G[9];
+  const int kg = (k0 + (lane < ne ? lane : 0)) % Kg;
+#pragma unroll
+  for (int c = 0; c < 9; ++c) G[c] = __ldg(vgeo + (size_t)kg * 9 + c);
+  __syncthreads();
+  for (int n = warp; n < Np; n += AW) {  // u, v, w -> contravariant components, in place
+    const float un = sX[(Np + n) * AS + lane], vn = sX[(2 * Np + n) * AS + lane],
+                wn = sX[(3 * Np + n) * AS + lane];
+    sX[(Np + n) * AS + lane] = un * G[0] + vn * G[1] + wn * G[2];
+    sX[(2 * Np + n) * AS + lane] = un * G[3] + vn * G[4] + wn * G[5];
+    sX[(3 * Np + n) * AS + lane] = un * G[6] + vn * G[7] + wn * G[8];
+  }
+  __syncthreads();
+  for (int nq = warp; nq < npq; nq += AW) {
+    float dr[4] = {0.f, 0.f, 0.f, 0.f}, ds[4] = {0.f, 0.f, 0.f, 0.f};
+    float dt[4] = {0.f, 0.f, 0.f, 0.f}, dv[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 5
+    for (int m = 0; m < Np; ++m) {
+      const float4 a = reinterpret_cast<const float4 *>(sD + m * ldp)[nq];
+      const float4 b = reinterpret_cast<const float4 *>(sD + (Np + m) * ldp)[nq];
+      const float4 c = reinterpret_cast<const float4 *>(sD + (2 * Np + m) * ldp)[nq];
+      const float p = sX[m * AS + lane], ur = sX[(Np + m) * AS + lane],
+                  us = sX[(2 * Np + m) * AS + lane], ut = sX[(3 * Np + m) * AS + lane];
+      fma4(dr, a, p);
+      fma4(ds, b, p);
+      fma4(dt, c, p);
+      fma4(dv, a, ur);
+      fma4(dv, b, us);
+      fma4(dv, c, ut);
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int n = 4 * nq + r;
+      if (n >= Np) continue;
+      sO[n * AS + lane] = -dv[r];
+      sO[(Np + n) * AS + lane] = -(G[0] * dr[r] + G[3] * ds[r] + G[6] * dt[r]);
+      sO[(2 * Np + n) * AS + lane] = -(G[1] * dr[r] + G[4] * ds[r] + G[7] * dt[r]);
+      sO[(3 * Np + n) * AS + lane] = -(G[2] * dr[r] + G[5] * ds[r] + G[8] * dt[r]);
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < ne * 4 * Np; i += AE * AW) {
+    const int e = i / (4 * Np), j = i - e * 4 * Np;
+    vol[(size_t)k0 * 4 * Np + i] = sO[j * AS + e];
+  }
 }
 
 // lamQ[k][.][n] += dt (vol[k][.][n] + surface adjoint at node n)
@@ -202,7 +339,9 @@ static bbw_status launch_adj_n(int S, int K, int Nq, const float *Vq, const floa
                                float dt, const float *vq, float *z, double *grad,
                                cudaStream_t st) {
   constexpr int Np = NP(N);
-  const size_t sm = sizeof(float) * (size_t)AS * (2 * Np + 2 * Nq);
+  const int ldq = (Nq + 3) & ~3, ldp = (Np + 3) & ~3;
+  const size_t sm = sizeof(float) * ((size_t)Np * ldq + (size_t)Nq * ldp +
+                                     (size_t)AS * (Np + 2 * Nq));
   if (sm > 200 * 1024) return set_error(BBW_ERR_UNSUPPORTED, "adjoint WADG: Nq too large");
   static bool attr = false;
   if (!attr) {
@@ -217,8 +356,10 @@ static bbw_status launch_adj_n(int S, int K, int Nq, const float *Vq, const floa
 template <int N>
 static bbw_status launch_sigma_n(int S, int K, const float *fgeo, const float *LIFT,
                                  const float *z, float *sigma, cudaStream_t st) {
-  constexpr int Np = NP(N), NF = 4 * NFP(N);
-  const size_t sm = sizeof(float) * ((size_t)AS * (4 * Np + NF) + AE * 16);
+  constexpr int Np = NP(N), NF = 4 * NFP(N), ldf = (NFP(N) + 3) & ~3;
+  const size_t sm =
+      sizeof(float) * ((size_t)4 * Np * ldf + (size_t)AS * (8 * Np + NF) + AE * 16);
+  if (sm > 200 * 1024) return set_error(BBW_ERR_UNSUPPORTED, "adjoint lift: N too large");
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_adj_sigma<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -226,6 +367,22 @@ static bbw_status launch_sigma_n(int S, int K, const float *fgeo, const float *L
   }
   k_adj_sigma<N><<<(S * K + AE - 1) / AE, AE * AW, sm, st>>>(S * K, K, fgeo, LIFT, z, sigma);
   return check_launch("adjoint lift");
+}
+
+template <int N>
+static bbw_status launch_volume_n(int S, int K, const float *vgeo, const float *Dr,
+                                  const float *Ds, const float *Dt, const float *z, float *vol,
+                                  cudaStream_t st) {
+  constexpr int Np = NP(N), ldp = (NP(N) + 3) & ~3;
+  const size_t sm = sizeof(float) * ((size_t)3 * Np * ldp + (size_t)8 * Np * AS);
+  if (sm > 200 * 1024) return set_error(BBW_ERR_UNSUPPORTED, "adjoint volume: N too large");
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_adj_volume<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr = true;
+  }
+  k_adj_volume<N><<<(S * K + AE - 1) / AE, AE * AW, sm, st>>>(S * K, K, vgeo, Dr, Ds, Dt, z, vol);
+  return check_launch("adjoint volume");
 }
 
 template <int N>
@@ -262,6 +419,13 @@ bbw_status adj_wadg(int N, int S, int K, int Nq, const float *Vq, const float *P
 bbw_status adj_sigma(int N, int S, int K, const float *fgeo, const float *LIFT, const float *z,
                      float *sigma, cudaStream_t st) {
 #define CALL(n) launch_sigma_n<n>(S, K, fgeo, LIFT, z, sigma, st)
+  BBW_N_SWITCH(CALL)
+#undef CALL
+}
+
+bbw_status adj_volume(int N, int S, int K, const float *vgeo, const float *Dr, const float *Ds,
+                      const float *Dt, const float *z, float *vol, cudaStream_t st) {
+#define CALL(n) launch_volume_n<n>(S, K, vgeo, Dr, Ds, Dt, z, vol, st)
   BBW_N_SWITCH(CALL)
 #undef CALL
 }
