@@ -49,13 +49,6 @@ bbw_status adj_gather(int N, int S, int K, int bc, float dt, const float *fgeo, 
 bbw_status adj_receivers(int S, int K, int Np, int R, const int *rec_elem, const float *rec_w,
                          const float *g, int nsteps, int n, float *lamQ, cudaStream_t st);
 bbw_status set_device_double(double *p, double v, cudaStream_t st);
-// kernel-level volume / surface over S shots of one K-element mesh (kernels_ref.cu)
-bbw_status rk_volume_shots(int N, int S, int K, const float *vgeo, const float *Dr,
-                           const float *Ds, const float *Dt, const float *Q, float *rhsQ,
-                           cudaStream_t st);
-bbw_status rk_surface_shots(int N, int S, int K, int bc, const float *fgeo, const int *Fmask,
-                            const int *vmapP, const float *LIFT, const float *Q, float *rhsQ,
-                            cudaStream_t st);
 
 }  // namespace bbw
 

@@ -679,44 +679,3 @@ extern "C" bbw_status bbw_rk_surface_bern_slice(int N, int K, int bc, const floa
 #undef CALL
   return set_error(BBW_ERR_UNSUPPORTED, "bbw_rk_surface_bern_slice: N out of range");
 }
-
-namespace bbw {
-
-// S shots of one mesh of K elements in one launch (state [S][K][4][Np])
-bbw_status rk_volume_shots(int N, int S, int K, const float *vgeo, const float *Dr,
-                           const float *Ds, const float *Dt, const float *Q, float *rhsQ,
-                           cudaStream_t st) {
-#define CALL(n) launch_volume<n>(S * K, K, vgeo, Dr, Ds, Dt, Q, rhsQ, st)
-  switch (N) {
-    case 1: return CALL(1);
-    case 2: return CALL(2);
-    case 3: return CALL(3);
-    case 4: return CALL(4);
-    case 5: return CALL(5);
-    case 6: return CALL(6);
-    case 7: return CALL(7);
-    case 8: return CALL(8);
-  }
-#undef CALL
-  return set_error(BBW_ERR_UNSUPPORTED, "volume: N out of range");
-}
-
-bbw_status rk_surface_shots(int N, int S, int K, int bc, const float *fgeo, const int *Fmask,
-                            const int *vmapP, const float *LIFT, const float *Q, float *rhsQ,
-                            cudaStream_t st) {
-#define CALL(n) launch_surface<n>(S * K, K, bc, fgeo, Fmask, vmapP, LIFT, Q, rhsQ, st)
-  switch (N) {
-    case 1: return CALL(1);
-    case 2: return CALL(2);
-    case 3: return CALL(3);
-    case 4: return CALL(4);
-    case 5: return CALL(5);
-    case 6: return CALL(6);
-    case 7: return CALL(7);
-    case 8: return CALL(8);
-  }
-#undef CALL
-  return set_error(BBW_ERR_UNSUPPORTED, "surface: N out of range");
-}
-
-}  // namespace bbw
