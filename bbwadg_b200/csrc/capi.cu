@@ -241,9 +241,11 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
   if (!out) return set_error(BBW_ERR_ARG, "bbw_create: out is NULL");
   *out = nullptr;
   if (!m || !o || (variant != BBW_NODAL && variant != BBW_BB) || (bc != 0 && bc != 1) ||
-      (precision != BBW_PREC_FP32 && precision != BBW_PREC_F16X3))
+      (precision != BBW_PREC_FP32 && precision != BBW_PREC_F16X3 &&
+       precision != BBW_PREC_BF16X3))
     return set_error(BBW_ERR_ARG, "bbw_create: bad argument");
-  if (precision == BBW_PREC_F16X3 && (variant != BBW_NODAL || !tc_supported(m->N, m->Nq)))
+  const bool tcp = precision == BBW_PREC_F16X3 || precision == BBW_PREC_BF16X3;
+  if (tcp && (variant != BBW_NODAL || !tc_supported(m->N, m->Nq)))
     return set_error(BBW_ERR_UNSUPPORTED,
                      "bbw_create: the split-FP16 tensor-core stage supports the nodal variant "
                      "with N in {3, 5} and Nq <= 128");
@@ -387,10 +389,11 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
     return s;
   }
   c->precision = precision;
-  if (precision == BBW_PREC_F16X3) {
-    // geometry records, split-FP16 operators in the canonical K-major layout
+  if (tcp) {
+    // geometry records, split-FP16 / split-BF16 operators in the canonical
+    // K-major layout
     TcPlan &tp = c->tc;
-    tp.N = N, tp.K = K, tp.Nq = Nq, tp.bc = bc;
+    tp.N = N, tp.K = K, tp.Nq = Nq, tp.bc = bc, tp.bf = precision == BBW_PREC_BF16X3;
     tp.table_ints = (int)tab.size(), tp.pat_off = pat_off;
     tp.L = tc_layout(N, Nq, tp.table_ints);
     const TcLayout &TL = tp.L;
@@ -399,17 +402,19 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
       std::memcpy(&geo[(size_t)k * TC_GEO], m->vgeo + (size_t)k * 9, 9 * sizeof(float));
       std::memcpy(&geo[(size_t)k * TC_GEO + 9], m->fgeo + (size_t)k * 16, 16 * sizeof(float));
     }
-    std::vector<__half> h(TL.ops_halfs);
+    std::vector<uint16_t> h(TL.ops_halfs);
     const float *Dd[3] = {o->Dr, o->Ds, o->Dt};
     for (int d = 0; d < 3; ++d)
       tc_pack_operator(Dd[d], Np, Np, 1, Np, 64, TL.KV, &h[TL.oD + 2 * d * 64 * TL.KV],
-                       &h[TL.oD + (2 * d + 1) * 64 * TL.KV]);
+                       &h[TL.oD + (2 * d + 1) * 64 * TL.KV], tp.bf);
     for (int f = 0; f < 4; ++f)
       tc_pack_operator(o->LIFT + (size_t)f * Nfp * Np, Np, Nfp, 1, Np, 64, TL.KF,
-                       &h[TL.oL + 2 * f * 64 * TL.KF], &h[TL.oL + (2 * f + 1) * 64 * TL.KF]);
-    tc_pack_operator(o->Vq, Nq, Np, 1, Nq, TL.MQ, TL.KV, &h[TL.oVq], &h[TL.oVq + TL.MQ * TL.KV]);
-    tc_pack_operator(o->Pq, Np, Nq, 1, Np, 64, TL.KQ, &h[TL.oPq], &h[TL.oPq + 64 * TL.KQ]);
-    __half *dops = nullptr;
+                       &h[TL.oL + 2 * f * 64 * TL.KF], &h[TL.oL + (2 * f + 1) * 64 * TL.KF],
+                       tp.bf);
+    tc_pack_operator(o->Vq, Nq, Np, 1, Nq, TL.MQ, TL.KV, &h[TL.oVq], &h[TL.oVq + TL.MQ * TL.KV],
+                     tp.bf);
+    tc_pack_operator(o->Pq, Np, Nq, 1, Np, 64, TL.KQ, &h[TL.oPq], &h[TL.oPq + 64 * TL.KQ], tp.bf);
+    uint16_t *dops = nullptr;
     if ((s = upload(&c->geo_tc, geo.data(), geo.size(), "bbw_create: geometry")) != BBW_OK ||
         (s = upload(&dops, h.data(), h.size(), "bbw_create: tensor-core operators")) != BBW_OK ||
         (s = upload<int>(&c->err, nullptr, 1, "bbw_create: status")) != BBW_OK) {
@@ -485,7 +490,7 @@ static void drop_graphs(bbw_ctx *c) {
 extern "C" bbw_status bbw_stage_ex(bbw_ctx *c, float fa, float fb, float fdt, float cstage) {
   if (!c) return set_error(BBW_ERR_ARG, "bbw_stage: ctx is NULL");
   bbw_status s =
-      c->precision == BBW_PREC_F16X3
+      c->precision != BBW_PREC_FP32
           ? tc_launch(c->tc, c->Q[c->cur], c->Q[c->cur ^ 1], c->res, fa, fb, fdt, c->stream)
           : fused_launch(c->plan, c->Q[c->cur], c->Q[c->cur ^ 1], c->res, fa, fb, fdt, cstage,
                          c->stream);

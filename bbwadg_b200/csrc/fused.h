@@ -1,6 +1,8 @@
 // Host-visible description of a prepared fused-stage launch (kernels_fused.cu).
 #pragma once
 #include <cuda_fp16.h>
+
+#include <cstdint>
 #include <cuda_runtime.h>
 
 #include <cstddef>
@@ -66,6 +68,7 @@ struct TcPlan {
   const float *geo = nullptr, *c2q = nullptr;
   const int *nbr = nullptr, *tables = nullptr;
   const void *ops = nullptr;
+  bool bf = false;  // split-BF16 operands instead of split-FP16
   int table_ints = 0, pat_off = 0;
   int *err = nullptr;
 };
@@ -76,7 +79,7 @@ bbw_status tc_prepare(TcPlan &pl);
 bbw_status tc_launch(const TcPlan &pl, const float *Qin, float *Qout, float *res, float fa,
                      float fb, float fdt, cudaStream_t st);
 void tc_pack_operator(const float *A, int nrows, int ncols, int ld_row, int ld_col, int rows,
-                      int kp, __half *hi, __half *lo);
+                      int kp, uint16_t *hi, uint16_t *lo, bool bf);
 bbw_status fused_prepare(FusedPlan &pl);
 bbw_status fused_launch(const FusedPlan &pl, const float *Qin, float *Qout, float *res, float fa,
                         float fb, float fdt, float cstage, cudaStream_t st);

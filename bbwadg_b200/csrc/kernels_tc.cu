@@ -12,7 +12,9 @@
 // significant bits) and s a per-tile power of two that maps the operand into
 // [-1, 1); the dropped A_lo x_lo term and the residual of the splits are
 // O(2^-22) relative to the tile maximum, i.e. FP32-class.  State, fluxes,
-// geometric factors and the LSRK update stay FP32.
+// geometric factors and the LSRK update stay FP32.  The same kernel with
+// BF16 pairs (BF = true; 16 significant bits, FP32's exponent range) gives
+// the split-BF16 form of the precision study: O(2^-16) per contraction.
 //
 // Orientation: operator rows on the MMA M dimension (64 or 128), the 32
 // elements of a tile on N, the reduction index on K.  Operators (A) are
@@ -28,11 +30,15 @@
 // the next tile's copies overlap the MMAs and epilogues.  The LSRK update
 // reads the old state and residual from global memory in the epilogues
 // (thread = node row, coalesced).
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include <algorithm>
 #include <cstdint>
+#include <cstring>
 
 #include "bbwadg.h"
 #include "device_common.cuh"
@@ -109,7 +115,7 @@ struct TcParams {
   const float *__restrict__ geo;  // [K][TC_GEO]: vgeo 9 | fgeo 16 | pad
   const int *__restrict__ nbr;    // [K][4]
   const float *__restrict__ c2q;  // [K][Nq]
-  const __half *__restrict__ ops;
+  const void *__restrict__ ops;  // split operators: __half, or __nv_bfloat16 (BF)
   const int *__restrict__ tables;
   int table_ints, pat_off;
   int *err;
@@ -129,22 +135,32 @@ __device__ __forceinline__ float pow2_scale(int bits_of_max) {
   return ldexpf(1.f, -E);
 }
 
-__device__ __forceinline__ void split_store4(__half *hi, __half *lo, float4 v, float s) {
+// float -> the operand type and back (round to nearest)
+__device__ __forceinline__ void to_e(float x, __half &h) { h = __float2half_rn(x); }
+__device__ __forceinline__ void to_e(float x, __nv_bfloat16 &h) { h = __float2bfloat16_rn(x); }
+__device__ __forceinline__ float from_e(__half h) { return __half2float(h); }
+__device__ __forceinline__ float from_e(__nv_bfloat16 h) { return __bfloat162float(h); }
+
+template <class E>
+__device__ __forceinline__ void split_store4(E *hi, E *lo, float4 v, float s) {
   const float x[4] = {v.x * s, v.y * s, v.z * s, v.w * s};
-  __half h[4], l[4];
+  E h[4], l[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    h[i] = __float2half_rn(x[i]);
-    l[i] = __float2half_rn(x[i] - __half2float(h[i]));
+    to_e(x[i], h[i]);
+    to_e(x[i] - from_e(h[i]), l[i]);
   }
   *reinterpret_cast<uint2 *>(hi) = *reinterpret_cast<uint2 *>(h);
   *reinterpret_cast<uint2 *>(lo) = *reinterpret_cast<uint2 *>(l);
 }
 
-__device__ __forceinline__ void split_store1(__half *hi, __half *lo, float x) {
-  const __half h = __float2half_rn(x);
+template <class E>
+__device__ __forceinline__ void split_store1(E *hi, E *lo, float x) {
+  E h, l;
+  to_e(x, h);
+  to_e(x - from_e(h), l);
   *hi = h;
-  *lo = __float2half_rn(x - __half2float(h));
+  *lo = l;
 }
 
 __device__ __forceinline__ float warp_max(float v) {
@@ -153,18 +169,22 @@ __device__ __forceinline__ float warp_max(float v) {
   return v;
 }
 
-template <int N>
+template <int N, bool BF>
 __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
+  // operand type; A and B of every MMA share it (the instruction descriptor
+  // sets both formats from FMT)
+  using E = typename std::conditional<BF, __nv_bfloat16, __half>::type;
+  constexpr int FMT = BF ? 1 : 0;
   using C = TcCfg<N>;
   constexpr int Np = C::Np, Nfp = C::Nfp, NF = C::NF, KV = C::KV, KF = C::KF, RS = C::RS;
   constexpr int FPW = C::FPW;
   extern __shared__ __align__(1024) unsigned char smem[];
   const TcLayout &L = P.L;
   const int KQ = L.KQ, MQ = L.MQ, Nq = P.Nq;
-  __half *sOps = reinterpret_cast<__half *>(smem + L.ops);
-  __half *sBp = reinterpret_cast<__half *>(smem + L.Bp);
-  __half *sBU = reinterpret_cast<__half *>(smem + L.BU);
-  __half *sBF = reinterpret_cast<__half *>(smem + L.BF);
+  E *sOps = reinterpret_cast<E *>(smem + L.ops);
+  E *sBp = reinterpret_cast<E *>(smem + L.Bp);
+  E *sBU = reinterpret_cast<E *>(smem + L.BU);
+  E *sBF = reinterpret_cast<E *>(smem + L.BF);
   float *sRaw = reinterpret_cast<float *>(smem + L.raw);
   float *sGeoB = reinterpret_cast<float *>(smem + L.geo);
   int *sNbr = reinterpret_cast<int *>(smem + L.nbr);
@@ -225,8 +245,8 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
   // one operator/operand product chain: D (+)= A B^T over ksteps, 3 products
   // descriptors of consecutive K steps differ only in the start-address field
   // (+256 bytes = +16 in 16-byte units)
-  auto chain = [&](uint32_t d, const __half *Ahi, const __half *Alo, int asbo, const __half *Bhi,
-                   const __half *Blo, int bsbo, int ksteps, uint32_t idesc, bool acc) {
+  auto chain = [&](uint32_t d, const E *Ahi, const E *Alo, int asbo, const E *Bhi,
+                   const E *Blo, int bsbo, int ksteps, uint32_t idesc, bool acc) {
     uint64_t ah = tc::smem_desc(tc::smem_u32(Ahi), 128, asbo);
     uint64_t al = tc::smem_desc(tc::smem_u32(Alo), 128, asbo);
     uint64_t bh = tc::smem_desc(tc::smem_u32(Bhi), 128, bsbo);
@@ -377,7 +397,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
     const int n = 16 * q4 + lane;  // M = 64 layout: lanes 0..15 of each sub-partition
     const bool rowok = lane < 16 && n < Np;
     if (tid == 0) {
-      const uint32_t id64 = tc::idesc_f16(64, TC_E, 0);
+      const uint32_t id64 = tc::idesc_f16(64, TC_E, FMT);
       const int sboV = (KV / 8) * 128, sboF = (KF / 8) * 128;
       for (int d = 0; d < 3; ++d)
         chain(tbase + 32 * d, sOps + L.oD + 2 * d * 64 * KV, sOps + L.oD + (2 * d + 1) * 64 * KV,
@@ -463,7 +483,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
     // ---- P4: Vq product; meanwhile c2/J of this thread's cubature row
     if (tid == 0) {
       chain(tbase + 0, sOps + L.oVq, sOps + L.oVq + MQ * KV, (KV / 8) * 128, sBp, sBp + TC_E * KV,
-            (KV / 8) * 128, KV / 16, tc::idesc_f16(MQ, TC_E, 0), false);
+            (KV / 8) * 128, KV / 16, tc::idesc_f16(MQ, TC_E, FMT), false);
       tc::mma_commit(mbarM);
     }
     const int q = MQ == 128 ? 32 * q4 + lane : (lane < 16 ? 16 * q4 + lane : MQ);
@@ -503,7 +523,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       // ---- P6: Pq product
       if (tid == 0) {
         chain(tbase + 32, sOps + L.oPq, sOps + L.oPq + 64 * KQ, (KQ / 8) * 128, sBU,
-              sBU + TC_E * KQ, (KQ / 8) * 128, KQ / 16, tc::idesc_f16(64, TC_E, 0), false);
+              sBU + TC_E * KQ, (KQ / 8) * 128, KQ / 16, tc::idesc_f16(64, TC_E, FMT), false);
         tc::mma_commit(mbarM);
       }
       float r7[8], q7[8];  // old residual and state of p, fetched during the MMAs
@@ -544,7 +564,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
 }
 
 // --------------------------------------------------------------- host side
-template <int N>
+template <int N, bool BF>
 static bbw_status tc_prepare_n(TcPlan &pl) {
   int dev = 0, maxsm = 0, nsm = 0;
   cudaGetDevice(&dev);
@@ -552,14 +572,14 @@ static bbw_status tc_prepare_n(TcPlan &pl) {
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (pl.L.total > maxsm)
     return set_error(BBW_ERR_UNSUPPORTED, "tensor-core stage: shared-memory footprint too large");
-  cudaError_t e = cudaFuncSetAttribute(k_tc_stage<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(k_tc_stage<N, BF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        pl.L.total);
   if (e != cudaSuccess) return set_cuda_error(e, "tensor-core stage attribute");
   pl.grid = std::min(cdv(pl.K, TC_E), nsm > 0 ? nsm : 148);
   return BBW_OK;
 }
 
-template <int N>
+template <int N, bool BF>
 static bbw_status tc_launch_n(const TcPlan &pl, const float *Qin, float *Qout, float *res, float fa,
                               float fb, float fdt, cudaStream_t st) {
   TcParams P;
@@ -567,11 +587,11 @@ static bbw_status tc_launch_n(const TcPlan &pl, const float *Qin, float *Qout, f
   P.fa = fa, P.fb = fb, P.fdt = fdt;
   P.Qin = Qin, P.Qout = Qout, P.res = res;
   P.geo = pl.geo, P.nbr = pl.nbr, P.c2q = pl.c2q;
-  P.ops = reinterpret_cast<const __half *>(pl.ops);
+  P.ops = pl.ops;
   P.tables = pl.tables, P.table_ints = pl.table_ints, P.pat_off = pl.pat_off;
   P.err = pl.err;
   P.L = pl.L;
-  k_tc_stage<N><<<pl.grid, TC_T, pl.L.total, st>>>(P);
+  k_tc_stage<N, BF><<<pl.grid, TC_T, pl.L.total, st>>>(P);
   return check_launch("tensor-core stage");
 }
 
@@ -580,34 +600,44 @@ bool tc_supported(int N, int Nq) {
 }
 
 bbw_status tc_prepare(TcPlan &pl) {
-  switch (pl.N) {
-    case 3: return tc_prepare_n<3>(pl);
-    case 5: return tc_prepare_n<5>(pl);
+  switch (pl.N * 2 + (pl.bf ? 1 : 0)) {
+    case 6: return tc_prepare_n<3, false>(pl);
+    case 7: return tc_prepare_n<3, true>(pl);
+    case 10: return tc_prepare_n<5, false>(pl);
+    case 11: return tc_prepare_n<5, true>(pl);
   }
   return set_error(BBW_ERR_UNSUPPORTED, "tensor-core stage: N must be 3 or 5");
 }
 
 bbw_status tc_launch(const TcPlan &pl, const float *Qin, float *Qout, float *res, float fa,
                      float fb, float fdt, cudaStream_t st) {
-  switch (pl.N) {
-    case 3: return tc_launch_n<3>(pl, Qin, Qout, res, fa, fb, fdt, st);
-    case 5: return tc_launch_n<5>(pl, Qin, Qout, res, fa, fb, fdt, st);
+  switch (pl.N * 2 + (pl.bf ? 1 : 0)) {
+    case 6: return tc_launch_n<3, false>(pl, Qin, Qout, res, fa, fb, fdt, st);
+    case 7: return tc_launch_n<3, true>(pl, Qin, Qout, res, fa, fb, fdt, st);
+    case 10: return tc_launch_n<5, false>(pl, Qin, Qout, res, fa, fb, fdt, st);
+    case 11: return tc_launch_n<5, true>(pl, Qin, Qout, res, fa, fb, fdt, st);
   }
   return set_error(BBW_ERR_UNSUPPORTED, "tensor-core stage: N must be 3 or 5");
 }
 
-// FP16 hi/lo split of an FP32 operator into the canonical K-major layout
-// (rows padded to `rows`, K padded to kp); host side
+// FP16 (or BF16, bf) hi/lo split of an FP32 operator into the canonical
+// K-major layout (rows padded to `rows`, K padded to kp), as raw 16-bit
+// words; host side
 void tc_pack_operator(const float *A, int nrows, int ncols, int ld_row, int ld_col, int rows,
-                      int kp, __half *hi, __half *lo) {
+                      int kp, uint16_t *hi, uint16_t *lo, bool bf) {
   for (int r = 0; r < rows; ++r)
     for (int k = 0; k < kp; ++k) {
       const float a = (r < nrows && k < ncols) ? A[(size_t)r * ld_row + (size_t)k * ld_col] : 0.f;
-      const __half h = __float2half_rn(a);
-      const __half l = __float2half_rn(a - __half2float(h));
       const int o = tc::kmajor_offset_f16(r, k, kp);
-      hi[o] = h;
-      lo[o] = l;
+      if (bf) {
+        const __nv_bfloat16 h = __float2bfloat16_rn(a);
+        const __nv_bfloat16 l = __float2bfloat16_rn(a - __bfloat162float(h));
+        std::memcpy(&hi[o], &h, 2), std::memcpy(&lo[o], &l, 2);
+      } else {
+        const __half h = __float2half_rn(a);
+        const __half l = __float2half_rn(a - __half2float(h));
+        std::memcpy(&hi[o], &h, 2), std::memcpy(&lo[o], &l, 2);
+      }
     }
 }
 

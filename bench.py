@@ -330,8 +330,8 @@ def precision_workload(args, torch):
     """Error study on the standing mode p = cos(pi x)cos(pi y)cos(pi z)
     cos(sqrt(3) pi t), c^2 = 1, p = 0 walls on [-1/2, 1/2]^3 (exact for the
     reference's boundary condition), h-refinement 8/16/24: FP32 stage at
-    N = 7 (the tensor-core form needs Np <= 64, Nq <= 128: N in {3, 5}), and
-    FP32 against the split-FP16 tensor-core form at N = 5.  Errors: relative
+    N = 7 (the tensor-core forms need Np <= 64, Nq <= 128: N in {3, 5}), and
+    FP32 against the split-FP16 and split-BF16 tensor-core forms at N = 5.  Errors: relative
     L2 against the exact solution at T (FP64 quadrature), and against the
     FP64 C restatement over the first 10 steps on the 8^3 mesh."""
     import math
@@ -340,7 +340,7 @@ def precision_workload(args, torch):
     from bbwadg_b200.problem import cavity_mode
     T = args.prec_time
     rows = []
-    for N, precs in ((7, ("fp32",)), (5, ("fp32", "f16x3"))):
+    for N, precs in ((7, ("fp32",)), (5, ("fp32", "f16x3", "bf16x3"))):
         cub, tri = reference_rule(N)
         for nh in (8, 16, 24):
             p = make_problem(N, nh, c2="one", ic="cavity", lo=-0.5, hi=0.5, cubature=cub,

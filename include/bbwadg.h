@@ -238,9 +238,10 @@ typedef struct bbw_ops_desc {
  * F16X3: the dense contractions (Dr/Ds/Dt, LIFT, Vq, Pq) on the tensor cores
  * as three FP16 products per split pair (A_hi x_hi + A_hi x_lo + A_lo x_hi,
  * per-tile power-of-two scaling, FP32 accumulation); state, fluxes and the
- * update stay FP32.  F16X3 supports the nodal variant with N in {3, 5},
- * Nq <= 128. */
-enum { BBW_PREC_FP32 = 0, BBW_PREC_F16X3 = 1 };
+ * update stay FP32.  BF16X3: the same with BF16 pairs (16 significant bits
+ * per pair instead of 22; the split-BF16 form of the precision study).  Both
+ * support the nodal variant with N in {3, 5}, Nq <= 128. */
+enum { BBW_PREC_FP32 = 0, BBW_PREC_F16X3 = 1, BBW_PREC_BF16X3 = 2 };
 
 /* Uploads mesh and operators (cpp/src/WaveOKL3d.cpp:1400-1615 and
  * :894-909) to the current CUDA device; state and residual start at zero.
