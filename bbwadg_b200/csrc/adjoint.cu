@@ -38,6 +38,7 @@ void adj_release(bbw_ctx *c) {
   for (int d = 0; d < 3; ++d) cudaFree(a.D[d]), cudaFree(a.DT[d]);
   cudaFree(a.LIFT), cudaFree(a.Vq), cudaFree(a.Pq);
   cudaFree(a.Fmask), cudaFree(a.vmapP), cudaFree(a.fidx), cudaFree(a.mapP);
+  cudaFree(a.PqT), cudaFree(a.VqT), cudaFree(a.DTp), cudaFree(a.LTp);
   a = AdjOps();
 }
 
@@ -101,6 +102,29 @@ bbw_status adj_setup(bbw_ctx *c) {
       (s = upload(&a.vmapP, c->hvmapP.data(), c->hvmapP.size(), "adjoint: vmapP")) != BBW_OK ||
       (s = upload(&a.fidx, fidx.data(), fidx.size(), "adjoint: face index")) != BBW_OK ||
       (s = upload(&a.mapP, mapP.data(), mapP.size(), "adjoint: mapP")) != BBW_OK)
+    return s;
+  // padded layouts of the reverse-stage kernels (see AdjOps)
+  const int Nq = c->Nq, Nfp = c->Nfp;
+  const int ldq = (Nq + 3) & ~3, ldp = (Np + 3) & ~3, ldf = (Nfp + 3) & ~3;
+  std::vector<float> pt((size_t)Np * ldq, 0.f), vt((size_t)Nq * ldp, 0.f),
+      dt((size_t)3 * Np * ldp, 0.f), lt((size_t)4 * Np * ldf, 0.f);
+  for (int n = 0; n < Np; ++n)
+    for (int q = 0; q < Nq; ++q) {
+      pt[(size_t)n * ldq + q] = c->hPq[n + (size_t)q * Np];  // Pq: Np x Nq column-major
+      vt[(size_t)q * ldp + n] = c->hVq[q + (size_t)n * Nq];  // Vq: Nq x Np column-major
+    }
+  for (int d = 0; d < 3; ++d)  // D^T column m, row n = D[m][n]
+    for (int m = 0; m < Np; ++m)
+      for (int n = 0; n < Np; ++n)
+        dt[((size_t)d * Np + m) * ldp + n] = c->hD[d][m + (size_t)n * Np];
+  for (int f = 0; f < 4; ++f)
+    for (int n = 0; n < Np; ++n)
+      for (int j = 0; j < Nfp; ++j)
+        lt[((size_t)f * Np + n) * ldf + j] = c->hLIFT[n + (size_t)(f * Nfp + j) * Np];
+  if ((s = upload(&a.PqT, pt.data(), pt.size(), "adjoint: Pq^T")) != BBW_OK ||
+      (s = upload(&a.VqT, vt.data(), vt.size(), "adjoint: Vq^T")) != BBW_OK ||
+      (s = upload(&a.DTp, dt.data(), dt.size(), "adjoint: D^T")) != BBW_OK ||
+      (s = upload(&a.LTp, lt.data(), lt.size(), "adjoint: LIFT^T")) != BBW_OK)
     return s;
   (void)NF;
   a.ready = true;
@@ -312,11 +336,10 @@ extern "C" bbw_status bbw_backward(bbw_ctx *c, bbw_tape *t, const float *dL_dtra
       }
       for (int i = 4; i >= 0; --i) {
         const float ai = (float)kRK4A[i], bi = (float)kRK4B[i];
-        if ((s = adj_wadg(N, S, K, Nq, a.Vq, a.Pq, pl.c2q, lamQ, lamR, ai, bi, dt,
+        if ((s = adj_wadg(N, S, K, Nq, a.PqT, a.VqT, pl.c2q, lamQ, lamR, ai, bi, dt,
                           vqs + (size_t)i * vqn, z, grad, st)) != BBW_OK ||
-            (s = adj_volume(N, S, K, c->vgeo, a.DT[0], a.DT[1], a.DT[2], z, rhs, st)) !=
-                BBW_OK ||
-            (s = adj_sigma(N, S, K, c->fgeo, a.LIFT, z, sigma, st)) != BBW_OK ||
+            (s = adj_volume(N, S, K, c->vgeo, a.DTp, z, rhs, st)) != BBW_OK ||
+            (s = adj_sigma(N, S, K, c->fgeo, a.LTp, z, sigma, st)) != BBW_OK ||
             (s = adj_gather(N, S, K, c->bc, dt, c->fgeo, a.fidx, a.mapP, sigma, rhs, lamQ, st)) !=
                 BBW_OK)
           return s;

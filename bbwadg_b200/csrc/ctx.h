@@ -21,6 +21,10 @@ struct AdjOps {
   int *Fmask = nullptr, *vmapP = nullptr;
   int *fidx = nullptr;  // [4][Np]: index of node n on face f, or -1
   int *mapP = nullptr;  // [K][4Nfp]: matching face node k2*4Nfp + m2, -1 on the boundary
+  // padded layouts read by the reverse-stage kernels (contraction index
+  // outer, rows padded to a multiple of 4): Pq^T [Np][ld(Nq)], Vq^T
+  // [Nq][ld(Np)], D^T [3][Np][ld(Np)], LIFT^T per face [4][Np][ld(Nfp)]
+  float *PqT = nullptr, *VqT = nullptr, *DTp = nullptr, *LTp = nullptr;
 };
 
 // LSRK45 coefficients (Carpenter-Kennedy), cpp/src/StartUp3d.cpp:517-537
@@ -36,13 +40,13 @@ bbw_status upload(T **dst, const T *src, size_t n, const char *what) {
 }
 
 // adjoint kernels (kernels_adj.cu)
-bbw_status adj_wadg(int N, int S, int K, int Nq, const float *Vq, const float *Pq, const float *c2q,
-                    const float *lamQ, float *lamR, float a, float b, float dt, const float *rhs,
-                    float *z, double *grad, cudaStream_t st);
-bbw_status adj_sigma(int N, int S, int K, const float *fgeo, const float *LIFT, const float *z,
+bbw_status adj_wadg(int N, int S, int K, int Nq, const float *PqT, const float *VqT,
+                    const float *c2q, const float *lamQ, float *lamR, float a, float b, float dt,
+                    const float *vq, float *z, double *grad, cudaStream_t st);
+bbw_status adj_sigma(int N, int S, int K, const float *fgeo, const float *LTp, const float *z,
                      float *sigma, cudaStream_t st);
-bbw_status adj_volume(int N, int S, int K, const float *vgeo, const float *Dr, const float *Ds,
-                      const float *Dt, const float *z, float *vol, cudaStream_t st);
+bbw_status adj_volume(int N, int S, int K, const float *vgeo, const float *DTp, const float *z,
+                      float *vol, cudaStream_t st);
 bbw_status adj_gather(int N, int S, int K, int bc, float dt, const float *fgeo, const int *fidx,
                       const int *mapP, const float *sigma, const float *vol, float *lamQ,
                       cudaStream_t st);

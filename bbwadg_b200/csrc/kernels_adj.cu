@@ -30,10 +30,12 @@ constexpr int AE = 32;   // elements per CTA (lane = element)
 constexpr int AW = 8;    // warps per CTA
 constexpr int AS = AE + 1;  // shared row stride
 
-// Operators are staged per CTA in shared memory with the contraction index
-// outer and four consecutive output rows contiguous (row stride padded to 4):
-// one warp-uniform 16-byte shared load then feeds four rows of the warp's
-// register block, each applied to the element values of the 32 lanes.
+// Operators come in padded layouts built once on the host (AdjOps): the
+// contraction index outer and four consecutive output rows contiguous (row
+// stride padded to 4), so one warp-uniform 16-byte load feeds four rows of
+// the warp's register block, each applied to the element values of the 32
+// lanes.  A CTA copies them into shared memory when they fit beside its
+// tiles (stage != 0), else reads them from global memory (L1-cached).
 __device__ __forceinline__ int pad4(int x) { return (x + 3) & ~3; }
 
 __device__ __forceinline__ void fma4(float (&acc)[4], const float4 a, float x) {
@@ -49,9 +51,9 @@ __device__ __forceinline__ void fma4(float (&acc)[4], const float4 a, float x) {
 // tile are done in turn, so every gradient entry is accumulated by one
 // thread in shot order.
 template <int N>
-__global__ void __launch_bounds__(AE * AW) k_adj_wadg(int S, int K, int Nq,
-                                                     const float *__restrict__ Vq,
-                                                     const float *__restrict__ Pq,
+__global__ void __launch_bounds__(AE * AW) k_adj_wadg(int S, int K, int Nq, int stage,
+                                                     const float *__restrict__ PqT,
+                                                     const float *__restrict__ VqT,
                                                      const float *__restrict__ c2q,
                                                      const float *__restrict__ lamQ,
                                                      float *__restrict__ lamR, float a, float b,
@@ -61,20 +63,20 @@ __global__ void __launch_bounds__(AE * AW) k_adj_wadg(int S, int K, int Nq,
   constexpr int Np = NP(N), ldp = (NP(N) + 3) & ~3;
   extern __shared__ float smem[];
   const int ldq = pad4(Nq);
-  float *sPt = smem;                // [Np][ldq]: Pq^T, row q of column n at n*ldq + q
-  float *sVt = sPt + Np * ldq;      // [Nq][ldp]: Vq^T, row n of column q at q*ldp + n
-  float *sMu = sVt + Nq * ldp;      // [Np][AS]
+  const int nops = stage ? Np * ldq + Nq * ldp : 0;
+  float *sMu = smem + nops;         // [Np][AS]
   float *sT = sMu + Np * AS;        // [Nq][AS]
   float *sC = sT + Nq * AS;         // [Nq][AS] c2/J
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int k0 = blockIdx.x * AE, ne = min(AE, K - k0);
-  for (int i = tid; i < Np * ldq; i += AE * AW) {
-    const int n = i / ldq, q = i - n * ldq;
-    sPt[i] = q < Nq ? __ldg(Pq + n + (size_t)q * Np) : 0.f;
-  }
-  for (int i = tid; i < Nq * ldp; i += AE * AW) {
-    const int q = i / ldp, n = i - q * ldp;
-    sVt[i] = n < Np ? __ldg(Vq + q + (size_t)n * Nq) : 0.f;
+  const float *sPt = PqT, *sVt = VqT;  // [Np][ldq] Pq^T, [Nq][ldp] Vq^T
+  if (stage) {
+    for (int i = tid; i < Np * ldq / 4; i += AE * AW)
+      reinterpret_cast<float4 *>(smem)[i] = __ldg(reinterpret_cast<const float4 *>(PqT) + i);
+    for (int i = tid; i < Nq * ldp / 4; i += AE * AW)
+      reinterpret_cast<float4 *>(smem + Np * ldq)[i] =
+          __ldg(reinterpret_cast<const float4 *>(VqT) + i);
+    sPt = smem, sVt = smem + Np * ldq;
   }
   for (int i = tid; i < ne * Nq; i += AE * AW) sC[(i % Nq) * AS + i / Nq] = c2q[(size_t)k0 * Nq + i];
   const int nqq = (Nq + 3) >> 2, npq = (Np + 3) >> 2;
@@ -100,10 +102,9 @@ __global__ void __launch_bounds__(AE * AW) k_adj_wadg(int S, int K, int Nq,
       for (int r = 0; r < 4; ++r) {
         const int q = 4 * qq + r;
         if (q < Nq && lane < ne) {
-          const size_t g = (size_t)q * K + k0 + lane;
           if (vq)
-            grad[g] += (double)dt * (double)t[r] *
-                       (double)vq[((size_t)sh * Nq + q) * K + k0 + lane];
+            grad[(size_t)q * K + k0 + lane] +=
+                (double)dt * (double)t[r] * (double)vq[((size_t)sh * Nq + q) * K + k0 + lane];
           sT[q * AS + lane] = sC[q * AS + lane] * t[r];
         } else if (q < Nq) {
           sT[q * AS + lane] = 0.f;
@@ -135,23 +136,25 @@ __global__ void __launch_bounds__(AE * AW) k_adj_wadg(int S, int K, int Nq,
 // combinations w_f = z_p - n_f . z_U are formed once per face, then each warp
 // takes quads of one face's rows.
 template <int N>
-__global__ void __launch_bounds__(AE * AW) k_adj_sigma(int K, int Kg,
+__global__ void __launch_bounds__(AE * AW) k_adj_sigma(int K, int Kg, int stage,
                                                       const float *__restrict__ fgeo,
-                                                      const float *__restrict__ LIFT,
+                                                      const float *__restrict__ LTp,
                                                       const float *__restrict__ z,
                                                       float *__restrict__ sigma) {
   constexpr int Np = NP(N), Nfp = NFP(N), NF = 4 * NFP(N), ldf = (NFP(N) + 3) & ~3;
   extern __shared__ float smem[];
-  float *sL = smem;                 // [4][Np][ldf]: LIFT^T per face
-  float *sZ = sL + 4 * Np * ldf;    // [4Np][AS]
+  const int nops = stage ? 4 * Np * ldf : 0;
+  float *sZ = smem + nops;          // [4Np][AS]
   float *sW = sZ + 4 * Np * AS;     // [4][Np][AS]
   float *sO = sW + 4 * Np * AS;     // [NF][AS]
   float *sG = sO + NF * AS;         // [AE][16]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int k0 = blockIdx.x * AE, ne = min(AE, K - k0);
-  for (int i = tid; i < 4 * Np * ldf; i += AE * AW) {
-    const int f = i / (Np * ldf), r = i - f * Np * ldf, n = r / ldf, j = r - n * ldf;
-    sL[i] = j < Nfp ? __ldg(LIFT + n + (size_t)(f * Nfp + j) * Np) : 0.f;
+  const float *sL = LTp;  // [4][Np][ldf]: LIFT^T per face
+  if (stage) {
+    for (int i = tid; i < nops / 4; i += AE * AW)
+      reinterpret_cast<float4 *>(smem)[i] = __ldg(reinterpret_cast<const float4 *>(LTp) + i);
+    sL = smem;
   }
   for (int i = tid; i < ne * 4 * Np; i += AE * AW)
     sZ[(i % (4 * Np)) * AS + i / (4 * Np)] = z[(size_t)k0 * 4 * Np + i];
@@ -190,30 +193,29 @@ __global__ void __launch_bounds__(AE * AW) k_adj_sigma(int K, int Kg,
 }
 
 // Volume part of S^T z: the forward volume form (rk_volume,
-// cpp/okl/WaveKernels.okl:44-153) with the given derivative operators (the
-// transposes of Dr, Ds, Dt), for the S*K elements of all shots (geometry row
+// cpp/okl/WaveKernels.okl:44-153) with the transposes of Dr, Ds, Dt (padded
+// layout DTp), for the S*K elements of all shots (geometry row
 // k % Kg).  Lane = element; each warp takes quads of output rows with the
 // four gradient / divergence sums in registers; per-output summation order
 // as in the forward kernel.
 template <int N>
-__global__ void __launch_bounds__(AE * AW) k_adj_volume(int K, int Kg,
+__global__ void __launch_bounds__(AE * AW) k_adj_volume(int K, int Kg, int stage,
                                                        const float *__restrict__ vgeo,
-                                                       const float *__restrict__ Dr,
-                                                       const float *__restrict__ Ds,
-                                                       const float *__restrict__ Dt,
+                                                       const float *__restrict__ DTp,
                                                        const float *__restrict__ z,
                                                        float *__restrict__ vol) {
   constexpr int Np = NP(N), ldp = (NP(N) + 3) & ~3, npq = (NP(N) + 3) >> 2;
   extern __shared__ float smem[];
-  float *sD = smem;                   // [3][Np][ldp]: column m of D_d at (d*Np + m)*ldp
-  float *sX = sD + 3 * Np * ldp;      // [4Np][AS]: p, then U in the rst directions
+  const int nops = stage ? 3 * Np * ldp : 0;
+  float *sX = smem + nops;            // [4Np][AS]: p, then U in the rst directions
   float *sO = sX + 4 * Np * AS;       // [4Np][AS]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int k0 = blockIdx.x * AE, ne = min(AE, K - k0);
-  for (int i = tid; i < 3 * Np * ldp; i += AE * AW) {
-    const int d = i / (Np * ldp), r = i - d * Np * ldp, m = r / ldp, n = r - m * ldp;
-    const float *D = d == 0 ? Dr : d == 1 ? Ds : Dt;
-    sD[i] = n < Np ? __ldg(D + n + (size_t)m * Np) : 0.f;
+  const float *sD = DTp;  // [3][Np][ldp]: column m of operator d at (d*Np + m)*ldp
+  if (stage) {
+    for (int i = tid; i < nops / 4; i += AE * AW)
+      reinterpret_cast<float4 *>(smem)[i] = __ldg(reinterpret_cast<const float4 *>(DTp) + i);
+    sD = smem;
   }
   for (int i = tid; i < AE * 4 * Np; i += AE * AW) {
     const int e = i / (4 * Np), j = i - e * 4 * Np;
@@ -333,55 +335,66 @@ __global__ void k_adj_receivers(int S, int K, int Np, int R, const int *__restri
 __global__ void k_set_double(double *p, double v) { *p = v; }
 
 // ------------------------------------------------------------- host side
+// shared memory of a launch: tiles, plus the staged operators when they fit
+static size_t stage_smem(size_t tiles, size_t ops, int *stage) {
+  *stage = tiles + ops <= 200 * 1024 ? 1 : 0;
+  return tiles + (*stage ? ops : 0);
+}
+
 template <int N>
-static bbw_status launch_adj_n(int S, int K, int Nq, const float *Vq, const float *Pq,
+static bbw_status launch_adj_n(int S, int K, int Nq, const float *PqT, const float *VqT,
                                const float *c2q, const float *lamQ, float *lamR, float a, float b,
                                float dt, const float *vq, float *z, double *grad,
                                cudaStream_t st) {
   constexpr int Np = NP(N);
   const int ldq = (Nq + 3) & ~3, ldp = (Np + 3) & ~3;
-  const size_t sm = sizeof(float) * ((size_t)Np * ldq + (size_t)Nq * ldp +
-                                     (size_t)AS * (Np + 2 * Nq));
+  int stage = 0;
+  const size_t sm = stage_smem(
+      sizeof(float) * (size_t)AS * (Np + 2 * Nq),
+      sizeof(float) * ((size_t)Np * ldq + (size_t)Nq * ldp), &stage);
   if (sm > 200 * 1024) return set_error(BBW_ERR_UNSUPPORTED, "adjoint WADG: Nq too large");
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_adj_wadg<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr = true;
   }
-  k_adj_wadg<N><<<(K + AE - 1) / AE, AE * AW, sm, st>>>(S, K, Nq, Vq, Pq, c2q, lamQ, lamR, a, b,
-                                                        dt, vq, z, grad);
+  k_adj_wadg<N><<<(K + AE - 1) / AE, AE * AW, sm, st>>>(S, K, Nq, stage, PqT, VqT, c2q, lamQ,
+                                                        lamR, a, b, dt, vq, z, grad);
   return check_launch("adjoint WADG");
 }
 
 template <int N>
-static bbw_status launch_sigma_n(int S, int K, const float *fgeo, const float *LIFT,
+static bbw_status launch_sigma_n(int S, int K, const float *fgeo, const float *LTp,
                                  const float *z, float *sigma, cudaStream_t st) {
   constexpr int Np = NP(N), NF = 4 * NFP(N), ldf = (NFP(N) + 3) & ~3;
-  const size_t sm =
-      sizeof(float) * ((size_t)4 * Np * ldf + (size_t)AS * (8 * Np + NF) + AE * 16);
+  int stage = 0;
+  const size_t sm = stage_smem(sizeof(float) * ((size_t)AS * (8 * Np + NF) + AE * 16),
+                               sizeof(float) * (size_t)4 * Np * ldf, &stage);
   if (sm > 200 * 1024) return set_error(BBW_ERR_UNSUPPORTED, "adjoint lift: N too large");
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_adj_sigma<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr = true;
   }
-  k_adj_sigma<N><<<(S * K + AE - 1) / AE, AE * AW, sm, st>>>(S * K, K, fgeo, LIFT, z, sigma);
+  k_adj_sigma<N><<<(S * K + AE - 1) / AE, AE * AW, sm, st>>>(S * K, K, stage, fgeo, LTp, z,
+                                                               sigma);
   return check_launch("adjoint lift");
 }
 
 template <int N>
-static bbw_status launch_volume_n(int S, int K, const float *vgeo, const float *Dr,
-                                  const float *Ds, const float *Dt, const float *z, float *vol,
-                                  cudaStream_t st) {
+static bbw_status launch_volume_n(int S, int K, const float *vgeo, const float *DTp,
+                                  const float *z, float *vol, cudaStream_t st) {
   constexpr int Np = NP(N), ldp = (NP(N) + 3) & ~3;
-  const size_t sm = sizeof(float) * ((size_t)3 * Np * ldp + (size_t)8 * Np * AS);
+  int stage = 0;
+  const size_t sm = stage_smem(sizeof(float) * (size_t)8 * Np * AS,
+                               sizeof(float) * (size_t)3 * Np * ldp, &stage);
   if (sm > 200 * 1024) return set_error(BBW_ERR_UNSUPPORTED, "adjoint volume: N too large");
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_adj_volume<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr = true;
   }
-  k_adj_volume<N><<<(S * K + AE - 1) / AE, AE * AW, sm, st>>>(S * K, K, vgeo, Dr, Ds, Dt, z, vol);
+  k_adj_volume<N><<<(S * K + AE - 1) / AE, AE * AW, sm, st>>>(S * K, K, stage, vgeo, DTp, z, vol);
   return check_launch("adjoint volume");
 }
 
@@ -408,24 +421,24 @@ static bbw_status launch_gather_n(int S, int K, int bc, float dt, const float *f
   }                                           \
   return set_error(BBW_ERR_UNSUPPORTED, "adjoint: N out of range");
 
-bbw_status adj_wadg(int N, int S, int K, int Nq, const float *Vq, const float *Pq, const float *c2q,
+bbw_status adj_wadg(int N, int S, int K, int Nq, const float *PqT, const float *VqT, const float *c2q,
                     const float *lamQ, float *lamR, float a, float b, float dt, const float *vq,
                     float *z, double *grad, cudaStream_t st) {
-#define CALL(n) launch_adj_n<n>(S, K, Nq, Vq, Pq, c2q, lamQ, lamR, a, b, dt, vq, z, grad, st)
+#define CALL(n) launch_adj_n<n>(S, K, Nq, PqT, VqT, c2q, lamQ, lamR, a, b, dt, vq, z, grad, st)
   BBW_N_SWITCH(CALL)
 #undef CALL
 }
 
-bbw_status adj_sigma(int N, int S, int K, const float *fgeo, const float *LIFT, const float *z,
+bbw_status adj_sigma(int N, int S, int K, const float *fgeo, const float *LTp, const float *z,
                      float *sigma, cudaStream_t st) {
-#define CALL(n) launch_sigma_n<n>(S, K, fgeo, LIFT, z, sigma, st)
+#define CALL(n) launch_sigma_n<n>(S, K, fgeo, LTp, z, sigma, st)
   BBW_N_SWITCH(CALL)
 #undef CALL
 }
 
-bbw_status adj_volume(int N, int S, int K, const float *vgeo, const float *Dr, const float *Ds,
-                      const float *Dt, const float *z, float *vol, cudaStream_t st) {
-#define CALL(n) launch_volume_n<n>(S, K, vgeo, Dr, Ds, Dt, z, vol, st)
+bbw_status adj_volume(int N, int S, int K, const float *vgeo, const float *DTp, const float *z,
+                      float *vol, cudaStream_t st) {
+#define CALL(n) launch_volume_n<n>(S, K, vgeo, DTp, z, vol, st)
   BBW_N_SWITCH(CALL)
 #undef CALL
 }

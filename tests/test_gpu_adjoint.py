@@ -17,8 +17,9 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-4
 
 
-def setup(variant, bc, S=2, N=3, n=2, seed=0):
-    p = make_problem(N, n, variant=variant, c2="sine", c2_jitter=0.3, seed=seed)
+def setup(variant, bc, S=2, N=3, n=2, seed=0, rules=(None, None)):
+    p = make_problem(N, n, variant=variant, c2="sine", c2_jitter=0.3, seed=seed,
+                     cubature=rules[0], tri_cubature=rules[1])
     pts = np.array([[0.1, 0.2, -0.3], [0.5, -0.5, 0.25], [-0.4, 0.0, 0.6], [0.0, 0.3, 0.0]])
     rec = receiver_weights(p, pts)
     centres = [(0.0, 0.0, 0.1), (0.3, -0.2, -0.1), (-0.3, 0.3, 0.2)][:S]
@@ -65,6 +66,23 @@ def test_gradient_matches_fp64_adjoint(cuda, variant, bc):
     nsteps = 12
     tr, grad, _ = gpu_gradient(p, rec, dense, bc, nsteps, 5, p.Q0)
     tr64, grad64, _ = oracle_gradient(p, rec, dense, bc, nsteps, p.Q0)
+    assert rel_l2(tr, tr64) < 1e-5
+    assert rel_l2(grad, grad64) < TOL
+
+
+@pytest.mark.parametrize("N", [5, 7])
+def test_gradient_matches_fp64_adjoint_higher_orders(cuda, N):
+    """The reference's cubature rules (Nq = 95, 214).  N = 5: the reverse-
+    stage kernels stage their operators in shared memory; N = 7: too large to
+    stage, they read them from global memory."""
+    from conftest import golden
+    g = golden("ops_N%d.npz" % N)
+    nfq = int(np.asarray(g["Nfq"]).ravel()[0])
+    rules = ((g["rq"], g["sq"], g["tq"], g["wq"]), (g["rfq"][:nfq], g["sfq"][:nfq], g["wfqFace"]))
+    p, rec, dense = setup("nodal", 0, S=1, N=N, rules=rules)
+    nsteps = 4
+    tr, grad, _ = gpu_gradient(p, rec, dense, 0, nsteps, 2, p.Q0)
+    tr64, grad64, _ = oracle_gradient(p, rec, dense, 0, nsteps, p.Q0)
     assert rel_l2(tr, tr64) < 1e-5
     assert rel_l2(grad, grad64) < TOL
 
