@@ -174,3 +174,23 @@ def test_bad_descriptions_are_rejected(cuda):
     with pytest.raises(BBWError):
         _lib.call("bbw_rk_volume_planar", p.N, -1, None, None, None, None, None, None, None,
                   None, None)
+
+
+def test_kernel_entries_accept_empty_lists(cuda):
+    """K = 0 (an all-planar or all-curved mesh leaves one list empty): the
+    entries return without touching rhsQ."""
+    import torch
+    p = make_curved_problem(2, 4)
+    a = {k: dev(v) for k, v in p.desc_arrays().items()}
+    r = torch.full((p.K * 4 * p.Np,), 7.0, device="cuda")
+    P = _lib.ptr
+    _lib.call("bbw_rk_volume_wadg_skew_combine", p.N, p.Nq, 0, None, None, None, None, None, None,
+              None, None, None, None, None, None, None, None, P(r), None)
+    _lib.call("bbw_rk_surface_wadg_skew_combine", p.N, p.Nfq, 0, None, None, None, None, None,
+              None, None, None, P(r), None)
+    _lib.call("bbw_rk_volume_planar", p.N, 0, None, None, None, None, None, None, None, P(r), None)
+    _lib.call("bbw_rk_surface_planar", p.N, 0, None, None, None, None, None, None, None, P(r),
+              None)
+    torch.cuda.synchronize()
+    assert bool((r == 7.0).all())
+    del a

@@ -173,3 +173,23 @@ def test_fused_n7_matches_oracle(cuda, variant):
     s.steps(p.dt, 3)
     assert rel_l2(s.get_data(), q_ref) < TOL, cfg
     s.close()
+
+
+def test_get_data_into_caller_buffer(cuda):
+    """WaveGetData3d into a caller's (pinned) buffer: same values as a fresh
+    array; wrong dtype or size is rejected."""
+    import torch
+    p = make_problem(3, 2)
+    s = WaveSolver(p)
+    s.set_data(p.Q0)
+    s.steps(p.dt, 2)
+    ref = s.get_data()
+    out = torch.empty(ref.size, dtype=torch.float32).pin_memory()
+    got = s.get_data(out=out.numpy())
+    assert got is not None and np.array_equal(out.numpy(), ref)
+    with pytest.raises(ValueError):
+        s.get_data(out=np.empty(ref.size, np.float64))
+    with pytest.raises(ValueError):
+        s.get_data(out=np.empty(ref.size - 1, np.float32))
+    s.close()
+
