@@ -456,6 +456,55 @@ def curved_workload(args, torch):
     return out
 
 
+def kernel_level_workload(args, torch):
+    """The headline workload through the kernel-level entry points, the
+    reference's three launches per stage (rk_volume, rk_surface,
+    rk_update_WADG; cpp/src/WaveOKL3d.cpp:2084-2109) with an rhs array in
+    HBM: what a kernel-for-kernel integration gets, beside the fused stage."""
+    from bbwadg_b200 import RK4A, RK4B, _lib, make_problem
+    cub, tri = reference_rule(N_ORDER)
+    p = make_problem(N_ORDER, args.hex, c2="sine", c2_jitter=0.5, seed=1234, cubature=cub,
+                     tri_cubature=tri, cfl=0.25)
+    o = p.ops_dict()
+
+    def dev(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    vgeo, fgeo, vmapP = dev(p.mesh["vgeo"]), dev(p.mesh["fgeo"]), dev(p.mesh["vmapP"])
+    Dr, Ds, Dt, LIFT = dev(o["Dr"]), dev(o["Ds"]), dev(o["Dt"]), dev(o["LIFT"])
+    Fmask, Vq, Pq, c2q = dev(o["Fmask"]), dev(o["Vq"]), dev(o["Pq"]), dev(p.c2q.ravel())
+    Jq = torch.ones(p.K * p.Nq, device="cuda")
+    Q = dev(p.Q0)
+    res = torch.zeros(p.Q0.size, device="cuda")
+    rhs = torch.empty(p.Q0.size, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    P = _lib.ptr
+    dt = float(np.float32(p.dt))
+
+    def step():
+        for i in range(5):
+            _lib.call("bbw_rk_volume", p.N, p.K, P(vgeo), P(Dr), P(Ds), P(Dt), P(Q), P(rhs), st)
+            _lib.call("bbw_rk_surface", p.N, p.K, 0, P(fgeo), P(Fmask), P(vmapP), P(LIFT), P(Q),
+                      P(rhs), st)
+            _lib.call("bbw_rk_update_wadg", p.N, p.K, p.Nq, P(Vq), P(Pq), P(Jq), P(c2q),
+                      float(np.float32(RK4A[i])), float(np.float32(RK4B[i])), dt, P(rhs), P(res),
+                      P(Q), st)
+    for _ in range(args.warmup):
+        step()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    steps = max(args.steps // 4, 5)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"workload": "same as the headline, kernel-level entry points (3 launches per stage)",
+            "value": p.K * p.Np * 4 * 5 * steps / (ms / 1e3), "unit": "DOF-stage/s",
+            "ms_per_step": ms / steps, "steps": steps, "gpu_launches": 15 * steps,
+            "finite": bool(torch.isfinite(Q).all().item())}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -467,9 +516,9 @@ def main():
     ap.add_argument("--hex", type=int, default=N_HEX, help="hexes per direction (profiling cases)")
     ap.add_argument("--variants", default="nodal,bb,nodal-f16x3",
                     help="variants to run, comma separated (nodal, bb, nodal-f16x3)")
-    ap.add_argument("--extra", default="shots,adjoint,precision,curved",
+    ap.add_argument("--extra", default="shots,adjoint,precision,curved,kernel_level",
                     help="extra workloads reported beside the headline: shots, adjoint, "
-                         "precision, curved")
+                         "precision, curved, kernel_level")
     ap.add_argument("--prec-time", type=float, default=0.02)
     ap.add_argument("--config", type=int, default=0,
                     help="pin the fused-stage configuration code instead of autotuning")
@@ -567,6 +616,7 @@ def main():
     adj = adjoint_workload(args, torch, dist, rank, world) if "adjoint" in extra else None
     prec = precision_workload(args, torch) if ("precision" in extra and rank == 0) else None
     curv = curved_workload(args, torch) if ("curved" in extra and rank == 0) else None
+    klev = kernel_level_workload(args, torch) if ("kernel_level" in extra and rank == 0) else None
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
@@ -625,6 +675,8 @@ def main():
         line["precision"] = prec
     if curv is not None:
         line["curved"] = curv
+    if klev is not None:
+        line["kernel_level"] = klev
     print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
