@@ -446,6 +446,26 @@ def curved_workload(args, torch):
            "alg_bytes_per_stage": alg,
            "gpu_launches": 5 * steps * ((KP > 0) + (KC > 0)),  # planar + curved stage kernels
            "finite": bool(np.isfinite(Q).all())}
+    # the reference's curved timing runs span N = 2..5 (cpp/runCurvedBlkTimings)
+    out["by_order"] = []
+    for No in (2, 4, 5):
+        cb, tr = reference_rule(No)
+        po = make_curved_problem(No, nh, cubature=cb, tri_cubature=tr)
+        so = CurvedSolver(po)
+        so.set_data(po.Q0)
+        so.steps(po.dt, args.warmup)
+        so.sync()
+        st = torch.cuda.ExternalStream(so.stream)
+        torch.cuda.synchronize()
+        e0.record(st)
+        so.steps(po.dt, 10)
+        e1.record(st)
+        torch.cuda.synchronize()
+        mso = e0.elapsed_time(e1)
+        out["by_order"].append({"N": No, "Nq": po.Nq, "value": po.K * po.Np * 4 * 50 / (mso / 1e3),
+                                "ms_per_step": mso / 10,
+                                "finite": bool(np.isfinite(so.get_data()).all())})
+        so.close()
     if not args.no_cpu_baseline:
         r, err = reference_curved_cpu(5, 1, 16)
         out["cpu_baseline"] = ({"value": r["dof_stage_per_s"], "unit": "DOF-stage/s",
