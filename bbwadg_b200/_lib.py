@@ -92,6 +92,9 @@ SIGNATURES = {
     "bbw_set_compute_range": (c_int, [c_void_p, c_int]),
     "bbw_gather_elements": (c_int, [c_void_p, c_int, P, P]),
     "bbw_scatter_elements": (c_int, [c_void_p, c_int, P, P]),
+    "bbw_stage_part": (c_int, [c_void_p, c_float, c_float, c_float, c_int, c_int]),
+    "bbw_stage_commit": (c_int, [c_void_p]),
+    "bbw_move_elements": (c_int, [c_void_p, c_int, c_int, c_int, P, P, c_void_p]),
     "bbw_autotune": (c_int, [c_void_p, c_float, c_int, ctypes.POINTER(c_int)]),
     "bbw_set_config": (c_int, [c_void_p, c_int]),
     "bbw_set_sources": (c_int, [c_void_p, c_int, P, P, P, c_float, c_float, c_float, c_int]),

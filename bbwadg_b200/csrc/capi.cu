@@ -673,6 +673,34 @@ extern "C" bbw_status bbw_gather_elements(bbw_ctx *c, int n, const int *idx, flo
   return gather_elements(c->Np, c->K, c->S, c->Q[c->cur], n, idx, buf, c->stream);
 }
 
+extern "C" bbw_status bbw_stage_part(bbw_ctx *c, float fa, float fb, float fdt, int K0, int K1) {
+  if (!c || K0 < 0 || K1 > c->K || K0 >= K1)
+    return set_error(BBW_ERR_ARG, "bbw_stage_part: need 0 <= K0 < K1 <= K");
+  if (c->precision != BBW_PREC_FP32)
+    return set_error(BBW_ERR_UNSUPPORTED, "bbw_stage_part: FP32 stage only");
+  FusedPlan p = c->plan;
+  p.K0 = K0, p.Kc = K1;
+  return fused_launch(p, c->Q[c->cur], c->Q[c->cur ^ 1], c->res, fa, fb, fdt, 0.f, c->stream);
+}
+
+extern "C" bbw_status bbw_stage_commit(bbw_ctx *c) {
+  if (!c) return set_error(BBW_ERR_ARG, "bbw_stage_commit: ctx is NULL");
+  c->cur ^= 1;
+  return BBW_OK;
+}
+
+extern "C" bbw_status bbw_move_elements(bbw_ctx *c, int which, int dir, int n, const int *idx,
+                                        float *buf, void *stream) {
+  bbw_status s = check_element_list(c, n, idx, buf, "bbw_move_elements: bad argument");
+  if (s != BBW_OK) return s;
+  if ((which != 0 && which != 1) || (dir != 0 && dir != 1))
+    return set_error(BBW_ERR_ARG, "bbw_move_elements: which and dir must be 0 or 1");
+  float *Q = c->Q[c->cur ^ which];
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  return dir == 0 ? gather_elements(c->Np, c->K, c->S, Q, n, idx, buf, st)
+                  : scatter_elements(c->Np, c->K, c->S, Q, n, idx, buf, st);
+}
+
 extern "C" bbw_status bbw_scatter_elements(bbw_ctx *c, int n, const int *idx, const float *buf) {
   bbw_status s = check_element_list(c, n, idx, buf, "bbw_scatter_elements: bad argument");
   if (s != BBW_OK) return s;

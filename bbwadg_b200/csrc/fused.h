@@ -19,6 +19,7 @@ struct FusedPlan {
   int N = 0, K = 0, Nq = 0, RQ = 0, PRQ = 0, bc = 0, npat = 0;
   int W = 0;                            // warps per CTA (8 or 16; 0 = default for N)
   int Kc = 0;                           // elements advanced (0 = all K; rest are halo copies)
+  int K0 = 0;                           // first element advanced (a launch covers [K0, Kc))
   int want_ops = -1, want_pipe = -1;    // requested placement (-1: first that fits)
   bool bb = false, pipe = false;
   int grid = 0;

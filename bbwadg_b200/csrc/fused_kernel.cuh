@@ -83,7 +83,7 @@ __device__ __forceinline__ float pick(const float2 *v, int i) { return (i & 1) ?
 // plus, for BB, the sparse tables.  Built on the host (fused_host.cu).
 struct FusedParams {
   int K, Nq, RQ, PRQ, bc, npat;
-  int Kc;  // elements [0, Kc) are advanced; [Kc, K) are halo copies (neighbour traces only)
+  int K0, Kc;  // elements [K0, Kc) are advanced; the others supply neighbour traces only
   int pat_off, bb_off;              // int offsets of the tables (multiples of 4)
   float fa, fb, fdt;
   const float *__restrict__ Qin;
@@ -194,13 +194,13 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
   const int *bbTab = OPS_SMEM ? sTab + P.bb_off : P.tables + P.bb_off;
 
   // asynchronous copies of one tile's inputs into buffer `buf`
-  const int ntiles = cdiv(P.Kc, TILE_E);
+  const int ntiles = cdiv(P.Kc - P.K0, TILE_E);
   const size_t sstride = (size_t)P.K * 4 * Np;  // floats per shot
   // parts of a tile's inputs: geometry + neighbour codes, state, c2
   constexpr int IN_GEO = 1, IN_Q = 2, IN_C2 = 4, IN_ALL = 7;
   auto issue_tile = [&](int vt, float *buf, int parts) {
     const int shot = vt / ntiles, tile = vt - shot * ntiles;
-    const int k0 = tile * TILE_E, ne = min(TILE_E, P.Kc - k0);
+    const int k0 = P.K0 + tile * TILE_E, ne = min(TILE_E, P.Kc - k0);
     float *bQ = buf + L::inQ, *bGeo = buf + L::inGeo, *bC2 = buf + L::inC2;
     int *bNbr = (int *)(buf + L::inNbr);
     if (parts & IN_GEO) {
@@ -237,7 +237,8 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
   // neighbour face traces of the tile in `buf` into registers
   auto load_traces = [&](const float *buf, int vt, float (&nb)[FIT][4]) {
     const int shot = vt / ntiles, tile_of_buf = vt - shot * ntiles;
-    const int ne_b = min(TILE_E, P.Kc - tile_of_buf * TILE_E);
+    const int kb = P.K0 + tile_of_buf * TILE_E;  // first element of the tile
+    const int ne_b = min(TILE_E, P.Kc - kb);
     const int *bNbr = (const int *)(buf + L::inNbr);
 #pragma unroll
     for (int j = 0; j < FIT; ++j) {
@@ -247,7 +248,7 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
         const int e = i & 31, m = i >> 5, f = m / Nfp;
         const int code = bNbr[e * 4 + f];
         const int pat = code & 255;
-        const unsigned rel = (unsigned)((code >> 8) - tile_of_buf * TILE_E);
+        const unsigned rel = (unsigned)((code >> 8) - kb);
         if (pat != 255 && rel >= (unsigned)ne_b) {  // neighbours inside the tile: from smem
           const float *q2 = P.Qin + shot * sstride + (size_t)(code >> 8) * 4 * Np +
                             sPat[pat * Nfp + (m - f * Nfp)];
@@ -272,7 +273,7 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
   }
   for (; vt < nvt; vt += gridDim.x) {
     const int shot = vt / ntiles, tile = vt - shot * ntiles;
-    const int k0 = tile * TILE_E;
+    const int k0 = P.K0 + tile * TILE_E;
     const int ne = min(TILE_E, P.Kc - k0);
     const int next = vt + gridDim.x;
     const size_t sbase = shot * sstride;
@@ -664,6 +665,7 @@ static bbw_status launch_fused(const FusedPlan &pl, const float *Qin, float *Qou
   FusedParams P;
   P.K = pl.K, P.Nq = pl.Nq, P.RQ = pl.RQ, P.PRQ = pl.PRQ, P.bc = pl.bc, P.npat = pl.npat;
   P.Kc = pl.Kc > 0 ? pl.Kc : pl.K;
+  P.K0 = pl.K0;
   P.pat_off = pl.pat_off, P.bb_off = pl.bb_off;
   P.fa = fa, P.fb = fb, P.fdt = fdt;
   P.Qin = Qin, P.Qout = Qout, P.res = res;
@@ -678,7 +680,8 @@ static bbw_status launch_fused(const FusedPlan &pl, const float *Qin, float *Qou
   P.vq_out = pl.vq_out;
   const bool os = pl.ops_smem > 0;
   const size_t sm = pl.smem;
-  const int grid = std::min(cdiv(pl.Kc > 0 ? pl.Kc : pl.K, TILE_E) * std::max(pl.S, 1), pl.nsm);
+  const int grid =
+      std::min(cdiv((pl.Kc > 0 ? pl.Kc : pl.K) - pl.K0, TILE_E) * std::max(pl.S, 1), pl.nsm);
   if (pl.W == 8) {
     constexpr int T = 256;
     if (os && pl.pipe) k_fused_stage<N, BB, true, true, 8><<<grid, T, sm, st>>>(P);

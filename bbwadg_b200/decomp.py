@@ -13,6 +13,14 @@ One exchange per stage carries 4 Np floats per halo element and shot.  The
 reference runs on one device (cpp/src/WaveOKL3d.cpp:1415); the per-element
 arithmetic is unchanged by the cut, so the decomposed run reproduces the
 single-device run.
+
+Overlap (``slab_partition(..., interface_first=True)`` and
+``run_decomposed(..., overlap=True)``): each part's owned elements are
+ordered interface first (those with a face neighbour in another part); a
+stage advances the interface elements, then the interior ones, while on a
+side stream the interface elements' new states are packed, copied and
+written into the other parts' halo slots of their next state; every part
+commits the stage once its incoming halos have landed.
 """
 from dataclasses import dataclass, field
 
@@ -34,6 +42,7 @@ class Part:
     c2q: np.ndarray              # [K][Nq]
     send: dict = field(default_factory=dict)   # part q -> local ids sent to q
     recv: dict = field(default_factory=dict)   # part q -> local halo ids received from q
+    Ki: int = 0                  # interface elements [0, Ki) of the owned ones (interface_first)
 
     @property
     def K(self):
@@ -48,8 +57,10 @@ class Part:
         return np.concatenate([self.owned, self.halo])
 
 
-def slab_partition(prob, nparts, axis=2):
-    """Cut prob's mesh into nparts slabs along `axis` (0, 1, 2 = x, y, z)."""
+def slab_partition(prob, nparts, axis=2, interface_first=False):
+    """Cut prob's mesh into nparts slabs along `axis` (0, 1, 2 = x, y, z).
+    interface_first: order each part's owned elements with those that have a
+    face neighbour in another part first (Part.Ki of them)."""
     N, K = prob.N, prob.K
     Np, NF = np_of(N), 4 * nfp_of(N)
     if not 1 <= nparts <= K:
@@ -69,6 +80,11 @@ def slab_partition(prob, nparts, axis=2):
     parts = []
     for p in range(nparts):
         owned = np.nonzero(part_of == p)[0]
+        ki = 0
+        if interface_first:
+            iface = (part_of[nbr[owned]] != p).any(1)
+            owned = np.concatenate([owned[iface], owned[~iface]])
+            ki = int(iface.sum())
         cand = np.unique(nbr[owned])
         halo = cand[part_of[cand] != p]
         ids = np.concatenate([owned, halo])
@@ -80,14 +96,16 @@ def slab_partition(prob, nparts, axis=2):
         lv[len(owned):] = hl[:, None] * 4 * Np + Fmask[None, :]  # halo faces: boundary
         parts.append(Part(p, owned, halo, np.ascontiguousarray(vgeo[ids]),
                           np.ascontiguousarray(fgeo[ids]), np.ascontiguousarray(lv, np.int32),
-                          np.ascontiguousarray(c2q[ids])))
+                          np.ascontiguousarray(c2q[ids]), Ki=ki))
     for q in parts:  # q's halo elements owned by p
         for p in parts:
             if p is q:
                 continue
             g = q.halo[part_of[q.halo] == p.index]
             if len(g):
-                p.send[q.index] = np.searchsorted(p.owned, g).astype(np.int32)
+                pos = np.full(K, -1, np.int64)  # global id -> position among p's owned
+                pos[p.owned] = np.arange(len(p.owned))
+                p.send[q.index] = pos[g].astype(np.int32)
                 q.recv[p.index] = (len(q.owned) + np.searchsorted(q.halo, g)).astype(np.int32)
     return parts
 
@@ -114,6 +132,7 @@ class LocalExchange:
         import torch
         self.parts, self.solvers = parts, solvers
         devices = devices or [0] * len(parts)
+        self.devices = devices
         self.links = []
         for p in parts:
             dp = torch.device("cuda", devices[p.index])
@@ -125,6 +144,41 @@ class LocalExchange:
                                    torch.from_numpy(recv).to(dq),
                                    torch.empty(n, dtype=torch.float32, device=dp),
                                    torch.empty(n, dtype=torch.float32, device=dq)))
+
+    def stage_overlapped(self, fa, fb, dt):
+        """One stage with the halo exchange overlapping the interior elements
+        (parts from slab_partition(..., interface_first=True))."""
+        import torch
+        if not hasattr(self, "_side"):
+            self._main = [torch.cuda.ExternalStream(s.device_state()[2],
+                                                    device=torch.device("cuda", d))
+                          for s, d in zip(self.solvers, self.devices)]
+            self._side = [torch.cuda.Stream(device=st.device) for st in self._main]
+        done = []
+        for part, s, main in zip(self.parts, self.solvers, self._main):
+            if part.Ki > 0:
+                s.stage_part(fa, fb, dt, 0, part.Ki)
+            ev = torch.cuda.Event()
+            ev.record(main)  # interface elements advanced
+            done.append(ev)
+            if part.Ki < part.Kc:
+                s.stage_part(fa, fb, dt, part.Ki, part.Kc)
+        touched = [[] for _ in self.solvers]
+        for p, q, si, ri, bp, bq in self.links:
+            side = self._side[p]
+            side.wait_event(done[p])
+            self.solvers[p].move_elements(1, 0, si, bp, side.cuda_stream)  # next state of p
+            with torch.cuda.stream(side):
+                bq.copy_(bp, non_blocking=True)
+            self.solvers[q].move_elements(1, 1, ri, bq, side.cuda_stream)  # q's next-state halo
+            ev = torch.cuda.Event()
+            ev.record(side)
+            touched[p].append(ev)
+            touched[q].append(ev)
+        for s, main, evs in zip(self.solvers, self._main, touched):
+            for ev in evs:  # halos in place; own buffers free again
+                main.wait_event(ev)
+            s.stage_commit()
 
     def __call__(self):
         for s in self.solvers:
@@ -146,9 +200,10 @@ class DistExchange:
     gather_elements / scatter_elements, with sync its sync."""
 
     def __init__(self, part, gather, scatter, floats_per_element, device, sync=None,
-                 group=None):
+                 group=None, solver=None):
         import torch
         self.gather, self.scatter, self.sync, self.group = gather, scatter, sync, group
+        self.part, self.solver = part, solver  # solver: for stage_overlapped (device buffers)
         n = floats_per_element
         self.sends = [(q, torch.from_numpy(i).to(device),
                        torch.empty(len(i) * n, dtype=torch.float32, device=device))
@@ -156,6 +211,41 @@ class DistExchange:
         self.recvs = [(q, torch.from_numpy(i).to(device),
                        torch.empty(len(i) * n, dtype=torch.float32, device=device))
                       for q, i in sorted(part.recv.items())]
+
+    def stage_overlapped(self, fa, fb, dt):
+        """One stage of this rank's part (cut interface first) with the
+        exchange on a side stream beside the interior elements: pack the
+        interface elements' next state, NCCL send / receive, write the
+        received halos into the next state, then commit.  Device buffers
+        (NCCL) only; not run here on several GPUs."""
+        import torch
+        import torch.distributed as dist
+        s, part = self.solver, self.part
+        if not hasattr(self, "_side"):
+            self._main = torch.cuda.ExternalStream(s.device_state()[2])
+            self._side = torch.cuda.Stream()
+        if part.Ki > 0:
+            s.stage_part(fa, fb, dt, 0, part.Ki)
+        ev = torch.cuda.Event()
+        ev.record(self._main)
+        if part.Ki < part.Kc:
+            s.stage_part(fa, fb, dt, part.Ki, part.Kc)
+        side = self._side
+        side.wait_event(ev)
+        with torch.cuda.stream(side):
+            for q, idx, buf in self.sends:
+                s.move_elements(1, 0, idx, buf, side.cuda_stream)
+            ops = [dist.P2POp(dist.isend, buf, q, self.group) for q, _, buf in self.sends]
+            ops += [dist.P2POp(dist.irecv, buf, q, self.group) for q, _, buf in self.recvs]
+            if ops:
+                for r in dist.batch_isend_irecv(ops):
+                    r.wait()  # the side stream waits for the transfers
+            for q, idx, buf in self.recvs:
+                s.move_elements(1, 1, idx, buf, side.cuda_stream)
+        done = torch.cuda.Event()
+        done.record(side)
+        self._main.wait_event(done)
+        s.stage_commit()
 
     def __call__(self):
         import torch.distributed as dist
@@ -175,11 +265,18 @@ class DistExchange:
             self.scatter(idx, buf)
 
 
-def run_decomposed(solvers, exchange, dt, nsteps):
-    """nsteps LSRK45 steps of every part, the halo refreshed after each stage."""
+def run_decomposed(solvers, exchange, dt, nsteps, overlap=False):
+    """nsteps LSRK45 steps of every part, the halo refreshed after each stage
+    (overlap: the exchange's stage_overlapped, parts cut interface first)."""
     for _ in range(nsteps):
         for i in range(5):
+            if overlap:
+                exchange.stage_overlapped(np.float32(RK4A[i]), np.float32(RK4B[i]), dt)
+                continue
             for s in solvers:
                 s.rk_stage(np.float32(RK4A[i]), np.float32(RK4B[i]), dt, 0.0)
             exchange()
+    if overlap:
+        for s in solvers:
+            s.sync()
     return solvers

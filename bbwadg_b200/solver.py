@@ -158,6 +158,20 @@ class WaveSolver:
         """State of element idx[j] in shot s = buf[s][j]."""
         _lib.call("bbw_scatter_elements", self._h, int(idx.numel()), _lib.ptr(idx), _lib.ptr(buf))
 
+    def stage_part(self, fa, fb, dt, K0, K1):
+        """Advance elements [K0, K1) into the next state (bbw_stage_part)."""
+        _lib.call("bbw_stage_part", self._h, float(fa), float(fb), float(dt), int(K0), int(K1))
+
+    def stage_commit(self):
+        """Make the next state current (bbw_stage_commit)."""
+        _lib.call("bbw_stage_commit", self._h)
+
+    def move_elements(self, which, dir, idx, buf, stream=None):
+        """Gather (dir 0) / scatter (dir 1) listed elements of the current
+        (which 0) or next (which 1) state on a CUDA stream handle."""
+        _lib.call("bbw_move_elements", self._h, int(which), int(dir), int(idx.numel()),
+                  _lib.ptr(idx), _lib.ptr(buf), stream)
+
     def autotune(self, dt, stages=10):
         """Pick the fastest fused-stage variant for this mesh and batch;
         returns dict(warps, ops_in_smem, pipelined)."""

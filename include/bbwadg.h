@@ -303,6 +303,21 @@ bbw_status bbw_set_compute_range(bbw_ctx *ctx, int Kc);
 bbw_status bbw_gather_elements(bbw_ctx *ctx, int n, const int *idx, float *buf);
 bbw_status bbw_scatter_elements(bbw_ctx *ctx, int n, const int *idx, const float *buf);
 
+/* Split stage for overlapping the halo exchange with interior work: each
+ * bbw_stage_part advances elements [K0, K1) from the current state into the
+ * next state (no buffer swap, context stream); bbw_stage_commit makes the
+ * next state current once every element of [0, Kc) has been advanced.
+ * Between them bbw_move_elements gathers (dir 0) or scatters (dir 1) listed
+ * elements of the current (which 0) or next (which 1) state on `stream`
+ * (NULL: the context stream): the interface elements can be packed and
+ * sent as soon as their part is done while the interior part runs.  FP32
+ * stage only; the caller orders the streams (events).  No reference
+ * counterpart. */
+bbw_status bbw_stage_part(bbw_ctx *ctx, float fa, float fb, float fdt, int K0, int K1);
+bbw_status bbw_stage_commit(bbw_ctx *ctx);
+bbw_status bbw_move_elements(bbw_ctx *ctx, int which, int dir, int n, const int *idx, float *buf,
+                             void *stream);
+
 /* ---- batched shots, sources, receivers (FP32 stage)
  * S independent shots share mesh, medium and operators; the state, residual
  * and traces hold S consecutive blocks and every stage launch advances all

@@ -94,3 +94,26 @@ def test_two_rank_decomposed_run_equals_single_mesh(tmp_path):
     full = Q.reshape(p.K, -1)
     for r, part in enumerate(slab_partition(p, 2)):
         assert np.array_equal(np.load(str(tmp_path / ("q%d.npy" % r))), full[part.owned])
+
+
+def test_interface_first_partition():
+    """Owned elements with a face neighbour in another part come first (Ki of
+    them); the send lists name exactly those, and the maps still agree."""
+    from bbwadg_b200 import make_problem
+    p = make_problem(3, 4)
+    parts = slab_partition(p, 3, interface_first=True)
+    K, Np = p.K, p.Np
+    nbr = np.asarray(p.mesh["vmapP"], np.int64).reshape(K, -1) // (4 * Np)
+    part_of = np.empty(K, np.int64)
+    for part in parts:
+        part_of[part.owned] = part.index
+    for part in parts:
+        iface = (part_of[nbr[part.owned]] != part.index).any(1)
+        assert iface[:part.Ki].all() and not iface[part.Ki:].any()
+        sent = np.unique(np.concatenate(list(part.send.values())))
+        assert np.array_equal(sent, np.arange(part.Ki))
+        for q, idx in part.send.items():  # element sent to q is the one q receives
+            g_sent = part.owned[idx]
+            g_recv = parts[q].ids[parts[q].recv[part.index]]
+            assert np.array_equal(g_sent, g_recv)
+

@@ -42,6 +42,50 @@ def test_three_slabs_equal_one_mesh(cuda, variant, shots):
         s.close()
 
 
+@pytest.mark.parametrize("shots", [1, 2])
+def test_overlapped_exchange_equals_one_mesh(cuda, shots):
+    """Interface elements first, halo exchange on side streams beside the
+    interior elements (bbw_stage_part / bbw_move_elements / bbw_stage_commit):
+    bit for bit the single-context run."""
+    from bbwadg_b200 import RK4A, RK4B
+    p = make_problem(4, 4, c2="sine", c2_jitter=0.5, seed=9)
+    rng = np.random.default_rng(5)
+    Q0 = np.stack([p.Q0 + 0.01 * s * rng.standard_normal(p.Q0.size) for s in range(shots)])
+    Q0 = Q0.astype(np.float32).reshape(shots, p.K, -1)
+    ref = WaveSolver(p)
+    ref.set_shots(shots)
+    ref.set_data(Q0)
+    for _ in range(3):
+        for i in range(5):
+            ref.rk_stage(np.float32(RK4A[i]), np.float32(RK4B[i]), p.dt, 0.0)
+    full = ref.get_data().reshape(shots, p.K, -1)
+    ref.close()
+    parts = slab_partition(p, 3, interface_first=True)
+    assert all(0 < part.Ki < part.Kc for part in parts)
+    solvers = []
+    for part in parts:
+        s = local_solver(p, part)
+        s.set_shots(shots)
+        s.set_compute_range(part.Kc)
+        s.set_data(np.stack([local_state(p, part, Q0[k]) for k in range(shots)]))
+        solvers.append(s)
+    run_decomposed(solvers, LocalExchange(parts, solvers), p.dt, 3, overlap=True)
+    for part, s in zip(parts, solvers):
+        q = s.get_data().reshape(shots, part.K, -1)[:, :part.Kc]
+        assert np.array_equal(q, full[:, part.owned])
+        s.close()
+
+
+def test_stage_part_arguments_are_validated(cuda):
+    from bbwadg_b200._lib import BBWError
+    p = make_problem(3, 2)
+    s = WaveSolver(p)
+    for k0, k1 in ((-1, 4), (4, 4), (0, p.K + 1)):
+        with pytest.raises(BBWError):
+            s.stage_part(0.0, 1.0, p.dt, k0, k1)
+    s.close()
+
+
 def test_compute_range_is_validated(cuda):
     from bbwadg_b200._lib import BBWError
     p = make_problem(3, 2)
