@@ -83,7 +83,7 @@ __device__ __forceinline__ float pick(const float2 *v, int i) { return (i & 1) ?
 // plus, for BB, the sparse tables.  Built on the host (fused_host.cu).
 struct FusedParams {
   int K, Nq, RQ, PRQ, bc, npat;
-  int K0, Kc;  // elements [K0, Kc) are advanced; the others supply neighbour traces only
+  int Kc;  // elements [K0, Kc) are advanced; the others supply neighbour traces only
   int pat_off, bb_off;              // int offsets of the tables (multiples of 4)
   float fa, fb, fdt;
   const float *__restrict__ Qin;
@@ -110,6 +110,8 @@ struct FusedParams {
   // optional: Vq (raw rhs_p) at the cubature points, before c2/J, stored as
   // [shot][Nq][K] (the c^2 gradient of the discrete adjoint needs it)
   float *__restrict__ vq_out;
+  int K0;  // first advanced element (read only by the WIN variants; kept last
+           // so the other fields keep their offsets)
 };
 
 // Ricker wavelet amp (1 - 2 a^2) exp(-a^2), a = pi f0 (t - tR)
@@ -155,9 +157,13 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // operator read is a shared-memory broadcast); otherwise they are read
 // through the read-only data path (large N or large cubature rules).
 // PIPE: two input-tile buffers (software pipelining across tiles).
-template <int N, bool BB, bool OPS_SMEM, bool PIPE, int W_>
+// WIN: the advanced elements start at P.K0 (a window of a split stage);
+// without it they start at 0, a constant, which keeps the window arithmetic
+// out of the whole-mesh stage.
+template <int N, bool BB, bool OPS_SMEM, bool PIPE, int W_, bool WIN = false>
 __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedParams P) {
   using C = FusedCfg<N, W_>;
+  const int K0 = WIN ? P.K0 : 0;  // first element advanced
   using L = FusedSmem<N, BB>;
   constexpr int Np = C::Np, Nfp = C::Nfp, NF = C::NF, W = C::W, T = C::T, R = C::R;
   constexpr int FIT = cdiv(TILE_E * NF, T);        // flux items per thread
@@ -194,13 +200,13 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
   const int *bbTab = OPS_SMEM ? sTab + P.bb_off : P.tables + P.bb_off;
 
   // asynchronous copies of one tile's inputs into buffer `buf`
-  const int ntiles = cdiv(P.Kc - P.K0, TILE_E);
+  const int ntiles = cdiv(P.Kc - K0, TILE_E);
   const size_t sstride = (size_t)P.K * 4 * Np;  // floats per shot
   // parts of a tile's inputs: geometry + neighbour codes, state, c2
   constexpr int IN_GEO = 1, IN_Q = 2, IN_C2 = 4, IN_ALL = 7;
   auto issue_tile = [&](int vt, float *buf, int parts) {
     const int shot = vt / ntiles, tile = vt - shot * ntiles;
-    const int k0 = P.K0 + tile * TILE_E, ne = min(TILE_E, P.Kc - k0);
+    const int k0 = K0 + tile * TILE_E, ne = min(TILE_E, P.Kc - k0);
     float *bQ = buf + L::inQ, *bGeo = buf + L::inGeo, *bC2 = buf + L::inC2;
     int *bNbr = (int *)(buf + L::inNbr);
     if (parts & IN_GEO) {
@@ -237,7 +243,7 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
   // neighbour face traces of the tile in `buf` into registers
   auto load_traces = [&](const float *buf, int vt, float (&nb)[FIT][4]) {
     const int shot = vt / ntiles, tile_of_buf = vt - shot * ntiles;
-    const int kb = P.K0 + tile_of_buf * TILE_E;  // first element of the tile
+    const int kb = K0 + tile_of_buf * TILE_E;  // first element of the tile
     const int ne_b = min(TILE_E, P.Kc - kb);
     const int *bNbr = (const int *)(buf + L::inNbr);
 #pragma unroll
@@ -273,7 +279,7 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
   }
   for (; vt < nvt; vt += gridDim.x) {
     const int shot = vt / ntiles, tile = vt - shot * ntiles;
-    const int k0 = P.K0 + tile * TILE_E;
+    const int k0 = K0 + tile * TILE_E;
     const int ne = min(TILE_E, P.Kc - k0);
     const int next = vt + gridDim.x;
     const size_t sbase = shot * sstride;
@@ -679,9 +685,20 @@ static bbw_status launch_fused(const FusedPlan &pl, const float *Qin, float *Qou
   P.time = pl.time;
   P.vq_out = pl.vq_out;
   const bool os = pl.ops_smem > 0;
-  const size_t sm = pl.smem;
+  size_t sm = pl.smem;
   const int grid =
       std::min(cdiv((pl.Kc > 0 ? pl.Kc : pl.K) - pl.K0, TILE_E) * std::max(pl.S, 1), pl.nsm);
+  if (pl.K0 > 0) {  // a window of a split stage: the single-buffered WIN variants
+    sm = smem_bytes<N, BB>(pl.Nq, false, os, pl.ops_floats, pl.table_ints, pl.bb_off);
+    if (pl.W == 8) {
+      if (os) k_fused_stage<N, BB, true, false, 8, true><<<grid, 256, sm, st>>>(P);
+      else k_fused_stage<N, BB, false, false, 8, true><<<grid, 256, sm, st>>>(P);
+    } else {
+      if (os) k_fused_stage<N, BB, true, false, 16, true><<<grid, 512, sm, st>>>(P);
+      else k_fused_stage<N, BB, false, false, 16, true><<<grid, 512, sm, st>>>(P);
+    }
+    return check_launch("fused stage (window)");
+  }
   if (pl.W == 8) {
     constexpr int T = 256;
     if (os && pl.pipe) k_fused_stage<N, BB, true, true, 8><<<grid, T, sm, st>>>(P);
@@ -713,6 +730,15 @@ static cudaError_t set_smem_attr(bool os, bool pipe, int bytes) {
                               cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
+// the window variants are single-buffered
+template <int N, bool BB, int W>
+static cudaError_t set_smem_attr_window(bool os, int bytes) {
+  return os ? cudaFuncSetAttribute(k_fused_stage<N, BB, true, false, W, true>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)
+            : cudaFuncSetAttribute(k_fused_stage<N, BB, false, false, W, true>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
 template <int N, bool BB>
 static bbw_status prepare(FusedPlan &pl) {
   int dev = 0, maxsm = 0, nsm = 0;
@@ -741,6 +767,12 @@ static bbw_status prepare(FusedPlan &pl) {
   cudaError_t e = pl.W == 8 ? set_smem_attr<N, BB, 8>(pl.ops_smem > 0, pl.pipe, (int)pl.smem)
                             : set_smem_attr<N, BB, 16>(pl.ops_smem > 0, pl.pipe, (int)pl.smem);
   if (e != cudaSuccess) return set_cuda_error(e, "fused stage attribute");
+  // the window variants (same operator placement)
+  const int smw = (int)smem_bytes<N, BB>(pl.Nq, false, pl.ops_smem > 0, pl.ops_floats,
+                                         pl.table_ints, pl.bb_off);
+  e = pl.W == 8 ? set_smem_attr_window<N, BB, 8>(pl.ops_smem > 0, smw)
+                : set_smem_attr_window<N, BB, 16>(pl.ops_smem > 0, smw);
+  if (e != cudaSuccess) return set_cuda_error(e, "fused stage window attribute");
   pl.nsm = nsm > 0 ? nsm : 148;
   pl.grid = std::min(cdiv(pl.Kc > 0 ? pl.Kc : pl.K, TILE_E) * std::max(pl.S, 1), pl.nsm);
   return BBW_OK;
