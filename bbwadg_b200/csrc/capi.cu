@@ -294,6 +294,11 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
   tab.resize(round4i((int)tab.size()), 0);
   const int pat_off = (int)tab.size();
   tab.insert(tab.end(), pats.begin(), pats.end());
+  // the fused stage zero-fills the neighbour codes past the last element of
+  // a ragged tile (neighbour 0, permutation 0) and reads their traces too;
+  // with no interior face (a single element) permutation 0 would not exist,
+  // so give it one row of valid node ids
+  if (npat == 0) tab.insert(tab.end(), (size_t)Nfp, 0);
   tab.resize(round4i((int)tab.size()), 0);
   const int bb_off = (int)tab.size();
   if (bb) {

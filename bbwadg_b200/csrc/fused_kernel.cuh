@@ -215,7 +215,9 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
     for (int i = tid; i < TILE_E * 16; i += T)
       cp_async4(&bGeo[(i / 16) * 25 + 9 + i % 16], P.fgeo + (size_t)k0 * 16 + (i < ne * 16 ? i : 0),
                 i < ne * 16);
-    for (int i = tid; i < TILE_E * 4; i += T)  // zero codes of absent elements: element 0, never used
+    // zero codes of absent elements: element 0, permutation 0 (the host
+    // always provides that table row); their fluxes are never used
+    for (int i = tid; i < TILE_E * 4; i += T)
       cp_async4(&bNbr[i], P.nbr + (size_t)k0 * 4 + (i < ne * 4 ? i : 0), i < ne * 4);
     }
     if (parts & IN_Q) {

@@ -193,3 +193,38 @@ def test_get_data_into_caller_buffer(cuda):
         s.get_data(out=np.empty(ref.size - 1, np.float32))
     s.close()
 
+
+
+def _tets(n_elems):
+    """One positively oriented tetrahedron, or two sharing the face (0,1,2)."""
+    VX = np.array([0.0, 1.0, 0.0, 0.0, 0.3])
+    VY = np.array([0.0, 0.0, 1.0, 0.0, 0.3])
+    VZ = np.array([0.0, 0.0, 0.0, 1.0, -0.9])
+    EToV = np.array([[0, 1, 2, 3], [0, 2, 1, 4]][:n_elems], np.int32)
+    return VX, VY, VZ, EToV
+
+
+@pytest.mark.parametrize("n_elems", [1, 2])
+@pytest.mark.parametrize("N", [3, 5])
+@pytest.mark.parametrize("form", ["nodal", "bb", "nodal-f16x3"])
+def test_one_and_two_element_meshes_match_oracle(cuda, n_elems, N, form):
+    """A tile holding one or two elements, every face but the shared one a
+    wall: the stage (FP32 fused, or the split-FP16 tensor-core form) against
+    the oracle over two steps."""
+    from oracle import Oracle
+    variant = form.split("-")[0]
+    g = golden("ops_N%d.npz" % N)  # the reference's rules (Nq = 31 / 95)
+    nfq = int(g["Nfq"][0])
+    p = make_problem(N, mesh=_tets(n_elems), variant=variant, c2="sine", seed=2,
+                     cubature=(g["rq"], g["sq"], g["tq"], g["wq"]),
+                     tri_cubature=(g["rfq"][:nfq], g["sfq"][:nfq], g["wfqFace"]))
+    assert p.K == n_elems
+    if n_elems == 2:
+        assert (p.mesh["EToE"].reshape(2, 4) != np.arange(2)[:, None]).sum() == 2
+    orc = Oracle(N, p.K, p.ops_dict(), p.geo_dict(), variant=variant)
+    q_ref, _ = orc.run(p.Q0.copy(), p.dt, 10)
+    s = WaveSolver(p, precision="f16x3" if form.endswith("f16x3") else "fp32")
+    s.set_data(p.Q0)
+    s.steps(p.dt, 2)
+    assert rel_l2(s.get_data(), q_ref) < TOL
+    s.close()
