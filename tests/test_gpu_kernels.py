@@ -168,3 +168,51 @@ def test_slice_lift_equals_sparse_lift_at_n7(cuda, bc):
               o["L0_ids"].size // Nfp, P(dev(o["L0_ids"])), P(dev(o["L0_vals"])),
               P(dev(o["cEL"])), P(Q), P(b), None)
     assert rel_l2(host(a) - r0, host(b) - r0) < 1e-5
+
+
+@pytest.mark.parametrize("n_elems", [1, 2])
+@pytest.mark.parametrize("N", [3, 5])
+@pytest.mark.parametrize("variant", ["nodal", "bb"])
+def test_kernels_on_one_and_two_elements(cuda, n_elems, N, variant):
+    """Volume, surface and WADG update on one element (all faces walls) and
+    on two sharing a face: partial element blocks against the restatement."""
+    from oracle import Oracle
+    from bbwadg_b200 import make_problem
+    VX = np.array([0.0, 1.0, 0.0, 0.0, 0.3])
+    VY = np.array([0.0, 0.0, 1.0, 0.0, 0.3])
+    VZ = np.array([0.0, 0.0, 0.0, 1.0, -0.9])
+    EToV = np.array([[0, 1, 2, 3], [0, 2, 1, 4]][:n_elems], np.int32)
+    p = make_problem(N, mesh=(VX, VY, VZ, EToV), variant=variant, c2="sine", seed=3)
+    ops, geo = p.ops_dict(), p.geo_dict()
+    orc = Oracle(N, p.K, ops, geo, variant=variant)
+    rng = np.random.default_rng(11)
+    q = rng.standard_normal(p.K * 4 * p.Np).astype(np.float32)
+    res0 = rng.standard_normal(q.size).astype(np.float32)
+    r0 = np.zeros_like(q)
+    orc.rk_volume(q, r0)
+    orc.rk_surface(q, r0)
+    rhs_ref = r0.copy()
+    res_ref, q_ref = res0.copy(), q.copy()
+    fa, fb, fdt = np.float32(-0.4), np.float32(0.37), np.float32(p.dt)
+    orc.rk_update_wadg(fa, fb, fdt, r0, res_ref, q_ref)
+    Q, rhs, res = dev(q), dev(np.zeros_like(q)), dev(res0)
+    if variant == "nodal":
+        _lib.call("bbw_rk_volume", N, p.K, P(dev(geo["vgeo"])), P(dev(ops["Dr"])),
+                  P(dev(ops["Ds"])), P(dev(ops["Dt"])), P(Q), P(rhs), None)
+        _lib.call("bbw_rk_surface", N, p.K, 0, P(dev(geo["fgeo"])), P(dev(ops["Fmask"])),
+                  P(dev(geo["vmapP"])), P(dev(ops["LIFT"])), P(Q), P(rhs), None)
+    else:
+        _lib.call("bbw_rk_volume_bern", N, p.K, P(dev(geo["vgeo"])), P(dev(ops["D_ids1"])),
+                  P(dev(ops["D_ids2"])), P(dev(ops["D_ids3"])), P(dev(ops["D_ids4"])),
+                  P(dev(ops["Dvals4"])), P(Q), P(rhs), None)
+        _lib.call("bbw_rk_surface_bern", N, p.K, 0, P(dev(geo["fgeo"])), P(dev(ops["Fmask"])),
+                  P(dev(geo["vmapP"])), P(dev(ops["slice_ids"])), ops["EEL_nnz"],
+                  P(dev(ops["EEL_ids"])), P(dev(ops["EEL_vals"])), ops["L0_nnz"],
+                  P(dev(ops["L0_ids"])), P(dev(ops["L0_vals"])), P(dev(ops["cEL"])), P(Q),
+                  P(rhs), None)
+    assert rel_l2(host(rhs), rhs_ref) < TOL
+    _lib.call("bbw_rk_update_wadg", N, p.K, p.Nq, P(dev(ops["Vq"])), P(dev(ops["Pq"])),
+              P(dev(geo["Jq"])), P(dev(geo["c2q"])), float(fa), float(fb), float(fdt), P(rhs),
+              P(res), P(Q), None)
+    assert rel_l2(host(res), res_ref) < TOL
+    assert rel_l2(host(Q), q_ref) < TOL
