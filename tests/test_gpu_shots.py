@@ -127,3 +127,30 @@ def test_bad_arguments_are_rejected(cuda):
     with pytest.raises(BBWError):
         t.set_shots(2)
     t.close()
+
+
+@pytest.mark.parametrize("n_elems", [1, 2])
+@pytest.mark.parametrize("N", [1, 2, 4])
+@pytest.mark.parametrize("variant", ["nodal", "bb"])
+def test_shots_on_one_and_two_elements(cuda, n_elems, N, variant):
+    """Three shots of a one- or two-element mesh: every (shot, tile) work
+    item is a partial tile; each shot against its own oracle run."""
+    VX = np.array([0.0, 1.0, 0.0, 0.0, 0.3])
+    VY = np.array([0.0, 0.0, 1.0, 0.0, 0.3])
+    VZ = np.array([0.0, 0.0, 0.0, 1.0, -0.9])
+    EToV = np.array([[0, 1, 2, 3], [0, 2, 1, 4]][:n_elems], np.int32)
+    p = make_problem(N, mesh=(VX, VY, VZ, EToV), variant=variant, c2="sine", seed=4)
+    rng = np.random.default_rng(N)
+    S = 3
+    Q0 = np.stack([p.Q0 * (1.0 - 0.3 * s) + 0.05 * rng.standard_normal(p.Q0.size)
+                   for s in range(S)]).astype(np.float32)
+    s = WaveSolver(p)
+    s.set_shots(S)
+    s.set_data(Q0)
+    s.steps(p.dt, 3)
+    out = s.get_data().reshape(S, -1)
+    s.close()
+    orc = oracle_for(p)
+    for i in range(S):
+        q, _ = orc.run(Q0[i].copy(), p.dt, 15)
+        assert rel_l2(out[i], q) < TOL, i
