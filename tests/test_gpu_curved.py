@@ -194,3 +194,39 @@ def test_kernel_entries_accept_empty_lists(cuda):
     torch.cuda.synchronize()
     assert bool((r == 7.0).all())
     del a
+
+
+@pytest.mark.parametrize("n_elems", [1, 2])
+@pytest.mark.parametrize("N", [2, 3])
+def test_one_and_two_curved_elements(cuda, n_elems, N):
+    """One curved tetrahedron (the centre and three points of the sphere:
+    its outer face is a whole octant) or two sharing a face: a partial
+    element block of the curved stage, no planar elements."""
+    VX = np.array([0.0, 1.0, 0.0, 0.0, 0.0])
+    VY = np.array([0.0, 0.0, 1.0, 0.0, 0.0])
+    VZ = np.array([0.0, 0.0, 0.0, 1.0, -1.0])
+    EToV = np.array([[0, 1, 2, 3], [0, 2, 1, 4]][:n_elems], np.int32)
+    p = make_curved_problem(N, mesh=(VX, VY, VZ, EToV), c2=c2_sine)
+    assert len(p.KlistCurved) == n_elems and len(p.KlistPlanar) == 0
+    s = CurvedSolver(p)
+    s.set_data(p.Q0)
+    stages(s, p.dt, 10)
+    Q = s.get_data()
+    s.close()
+    assert rel_l2(Q, oracle_of(p).run(p.Q0, p.dt, 10)[0]) < TOL
+
+
+def test_one_planar_element(cuda):
+    """A single element inside the ball (no vertex on the sphere): the
+    fused affine stage over a one-element planar prefix."""
+    VX = np.array([0.0, 0.5, 0.0, 0.0])
+    VY = np.array([0.0, 0.0, 0.5, 0.0])
+    VZ = np.array([0.0, 0.0, 0.0, 0.5])
+    p = make_curved_problem(3, mesh=(VX, VY, VZ, np.array([[0, 1, 2, 3]], np.int32)), c2=c2_sine)
+    assert len(p.KlistCurved) == 0 and len(p.KlistPlanar) == 1
+    s = CurvedSolver(p)
+    s.set_data(p.Q0)
+    stages(s, p.dt, 10)
+    Q = s.get_data()
+    s.close()
+    assert rel_l2(Q, oracle_of(p).run(p.Q0, p.dt, 10)[0]) < TOL
