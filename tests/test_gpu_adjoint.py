@@ -156,3 +156,24 @@ def test_adjoint_errors(cuda):
     with pytest.raises(BBWError):
         t.forward(p.dt, 4, 2)
     t.close()
+
+
+@pytest.mark.parametrize("n_elems", [1, 2])
+@pytest.mark.parametrize("variant", ["nodal", "bb"])
+def test_gradient_on_one_and_two_elements(cuda, n_elems, variant):
+    """Partial element tiles in every forward and reverse kernel: one
+    element (all faces walls) or two sharing a face, two shots."""
+    VX = np.array([0.0, 1.0, 0.0, 0.0, 0.3])
+    VY = np.array([0.0, 0.0, 1.0, 0.0, 0.3])
+    VZ = np.array([0.0, 0.0, 0.0, 1.0, -0.9])
+    EToV = np.array([[0, 1, 2, 3], [0, 2, 1, 4]][:n_elems], np.int32)
+    p = make_problem(3, mesh=(VX, VY, VZ, EToV), variant=variant, c2="sine", c2_jitter=0.3,
+                     seed=6)
+    pts = np.array([[0.2, 0.2, 0.2], [0.1, 0.3, 0.1], [0.3, 0.3, -0.2]][:2 + (n_elems - 1)])
+    rec = receiver_weights(p, pts)
+    dense = [gaussian_source(p, x0, a=3.0) for x0 in ((0.2, 0.2, 0.1), (0.1, 0.1, 0.3))]
+    nsteps = 10
+    tr, grad, _ = gpu_gradient(p, rec, dense, 0, nsteps, 4, p.Q0)
+    tr64, grad64, _ = oracle_gradient(p, rec, dense, 0, nsteps, p.Q0)
+    assert rel_l2(tr, tr64) < 1e-5
+    assert rel_l2(grad, grad64) < TOL
