@@ -47,3 +47,20 @@ def test_argument_validation_without_gpu():
     assert b"NULL" in L.bbw_last_error() or L.bbw_last_error() != b""
     # K = 0 is a valid no-op, as an OCCA launch over an empty outer loop
     assert L.bbw_rk_volume(5, 0, None, None, None, None, None, None, None) == 0
+
+
+def test_context_size_limits_without_gpu():
+    """K and N outside the supported range are refused before any CUDA call:
+    the neighbour code packs the element index above an 8-bit face
+    permutation id, so K < 2^23."""
+    import ctypes
+    L = _lib.lib()
+    h = ctypes.c_void_p()
+    od = _lib.OpsDesc()
+    for N, K, code in ((3, 1 << 23, 1), (3, 0, 1), (3, -5, 1), (0, 10, 7), (99, 10, 7)):
+        md = _lib.MeshDesc(N=N, K=K, Nq=31)
+        assert L.bbw_create(ctypes.byref(md), ctypes.byref(od), 0, 0, ctypes.byref(h)) == code
+        assert not h.value
+    md = _lib.MeshDesc(N=3, K=1 << 23, Nq=31)
+    L.bbw_create(ctypes.byref(md), ctypes.byref(od), 0, 0, ctypes.byref(h))
+    assert b"2^23" in L.bbw_last_error()
