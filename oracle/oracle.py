@@ -84,6 +84,10 @@ class Oracle:
         self.c2q, self.Jq = _c(geo["c2q"], d), _c(geo["Jq"], d)
         self.Vq, self.Pq = _c(ops["Vq"], d), _c(ops["Pq"], d)
         self.Nq = self.Vq.size // self.Np
+        # the restatement keeps per-element work arrays of fixed size
+        if self.Np > lib().ora_maxnp() or self.Nq > lib().ora_maxnq():
+            raise ValueError("oracle: Np = %d, Nq = %d exceed the compiled limits (%d, %d)"
+                             % (self.Np, self.Nq, lib().ora_maxnp(), lib().ora_maxnq()))
         if variant == "nodal":
             self.Dr, self.Ds, self.Dt = (_c(ops[k], d) for k in ("Dr", "Ds", "Dt"))
             self.LIFT = _c(ops["LIFT"], d)

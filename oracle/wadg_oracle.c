@@ -16,7 +16,7 @@
  */
 #define MAXNP 220   /* N <= 9 */
 #define MAXNFP 55
-#define MAXNQ 560
+#define MAXNQ 1000  /* Stroud rule of degree 2N+1 at N = 9 */
 
 #define REAL float
 #define SFX _f32

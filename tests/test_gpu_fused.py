@@ -228,3 +228,30 @@ def test_one_and_two_element_meshes_match_oracle(cuda, n_elems, N, form):
     s.steps(p.dt, 2)
     assert rel_l2(s.get_data(), q_ref) < TOL
     s.close()
+
+
+@pytest.mark.parametrize("variant", ["nodal", "bb"])
+def test_fused_n6_matches_oracle(cuda, variant):
+    """N = 6 (Np = 84) with the 343-point Stroud rule: operators read through
+    the cache, the cubature arrays of the tile in shared memory."""
+    from oracle import Oracle
+    p = make_problem(6, 2, variant=variant, c2="sine", c2_jitter=0.5, seed=3)
+    s = WaveSolver(p)
+    s.set_data(p.Q0)
+    s.steps(p.dt, 2)
+    q = s.get_data()
+    s.close()
+    q_ref, _ = Oracle(6, p.K, p.ops_dict(), p.geo_dict(), variant=variant).run(p.Q0.copy(), p.dt, 10)
+    assert rel_l2(q, q_ref) < TOL
+
+
+def test_fused_n8_with_729_point_rule_is_refused(cuda):
+    """N = 8 with the 729-point Stroud rule: a 32-element tile's cubature
+    arrays alone exceed one SM's shared memory, so the context is refused
+    (BBW_ERR_UNSUPPORTED) rather than run out of bounds; the kernel-level
+    entry points still take it."""
+    from bbwadg_b200._lib import BBWError
+    p = make_problem(8, 2, variant="nodal", c2="sine", seed=3)
+    assert p.Nq == 729
+    with pytest.raises(BBWError, match="shared memory"):
+        WaveSolver(p)

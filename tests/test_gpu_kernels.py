@@ -216,3 +216,46 @@ def test_kernels_on_one_and_two_elements(cuda, n_elems, N, variant):
               P(res), P(Q), None)
     assert rel_l2(host(res), res_ref) < TOL
     assert rel_l2(host(Q), q_ref) < TOL
+
+
+@pytest.mark.parametrize("variant", ["nodal", "bb"])
+def test_kernels_at_n8(cuda, variant):
+    """The highest order (N = 8, Np = 165, Nq = 729): volume, surface and WADG
+    update against the restatement."""
+    from oracle import Oracle
+    from bbwadg_b200 import make_problem
+    N = 8
+    p = make_problem(N, 2, variant=variant, c2="sine", seed=3)
+    ops, geo = p.ops_dict(), p.geo_dict()
+    orc = Oracle(N, p.K, ops, geo, variant=variant)
+    rng = np.random.default_rng(8)
+    q = rng.standard_normal(p.K * 4 * p.Np).astype(np.float32)
+    res0 = rng.standard_normal(q.size).astype(np.float32)
+    r0 = np.zeros_like(q)
+    orc.rk_volume(q, r0)
+    orc.rk_surface(q, r0)
+    rhs_ref = r0.copy()
+    res_ref, q_ref = res0.copy(), q.copy()
+    fa, fb, fdt = np.float32(-0.4), np.float32(0.37), np.float32(p.dt)
+    orc.rk_update_wadg(fa, fb, fdt, r0, res_ref, q_ref)
+    Q, rhs, res = dev(q), dev(np.zeros_like(q)), dev(res0)
+    if variant == "nodal":
+        _lib.call("bbw_rk_volume", N, p.K, P(dev(geo["vgeo"])), P(dev(ops["Dr"])),
+                  P(dev(ops["Ds"])), P(dev(ops["Dt"])), P(Q), P(rhs), None)
+        _lib.call("bbw_rk_surface", N, p.K, 0, P(dev(geo["fgeo"])), P(dev(ops["Fmask"])),
+                  P(dev(geo["vmapP"])), P(dev(ops["LIFT"])), P(Q), P(rhs), None)
+    else:
+        _lib.call("bbw_rk_volume_bern", N, p.K, P(dev(geo["vgeo"])), P(dev(ops["D_ids1"])),
+                  P(dev(ops["D_ids2"])), P(dev(ops["D_ids3"])), P(dev(ops["D_ids4"])),
+                  P(dev(ops["Dvals4"])), P(Q), P(rhs), None)
+        _lib.call("bbw_rk_surface_bern", N, p.K, 0, P(dev(geo["fgeo"])), P(dev(ops["Fmask"])),
+                  P(dev(geo["vmapP"])), P(dev(ops["slice_ids"])), ops["EEL_nnz"],
+                  P(dev(ops["EEL_ids"])), P(dev(ops["EEL_vals"])), ops["L0_nnz"],
+                  P(dev(ops["L0_ids"])), P(dev(ops["L0_vals"])), P(dev(ops["cEL"])), P(Q),
+                  P(rhs), None)
+    assert rel_l2(host(rhs), rhs_ref) < TOL
+    _lib.call("bbw_rk_update_wadg", N, p.K, p.Nq, P(dev(ops["Vq"])), P(dev(ops["Pq"])),
+              P(dev(geo["Jq"])), P(dev(geo["c2q"])), float(fa), float(fb), float(fdt), P(rhs),
+              P(res), P(Q), None)
+    assert rel_l2(host(res), res_ref) < TOL
+    assert rel_l2(host(Q), q_ref) < TOL

@@ -128,3 +128,17 @@ def test_wadg_projection_is_identity_on_polynomials(N, variant):
     Vq = np.asarray(g["Vq_" + variant], np.float64).reshape(Np, Nq).T
     Pq = np.asarray(g["Pq_" + variant], np.float64).reshape(Nq, Np).T
     assert np.abs(Pq @ Vq - np.eye(Np)).max() < 1e-5
+
+
+def test_oracle_refuses_sizes_beyond_its_arrays():
+    """The restatement's per-element work arrays have fixed sizes; a rule
+    with more points is refused instead of overrunning them, and the
+    729-point rule of N = 8 fits."""
+    from oracle import lib
+    from bbwadg_b200 import make_problem
+    assert lib().ora_maxnq() >= 729
+    p = make_problem(3, 2)
+    ops = dict(p.ops_dict())
+    ops["Vq"] = np.zeros(p.Np * (lib().ora_maxnq() + 1), np.float32)
+    with pytest.raises(ValueError, match="compiled limits"):
+        Oracle(3, p.K, ops, p.geo_dict())
