@@ -230,12 +230,22 @@ def test_one_and_two_element_meshes_match_oracle(cuda, n_elems, N, form):
     s.close()
 
 
+@pytest.mark.parametrize("rule", ["reference", "stroud"])
 @pytest.mark.parametrize("variant", ["nodal", "bb"])
-def test_fused_n6_matches_oracle(cuda, variant):
-    """N = 6 (Np = 84) with the 343-point Stroud rule: operators read through
-    the cache, the cubature arrays of the tile in shared memory."""
+def test_fused_n6_matches_oracle(cuda, variant, rule):
+    """N = 6 (Np = 84) with the reference's 146-point rule or the 343-point
+    Stroud rule: operators read through the cache, the cubature arrays of
+    the tile in shared memory."""
     from oracle import Oracle
-    p = make_problem(6, 2, variant=variant, c2="sine", c2_jitter=0.5, seed=3)
+    cub = tri = None
+    if rule == "reference":
+        g = golden("ops_N6.npz")
+        nfq = int(g["Nfq"][0])
+        cub = (g["rq"], g["sq"], g["tq"], g["wq"])
+        tri = (g["rfq"][:nfq], g["sfq"][:nfq], g["wfqFace"])
+    p = make_problem(6, 2, variant=variant, c2="sine", c2_jitter=0.5, seed=3, cubature=cub,
+                     tri_cubature=tri)
+    assert p.Nq == (146 if rule == "reference" else 343)
     s = WaveSolver(p)
     s.set_data(p.Q0)
     s.steps(p.dt, 2)

@@ -22,7 +22,7 @@ def maxrel(a, b):
     return float(np.abs(a - b).max() / np.abs(b).max())
 
 
-@pytest.mark.parametrize("N", [3, 4, 5, 7])
+@pytest.mark.parametrize("N", [3, 4, 5, 6, 7])
 def test_integer_maps_bit_exact(N):
     o, g = ref_rule_ops(N)
     for k in ["Fmask", "D_ids1", "D_ids2", "D_ids3", "D_ids4", "EEL_ids", "L0_ids", "slice_ids",
@@ -32,7 +32,7 @@ def test_integer_maps_bit_exact(N):
     assert np.array_equal(o["faceVolPerm"], g["faceVolPerm"].reshape(3, -1).T.ravel())
 
 
-@pytest.mark.parametrize("N", [3, 4, 5, 7])
+@pytest.mark.parametrize("N", [3, 4, 5, 6, 7])
 def test_operators_match_reference(N):
     o, g = ref_rule_ops(N)
     for k in ["r", "s", "t"]:
@@ -56,7 +56,7 @@ def test_fp64_operators_match_reference(N):
         assert maxrel(o[k + "64"], g[k + "64"]) < 1e-6, k
 
 
-@pytest.mark.parametrize("N", [3, 4, 5, 7])
+@pytest.mark.parametrize("N", [3, 4, 5, 6, 7])
 def test_connectivity_and_geometry_bit_exact(N):
     o, _ = ref_rule_ops(N)
     m = golden("mesh_box2_N%d.npz" % N)
