@@ -104,7 +104,7 @@ def reference_rules(N):
     return (g["rq"], g["sq"], g["tq"], g["wq"]), (g["rfq"][:nfq], g["sfq"][:nfq], g["wfqFace"])
 
 
-@pytest.mark.parametrize("N", [1, 4, 5, 7])
+@pytest.mark.parametrize("N", [1, 4, 5, 6, 7])
 def test_matches_oracle_at_higher_orders(cuda, N):
     cub, tri = reference_rules(N)
     p = make_curved_problem(N, 4, c2=c2_sine, cubature=cub, tri_cubature=tri)
