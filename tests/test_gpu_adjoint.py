@@ -70,11 +70,11 @@ def test_gradient_matches_fp64_adjoint(cuda, variant, bc):
     assert rel_l2(grad, grad64) < TOL
 
 
-@pytest.mark.parametrize("N", [5, 7])
+@pytest.mark.parametrize("N", [5, 6, 7])
 def test_gradient_matches_fp64_adjoint_higher_orders(cuda, N):
-    """The reference's cubature rules (Nq = 95, 214).  N = 5: the reverse-
-    stage kernels stage their operators in shared memory; N = 7: too large to
-    stage, they read them from global memory."""
+    """The reference's cubature rules (Nq = 95, 146, 214).  N = 5: the
+    reverse-stage kernels stage their operators in shared memory; N = 7: too
+    large to stage, they read them from global memory."""
     from conftest import golden
     g = golden("ops_N%d.npz" % N)
     nfq = int(np.asarray(g["Nfq"]).ravel()[0])
