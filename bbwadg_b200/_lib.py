@@ -123,6 +123,7 @@ SIGNATURES = {
     "bbw_curved_steps": (c_int, [c_void_p, c_float, c_int]),
     "bbw_curved_sync": (c_int, [c_void_p]),
     "bbw_curved_stream": (c_void_p, [c_void_p]),
+    "bbw_curved_autotune": (c_int, [c_void_p, c_float, c_int, ctypes.POINTER(c_int)]),
 }
 
 _lib = None

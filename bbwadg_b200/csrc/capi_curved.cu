@@ -327,3 +327,68 @@ extern "C" bbw_status bbw_curved_sync(bbw_curved *h) {
 }
 
 extern "C" void *bbw_curved_stream(bbw_curved *h) { return h ? (void *)h->stream : nullptr; }
+
+extern "C" bbw_status bbw_curved_autotune(bbw_curved *h, float dt, int stages, int *config) {
+  if (!h || !(dt > 0.f) || stages < 1)
+    return set_error(BBW_ERR_ARG, "bbw_curved_autotune: bad argument");
+  if (config) *config = 0;
+  if (!h->aff) return BBW_OK;  // no planar element: nothing to choose
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->side);
+  if (e != cudaSuccess) return set_cuda_error(e, "bbw_curved_autotune");
+  // the captured steps hold the planar variant's operator buffer, which
+  // bbw_set_config frees: recapture after tuning
+  drop_graphs(h);
+  const size_t n = (size_t)h->K * 4 * h->Np;
+  float *saveQ = nullptr, *saveR = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  auto cleanup = [&]() {
+    cudaFree(saveQ), cudaFree(saveR);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  };
+  e = cudaMalloc(&saveQ, n * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&saveR, n * sizeof(float));
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  const int cur0 = h->cur;
+  if (e == cudaSuccess)
+    e = cudaMemcpy(saveQ, h->Q[cur0], n * sizeof(float), cudaMemcpyDeviceToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(saveR, h->res, n * sizeof(float), cudaMemcpyDeviceToDevice);
+  if (e != cudaSuccess) {
+    cleanup();
+    return set_cuda_error(e, "bbw_curved_autotune: scratch");
+  }
+  float best_ms = 0.f;
+  int best = -1;
+  bbw_status s = BBW_OK;
+  for (int W = 8; W <= 16 && s == BBW_OK; W += 8)
+    for (int v = 0; v < 4 && s == BBW_OK; ++v) {
+      const int code = W | (v < 2 ? 1 << 8 : 0) | (v % 2 == 0 ? 1 << 9 : 0);
+      if (bbw_set_config(h->aff, code) != BBW_OK) continue;  // does not fit
+      for (int i = 0; i < 2 && s == BBW_OK; ++i) s = stage(h, 0.f, (float)kRK4B[0], dt);
+      if (s == BBW_OK) e = cudaEventRecord(e0, h->stream);
+      for (int i = 0; i < stages && s == BBW_OK && e == cudaSuccess; ++i)
+        s = stage(h, (float)kRK4A[i % 5], (float)kRK4B[i % 5], dt);
+      if (s == BBW_OK && e == cudaSuccess) e = cudaEventRecord(e1, h->stream);
+      if (s == BBW_OK && e == cudaSuccess) e = cudaEventSynchronize(e1);
+      if (s == BBW_OK && e != cudaSuccess) s = set_cuda_error(e, "bbw_curved_autotune: timing");
+      float ms = 0.f;
+      if (s == BBW_OK) cudaEventElapsedTime(&ms, e0, e1);
+      if (s == BBW_OK && (best < 0 || ms < best_ms)) best = code, best_ms = ms;
+    }
+  // the state and residual as they were, the fastest variant kept
+  h->cur = cur0;
+  e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->side);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(h->Q[cur0], saveQ, n * sizeof(float), cudaMemcpyDeviceToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(h->res, saveR, n * sizeof(float), cudaMemcpyDeviceToDevice);
+  cleanup();
+  if (s != BBW_OK) return s;
+  if (e != cudaSuccess) return set_cuda_error(e, "bbw_curved_autotune: restore");
+  if (best < 0) return set_error(BBW_ERR_UNSUPPORTED, "bbw_curved_autotune: no variant fits");
+  if ((s = bbw_set_config(h->aff, best)) != BBW_OK) return s;
+  if (config) *config = best;
+  return BBW_OK;
+}

@@ -199,6 +199,14 @@ class CurvedSolver:
     def sync(self):
         _lib.call("bbw_curved_sync", self._h)
 
+    def autotune(self, dt, stages=10):
+        """Pick the fastest fused variant for the planar elements, timed
+        inside whole curved stages (bbw_curved_autotune); returns its
+        configuration code (0: no planar element)."""
+        cfg = ctypes.c_int(0)
+        _lib.call("bbw_curved_autotune", self._h, float(dt), int(stages), ctypes.byref(cfg))
+        return cfg.value
+
     @property
     def stream(self):
         return _lib.lib().bbw_curved_stream(self._h)

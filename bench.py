@@ -419,6 +419,7 @@ def curved_workload(args, torch):
     p = make_curved_problem(N, nh, cubature=cub, tri_cubature=tri)
     s = CurvedSolver(p)
     s.set_data(p.Q0)
+    tuned = s.autotune(p.dt, 10)  # planar variant, timed inside whole stages
     stream = torch.cuda.ExternalStream(s.stream)
     s.steps(p.dt, args.warmup)
     s.sync()
@@ -445,7 +446,7 @@ def curved_workload(args, torch):
            "steps": steps, "hbm_frac_of_stage": alg / stage_s / 1e9 / peak, "peak_kind": kind,
            "alg_bytes_per_stage": alg,
            "gpu_launches": 5 * steps * ((KP > 0) + (KC > 0)),  # planar + curved stage kernels
-           "finite": bool(np.isfinite(Q).all())}
+           "planar_config": tuned, "finite": bool(np.isfinite(Q).all())}
     # the reference's curved timing runs span N = 2..5 (cpp/runCurvedBlkTimings)
     out["by_order"] = []
     for No in (2, 4, 5):
@@ -453,6 +454,7 @@ def curved_workload(args, torch):
         po = make_curved_problem(No, nh, cubature=cb, tri_cubature=tr)
         so = CurvedSolver(po)
         so.set_data(po.Q0)
+        tuned_o = so.autotune(po.dt, 10)
         so.steps(po.dt, args.warmup)
         so.sync()
         st = torch.cuda.ExternalStream(so.stream)
@@ -463,7 +465,7 @@ def curved_workload(args, torch):
         torch.cuda.synchronize()
         mso = e0.elapsed_time(e1)
         out["by_order"].append({"N": No, "Nq": po.Nq, "value": po.K * po.Np * 4 * 50 / (mso / 1e3),
-                                "ms_per_step": mso / 10,
+                                "ms_per_step": mso / 10, "planar_config": tuned_o,
                                 "finite": bool(np.isfinite(so.get_data()).all())})
         so.close()
     if not args.no_cpu_baseline:

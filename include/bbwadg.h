@@ -438,6 +438,13 @@ bbw_status bbw_curved_steps(bbw_curved *h, float dt, int nsteps);
 bbw_status bbw_curved_sync(bbw_curved *h);
 /* The handle's CUDA stream (cudaStream_t). */
 void *bbw_curved_stream(bbw_curved *h);
+/* Times `stages` whole curved stages (fused planar stage beside the curved
+ * kernel) for every fused-stage variant that fits and keeps the fastest;
+ * the state and residual are restored.  *config (may be NULL) receives the
+ * code bbw_set_config takes, 0 when there is no planar element.  Replaces
+ * the reference's hand-run element-block timings of the curved kernels
+ * (cpp/runCurvedBlkTimings). */
+bbw_status bbw_curved_autotune(bbw_curved *h, float dt, int stages, int *config);
 
 typedef struct bbw_tape bbw_tape;
 

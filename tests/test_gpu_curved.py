@@ -230,3 +230,31 @@ def test_one_planar_element(cuda):
     Q = s.get_data()
     s.close()
     assert rel_l2(Q, oracle_of(p).run(p.Q0, p.dt, 10)[0]) < TOL
+
+
+def test_autotune_restores_state_and_steps_match_oracle(cuda):
+    """bbw_curved_autotune: the state and residual come back unchanged, the
+    step graph captured before tuning is not reused (the variant's operator
+    buffer changed), and the tuned steps equal the oracle's."""
+    cub, tri = reference_rules(3)
+    p = make_curved_problem(3, 4, c2=c2_sine, cubature=cub, tri_cubature=tri)
+    s = CurvedSolver(p)
+    s.set_data(p.Q0)
+    s.steps(p.dt, 1)
+    q, r = s.get_data(), s.get_residual()
+    cfg = s.autotune(p.dt, 5)
+    assert cfg & 255 in (8, 16)
+    assert np.array_equal(s.get_data(), q)
+    assert np.array_equal(s.get_residual(), r)
+    s.steps(p.dt, 1)
+    Q = s.get_data()
+    s.close()
+    assert rel_l2(Q, oracle_of(p).run(p.Q0, p.dt, 10)[0]) < TOL
+
+
+def test_autotune_without_planar_elements(cuda):
+    p = make_curved_problem(3, mesh=kuhn_ball(2), c2=c2_sine)
+    assert len(p.KlistPlanar) == 0
+    s = CurvedSolver(p)
+    assert s.autotune(p.dt, 2) == 0
+    s.close()
