@@ -515,11 +515,16 @@ static bbw_status launch_surface_bern_slice(int K, int bc, const float *fgeo, co
 
 using namespace bbw;
 
+// node indices are int32, as the reference's vmapP: K * 4 * Np < 2^31
+static bool too_many_nodes(int N, int K) { return (long long)K * 4 * NP(N) >= (1LL << 31); }
+
 extern "C" bbw_status bbw_rk_volume(int N, int K, const float *vgeo, const float *Dr,
                                     const float *Ds, const float *Dt, const float *Q, float *rhsQ,
                                     void *stream) {
   if (K < 0 || (K > 0 && (!vgeo || !Dr || !Ds || !Dt || !Q || !rhsQ)))
     return set_error(BBW_ERR_ARG, "bbw_rk_volume: bad argument");
+  if (too_many_nodes(N, K))
+    return set_error(BBW_ERR_UNSUPPORTED, "bbw_rk_volume: K * 4 * Np must be below 2^31");
   if (K == 0) return BBW_OK;
   cudaStream_t st = (cudaStream_t)stream;
 #define CALL(n) launch_volume<n>(K, K, vgeo, Dr, Ds, Dt, Q, rhsQ, st)
@@ -543,6 +548,8 @@ extern "C" bbw_status bbw_rk_surface(int N, int K, int bc, const float *fgeo, co
   if (K < 0 || (bc != 0 && bc != 1) ||
       (K > 0 && (!fgeo || !Fmask || !vmapP || !LIFT || !Q || !rhsQ)))
     return set_error(BBW_ERR_ARG, "bbw_rk_surface: bad argument");
+  if (too_many_nodes(N, K))
+    return set_error(BBW_ERR_UNSUPPORTED, "bbw_rk_surface: K * 4 * Np must be below 2^31");
   if (K == 0) return BBW_OK;
   cudaStream_t st = (cudaStream_t)stream;
 #define CALL(n) launch_surface<n>(K, K, bc, fgeo, Fmask, vmapP, LIFT, Q, rhsQ, st)
@@ -565,6 +572,8 @@ extern "C" bbw_status bbw_rk_update(int N, int K, float fa, float fb, float fdt,
   if (N < 1 || N > BBW_MAX_N) return set_error(BBW_ERR_UNSUPPORTED, "bbw_rk_update: N");
   if (K < 0 || (K > 0 && (!rhsQ || !resQ || !Q)))
     return set_error(BBW_ERR_ARG, "bbw_rk_update: bad argument");
+  if (too_many_nodes(N, K))
+    return set_error(BBW_ERR_UNSUPPORTED, "bbw_rk_update: K * 4 * Np must be below 2^31");
   if (K == 0) return BBW_OK;
   const long long n4 = (long long)K * 4 * NP(N) / 4;  // 4*Np floats per element: multiple of 4
   const int blocks = (int)std::min<long long>((n4 + 255) / 256, 148LL * 16);
@@ -579,6 +588,8 @@ extern "C" bbw_status bbw_rk_update_wadg(int N, int K, int Nq, const float *Vq, 
                                          void *stream) {
   if (K < 0 || Nq <= 0 || (K > 0 && (!Vq || !Pq || !Jq || !c2q || !rhsQ || !resQ || !Q)))
     return set_error(BBW_ERR_ARG, "bbw_rk_update_wadg: bad argument");
+  if (too_many_nodes(N, K))
+    return set_error(BBW_ERR_UNSUPPORTED, "bbw_rk_update_wadg: K * 4 * Np must be below 2^31");
   if (K == 0) return BBW_OK;
   cudaStream_t st = (cudaStream_t)stream;
 #define CALL(n) launch_wadg<n>(K, Nq, Vq, Pq, Jq, c2q, fa, fb, fdt, rhsQ, resQ, Q, st)
@@ -603,6 +614,8 @@ extern "C" bbw_status bbw_rk_volume_bern(int N, int K, const float *vgeo, const 
   if (K < 0 ||
       (K > 0 && (!vgeo || !D_ids1 || !D_ids2 || !D_ids3 || !D_ids4 || !Dvals4 || !Q || !rhsQ)))
     return set_error(BBW_ERR_ARG, "bbw_rk_volume_bern: bad argument");
+  if (too_many_nodes(N, K))
+    return set_error(BBW_ERR_UNSUPPORTED, "bbw_rk_volume_bern: K * 4 * Np must be below 2^31");
   if (K == 0) return BBW_OK;
   cudaStream_t st = (cudaStream_t)stream;
 #define CALL(n) launch_volume_bern<n>(K, vgeo, D_ids1, D_ids2, D_ids3, D_ids4, Dvals4, Q, rhsQ, st)
@@ -631,6 +644,8 @@ extern "C" bbw_status bbw_rk_surface_bern(int N, int K, int bc, const float *fge
       (K > 0 && (!fgeo || !Fmask || !vmapP || !EEL_ids || !EEL_vals || !L0_ids || !L0_vals ||
                  !Q || !rhsQ)))
     return set_error(BBW_ERR_ARG, "bbw_rk_surface_bern: bad argument");
+  if (too_many_nodes(N, K))
+    return set_error(BBW_ERR_UNSUPPORTED, "bbw_rk_surface_bern: K * 4 * Np must be below 2^31");
   if (K == 0) return BBW_OK;
   cudaStream_t st = (cudaStream_t)stream;
 #define CALL(n)                                                                                \
@@ -661,6 +676,8 @@ extern "C" bbw_status bbw_rk_surface_bern_slice(int N, int K, int bc, const floa
       (K > 0 && (!fgeo || !Fmask || !vmapP || !slice_ids || !EEL_ids || !EEL_vals || !L0_ids ||
                  !L0_vals || !cEL || !Q || !rhsQ)))
     return set_error(BBW_ERR_ARG, "bbw_rk_surface_bern_slice: bad argument");
+  if (too_many_nodes(N, K))
+    return set_error(BBW_ERR_UNSUPPORTED, "bbw_rk_surface_bern_slice: K * 4 * Np must be below 2^31");
   if (K == 0) return BBW_OK;
   cudaStream_t st = (cudaStream_t)stream;
 #define CALL(n)                                                                             \

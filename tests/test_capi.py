@@ -64,3 +64,15 @@ def test_context_size_limits_without_gpu():
     md = _lib.MeshDesc(N=3, K=1 << 23, Nq=31)
     L.bbw_create(ctypes.byref(md), ctypes.byref(od), 0, 0, ctypes.byref(h))
     assert b"2^23" in L.bbw_last_error()
+
+
+def test_kernel_level_node_index_limit_without_gpu():
+    """Node indices are int32 (as the reference's vmapP): K * 4 * Np >= 2^31
+    is refused before any CUDA call; the arrays are never touched."""
+    L = _lib.lib()
+    Np = 56  # N = 5
+    K = (1 << 31) // (4 * Np) + 1
+    assert L.bbw_rk_volume(5, K, 1, 1, 1, 1, 1, 1, None) == 7
+    assert b"2^31" in L.bbw_last_error()
+    assert L.bbw_rk_update(5, K, 0.0, 0.0, 0.0, 1, 1, 1, None) == 7
+    assert L.bbw_rk_update_wadg(5, K, 95, 1, 1, 1, 1, 0.0, 0.0, 0.0, 1, 1, 1, None) == 7
