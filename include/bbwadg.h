@@ -139,7 +139,9 @@ bbw_status bbw_basis_eval(int N, int variant, int npts, const double *r, const d
 
 /* ------------------------------------------------ kernel-level entry points
  * One-to-one replacements of the reference's OKL kernels; same argument
- * order and meaning, device pointers, N at run time. */
+ * order and meaning, device pointers, N at run time.  Node indices are
+ * int32 as in the reference's vmapP: K * 4 * Np >= 2^31 returns
+ * BBW_ERR_UNSUPPORTED. */
 
 /* cpp/okl/WaveKernels.okl:44-153  rk_volume(K, vgeo, Dr, Ds, Dt, Q, rhsQ) */
 bbw_status bbw_rk_volume(int N, int K, const float *vgeo, const float *Dr, const float *Ds,
