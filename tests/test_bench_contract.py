@@ -42,3 +42,24 @@ def test_reference_arm_other_ranks_exit_without_work():
                   env={"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert r.returncode == 0, r.stderr[-2000:]
     assert r.stdout.strip() == ""
+
+
+@pytest.mark.gpu
+def test_bench_line_on_the_gpu(cuda):
+    """A small run of the product arm: one JSON line with the roofline,
+    end-to-end, launch-count and clock records."""
+    r = run_bench("--steps", "2", "--warmup", "3", "--extra", "none", "--no-cpu-baseline",
+                  "--hex", "8", "--variants", "nodal")
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.strip()]
+    d = json.loads(lines[-1])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+              "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config", "roofline",
+              "e2e", "gpu_launches", "clocks"):
+        assert k in d, k
+    assert d["n_gpus"] == 1 and d["steps"] == 2 and d["warmup"] == 3 and d["value"] > 0
+    assert d["gpu_launches"] == 6 * 2
+    for k in ("bound", "achieved", "peak", "unit", "frac", "traffic"):
+        assert k in d["roofline"], k
+    assert d["e2e"]["h2d_bytes_per_step"] > 0 and d["e2e"]["d2h_bytes_per_step"] > 0
+    assert "sm_mhz" in d["clocks"] and "reasons" in d["clocks"]
