@@ -97,6 +97,7 @@ SIGNATURES = {
     "bbw_move_elements": (c_int, [c_void_p, c_int, c_int, c_int, P, P, c_void_p]),
     "bbw_autotune": (c_int, [c_void_p, c_float, c_int, ctypes.POINTER(c_int)]),
     "bbw_set_config": (c_int, [c_void_p, c_int]),
+    "bbw_set_grid_limit": (c_int, [c_void_p, c_int]),
     "bbw_set_sources": (c_int, [c_void_p, c_int, P, P, P, c_float, c_float, c_float, c_int]),
     "bbw_set_receivers": (c_int, [c_void_p, c_int, P, P, c_int]),
     "bbw_get_traces": (c_int, [c_void_p, P, ctypes.POINTER(c_int)]),

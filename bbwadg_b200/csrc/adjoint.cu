@@ -147,6 +147,7 @@ struct DevBuf {  // freed on scope exit
 }  // namespace
 
 extern "C" bbw_status bbw_set_c2q(bbw_ctx *c, const float *c2q) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c || !c2q) return set_error(BBW_ERR_ARG, "bbw_set_c2q: NULL");
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e == cudaSuccess)
@@ -163,6 +164,7 @@ extern "C" bbw_status bbw_tape_free(bbw_tape *t) {
 
 extern "C" bbw_status bbw_forward(bbw_ctx *c, float dt, int nsteps, int checkpoint_every,
                                   bbw_tape **out) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c || !out || nsteps < 1 || checkpoint_every < 1 || !(dt > 0.f))
     return set_error(BBW_ERR_ARG, "bbw_forward: bad argument");
   *out = nullptr;
@@ -212,6 +214,7 @@ extern "C" bbw_status bbw_forward(bbw_ctx *c, float dt, int nsteps, int checkpoi
 
 extern "C" bbw_status bbw_backward(bbw_ctx *c, bbw_tape *t, const float *dL_dtraces,
                                    double *dL_dc2q, float *dL_dQ0) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c || !t || !dL_dtraces || !dL_dc2q) return set_error(BBW_ERR_ARG, "bbw_backward: NULL");
   if (t->state != (size_t)c->S * c->K * 4 * c->Np)
     return set_error(BBW_ERR_STATE, "bbw_backward: tape does not match the context");

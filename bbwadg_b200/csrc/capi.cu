@@ -440,6 +440,7 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
 }
 
 extern "C" bbw_status bbw_check(bbw_ctx *c) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c) return set_error(BBW_ERR_ARG, "bbw_check: ctx is NULL");
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return set_cuda_error(e, "bbw_check");
@@ -452,6 +453,7 @@ extern "C" bbw_status bbw_check(bbw_ctx *c) {
 }
 
 extern "C" bbw_status bbw_destroy(bbw_ctx *c) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c) return BBW_OK;
   cudaStreamSynchronize(c->stream);
   release(c);
@@ -469,18 +471,22 @@ static bbw_status copy_state(bbw_ctx *c, float *dev, const float *src, float *ds
 }
 
 extern "C" bbw_status bbw_set_state(bbw_ctx *c, const float *Q) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c || !Q) return set_error(BBW_ERR_ARG, "bbw_set_state: NULL");
   return copy_state(c, c->Q[c->cur], Q, nullptr);
 }
 extern "C" bbw_status bbw_get_state(bbw_ctx *c, float *Q) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c || !Q) return set_error(BBW_ERR_ARG, "bbw_get_state: NULL");
   return copy_state(c, c->Q[c->cur], nullptr, Q);
 }
 extern "C" bbw_status bbw_set_residual(bbw_ctx *c, const float *r) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c || !r) return set_error(BBW_ERR_ARG, "bbw_set_residual: NULL");
   return copy_state(c, c->res, r, nullptr);
 }
 extern "C" bbw_status bbw_get_residual(bbw_ctx *c, float *r) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c || !r) return set_error(BBW_ERR_ARG, "bbw_get_residual: NULL");
   return copy_state(c, c->res, nullptr, r);
 }
@@ -493,6 +499,7 @@ static void drop_graphs(bbw_ctx *c) {
 }
 
 extern "C" bbw_status bbw_stage_ex(bbw_ctx *c, float fa, float fb, float fdt, float cstage) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c) return set_error(BBW_ERR_ARG, "bbw_stage: ctx is NULL");
   bbw_status s =
       c->precision != BBW_PREC_FP32
@@ -504,6 +511,7 @@ extern "C" bbw_status bbw_stage_ex(bbw_ctx *c, float fa, float fb, float fdt, fl
 }
 
 extern "C" bbw_status bbw_stage(bbw_ctx *c, float fa, float fb, float fdt) {
+  DeviceGuard dg(c ? c->device : -1);
   return bbw_stage_ex(c, fa, fb, fdt, 0.f);
 }
 
@@ -520,6 +528,7 @@ static bbw_status one_step(bbw_ctx *c, float dt) {
 }
 
 extern "C" bbw_status bbw_steps(bbw_ctx *c, float dt, int nsteps) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c || nsteps < 0) return set_error(BBW_ERR_ARG, "bbw_steps: bad argument");
   uint32_t bits;
   std::memcpy(&bits, &dt, 4);
@@ -571,6 +580,7 @@ static int config_code(const FusedPlan &p) {
 }
 
 extern "C" bbw_status bbw_set_config(bbw_ctx *c, int config) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c) return set_error(BBW_ERR_ARG, "bbw_set_config: ctx is NULL");
   const int W = config & 255;
   if ((W != 8 && W != 16) || (config >> 10) != 0)
@@ -593,6 +603,7 @@ extern "C" bbw_status bbw_set_config(bbw_ctx *c, int config) {
 }
 
 extern "C" bbw_status bbw_autotune(bbw_ctx *c, float dt, int stages, int *config) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c || !(dt > 0.f) || stages < 1) return set_error(BBW_ERR_ARG, "bbw_autotune: bad argument");
   if (c->precision != BBW_PREC_FP32) {  // nothing to choose for the tensor-core stage
     if (config) *config = 0;
@@ -655,7 +666,19 @@ extern "C" bbw_status bbw_autotune(bbw_ctx *c, float dt, int stages, int *config
   return BBW_OK;
 }
 
+extern "C" bbw_status bbw_set_grid_limit(bbw_ctx *c, int max_ctas) {
+  DeviceGuard dg(c ? c->device : -1);
+  if (!c || max_ctas < 0) return set_error(BBW_ERR_ARG, "bbw_set_grid_limit: bad argument");
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return set_cuda_error(e, "bbw_set_grid_limit");
+  c->plan.max_ctas = max_ctas;
+  c->tc.max_ctas = max_ctas;
+  drop_graphs(c);
+  return BBW_OK;
+}
+
 extern "C" bbw_status bbw_set_compute_range(bbw_ctx *c, int Kc) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c || Kc < 1 || Kc > c->K) return set_error(BBW_ERR_ARG, "bbw_set_compute_range: bad Kc");
   if (Kc < c->K && c->precision != BBW_PREC_FP32)
     return set_error(BBW_ERR_UNSUPPORTED, "bbw_set_compute_range: halo elements need BBW_PREC_FP32");
@@ -673,12 +696,14 @@ static bbw_status check_element_list(bbw_ctx *c, int n, const int *idx, const vo
 }
 
 extern "C" bbw_status bbw_gather_elements(bbw_ctx *c, int n, const int *idx, float *buf) {
+  DeviceGuard dg(c ? c->device : -1);
   bbw_status s = check_element_list(c, n, idx, buf, "bbw_gather_elements: bad argument");
   if (s != BBW_OK) return s;
   return gather_elements(c->Np, c->K, c->S, c->Q[c->cur], n, idx, buf, c->stream);
 }
 
 extern "C" bbw_status bbw_stage_part(bbw_ctx *c, float fa, float fb, float fdt, int K0, int K1) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c || K0 < 0 || K1 > c->K || K0 >= K1)
     return set_error(BBW_ERR_ARG, "bbw_stage_part: need 0 <= K0 < K1 <= K");
   if (c->precision != BBW_PREC_FP32)
@@ -689,6 +714,7 @@ extern "C" bbw_status bbw_stage_part(bbw_ctx *c, float fa, float fb, float fdt, 
 }
 
 extern "C" bbw_status bbw_stage_commit(bbw_ctx *c) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c) return set_error(BBW_ERR_ARG, "bbw_stage_commit: ctx is NULL");
   c->cur ^= 1;
   return BBW_OK;
@@ -696,6 +722,7 @@ extern "C" bbw_status bbw_stage_commit(bbw_ctx *c) {
 
 extern "C" bbw_status bbw_move_elements(bbw_ctx *c, int which, int dir, int n, const int *idx,
                                         float *buf, void *stream) {
+  DeviceGuard dg(c ? c->device : -1);
   bbw_status s = check_element_list(c, n, idx, buf, "bbw_move_elements: bad argument");
   if (s != BBW_OK) return s;
   if ((which != 0 && which != 1) || (dir != 0 && dir != 1))
@@ -707,12 +734,14 @@ extern "C" bbw_status bbw_move_elements(bbw_ctx *c, int which, int dir, int n, c
 }
 
 extern "C" bbw_status bbw_scatter_elements(bbw_ctx *c, int n, const int *idx, const float *buf) {
+  DeviceGuard dg(c ? c->device : -1);
   bbw_status s = check_element_list(c, n, idx, buf, "bbw_scatter_elements: bad argument");
   if (s != BBW_OK) return s;
   return scatter_elements(c->Np, c->K, c->S, c->Q[c->cur], n, idx, buf, c->stream);
 }
 
 extern "C" bbw_status bbw_set_shots(bbw_ctx *c, int S) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c || S < 1) return set_error(BBW_ERR_ARG, "bbw_set_shots: bad argument");
   if (S > 1 && c->precision != BBW_PREC_FP32)
     return set_error(BBW_ERR_UNSUPPORTED, "bbw_set_shots: batched shots need BBW_PREC_FP32");
@@ -756,6 +785,7 @@ extern "C" bbw_status bbw_set_shots(bbw_ctx *c, int S) {
 extern "C" bbw_status bbw_set_sources(bbw_ctx *c, int nent, const int *shot, const int *elem,
                                       const float *vec, float f0, float t_delay, float amplitude,
                                       int stage_times) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c || nent < 0 || (nent > 0 && (!shot || !elem || !vec)))
     return set_error(BBW_ERR_ARG, "bbw_set_sources: bad argument");
   if (nent > 0 && c->precision != BBW_PREC_FP32)
@@ -798,6 +828,7 @@ extern "C" bbw_status bbw_set_sources(bbw_ctx *c, int nent, const int *shot, con
 
 extern "C" bbw_status bbw_set_receivers(bbw_ctx *c, int R, const int *elem, const float *w,
                                         int max_steps) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c || R < 0 || max_steps < 0 || (R > 0 && (!elem || !w)))
     return set_error(BBW_ERR_ARG, "bbw_set_receivers: bad argument");
   cudaStreamSynchronize(c->stream);
@@ -820,6 +851,7 @@ extern "C" bbw_status bbw_set_receivers(bbw_ctx *c, int R, const int *elem, cons
 }
 
 extern "C" bbw_status bbw_get_traces(bbw_ctx *c, float *out, int *nsteps) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c || !out) return set_error(BBW_ERR_ARG, "bbw_get_traces: bad argument");
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return set_cuda_error(e, "bbw_get_traces");
@@ -834,6 +866,7 @@ extern "C" bbw_status bbw_get_traces(bbw_ctx *c, float *out, int *nsteps) {
 }
 
 extern "C" bbw_status bbw_set_time(bbw_ctx *c, double t) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c) return set_error(BBW_ERR_ARG, "bbw_set_time: ctx is NULL");
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e == cudaSuccess) e = cudaMemcpy(c->d_time, &t, sizeof(double), cudaMemcpyHostToDevice);
@@ -842,6 +875,7 @@ extern "C" bbw_status bbw_set_time(bbw_ctx *c, double t) {
 }
 
 extern "C" bbw_status bbw_get_time(bbw_ctx *c, double *t, int *step) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c) return set_error(BBW_ERR_ARG, "bbw_get_time: ctx is NULL");
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e == cudaSuccess && t) e = cudaMemcpy(t, c->d_time, sizeof(double), cudaMemcpyDeviceToHost);
@@ -850,6 +884,7 @@ extern "C" bbw_status bbw_get_time(bbw_ctx *c, double *t, int *step) {
 }
 
 extern "C" bbw_status bbw_run(bbw_ctx *c, double final_time, float dt) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c || !(dt > 0.f) || final_time < 0) return set_error(BBW_ERR_ARG, "bbw_run: bad argument");
   double time = 0;
   while (time < final_time) {
@@ -862,11 +897,13 @@ extern "C" bbw_status bbw_run(bbw_ctx *c, double final_time, float dt) {
 }
 
 extern "C" bbw_status bbw_sync(bbw_ctx *c) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c) return set_error(BBW_ERR_ARG, "bbw_sync: ctx is NULL");
   return set_cuda_error(cudaStreamSynchronize(c->stream), "bbw_sync");
 }
 
 extern "C" bbw_status bbw_device_state(bbw_ctx *c, float **Q, float **res, void **stream) {
+  DeviceGuard dg(c ? c->device : -1);
   if (!c) return set_error(BBW_ERR_ARG, "bbw_device_state: ctx is NULL");
   if (Q) *Q = c->Q[c->cur];
   if (res) *res = c->res;

@@ -166,8 +166,12 @@ extern "C" bbw_status bbw_curved_create(const bbw_curved_desc *d, int device, bb
         return set_error(BBW_ERR_ARG, "bbw_curved_create: vmapP entry out of range");
       vmapP[(size_t)i * NF + m] = inv[v / (4 * Np)] * 4 * Np + v % (4 * Np);
     }
-  cudaError_t e = cudaSetDevice(device);
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess) return set_cuda_error(e, "bbw_curved_create: device");
+  if (device < 0 || device >= ndev)
+    return set_error(BBW_ERR_ARG, "bbw_curved_create: no such device");
+  DeviceGuard dg(device);  // the caller's current device is restored on return
   bbw_curved *h = new bbw_curved;
   h->N = N, h->K = K, h->Np = Np, h->KC = d->KCurved, h->KP = d->KPlanar, h->device = device;
   h->perm = perm;
@@ -234,7 +238,7 @@ extern "C" bbw_status bbw_curved_create(const bbw_curved_desc *d, int device, bb
 
 extern "C" bbw_status bbw_curved_destroy(bbw_curved *h) {
   if (!h) return BBW_OK;
-  cudaSetDevice(h->device);
+  DeviceGuard dg(h->device);
   cudaStreamSynchronize(h->stream);
   drop_graphs(h);
   release(h);
@@ -266,6 +270,7 @@ static bbw_status copy_state(bbw_curved *h, float *dev, const float *src, float 
 }
 
 extern "C" bbw_status bbw_curved_set_state(bbw_curved *h, const float *Q) {
+  DeviceGuard dg(h ? h->device : -1);
   bbw_status s = copy_state(h, h ? h->Q[h->cur] : nullptr, Q, nullptr, "bbw_curved_set_state");
   if (s != BBW_OK) return s;
   const size_t n = (size_t)h->K * 4 * h->Np * sizeof(float);
@@ -275,19 +280,23 @@ extern "C" bbw_status bbw_curved_set_state(bbw_curved *h, const float *Q) {
 }
 
 extern "C" bbw_status bbw_curved_get_state(bbw_curved *h, float *Q) {
+  DeviceGuard dg(h ? h->device : -1);
   return copy_state(h, h ? h->Q[h->cur] : nullptr, nullptr, Q, "bbw_curved_get_state");
 }
 
 extern "C" bbw_status bbw_curved_get_residual(bbw_curved *h, float *r) {
+  DeviceGuard dg(h ? h->device : -1);
   return copy_state(h, h ? h->res : nullptr, nullptr, r, "bbw_curved_get_residual");
 }
 
 extern "C" bbw_status bbw_curved_stage(bbw_curved *h, float fa, float fb, float fdt) {
+  DeviceGuard dg(h ? h->device : -1);
   if (!h) return set_error(BBW_ERR_ARG, "bbw_curved_stage: NULL handle");
   return stage(h, fa, fb, fdt);
 }
 
 extern "C" bbw_status bbw_curved_steps(bbw_curved *h, float dt, int nsteps) {
+  DeviceGuard dg(h ? h->device : -1);
   if (!h || nsteps < 0) return set_error(BBW_ERR_ARG, "bbw_curved_steps: bad argument");
   uint32_t bits;
   std::memcpy(&bits, &dt, 4);
@@ -322,6 +331,7 @@ extern "C" bbw_status bbw_curved_steps(bbw_curved *h, float dt, int nsteps) {
 }
 
 extern "C" bbw_status bbw_curved_sync(bbw_curved *h) {
+  DeviceGuard dg(h ? h->device : -1);
   if (!h) return set_error(BBW_ERR_ARG, "bbw_curved_sync: NULL handle");
   return set_cuda_error(cudaStreamSynchronize(h->stream), "bbw_curved_sync");
 }
@@ -329,6 +339,7 @@ extern "C" bbw_status bbw_curved_sync(bbw_curved *h) {
 extern "C" void *bbw_curved_stream(bbw_curved *h) { return h ? (void *)h->stream : nullptr; }
 
 extern "C" bbw_status bbw_curved_autotune(bbw_curved *h, float dt, int stages, int *config) {
+  DeviceGuard dg(h ? h->device : -1);
   if (!h || !(dt > 0.f) || stages < 1)
     return set_error(BBW_ERR_ARG, "bbw_curved_autotune: bad argument");
   if (config) *config = 0;

@@ -92,4 +92,23 @@ struct bbw_ctx {
 
 namespace bbw {
 void adj_release(bbw_ctx *c);
+
+// Makes a context's device current for the duration of one entry point and
+// restores the caller's device on return: contexts of one process may live
+// on different devices, and their streams, buffers and launches belong to
+// that device.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int device) {  // device < 0: nothing to do
+    int cur = -1;
+    if (device >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != device &&
+        cudaSetDevice(device) == cudaSuccess)
+      prev = cur;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+  DeviceGuard(const DeviceGuard &) = delete;
+  DeviceGuard &operator=(const DeviceGuard &) = delete;
+};
 }  // namespace bbw

@@ -1,6 +1,9 @@
 // Status strings and the per-thread last-error record of the C ABI.
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "device_common.cuh"
 
@@ -20,6 +23,29 @@ bbw_status set_cuda_error(cudaError_t e, const char *where) {
 }
 
 bbw_status check_launch(const char *what) { return set_cuda_error(cudaGetLastError(), what); }
+
+bbw_status ensure_smem_limit(const void *func, int bytes, const char *what) {
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, int> done;  // (kernel, device) -> limit set
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return set_cuda_error(e, what);
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = done.find(std::make_pair(func, dev));
+  if (it != done.end() && it->second >= bytes) return BBW_OK;
+  e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return set_cuda_error(e, what);
+  done[std::make_pair(func, dev)] = bytes;
+  return BBW_OK;
+}
+
+int device_smem_optin() {
+  int dev = 0, v = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 48 * 1024;
+  if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+    return 48 * 1024;
+  return v;
+}
 
 }  // namespace bbw
 

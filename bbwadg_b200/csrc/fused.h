@@ -32,6 +32,7 @@ struct FusedPlan {
   const int *tables = nullptr;
   int table_ints = 0, pat_off = 0, bb_off = 0;
   int S = 1, nsm = 148;  // shots per launch, SM count
+  int max_ctas = 0;      // cap on the persistent grid (0: one CTA per SM)
   const int *src_off = nullptr, *src_elem = nullptr;  // sources (null: none)
   const float *src_vec = nullptr;
   float f0 = 0.f, tR = 0.f, samp = 0.f;
@@ -64,7 +65,8 @@ struct TcLayout {
 };
 
 struct TcPlan {
-  int N = 0, K = 0, Nq = 0, bc = 0, grid = 0;
+  int N = 0, K = 0, Nq = 0, bc = 0, grid = 0, nsm = 148;
+  int max_ctas = 0;  // cap on the persistent grid (0: one CTA per SM)
   TcLayout L;
   const float *geo = nullptr, *c2q = nullptr;
   const int *nbr = nullptr, *tables = nullptr;

@@ -688,8 +688,9 @@ static bbw_status launch_fused(const FusedPlan &pl, const float *Qin, float *Qou
   P.vq_out = pl.vq_out;
   const bool os = pl.ops_smem > 0;
   size_t sm = pl.smem;
+  const int ctas = pl.max_ctas > 0 ? std::min(pl.max_ctas, pl.nsm) : pl.nsm;
   const int grid =
-      std::min(cdiv((pl.Kc > 0 ? pl.Kc : pl.K) - pl.K0, TILE_E) * std::max(pl.S, 1), pl.nsm);
+      std::min(cdiv((pl.Kc > 0 ? pl.Kc : pl.K) - pl.K0, TILE_E) * std::max(pl.S, 1), ctas);
   if (pl.K0 > 0) {  // a window of a split stage: the single-buffered WIN variants
     sm = smem_bytes<N, BB>(pl.Nq, false, os, pl.ops_floats, pl.table_ints, pl.bb_off);
     if (pl.W == 8) {
@@ -717,28 +718,23 @@ static bbw_status launch_fused(const FusedPlan &pl, const float *Qin, float *Qou
   return check_launch("fused stage");
 }
 
+// The dynamic shared-memory limit is a per-kernel, per-device attribute
+// while a plan's size depends on its mesh (the face-permutation table), so
+// every variant's limit is raised to the device maximum once: contexts on
+// different meshes then never undercut each other's launches.
 template <int N, bool BB, int W>
-static cudaError_t set_smem_attr(bool os, bool pipe, int bytes) {
-  if (os && pipe)
-    return cudaFuncSetAttribute(k_fused_stage<N, BB, true, true, W>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  if (os)
-    return cudaFuncSetAttribute(k_fused_stage<N, BB, true, false, W>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  if (pipe)
-    return cudaFuncSetAttribute(k_fused_stage<N, BB, false, true, W>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  return cudaFuncSetAttribute(k_fused_stage<N, BB, false, false, W>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-}
-
-// the window variants are single-buffered
-template <int N, bool BB, int W>
-static cudaError_t set_smem_attr_window(bool os, int bytes) {
-  return os ? cudaFuncSetAttribute(k_fused_stage<N, BB, true, false, W, true>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)
-            : cudaFuncSetAttribute(k_fused_stage<N, BB, false, false, W, true>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+static bbw_status set_smem_attr(int bytes) {
+  const void *fn[6] = {(const void *)k_fused_stage<N, BB, true, true, W>,
+                       (const void *)k_fused_stage<N, BB, true, false, W>,
+                       (const void *)k_fused_stage<N, BB, false, true, W>,
+                       (const void *)k_fused_stage<N, BB, false, false, W>,
+                       (const void *)k_fused_stage<N, BB, true, false, W, true>,
+                       (const void *)k_fused_stage<N, BB, false, false, W, true>};
+  for (const void *f : fn) {
+    const bbw_status s = ensure_smem_limit(f, bytes, "fused stage attribute");
+    if (s != BBW_OK) return s;
+  }
+  return BBW_OK;
 }
 
 template <int N, bool BB>
@@ -766,15 +762,8 @@ static bbw_status prepare(FusedPlan &pl) {
   pl.pipe = cand[pick][1];
   pl.smem = smem_bytes<N, BB>(pl.Nq, pl.pipe, pl.ops_smem > 0, pl.ops_floats, pl.table_ints,
                               pl.bb_off);
-  cudaError_t e = pl.W == 8 ? set_smem_attr<N, BB, 8>(pl.ops_smem > 0, pl.pipe, (int)pl.smem)
-                            : set_smem_attr<N, BB, 16>(pl.ops_smem > 0, pl.pipe, (int)pl.smem);
-  if (e != cudaSuccess) return set_cuda_error(e, "fused stage attribute");
-  // the window variants (same operator placement)
-  const int smw = (int)smem_bytes<N, BB>(pl.Nq, false, pl.ops_smem > 0, pl.ops_floats,
-                                         pl.table_ints, pl.bb_off);
-  e = pl.W == 8 ? set_smem_attr_window<N, BB, 8>(pl.ops_smem > 0, smw)
-                : set_smem_attr_window<N, BB, 16>(pl.ops_smem > 0, smw);
-  if (e != cudaSuccess) return set_cuda_error(e, "fused stage window attribute");
+  bbw_status st = pl.W == 8 ? set_smem_attr<N, BB, 8>(maxsm) : set_smem_attr<N, BB, 16>(maxsm);
+  if (st != BBW_OK) return st;
   pl.nsm = nsm > 0 ? nsm : 148;
   pl.grid = std::min(cdiv(pl.Kc > 0 ? pl.Kc : pl.K, TILE_E) * std::max(pl.S, 1), pl.nsm);
   return BBW_OK;

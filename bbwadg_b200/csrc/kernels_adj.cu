@@ -353,11 +353,8 @@ static bbw_status launch_adj_n(int S, int K, int Nq, const float *PqT, const flo
       sizeof(float) * (size_t)AS * (Np + 2 * Nq),
       sizeof(float) * ((size_t)Np * ldq + (size_t)Nq * ldp), &stage);
   if (sm > 200 * 1024) return set_error(BBW_ERR_UNSUPPORTED, "adjoint WADG: Nq too large");
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_adj_wadg<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  bbw_status s = ensure_smem_limit(k_adj_wadg<N>, 200 * 1024, "adjoint WADG attribute");
+  if (s != BBW_OK) return s;
   k_adj_wadg<N><<<(K + AE - 1) / AE, AE * AW, sm, st>>>(S, K, Nq, stage, PqT, VqT, c2q, lamQ,
                                                         lamR, a, b, dt, vq, z, grad);
   return check_launch("adjoint WADG");
@@ -371,11 +368,8 @@ static bbw_status launch_sigma_n(int S, int K, const float *fgeo, const float *L
   const size_t sm = stage_smem(sizeof(float) * ((size_t)AS * (8 * Np + NF) + AE * 16),
                                sizeof(float) * (size_t)4 * Np * ldf, &stage);
   if (sm > 200 * 1024) return set_error(BBW_ERR_UNSUPPORTED, "adjoint lift: N too large");
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_adj_sigma<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  bbw_status s = ensure_smem_limit(k_adj_sigma<N>, 200 * 1024, "adjoint lift attribute");
+  if (s != BBW_OK) return s;
   k_adj_sigma<N><<<(S * K + AE - 1) / AE, AE * AW, sm, st>>>(S * K, K, stage, fgeo, LTp, z,
                                                                sigma);
   return check_launch("adjoint lift");
@@ -389,11 +383,8 @@ static bbw_status launch_volume_n(int S, int K, const float *vgeo, const float *
   const size_t sm = stage_smem(sizeof(float) * (size_t)8 * Np * AS,
                                sizeof(float) * (size_t)3 * Np * ldp, &stage);
   if (sm > 200 * 1024) return set_error(BBW_ERR_UNSUPPORTED, "adjoint volume: N too large");
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_adj_volume<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  bbw_status s = ensure_smem_limit(k_adj_volume<N>, 200 * 1024, "adjoint volume attribute");
+  if (s != BBW_OK) return s;
   k_adj_volume<N><<<(S * K + AE - 1) / AE, AE * AW, sm, st>>>(S * K, K, stage, vgeo, DTp, z, vol);
   return check_launch("adjoint volume");
 }

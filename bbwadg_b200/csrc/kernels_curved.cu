@@ -454,12 +454,9 @@ bbw_status launch_curved_stage(CurvedStageArgs A, const float *Qold, float *Qnew
   A.EB = curved_eb(width, per);
   if (A.EB * per > kCurvedSmemMax)
     return set_error(BBW_ERR_UNSUPPORTED, "curved stage: cubature too large for shared memory");
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_curved_stage<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)kCurvedSmemMax);
-    attr = true;
-  }
+  bbw_status s =
+      ensure_smem_limit(k_curved_stage<N>, (int)kCurvedSmemMax, "curved stage attribute");
+  if (s != BBW_OK) return s;
   k_curved_stage<N><<<(A.KC + A.EB - 1) / A.EB, kCurvedThreads, A.EB * per, st>>>(A, Qold, Qnew,
                                                                                    res);
   return check_launch("curved stage");
@@ -477,12 +474,9 @@ bbw_status launch_volume_skew(int K, const int *Klist, int Nq, const float *vgeo
   const int eb = curved_eb(std::max(Nq, Np), per);
   if (eb * per > kCurvedSmemMax)
     return set_error(BBW_ERR_UNSUPPORTED, "rk_volume_WADG_skew_combine: Nq too large");
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_volume_skew<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)kCurvedSmemMax);
-    attr = true;
-  }
+  bbw_status s = ensure_smem_limit(k_volume_skew<N>, (int)kCurvedSmemMax,
+                                   "rk_volume_WADG_skew_combine attribute");
+  if (s != BBW_OK) return s;
   k_volume_skew<N><<<(K + eb - 1) / eb, kCurvedThreads, eb * per, st>>>(
       K, Klist, Nq, eb, vgeoq, Jq, Vq, Vrq, Vsq, Vtq, Pq, Prq, Psq, Ptq, Q, rhsQ);
   return check_launch("rk_volume_WADG_skew_combine");
@@ -497,12 +491,9 @@ bbw_status launch_surface_skew(int K, const int *Klist, int Nfq, const float *fg
   const int eb = curved_eb(std::max(4 * Nfq, NF), per);
   if (eb * per > kCurvedSmemMax)
     return set_error(BBW_ERR_UNSUPPORTED, "rk_surface_WADG_skew_combine: Nfq too large");
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_surface_skew<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)kCurvedSmemMax);
-    attr = true;
-  }
+  bbw_status s = ensure_smem_limit(k_surface_skew<N>, (int)kCurvedSmemMax,
+                                   "rk_surface_WADG_skew_combine attribute");
+  if (s != BBW_OK) return s;
   k_surface_skew<N><<<(K + eb - 1) / eb, kCurvedThreads, eb * per, st>>>(
       K, Klist, Nfq, eb, fgeoq, VfqFace, Pfq, Fmask, vmapP, Q, rhsQ);
   return check_launch("rk_surface_WADG_skew_combine");

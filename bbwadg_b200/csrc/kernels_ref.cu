@@ -463,12 +463,9 @@ static bbw_status launch_wadg(int K, int Nq, const float *Vq, const float *Pq, c
   constexpr int Np = NP(N), EB = UPD_EB(N);
   const size_t sm = sizeof(float) * EB * 4 * (Np + Nq);
   if (sm > 200 * 1024) return set_error(BBW_ERR_UNSUPPORTED, "rk_update_WADG: Nq too large");
-  static bool attr[BBW_MAX_N + 1] = {};
-  if (!attr[N]) {
-    cudaFuncSetAttribute(k_rk_update_wadg<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         200 * 1024);
-    attr[N] = true;
-  }
+  bbw_status s =
+      ensure_smem_limit(k_rk_update_wadg<N>, 200 * 1024, "rk_update_WADG attribute");
+  if (s != BBW_OK) return s;
   k_rk_update_wadg<N><<<(K + EB - 1) / EB, 256, sm, st>>>(K, Nq, Vq, Pq, Jq, c2q, fa, fb, fdt,
                                                           rhsQ, resQ, Q);
   return check_launch("rk_update_WADG");

@@ -220,10 +220,20 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
   const int *sFmask = sTab;
   const int *sPat = sTab + P.pat_off;
   const int ntiles = cdv(P.K, TC_E);
+  // Failure path: a bounded wait that gives up sets `fail` (made warp
+  // uniform at once, so the warp-collective TMEM loads stay converged); the
+  // thread then skips every shared-memory, TMEM and global access that
+  // depends on the awaited data.  At the next CTA barrier the whole CTA
+  // votes, stops issuing copies and MMAs, and leaves the tile loop; thread 0
+  // then waits (bounded again) for the copies and MMAs it still has in
+  // flight before the TMEM is freed, and the error flag is raised.
   bool fail = false;
+  bool tma_pend = false, mma_pend = false;  // thread 0: issued, completion not yet seen
+  uint32_t tma_par = 0, mma_par = 0;        // their mbarrier phases
 
-  auto issue_tma = [&](int tile, int gb) {  // thread 0
+  auto issue_tma = [&](int tile, int gb, uint32_t parity) {  // thread 0
     const int k0 = tile * TC_E, ne = min(TC_E, P.K - k0);
+    tma_pend = true, tma_par = parity;
     const uint32_t bytes = (uint32_t)ne * (4 * Np * 4 + TC_GEO * 4 + 16);
     tc::mbar_expect_tx(mbarT, bytes);
     for (int e = 0; e < ne; ++e)
@@ -231,9 +241,16 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
     tc::bulk_g2s(sGeoB + gb * TC_E * TC_GEO, P.geo + (size_t)k0 * TC_GEO, ne * TC_GEO * 4, mbarT);
     tc::bulk_g2s(sNbr, P.nbr + (size_t)k0 * 4, ne * 16, mbarT);
   };
-  auto mma_wait = [&](uint32_t &ph) {
-    if (!tc::mbar_wait(mbarM, ph, TC_WAIT)) fail = true;
-    ph ^= 1u;
+  uint32_t tphase = 0, mphase = 0;
+  auto mma_commit = [&]() {  // thread 0
+    tc::mma_commit(mbarM);
+    mma_pend = true, mma_par = mphase;
+  };
+  auto mma_wait = [&]() {
+    const bool ok = tc::mbar_wait(mbarM, mphase, TC_WAIT);
+    if (ok && tid == 0) mma_pend = false;
+    fail = __any_sync(0xffffffffu, fail || !ok);
+    mphase ^= 1u;
     tc::fence_after_sync();
   };
   auto sync_for_mma = [&]() {  // generic smem writes -> tensor core
@@ -283,8 +300,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
     }
   };
 
-  uint32_t tphase = 0, mphase = 0;
-  if (blockIdx.x < ntiles && tid == 0) issue_tma(blockIdx.x, 0);
+  if (blockIdx.x < ntiles && tid == 0) issue_tma(blockIdx.x, 0, tphase);
   int it = 0;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
     const int k0 = tile * TC_E, ne = min(TC_E, P.K - k0), gb = it & 1;
@@ -293,11 +309,18 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
 
     // ---- P0: tile inputs (issued during the previous tile's epilogues);
     //          outside neighbour traces in flight through the first half of P1
-    if (!tc::mbar_wait(mbarT, tphase, TC_WAIT)) fail = true;
+    {
+      const bool ok = tc::mbar_wait(mbarT, tphase, TC_WAIT);
+      if (ok && tid == 0) tma_pend = false;
+      fail = __any_sync(0xffffffffu, fail || !ok);
+    }
     tphase ^= 1u;
-    load_traces(tile);
+    if (!fail) load_traces(tile);
     if (tid < 8) sRed[tid] = 0;
-    __syncthreads();
+    if (__syncthreads_or(fail)) {
+      fail = true;
+      break;
+    }
 
     // ---- P1: p and contravariant velocities (4 nodes x 1 element per item),
     //          then the upwind flux; maxima
@@ -409,7 +432,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
         chain(tbase + 128 + 32 * f, sOps + L.oL + 2 * f * 64 * KF,
               sOps + L.oL + (2 * f + 1) * 64 * KF, sboF, sBF + 2 * f * TC_E * KF,
               sBF + (2 * f + 1) * TC_E * KF, sboF, KF / 16, id64, false);
-      tc::mma_commit(mbarM);
+      mma_commit();
     }
     float ro[8][3];
 #pragma unroll
@@ -419,14 +442,14 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
 #pragma unroll
       for (int fl = 1; fl < 4; ++fl) ro[j][fl - 1] = rowok && e < ne ? P.res[id + fl * Np] : 0.f;
     }
-    mma_wait(mphase);
+    mma_wait();
 
     // ---- P3: epilogue 1 (thread = node row n, 8 elements): rhs of p, u, v, w;
     //          LSRK update of u, v, w (old state from the tile in shared
     //          memory); rhs_p -> B operand of the Vq product
     const uint32_t trow = tbase + ((uint32_t)(32 * q4) << 16) + 8 * g8;
-    float rp[8];
-    {
+    float rp[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (!fail) {
       float gr[8], gs[8], gt[8], dv[8], lf[4][8];
       tc::tmem_ld8x4(trow + 0, trow + 32, trow + 64, trow + 96, gr, gs, gt, dv);
       tc::tmem_ld8x4(trow + 128, trow + 160, trow + 192, trow + 224, lf[0], lf[1], lf[2], lf[3]);
@@ -466,9 +489,12 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       mr = warp_max(mr);
       if (lane == 0) atomicMax(&sRed[3], __float_as_int(mr));
     }
-    __syncthreads();
+    if (__syncthreads_or(fail)) {
+      fail = true;
+      break;
+    }
     // the state tile is dead: the next tile's copies overlap the rest
-    if (tid == 0 && next < ntiles) issue_tma(next, gb ^ 1);
+    if (tid == 0 && next < ntiles) issue_tma(next, gb ^ 1, tphase);
     const float srp = pow2_scale(sRed[3]);
     if (lane < 16) {
 #pragma unroll
@@ -484,7 +510,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
     if (tid == 0) {
       chain(tbase + 0, sOps + L.oVq, sOps + L.oVq + MQ * KV, (KV / 8) * 128, sBp, sBp + TC_E * KV,
             (KV / 8) * 128, KV / 16, tc::idesc_f16(MQ, TC_E, FMT), false);
-      tc::mma_commit(mbarM);
+      mma_commit();
     }
     const int q = MQ == 128 ? 32 * q4 + lane : (lane < 16 ? 16 * q4 + lane : MQ);
     float c2v[8];
@@ -493,12 +519,12 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       const int e = 8 * g8 + j;
       c2v[j] = q < Nq && e < ne ? __ldg(P.c2q + (size_t)(k0 + e) * Nq + q) : 0.f;
     }
-    mma_wait(mphase);
+    mma_wait();
 
     // ---- P5: epilogue 2 (thread = cubature row q): c2/J * p_q -> B operand
     {
-      float v[8];
-      tc::tmem_ld8(tbase + ((uint32_t)(32 * q4) << 16) + 8 * g8, v);
+      float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      if (!fail) tc::tmem_ld8(tbase + ((uint32_t)(32 * q4) << 16) + 8 * g8, v);
       const float isr = 1.f / srp;
       float mc = 0.f;
 #pragma unroll
@@ -508,7 +534,10 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       }
       mc = warp_max(mc);
       if (lane == 0) atomicMax(&sRed[4], __float_as_int(mc));
-      __syncthreads();
+      if (__syncthreads_or(fail)) {
+        fail = true;
+        break;
+      }
       const float sc = pow2_scale(sRed[4]);
       if (q < KQ) {
 #pragma unroll
@@ -524,7 +553,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       if (tid == 0) {
         chain(tbase + 32, sOps + L.oPq, sOps + L.oPq + 64 * KQ, (KQ / 8) * 128, sBU,
               sBU + TC_E * KQ, (KQ / 8) * 128, KQ / 16, tc::idesc_f16(64, TC_E, FMT), false);
-        tc::mma_commit(mbarM);
+        mma_commit();
       }
       float r7[8], q7[8];  // old residual and state of p, fetched during the MMAs
 #pragma unroll
@@ -534,13 +563,13 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
         r7[j] = rowok && e < ne ? P.res[id] : 0.f;
         q7[j] = rowok && e < ne ? __ldg(P.Qin + id) : 0.f;
       }
-      mma_wait(mphase);
+      mma_wait();
 
       // ---- P7: epilogue 3: rhs_p = Pq (c2 p_q); LSRK update of p
       float w[8];
-      tc::tmem_ld8(tbase + ((uint32_t)(32 * q4) << 16) + 32 + 8 * g8, w);
+      if (!fail) tc::tmem_ld8(tbase + ((uint32_t)(32 * q4) << 16) + 32 + 8 * g8, w);
       const float isc = 1.f / sc;
-      if (rowok) {
+      if (rowok && !fail) {
         const float *ro = r7, *qo = q7;
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
@@ -554,10 +583,20 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       }
     }
     tc::fence_before_sync();
-    __syncthreads();  // TMEM, B operands and reduction slots free for the next tile
+    // TMEM, B operands and reduction slots free for the next tile
+    if (__syncthreads_or(fail)) {
+      fail = true;
+      break;
+    }
     tc::fence_after_sync();
   }
-  if (fail) atomicAdd(P.err, 1);
+  if (fail && tid == 0) {
+    // drain this CTA's own copies and MMAs still in flight (bounded), so
+    // nothing lands in shared memory or TMEM after they are released
+    if (tma_pend) tc::mbar_wait(mbarT, tma_par, TC_WAIT);
+    if (mma_pend) tc::mbar_wait(mbarM, mma_par, TC_WAIT);
+    atomicAdd(P.err, 1);
+  }
   tc::fence_before_sync();
   __syncthreads();
   if (warp == 0) tc::tmem_dealloc(tbase, 256);
@@ -572,10 +611,12 @@ static bbw_status tc_prepare_n(TcPlan &pl) {
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (pl.L.total > maxsm)
     return set_error(BBW_ERR_UNSUPPORTED, "tensor-core stage: shared-memory footprint too large");
-  cudaError_t e = cudaFuncSetAttribute(k_tc_stage<N, BF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       pl.L.total);
-  if (e != cudaSuccess) return set_cuda_error(e, "tensor-core stage attribute");
-  pl.grid = std::min(cdv(pl.K, TC_E), nsm > 0 ? nsm : 148);
+  // the limit is per kernel and device while the footprint depends on the
+  // mesh (face-permutation table): raise it to the device maximum once
+  const bbw_status s = ensure_smem_limit(k_tc_stage<N, BF>, maxsm, "tensor-core stage attribute");
+  if (s != BBW_OK) return s;
+  pl.nsm = nsm > 0 ? nsm : 148;
+  pl.grid = std::min(cdv(pl.K, TC_E), pl.nsm);
   return BBW_OK;
 }
 
@@ -591,7 +632,8 @@ static bbw_status tc_launch_n(const TcPlan &pl, const float *Qin, float *Qout, f
   P.tables = pl.tables, P.table_ints = pl.table_ints, P.pat_off = pl.pat_off;
   P.err = pl.err;
   P.L = pl.L;
-  k_tc_stage<N, BF><<<pl.grid, TC_T, pl.L.total, st>>>(P);
+  const int grid = pl.max_ctas > 0 ? std::min(pl.grid, pl.max_ctas) : pl.grid;
+  k_tc_stage<N, BF><<<grid, TC_T, pl.L.total, st>>>(P);
   return check_launch("tensor-core stage");
 }
 

@@ -16,9 +16,12 @@
 // * The scratch holds kNoAllocScratchFloats floats (16 MiB): K * 4 * Np
 //   must not exceed it (N = 3: K <= 52 428; N = 5: K <= 18 724); larger
 //   meshes are rejected with BBW_ERR_UNSUPPORTED before anything runs.
-// * The first call on each device looks the scratch address up
-//   (cudaGetSymbolAddress with that device current); make that first call
-//   outside any stream capture.
+// * The scratch address is looked up (cudaGetSymbolAddress, with the
+//   device current) and cached per device.  The first call on each device
+//   does this set-up and must come before any stream capture.  Every later
+//   call whose stream is not capturing looks the address up again, so after
+//   a cudaDeviceReset (which reloads the module and may move the array) the
+//   next such call picks up the new address.
 // * Nothing in the scratch has to start at zero: rk_volume overwrites every
 //   rhs entry of the K elements before rk_surface accumulates into it.
 // * There is one scratch per device: calls that overlap in time on the same
@@ -42,14 +45,21 @@ __device__ __align__(256) float g_stage_scratch[kNoAllocScratchFloats];
 std::mutex g_scratch_mu;
 float *g_scratch_ptr[kMaxDevices] = {};
 
-bbw_status scratch_for_current_device(float **out) {
+bbw_status scratch_for_current_device(cudaStream_t stream, float **out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return bbw::set_cuda_error(e, "bbw_rk_stage_noalloc: current device");
   if (dev < 0 || dev >= kMaxDevices)
     return bbw::set_error(BBW_ERR_UNSUPPORTED, "bbw_rk_stage_noalloc: device index above 63");
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(stream, &cap);
+  if (e != cudaSuccess) return bbw::set_cuda_error(e, "bbw_rk_stage_noalloc: stream");
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_ptr[dev]) {
+  if (cap == cudaStreamCaptureStatusNone || !g_scratch_ptr[dev]) {
+    if (cap != cudaStreamCaptureStatusNone)
+      return bbw::set_error(BBW_ERR_STATE,
+                            "bbw_rk_stage_noalloc: first call on a device inside a stream "
+                            "capture; make one call outside the capture first");
     void *p = nullptr;
     e = cudaGetSymbolAddress(&p, g_stage_scratch);
     if (e != cudaSuccess)
@@ -83,7 +93,7 @@ extern "C" bbw_status bbw_rk_stage_noalloc(int N, int K, int Nq, int bc, const f
                           "(4 Mi floats); use the kernel-level entry points with your own rhs "
                           "buffer or a bbw_ctx");
   float *rhs = nullptr;
-  bbw_status s = scratch_for_current_device(&rhs);
+  bbw_status s = scratch_for_current_device(static_cast<cudaStream_t>(stream), &rhs);
   if (s != BBW_OK) return s;
   if ((s = bbw_rk_volume(N, K, vgeo, Dr, Ds, Dt, Q, rhs, stream)) != BBW_OK) return s;
   if ((s = bbw_rk_surface(N, K, bc, fgeo, Fmask, vmapP, LIFT, Q, rhs, stream)) != BBW_OK) return s;

@@ -170,10 +170,16 @@ class LocalExchange:
             self.solvers[p].move_elements(1, 0, si, bp, side.cuda_stream)  # next state of p
             with torch.cuda.stream(side):
                 bq.copy_(bp, non_blocking=True)
-            self.solvers[q].move_elements(1, 1, ri, bq, side.cuda_stream)  # q's next-state halo
+            copied = torch.cuda.Event()
+            copied.record(side)
+            # the scatter is a launch on q's device: on one of q's streams
+            side_q = self._side[q] if self.devices[q] != self.devices[p] else side
+            if side_q is not side:
+                side_q.wait_event(copied)
+            self.solvers[q].move_elements(1, 1, ri, bq, side_q.cuda_stream)  # q's next-state halo
             ev = torch.cuda.Event()
-            ev.record(side)
-            touched[p].append(ev)
+            ev.record(side_q)
+            touched[p].append(copied)
             touched[q].append(ev)
         for s, main, evs in zip(self.solvers, self._main, touched):
             for ev in evs:  # halos in place; own buffers free again
@@ -202,6 +208,10 @@ class DistExchange:
     def __init__(self, part, gather, scatter, floats_per_element, device, sync=None,
                  group=None, solver=None):
         import torch
+        if torch.device(device).type == "cuda" and sync is None:
+            # the gather kernels run on the solver's stream, NCCL reads the
+            # buffers on another: without sync the send could read them early
+            raise ValueError("DistExchange: device buffers need sync (the solver's sync)")
         self.gather, self.scatter, self.sync, self.group = gather, scatter, sync, group
         self.part, self.solver = part, solver  # solver: for stage_overlapped (device buffers)
         n = floats_per_element

@@ -186,6 +186,10 @@ class WaveSolver:
         _lib.call("bbw_set_config", self._h,
                   int(warps) | (int(bool(ops_in_smem)) << 8) | (int(bool(pipelined)) << 9))
 
+    def set_grid_limit(self, max_ctas):
+        """Cap the persistent stage kernels at max_ctas CTAs (0: one per SM)."""
+        _lib.call("bbw_set_grid_limit", self._h, int(max_ctas))
+
     # ---- batched shots, sources, receivers
     def set_shots(self, S):
         """S independent shots per launch (state [S][K][4][Np], zeroed)."""

@@ -22,10 +22,13 @@ steps.
 * roofline   the fused stage kernel against the measured HBM copy bandwidth;
              algorithmic bytes per element-stage 64 Np + 4 Nq + 132;
 * cpu_baseline  the reference's own OKL kernels (oracle/_ref, built from the
-             reference sources, OpenMP over elements) on this host's cores,
-             on a bounded sample (16^3 x 6 tets, same N and operators).
+             reference sources, OpenMP over elements) on all of this host's
+             cores, on the same 32^3 x 6 mesh, N and operators, one LSRK45
+             step (a bounded sample of the run).
 
---impl reference runs only that CPU path (rank 0; other ranks exit 0).
+--impl reference runs only that CPU path on the same workload (rank 0;
+other ranks exit 0): --warmup untimed steps (at most 2) then --steps timed
+steps (at most 30), each a full LSRK45 step of the 32^3 x 6 mesh.
 """
 import argparse
 import json
@@ -44,7 +47,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 N_ORDER, N_HEX = 5, 32
-SAMPLE_HEX = 16
+REF_MAX_STEPS, REF_MAX_WARMUP = 30, 2  # bound on the reference arm's CPU time
 
 
 def algorithmic_bytes_per_element(Np, Nq):
@@ -115,12 +118,23 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def dist_env():
     return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
             int(os.environ.get("LOCAL_RANK", 0)))
 
 
-def reference_cpu(steps, warmup, nhex=SAMPLE_HEX, N=N_ORDER, bern=0, timeout=900):
+def reference_cpu(steps, warmup, nhex=N_HEX, N=N_ORDER, bern=0, timeout=900):
     """The reference's own CPU path: oracle/_ref driver (reference host code +
     OKL kernels translated and JIT-compiled with OpenMP), all host threads."""
     from bbwadg_b200.mesh import kuhn_box, write_gmsh22
@@ -138,6 +152,7 @@ def reference_cpu(steps, warmup, nhex=SAMPLE_HEX, N=N_ORDER, bern=0, timeout=900
         return None, "reference run failed: " + p.stderr[-200:]
     r = json.loads(p.stdout.strip().splitlines()[-1])
     r["cores"] = cores
+    r["cpu_model"] = cpu_model()
     return r, None
 
 
@@ -145,21 +160,24 @@ def run_reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    r, err = reference_cpu(max(args.steps, 1), max(args.warmup, 0))
+    steps = min(max(args.steps, 1), REF_MAX_STEPS)
+    warm = min(max(args.warmup, 0), REF_MAX_WARMUP)
+    r, err = reference_cpu(steps, warm)
     if r is None:
         print(json.dumps({"impl": "reference", "unavailable": err}))
         return 0
     v = r["dof_stage_per_s"]
-    sample = "N=%d, %d^3 x 6 tets (K=%d), %d LSRK45 steps after %d warm-up" % (
-        N_ORDER, SAMPLE_HEX, r["K"], r["steps"], args.warmup)
+    sample = ("N=%d, %d^3 x 6 tets (K=%d, the full workload), %d LSRK45 steps timed after %d "
+              "warm-up (steps capped at %d)" % (N_ORDER, N_HEX, r["K"], r["steps"], warm,
+                                                REF_MAX_STEPS))
     print(json.dumps({
         "metric": "DOF-stage updates/s (acoustic WADG, affine tets, N=5)", "impl": "reference",
         "value": v, "unit": "DOF-stage/s", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * r["seconds"] / r["steps"],
+        "warmup": warm, "ms_per_step": 1e3 * r["seconds"] / r["steps"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic", "config": workload_config(args, "nodal"),
         "cpu_baseline": {"value": v, "unit": "DOF-stage/s", "cores": r["cores"],
-                         "kind": "reference", "sample": sample},
+                         "cpu_model": r["cpu_model"], "kind": "reference", "sample": sample},
         "e2e": {"value": v, "unit": "DOF-stage/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0}}))
     return 0
@@ -594,17 +612,20 @@ def main():
             tuned = s.autotune(prob.dt, 10)
         qptr, rptr, stream_ptr = s.device_state()
         stream = torch.cuda.ExternalStream(stream_ptr)
+        # clocks are sampled every 100 ms from the warm-up through the timed
+        # and end-to-end regions (a timed region alone can be shorter than
+        # one sample)
+        clk = ClockSampler(local).__enter__()
         s.steps(prob.dt, args.warmup)
         s.sync()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
-        with ClockSampler(local) as clk:
-            e0.record(stream)
-            s.steps(prob.dt, args.steps)
-            e1.record(stream)
-            torch.cuda.synchronize()
+        e0.record(stream)
+        s.steps(prob.dt, args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         if world > 1:
             t = torch.tensor([ms], device="cuda")
@@ -623,6 +644,7 @@ def main():
         s.steps(prob.dt, args.steps)
         s.get_data(out=out.numpy())
         t_e2e = time.perf_counter() - t0
+        clk.__exit__(None, None, None)
         if world > 1:
             t = torch.tensor([t_e2e], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -670,7 +692,11 @@ def main():
                      "peak_kind": peak_kind},
         "e2e": {"value": world * head["dofs"] / head["e2e_s"], "unit": "DOF-stage/s",
                 "h2d_bytes_per_step": head["state_bytes"] / args.steps,
-                "d2h_bytes_per_step": head["state_bytes"] / args.steps},
+                "d2h_bytes_per_step": head["state_bytes"] / args.steps,
+                "copies": "per run, as the reference's WaveSetData3d -> Wave_RK -> "
+                          "WaveGetData3d: the state in from pinned host memory once, the "
+                          "timed steps, the state out once; bytes per step = state bytes / "
+                          "steps"},
         "gpu_launches": head["launches"],
         "clocks": head["clocks"],
         "side_by_side": {v: {"value": world * r["dofs"] / (r["ms"] / 1e3),
@@ -684,9 +710,9 @@ def main():
         if r is not None:
             line["cpu_baseline"] = {
                 "value": r["dof_stage_per_s"], "unit": "DOF-stage/s", "cores": r["cores"],
-                "kind": "reference",
-                "sample": "N=5, %d^3 x 6 tets (K=%d), %d LSRK45 step, reference OKL kernels "
-                          "via oracle/_ref" % (SAMPLE_HEX, r["K"], r["steps"])}
+                "cpu_model": r["cpu_model"], "kind": "reference",
+                "sample": "N=5, %d^3 x 6 tets (K=%d, the full workload), %d LSRK45 step, "
+                          "reference OKL kernels via oracle/_ref" % (N_HEX, r["K"], r["steps"])}
         else:
             line["cpu_baseline"] = {"value": None, "unavailable": err}
     if shots is not None:

@@ -197,9 +197,10 @@ bbw_status bbw_rk_surface_bern_slice(int N, int K, int bc, const float *fgeo, co
  * library (K * 4 * Np <= 4 Mi floats, else BBW_ERR_UNSUPPORTED).  No
  * reference counterpart (the reference allocates rhsQ at setup).  Make the
  * first call on each device outside stream capture (it looks the scratch
- * address up); nothing in the scratch needs to start at zero; calls that
- * overlap on the same device race on the one scratch; it makes no
- * allocation. */
+ * address up); calls outside a capture look it up again, so after a
+ * cudaDeviceReset make one such call first; nothing in the scratch needs to
+ * start at zero; calls that overlap on the same device race on the one
+ * scratch; it makes no allocation. */
 bbw_status bbw_rk_stage_noalloc(int N, int K, int Nq, int bc, const float *vgeo, const float *Dr,
                                 const float *Ds, const float *Dt, const float *fgeo,
                                 const int *Fmask, const int *vmapP, const float *LIFT,
@@ -291,6 +292,13 @@ bbw_status bbw_autotune(bbw_ctx *ctx, float dt, int stages, int *config);
 /* Applies a configuration code as returned by bbw_autotune (for instance one
  * cached from an earlier run); BBW_ERR_UNSUPPORTED if it does not fit. */
 bbw_status bbw_set_config(bbw_ctx *ctx, int config);
+/* Caps the persistent stage kernels (FP32 fused and tensor-core forms) at
+ * max_ctas CTAs, each then looping over more element tiles; 0 restores one
+ * CTA per SM.  For leaving SMs to concurrent work on other streams, and for
+ * checking the per-CTA tile loop on small meshes.  A launch-shape control
+ * like the reference's KblkV/KblkS/KblkU (cpp/src/WaveOKL3d.cpp:1618-1650);
+ * results do not depend on it. */
+bbw_status bbw_set_grid_limit(bbw_ctx *ctx, int max_ctas);
 
 /* ---- element (slab) decomposition across devices.  Elements [0, Kc) of
  * the context are advanced by each stage; elements [Kc, K) are halo copies of

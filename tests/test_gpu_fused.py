@@ -265,3 +265,26 @@ def test_fused_n8_with_729_point_rule_is_refused(cuda):
     assert p.Nq == 729
     with pytest.raises(BBWError, match="shared memory"):
         WaveSolver(p)
+
+
+@pytest.mark.parametrize("form", ["fp32", "f16x3"])
+def test_contexts_on_different_meshes_do_not_undercut_each_other(cuda, form):
+    """Two contexts of the same order on meshes with different numbers of
+    face permutations (hence different shared-memory footprints): creating
+    the second must not break the first one's launches."""
+    from oracle import Oracle
+    g = golden("ops_N3.npz")
+    nfq = int(g["Nfq"][0])
+    rule = dict(cubature=(g["rq"], g["sq"], g["tq"], g["wq"]),
+                tri_cubature=(g["rfq"][:nfq], g["sfq"][:nfq], g["wfqFace"]))
+    a = make_problem(3, 3, variant="nodal", c2="sine", seed=2, **rule)
+    b = make_problem(3, mesh=_tets(2), variant="nodal", c2="sine", seed=2, **rule)
+    sa = WaveSolver(a, precision=form)
+    sb = WaveSolver(b, precision=form)
+    for s, p in ((sa, a), (sb, b)):
+        s.set_data(p.Q0)
+        s.steps(p.dt, 2)
+        q_ref, _ = Oracle(3, p.K, p.ops_dict(), p.geo_dict()).run(p.Q0.copy(), p.dt, 10)
+        assert rel_l2(s.get_data(), q_ref) < TOL
+    sa.close()
+    sb.close()

@@ -1,0 +1,141 @@
+"""Persistent CTAs that loop over many element tiles, against the C
+restatement.
+
+Every stage kernel runs one CTA per SM and walks the (shot, tile) work items
+with a grid stride, so a mesh of more than 148 tiles (or a capped grid) is
+needed before the cross-tile machinery runs: the next tile's inputs copied
+while the current one computes (double buffer), or the single buffer refilled
+part by part as the tile is done with it, and the neighbour traces fetched a
+tile ahead.  Each case compares the state after two LSRK45 steps (ten
+stages, cpp/src/WaveOKL3d.cpp:2084-2109) with the oracle.  FP32 tolerance:
+1e-5 relative L2."""
+import numpy as np
+import pytest
+from conftest import golden, rel_l2
+
+from bbwadg_b200 import WaveSolver, make_problem
+from bbwadg_b200._lib import BBWError
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+# split-BF16 keeps 16 significant bits per hi/lo pair; over ten stages it
+# stays within 1e-6 of the FP32 restatement, so it shares the FP32 bar here
+BF16X3_TOL = 1e-5
+
+
+def ref_rule(N):
+    g = golden("ops_N%d.npz" % N)
+    nfq = int(g["Nfq"][0])
+    return (g["rq"], g["sq"], g["tq"], g["wq"]), (g["rfq"][:nfq], g["sfq"][:nfq], g["wfqFace"])
+
+
+def oracle_run(p, stages, Q0=None):
+    from oracle import Oracle
+    orc = Oracle(p.N, p.K, p.ops_dict(), p.geo_dict(), variant=p.variant)
+    if Q0 is None:
+        return orc.run(p.Q0.copy(), p.dt, stages)[0]
+    return [orc.run(q.copy(), p.dt, stages)[0] for q in Q0]
+
+
+CONFIGS = [(w, ops, pipe) for w in (8, 16) for ops in (True, False) for pipe in (True, False)]
+
+
+@pytest.mark.parametrize("N", [3, 5])
+@pytest.mark.parametrize("variant", ["nodal", "bb"])
+def test_every_configuration_over_many_tiles(cuda, N, variant):
+    """10^3 x 6 tets (K = 6000, 188 tiles on 148 CTAs) with the full grid,
+    and the same mesh on 7 CTAs (27 tiles each), for every warps /
+    operator-placement / buffering variant the autotuner can pick
+    (including the single-buffered form the N = 5 headline runs)."""
+    cub, tri = ref_rule(N)
+    p = make_problem(N, 10, variant=variant, c2="sine", c2_jitter=0.5, seed=11, cubature=cub,
+                     tri_cubature=tri)
+    assert p.K == 6000
+    q_ref = oracle_run(p, 10)
+    ran = []
+    for warps, ops, pipe in CONFIGS:
+        for limit in (0, 7):
+            s = WaveSolver(p)
+            try:
+                s.set_config(warps, ops, pipe)
+            except BBWError:  # does not fit in shared memory
+                s.close()
+                break
+            s.set_grid_limit(limit)
+            s.set_data(p.Q0)
+            s.steps(p.dt, 2)
+            err = rel_l2(s.get_data(), q_ref)
+            s.close()
+            assert err < TOL, (warps, ops, pipe, limit, err)
+            ran.append((warps, ops, pipe, limit))
+    assert len(ran) >= 8, ran
+    if N == 5:  # the headline form: 8 warps, operators in shared memory, one buffer
+        assert (8, True, False, 0) in ran
+
+
+@pytest.mark.parametrize("variant", ["nodal", "bb"])
+def test_shots_over_many_tiles_on_a_capped_grid(cuda, variant):
+    """Three shots of a 6^3 x 6 mesh (41 tiles each, 123 work items) on 5
+    CTAs: every CTA's loop crosses shot boundaries and ragged last tiles."""
+    N = 4
+    cub, tri = ref_rule(N)
+    p = make_problem(N, 6, variant=variant, c2="sine", c2_jitter=0.5, seed=4, cubature=cub,
+                     tri_cubature=tri)
+    rng = np.random.default_rng(1)
+    S = 3
+    Q0 = np.stack([p.Q0 * (1.0 - 0.3 * i) + 0.01 * rng.standard_normal(p.Q0.size)
+                   for i in range(S)]).astype(np.float32)
+    refs = oracle_run(p, 10, Q0=Q0)
+    for warps, ops, pipe in CONFIGS:
+        s = WaveSolver(p)
+        try:
+            s.set_config(warps, ops, pipe)
+        except BBWError:
+            s.close()
+            continue
+        s.set_shots(S)
+        s.set_grid_limit(5)
+        s.set_data(Q0)
+        s.steps(p.dt, 2)
+        out = s.get_data().reshape(S, -1)
+        s.close()
+        for i in range(S):
+            assert rel_l2(out[i], refs[i]) < TOL, (warps, ops, pipe, i)
+
+
+@pytest.mark.parametrize("prec,tol", [("f16x3", TOL), ("bf16x3", BF16X3_TOL)])
+@pytest.mark.parametrize("limit", [0, 3])
+def test_tensor_core_stage_over_many_tiles(cuda, prec, tol, limit):
+    """The tensor-core stage at N = 5 (reference rule, Nq = 95) on 10^3 x 6
+    tets: 188 tiles with the full grid, about 63 per CTA on 3 CTAs."""
+    cub, tri = ref_rule(5)
+    p = make_problem(5, 10, variant="nodal", c2="sine", c2_jitter=0.5, seed=12, cubature=cub,
+                     tri_cubature=tri)
+    q_ref = oracle_run(p, 10)
+    s = WaveSolver(p, precision=prec)
+    s.set_grid_limit(limit)
+    s.set_data(p.Q0)
+    s.steps(p.dt, 2)
+    s.check()
+    err = rel_l2(s.get_data(), q_ref)
+    s.close()
+    assert err < tol, err
+
+
+def test_grid_limit_does_not_change_results(cuda):
+    """The grid cap only changes which CTA runs which tile: results are
+    bit-identical for any cap, and a negative cap is refused."""
+    p = make_problem(3, 4, variant="nodal", c2="sine", c2_jitter=0.5, seed=2)
+    out = []
+    for limit in (0, 1, 2, 5):
+        s = WaveSolver(p)
+        s.set_grid_limit(limit)
+        s.set_data(p.Q0)
+        s.steps(p.dt, 3)
+        out.append(s.get_data())
+        if limit == 5:
+            with pytest.raises(BBWError):
+                s.set_grid_limit(-1)
+        s.close()
+    for q in out[1:]:
+        assert np.array_equal(q, out[0])
