@@ -13,6 +13,9 @@
 // fa=(float)rk4a[s], fb=(float)rk4b[s], fdt=dt.
 //
 // Usage:
+//   ref_driver mesh  MESH OUT.bin                ReadGmsh3d + FacePair3d + StartUp3d
+//                                                 outputs (vertices, EToV, EToE,
+//                                                 EToF, vmapM/vmapP, nodes)
 //   ref_driver dump  MESH OUT.bin [opts]         operators + connectivity
 //   ref_driver run   MESH OUT.bin [opts]         IC + stages, final state
 //   ref_driver kernel MESH OUT.bin --which NAME  one kernel on given inputs
@@ -38,6 +41,7 @@ extern occa::memory c_Vq_reduced, c_Pq_reduced, c_c2q, c_Jq_reduced;
 extern occa::kernel rk_volume, rk_surface, rk_volume_bern, rk_surface_bern, rk_update,
     rk_update_WADG;
 extern occa::device device;
+extern double *VX, *VY, *VZ;  // cpp/src/Mesh3d.cpp:6
 extern occa::kernelInfo dgInfo;
 dfloat WaveInitOCCA3d(Mesh *mesh, int KblkV, int KblkS, int KblkU, int KblkQ, int KblkQf);
 
@@ -86,6 +90,41 @@ int main(int argc, char **argv) {
   if (!kb.empty()) sscanf(kb.c_str(), "%d,%d,%d", &KblkV, &KblkS, &KblkU);
   FacePair3d(mesh);
   StartUp3d(mesh);
+  if (mode == "mesh") {  // the mesh reader's and connectivity's own outputs
+    fflush(stdout);
+    dup2(saved_stdout, 1);
+    const int K = mesh->K;
+    Writer w(argv[3]);
+    w.scal("N", p_N);
+    w.scal("K", K);
+    w.scal("Nv", mesh->Nv);
+    w.rec("VX", 1, VX, (uint64_t)mesh->Nv);
+    w.rec("VY", 1, VY, (uint64_t)mesh->Nv);
+    w.rec("VZ", 1, VZ, (uint64_t)mesh->Nv);
+    std::vector<int> e2v((size_t)K * 4), e2e((size_t)K * 4), e2f((size_t)K * 4);
+    std::vector<double> gx((size_t)K * 4), gy((size_t)K * 4), gz((size_t)K * 4);
+    for (int k = 0; k < K; ++k)
+      for (int f = 0; f < 4; ++f) {
+        e2v[4 * k + f] = mesh->EToV[k][f];
+        e2e[4 * k + f] = mesh->EToE[k][f];
+        e2f[4 * k + f] = mesh->EToF[k][f];
+        gx[4 * k + f] = mesh->GX(k, f);
+        gy[4 * k + f] = mesh->GY(k, f);
+        gz[4 * k + f] = mesh->GZ(k, f);
+      }
+    w.rec("EToV", 2, e2v.data(), e2v.size());
+    w.rec("EToE", 2, e2e.data(), e2e.size());
+    w.rec("EToF", 2, e2f.data(), e2f.size());
+    w.rec("GX", 1, gx.data(), gx.size());
+    w.rec("GY", 1, gy.data(), gy.size());
+    w.rec("GZ", 1, gz.data(), gz.size());
+    w.rec("vmapM_raw", 2, mesh->vmapM, (uint64_t)K * p_Nfp * p_Nfaces);
+    w.rec("vmapP_raw", 2, mesh->vmapP, (uint64_t)K * p_Nfp * p_Nfaces);
+    w.f64("x", mesh->x);
+    w.f64("y", mesh->y);
+    w.f64("z", mesh->z);
+    return 0;
+  }
   dfloat dt = WaveInitOCCA3d(mesh, KblkV, KblkS, KblkU, 1, 1);
   InitQuadratureArrays(mesh);
   std::string c2 = opt(argc, argv, "--c2", "one");
