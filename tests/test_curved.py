@@ -1,8 +1,9 @@
 """Curvilinear WADG path on the CPU: the native setup (Gordon-Hall curving,
 geometric factors at the cubature, curved operators) against the reference's
 own setup, and the FP64 restatement of the curved stage (oracle/curved.py)
-pinned to the reference's kernels (tests/golden/curved_ball4_N*.npz, from
-oracle/_ref/ref_curved_N* on kuhn_ball(4): K = 384, 288 curved)."""
+pinned to the reference's kernels (tests/golden/curved_*_N*.npz, from
+oracle/_ref/ref_curved_N* on kuhn_ball(4): K = 384, 288 curved, and on the
+reference's own sphere meshes sphere48.msh and sphere385.msh)."""
 import numpy as np
 import pytest
 from conftest import golden, rel_l2
@@ -18,12 +19,22 @@ def ref_rules(g):
     return ((g["rq"], g["sq"], g["tq"], g["wq"]), (g["rfq"][:Nfq], g["sfq"][:Nfq], g["wfqFace"]))
 
 
-def problem_like_reference(N):
-    g = golden("curved_ball4_N%d.npz" % N)
+def problem_like_reference(N, mesh="ball4"):
+    """The reference's curved setup on kuhn_ball(4) or on one of its own
+    sphere meshes (sphere48 / sphere385, read as ReadGmsh3d reads them)."""
+    g = golden("curved_%s_N%d.npz" % (mesh, N))
     cub, tri = ref_rules(g)
-    p = make_curved_problem(N, 4, cubature=cub, tri_cubature=tri)
+    if mesh == "ball4":
+        p = make_curved_problem(N, 4, cubature=cub, tri_cubature=tri)
+    else:
+        m = golden("gmsh_%s.npz" % mesh)
+        p = make_curved_problem(N, mesh=(m["VX"], m["VY"], m["VZ"], m["EToV"]), cubature=cub,
+                                tri_cubature=tri)
     p.c2q = g["c2q_in"].reshape(p.K, p.Nq)
     return p, g
+
+
+MESHES = ["ball4", "sphere48", "sphere385"]
 
 
 def oracle_of(p):
@@ -31,35 +42,42 @@ def oracle_of(p):
     return CurvedOracle(p.N, p.K, p.Nq, p.Nfq, p.desc_arrays())
 
 
+@pytest.mark.parametrize("mesh", MESHES)
 @pytest.mark.parametrize("N", [2, 3])
-def test_gordon_hall_matches_reference(N):
-    p, g = problem_like_reference(N)
+def test_gordon_hall_matches_reference(N, mesh):
+    p, g = problem_like_reference(N, mesh)
     assert np.array_equal(p.KlistCurved, g["KlistCurved"])
-    assert np.array_equal(p.KlistPlanar, g["KlistPlanar"])
+    # the reference sizes its planar list max(1, KPlanar) (cpp/src/WaveOKL3d.cpp:1239):
+    # with every element curved (sphere48) it holds one unused 0
+    KP = p.K - len(g["KlistCurved"])
+    assert np.array_equal(p.KlistPlanar, g["KlistPlanar"][:KP])
     for c in ("x", "y", "z"):
         assert np.abs(p.mesh[c] - g[c]).max() < 1e-13, c
     assert abs(p.dt - float(g["dt"][0])) <= 1e-7 * p.dt
 
 
+@pytest.mark.parametrize("mesh", MESHES)
 @pytest.mark.parametrize("N", [2, 3])
-def test_curved_geometry_matches_reference(N):
-    p, g = problem_like_reference(N)
+def test_curved_geometry_matches_reference(N, mesh):
+    p, g = problem_like_reference(N, mesh)
     n = len(g["Jq_sub"])
     for ours, ref in ((p.vgeoq, g["vgeoq_sub"]), (p.Jq, g["Jq_sub"]), (p.fgeoq, g["fgeoq_sub"])):
         a = ours.reshape(p.K, -1)[:n]
         assert np.abs(a - ref).max() <= 1e-6 * np.abs(ref).max()
 
 
+@pytest.mark.parametrize("mesh", MESHES)
 @pytest.mark.parametrize("N", [2, 3])
-def test_curved_operators_match_reference(N):
-    p, g = problem_like_reference(N)
+def test_curved_operators_match_reference(N, mesh):
+    p, g = problem_like_reference(N, mesh)
     for k in OPS:
         assert np.abs(p.ops[k] - g[k]).max() <= 1e-6 * np.abs(g[k]).max(), k
 
 
+@pytest.mark.parametrize("mesh", MESHES)
 @pytest.mark.parametrize("N", [2, 3])
-def test_oracle_run_matches_reference(N):
-    p, g = problem_like_reference(N)
+def test_oracle_run_matches_reference(N, mesh):
+    p, g = problem_like_reference(N, mesh)
     Q, res = oracle_of(p).run(p.Q0, float(g["dt"][0]), int(g["stages"]))
     assert rel_l2(Q, g["Q_run"]) < 1e-6
     assert rel_l2(res, g["res_run"]) < 1e-4  # small residual: FP32 noise of the reference

@@ -1,5 +1,6 @@
 """Curvilinear WADG path on the GPU against the reference's own kernels
-(tests/golden/curved_ball4_N*.npz) and the FP64 restatement
+and runs (tests/golden/curved_*_N*.npz: kuhn_ball(4) and the reference's
+sphere48 / sphere385 meshes) and the FP64 restatement
 (oracle/curved.py) at orders the reference's curving does not define.
 
 FP32 tolerance: 1e-5 relative L2 on states and kernel outputs; 1e-3 on the
@@ -63,9 +64,13 @@ def test_kernel_entries_match_reference(cuda, kernel):
     assert rel_l2(r.cpu().numpy(), g[kernel + ".rhsQ"]) < TOL
 
 
+@pytest.mark.parametrize("mesh", ["ball4", "sphere48", "sphere385"])
 @pytest.mark.parametrize("N", [2, 3])
-def test_stages_match_reference(cuda, N):
-    p, g = problem_like_reference(N)
+def test_stages_match_reference(cuda, N, mesh):
+    """50 stages on kuhn_ball(4) and on the reference's own sphere meshes
+    (sphere48.msh: every element curved; sphere385.msh) against the
+    reference's RK_step_WADG run on them."""
+    p, g = problem_like_reference(N, mesh)
     s = CurvedSolver(p)
     s.set_data(p.Q0)
     stages(s, float(g["dt"][0]), int(g["stages"]))
