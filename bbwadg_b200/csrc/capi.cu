@@ -248,7 +248,7 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
   if (tcp && (variant != BBW_NODAL || !tc_supported(m->N, m->Nq)))
     return set_error(BBW_ERR_UNSUPPORTED,
                      "bbw_create: the split-FP16 tensor-core stage supports the nodal variant "
-                     "with N in {3, 5} and Nq <= 128");
+                     "with N in [2, 5] and Nq <= 128");
   const int N = m->N, K = m->K, Nq = m->Nq;
   if (N < 1 || N > BBW_MAX_N) return set_error(BBW_ERR_UNSUPPORTED, "bbw_create: N out of range");
   if (K <= 0 || K >= (1 << 23) || Nq <= 0)
@@ -407,18 +407,20 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
       std::memcpy(&geo[(size_t)k * TC_GEO], m->vgeo + (size_t)k * 9, 9 * sizeof(float));
       std::memcpy(&geo[(size_t)k * TC_GEO + 9], m->fgeo + (size_t)k * 16, 16 * sizeof(float));
     }
+    // operator planes with MR (MRQ) stored rows, see tc_layout
     std::vector<uint16_t> h(TL.ops_halfs);
+    const int MR = TL.MR, MRQ = TL.MRQ;
     const float *Dd[3] = {o->Dr, o->Ds, o->Dt};
     for (int d = 0; d < 3; ++d)
-      tc_pack_operator(Dd[d], Np, Np, 1, Np, 64, TL.KV, &h[TL.oD + 2 * d * 64 * TL.KV],
-                       &h[TL.oD + (2 * d + 1) * 64 * TL.KV], tp.bf);
+      tc_pack_operator(Dd[d], Np, Np, 1, Np, MR, TL.KV, &h[TL.oD + 2 * d * MR * TL.KV],
+                       &h[TL.oD + (2 * d + 1) * MR * TL.KV], tp.bf);
     for (int f = 0; f < 4; ++f)
-      tc_pack_operator(o->LIFT + (size_t)f * Nfp * Np, Np, Nfp, 1, Np, 64, TL.KF,
-                       &h[TL.oL + 2 * f * 64 * TL.KF], &h[TL.oL + (2 * f + 1) * 64 * TL.KF],
+      tc_pack_operator(o->LIFT + (size_t)f * Nfp * Np, Np, Nfp, 1, Np, MR, TL.KF,
+                       &h[TL.oL + 2 * f * MR * TL.KF], &h[TL.oL + (2 * f + 1) * MR * TL.KF],
                        tp.bf);
-    tc_pack_operator(o->Vq, Nq, Np, 1, Nq, TL.MQ, TL.KV, &h[TL.oVq], &h[TL.oVq + TL.MQ * TL.KV],
+    tc_pack_operator(o->Pq, Np, Nq, 1, Np, MR, TL.KQ, &h[TL.oPq], &h[TL.oPq + MR * TL.KQ], tp.bf);
+    tc_pack_operator(o->Vq, Nq, Np, 1, Nq, MRQ, TL.KV, &h[TL.oVq], &h[TL.oVq + MRQ * TL.KV],
                      tp.bf);
-    tc_pack_operator(o->Pq, Np, Nq, 1, Np, 64, TL.KQ, &h[TL.oPq], &h[TL.oPq + 64 * TL.KQ], tp.bf);
     uint16_t *dops = nullptr;
     if ((s = upload(&c->geo_tc, geo.data(), geo.size(), "bbw_create: geometry")) != BBW_OK ||
         (s = upload(&dops, h.data(), h.size(), "bbw_create: tensor-core operators")) != BBW_OK ||
@@ -429,7 +431,7 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
     }
     c->ops_tc = dops;
     tp.geo = c->geo_tc, tp.c2q = c->c2q, tp.nbr = c->nbr, tp.tables = c->tables;
-    tp.ops = c->ops_tc, tp.err = c->err;
+    tp.ops = c->ops_tc, tp.err = c->err, tp.time = c->d_time;
     if ((s = tc_prepare(tp)) != BBW_OK) {
       release(c);
       return s;
@@ -503,7 +505,8 @@ extern "C" bbw_status bbw_stage_ex(bbw_ctx *c, float fa, float fb, float fdt, fl
   if (!c) return set_error(BBW_ERR_ARG, "bbw_stage: ctx is NULL");
   bbw_status s =
       c->precision != BBW_PREC_FP32
-          ? tc_launch(c->tc, c->Q[c->cur], c->Q[c->cur ^ 1], c->res, fa, fb, fdt, c->stream)
+          ? tc_launch(c->tc, c->Q[c->cur], c->Q[c->cur ^ 1], c->res, fa, fb, fdt, cstage,
+                      c->stream)
           : fused_launch(c->plan, c->Q[c->cur], c->Q[c->cur ^ 1], c->res, fa, fb, fdt, cstage,
                          c->stream);
   if (s == BBW_OK) c->cur ^= 1;
@@ -743,8 +746,6 @@ extern "C" bbw_status bbw_scatter_elements(bbw_ctx *c, int n, const int *idx, co
 extern "C" bbw_status bbw_set_shots(bbw_ctx *c, int S) {
   DeviceGuard dg(c ? c->device : -1);
   if (!c || S < 1) return set_error(BBW_ERR_ARG, "bbw_set_shots: bad argument");
-  if (S > 1 && c->precision != BBW_PREC_FP32)
-    return set_error(BBW_ERR_UNSUPPORTED, "bbw_set_shots: batched shots need BBW_PREC_FP32");
   cudaStreamSynchronize(c->stream);
   const size_t n = (size_t)S * c->K * 4 * c->Np;
   if ((size_t)S * c->K * 4 * c->Np > ((size_t)1 << 40))
@@ -765,10 +766,12 @@ extern "C" bbw_status bbw_set_shots(bbw_ctx *c, int S) {
   c->Q[0] = q0, c->Q[1] = q1, c->res = r, c->cur = 0;
   c->S = S;
   c->plan.S = S;
+  c->tc.S = S;
   if (c->src_off) {  // source table is per shot: drop it
     cudaFree(c->src_off), cudaFree(c->src_elem), cudaFree(c->src_vec);
     c->src_off = c->src_elem = nullptr, c->src_vec = nullptr;
     c->plan.src_off = c->plan.src_elem = nullptr, c->plan.src_vec = nullptr;
+    c->tc.src_off = c->tc.src_elem = nullptr, c->tc.src_vec = nullptr;
   }
   if (c->traces) {
     cudaFree(c->traces);
@@ -788,12 +791,11 @@ extern "C" bbw_status bbw_set_sources(bbw_ctx *c, int nent, const int *shot, con
   DeviceGuard dg(c ? c->device : -1);
   if (!c || nent < 0 || (nent > 0 && (!shot || !elem || !vec)))
     return set_error(BBW_ERR_ARG, "bbw_set_sources: bad argument");
-  if (nent > 0 && c->precision != BBW_PREC_FP32)
-    return set_error(BBW_ERR_UNSUPPORTED, "bbw_set_sources: sources need BBW_PREC_FP32");
   cudaStreamSynchronize(c->stream);
   cudaFree(c->src_off), cudaFree(c->src_elem), cudaFree(c->src_vec);
   c->src_off = c->src_elem = nullptr, c->src_vec = nullptr;
   c->plan.src_off = c->plan.src_elem = nullptr, c->plan.src_vec = nullptr;
+  c->tc.src_off = c->tc.src_elem = nullptr, c->tc.src_vec = nullptr;
   drop_graphs(c);
   if (nent == 0) return BBW_OK;
   const int Np = c->Np;
@@ -822,6 +824,8 @@ extern "C" bbw_status bbw_set_sources(bbw_ctx *c, int nent, const int *shot, con
     return s;
   c->plan.src_off = c->src_off, c->plan.src_elem = c->src_elem, c->plan.src_vec = c->src_vec;
   c->plan.f0 = f0, c->plan.tR = t_delay, c->plan.samp = amplitude;
+  c->tc.src_off = c->src_off, c->tc.src_elem = c->src_elem, c->tc.src_vec = c->src_vec;
+  c->tc.f0 = f0, c->tc.tR = t_delay, c->tc.samp = amplitude;
   c->src_stage_times = stage_times != 0;
   return BBW_OK;
 }

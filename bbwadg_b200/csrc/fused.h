@@ -57,15 +57,17 @@ void pack_fused_ops(int N, int Nq, int W, bool bb, const float *Dr, const float 
 constexpr int TC_GEO = 28;  // floats per element geometry record: vgeo 9 | fgeo 16 | pad 3
 
 struct TcLayout {
-  int KV = 0, KF = 0, KQ = 0, MQ = 0;         // padded K extents, Vq rows
-  int oD = 0, oL = 0, oVq = 0, oPq = 0;       // operator offsets (halves)
+  int KV = 0, KF = 0, KQ = 0, MQ = 0;   // padded K extents, rows of the Vq MMA (64 or 128)
+  int MR = 0, MRQ = 0;                  // operator rows stored: Np and Nq rounded up (see tc_layout)
+  int oD = 0, oL = 0, oPq = 0, oVq = 0; // operator offsets (halves)
   int ops_halfs = 0;
-  int ops = 0, Bp = 0, BU = 0, BF = 0, raw = 0, geo = 0, nbr = 0, tab = 0, misc = 0;  // bytes
+  int ops = 0, Bp = 0, BU = 0, BF = 0, BW = 0, raw = 0, geo = 0, nbr = 0, tab = 0, misc = 0;  // bytes
   int total = 0;
 };
 
 struct TcPlan {
   int N = 0, K = 0, Nq = 0, bc = 0, grid = 0, nsm = 148;
+  int S = 1;         // shots per launch (state [S][K][4][Np])
   int max_ctas = 0;  // cap on the persistent grid (0: one CTA per SM)
   TcLayout L;
   const float *geo = nullptr, *c2q = nullptr;
@@ -74,13 +76,18 @@ struct TcPlan {
   bool bf = false;  // split-BF16 operands instead of split-FP16
   int table_ints = 0, pat_off = 0;
   int *err = nullptr;
+  // sources, as FusedPlan (null: none)
+  const int *src_off = nullptr, *src_elem = nullptr;
+  const float *src_vec = nullptr;
+  float f0 = 0.f, tR = 0.f, samp = 0.f;
+  const double *time = nullptr;
 };
 
 TcLayout tc_layout(int N, int Nq, int table_ints);
 bool tc_supported(int N, int Nq);
 bbw_status tc_prepare(TcPlan &pl);
 bbw_status tc_launch(const TcPlan &pl, const float *Qin, float *Qout, float *res, float fa,
-                     float fb, float fdt, cudaStream_t st);
+                     float fb, float fdt, float cstage, cudaStream_t st);
 void tc_pack_operator(const float *A, int nrows, int ncols, int ld_row, int ld_col, int rows,
                       int kp, uint16_t *hi, uint16_t *lo, bool bf);
 bbw_status fused_prepare(FusedPlan &pl);

@@ -18,18 +18,40 @@
 //
 // Orientation: operator rows on the MMA M dimension (64 or 128), the 32
 // elements of a tile on N, the reduction index on K.  Operators (A) are
-// staged once per CTA; element operands (B) are written per tile by the
-// CUDA-core producer phase.  Accumulators: TMEM columns [0,96) gradient
-// (r,s,t), [96,128) divergence, [128,256) lift per face; then [0,32) Vq and
-// [32,64) Pq.
+// staged once per CTA with only round8(Np) rows (round16(Nq) for Vq) stored:
+// an M = 64 (128) MMA reads its remaining rows from whatever follows in
+// shared memory, and those rows only feed accumulator rows that are never
+// read.  The operators' K padding is stored as zeros, so it meets the zero K
+// padding of the element operands (B) in exact zero products.
 //
-// Inputs arrive by 1-D TMA bulk copies: each element's 4 Np state record
-// into a row of stride RS (RS/4 odd, so lane-per-element float4 reads are
-// conflict-free), the packed geometry record and the neighbour codes.  The
-// state buffer is released as soon as the producers have consumed it, so
-// the next tile's copies overlap the MMAs and epilogues.  The LSRK update
-// reads the old state and residual from global memory in the epilogues
-// (thread = node row, coalesced).
+// Work items are (shot, tile of 32 elements); a persistent CTA walks them
+// with a grid stride and keeps two in flight in one instruction stream:
+//
+//   a. epilogue 1 of tile T: rhs of u, v, w and the LSRK update of u, v, w
+//      from the gradient / divergence / lift accumulators; rhs_p split into
+//      the B operand of Vq; issue the Vq MMAs
+//   b. while they run: tile T+1 (its bulk copies were issued one tile
+//      earlier) - neighbour traces, upwind flux, B operands of its first
+//      MMA group
+//   c. epilogue 2 of T: c^2 / J at the cubature points -> B operand of Pq;
+//      issue the Pq MMAs of T, the first MMA group of T+1, the bulk copies
+//      of T+2
+//   d. epilogue 3 of T: rhs_p, sources, LSRK update of p, while T+1's MMAs
+//      run.
+//
+// TMEM (512 columns): [0,96) gradient r,s,t, [96,128) divergence,
+// [128,256) lift per face, [256,288) Vq, [288,320) Pq.  For M = 64 an
+// accumulator row m lives in lane (m % 16) + 32 (m / 16); the epilogues read
+// those with the 16x64b shape, so all 32 threads of a warp hold a (row,
+// element) pair.  The LSRK update reads the old state and residual from
+// global memory (L2), so the state tile in shared memory is free for the
+// next copies as soon as the tile's B operands are built.
+//
+// Every mbarrier wait is bounded.  A wait that gives up sets a warp-uniform
+// failure flag; the thread then skips every access that depends on the
+// awaited data, the CTA votes at its next barrier, issues no further copy or
+// MMA and leaves the loop; thread 0 waits (bounded) for what it still has
+// in flight before the TMEM is freed and the error flag is raised.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -50,21 +72,26 @@ namespace bbw {
 constexpr int TC_E = 32;   // elements per tile (MMA N)
 constexpr int TC_T = 512;  // threads per CTA (16 warps)
 constexpr uint32_t TC_WAIT = 1u << 22;  // bounded mbarrier polls
+constexpr uint32_t TC_COLS = 512;       // TMEM columns allocated
+constexpr uint32_t cGrad = 0, cDiv = 96, cLift = 128, cVq = 256, cPq = 288;
 
 __host__ __device__ constexpr int r16(int x) { return (x + 15) & ~15; }
+__host__ __device__ constexpr int r8(int x) { return (x + 7) & ~7; }
 __host__ __device__ constexpr int cdv(int a, int b) { return (a + b - 1) / b; }
 
 template <int N>
 struct TcCfg {
   static constexpr int Np = NP(N), Nfp = NFP(N), NF = 4 * NFP(N);
   static constexpr int KV = r16(Np), KF = r16(Nfp);
-  // raw state row stride (floats): multiple of 4 with RS/4 odd
+  // raw state row stride (floats): multiple of 4 with RS/4 odd, so the
+  // lane-per-element reads of one node hit distinct bank groups
   static constexpr int RS = (Np % 2) ? 4 * Np : 4 * Np + 4;
+  static constexpr bool V4 = Np % 4 == 0;  // field rows 16-byte aligned in the raw tile
   // flux items with lane = face node: (element, face) pairs per warp
   static constexpr int FPW = (4 * TC_E) / (TC_T / 32);
   static_assert((4 * TC_E) % (TC_T / 32) == 0, "face pairs per warp");
   static_assert(NFP(N) <= 32, "one face per warp pass");
-  static_assert(Np <= 64 && Np % 4 == 0, "tensor-core stage: Np <= 64, Np % 4 == 0");
+  static_assert(Np <= 64, "tensor-core stage: Np <= 64 (operator rows of one M = 64 MMA)");
 };
 
 TcLayout tc_layout(int N, int Nq, int table_ints) {
@@ -74,14 +101,16 @@ TcLayout tc_layout(int N, int Nq, int table_ints) {
   L.KF = r16(Nfp);
   L.KQ = r16(Nq);
   L.MQ = Nq <= 64 ? 64 : 128;
+  L.MR = r8(Np);
+  L.MRQ = L.KQ;  // Vq rows [Nq, KQ) are stored zeros: they reach Pq's K padding
   const int RS = (Np % 2) ? 4 * Np : 4 * Np + 4;
-  // operator halves: D_d hi/lo [64][KV] x3, LIFT_f hi/lo [64][KF] x4,
-  // Vq hi/lo [MQ][KV], Pq hi/lo [64][KQ]
+  // operator planes (hi, lo): D_d [MR][KV] x3, LIFT_f [MR][KF] x4, Pq [MR][KQ],
+  // Vq [MRQ][KV]; each MMA reads 64 - MR (MQ - MRQ) rows past its plane
   L.oD = 0;
-  L.oL = L.oD + 6 * 64 * L.KV;
-  L.oVq = L.oL + 8 * 64 * L.KF;
-  L.oPq = L.oVq + 2 * L.MQ * L.KV;
-  L.ops_halfs = L.oPq + 2 * 64 * L.KQ;
+  L.oL = L.oD + 6 * L.MR * L.KV;
+  L.oPq = L.oL + 8 * L.MR * L.KF;
+  L.oVq = L.oPq + 2 * L.MR * L.KQ;
+  L.ops_halfs = L.oVq + 2 * L.MRQ * L.KV;
   auto al = [](int b) { return (b + 127) & ~127; };
   int o = 0;
   L.ops = o;
@@ -89,9 +118,11 @@ TcLayout tc_layout(int N, int Nq, int table_ints) {
   L.Bp = o;
   o = al(o + 2 * (2 * TC_E * L.KV));
   L.BU = o;
-  o = al(o + 2 * std::max(6 * TC_E * L.KV, 2 * TC_E * L.KQ));
+  o = al(o + 2 * (6 * TC_E * L.KV));
   L.BF = o;
   o = al(o + 2 * (8 * TC_E * L.KF));
+  L.BW = o;
+  o = al(o + 2 * std::max(2 * TC_E * L.KV, 2 * TC_E * L.KQ));
   L.raw = o;
   o = al(o + 4 * TC_E * RS);
   L.geo = o;
@@ -101,24 +132,32 @@ TcLayout tc_layout(int N, int Nq, int table_ints) {
   L.tab = o;
   o = al(o + 4 * table_ints);
   L.misc = o;
-  o = al(o + 64);
+  o = al(o + 128);
   L.total = o;
   return L;
 }
 
 struct TcParams {
-  int K, Nq, bc;
-  float fa, fb, fdt;
+  int K, Nq, bc, S;
+  float fa, fb, fdt, cstage;
   const float *__restrict__ Qin;
   float *__restrict__ Qout;
   float *__restrict__ res;
   const float *__restrict__ geo;  // [K][TC_GEO]: vgeo 9 | fgeo 16 | pad
   const int *__restrict__ nbr;    // [K][4]
   const float *__restrict__ c2q;  // [K][Nq]
-  const void *__restrict__ ops;  // split operators: __half, or __nv_bfloat16 (BF)
+  const void *__restrict__ ops;   // split operators: __half, or __nv_bfloat16 (BF)
   const int *__restrict__ tables;
   int table_ints, pat_off;
   int *err;
+  // sources: entries [src_off[s], src_off[s+1]) of shot s, sorted by element,
+  // add ricker(t) * src_vec[j][:] to the projected rhs_p of element
+  // src_elem[j], t = *time + cstage * fdt (as the FP32 fused stage)
+  const int *__restrict__ src_off;
+  const int *__restrict__ src_elem;
+  const float *__restrict__ src_vec;
+  float f0, tR, samp;
+  const double *__restrict__ time;
   TcLayout L;
 };
 
@@ -169,6 +208,20 @@ __device__ __forceinline__ float warp_max(float v) {
   return v;
 }
 
+// Ricker wavelet amp (1 - 2 a^2) exp(-a^2), a = pi f0 (t - tR)
+__device__ __forceinline__ float tc_ricker(float t, float f0, float tR, float amp) {
+  const float a = 3.14159265358979f * f0 * (t - tR);
+  return amp * (1.f - 2.f * a * a) * expf(-a * a);
+}
+
+// An M = 64 accumulator block read with tcgen05.ld.16x64b.x4: the warp
+// reads the 16 lanes of its sub-partition (rows 16 q .. 16 q + 15) and 8
+// element columns; register j of thread t holds TMEM lane (t / 4) + 8 (t % 2)
+// of the sub-partition and column 2 j + (t / 2) % 2 (measured on the B200
+// with a store / load round trip of known values).
+__device__ __forceinline__ int ep_row(int lane) { return (lane >> 2) + 8 * (lane & 1); }
+__device__ __forceinline__ int ep_col(int lane, int j) { return 2 * j + ((lane >> 1) & 1); }
+
 template <int N, bool BF>
 __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
   // operand type; A and B of every MMA share it (the instruction descriptor
@@ -176,34 +229,38 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
   using E = typename std::conditional<BF, __nv_bfloat16, __half>::type;
   constexpr int FMT = BF ? 1 : 0;
   using C = TcCfg<N>;
-  constexpr int Np = C::Np, Nfp = C::Nfp, NF = C::NF, KV = C::KV, KF = C::KF, RS = C::RS;
+  constexpr int Np = C::Np, Nfp = C::Nfp, KV = C::KV, KF = C::KF, RS = C::RS;
   constexpr int FPW = C::FPW;
   extern __shared__ __align__(1024) unsigned char smem[];
   const TcLayout &L = P.L;
-  const int KQ = L.KQ, MQ = L.MQ, Nq = P.Nq;
+  const int KQ = L.KQ, MQ = L.MQ, MR = L.MR, MRQ = L.MRQ, Nq = P.Nq;
   E *sOps = reinterpret_cast<E *>(smem + L.ops);
   E *sBp = reinterpret_cast<E *>(smem + L.Bp);
   E *sBU = reinterpret_cast<E *>(smem + L.BU);
   E *sBF = reinterpret_cast<E *>(smem + L.BF);
+  E *sBW = reinterpret_cast<E *>(smem + L.BW);
   float *sRaw = reinterpret_cast<float *>(smem + L.raw);
   float *sGeoB = reinterpret_cast<float *>(smem + L.geo);
   int *sNbr = reinterpret_cast<int *>(smem + L.nbr);
   int *sTab = reinterpret_cast<int *>(smem + L.tab);
-  uint64_t *mbarT = reinterpret_cast<uint64_t *>(smem + L.misc);
-  uint64_t *mbarM = mbarT + 1;
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(mbarT + 2);
-  int *sRed = reinterpret_cast<int *>(tslot + 2);  // [8] maxima as float bits
+  uint64_t *mbT = reinterpret_cast<uint64_t *>(smem + L.misc);  // tile copies
+  uint64_t *mbM = mbT + 1;                                      // gradient/divergence/lift MMAs
+  uint64_t *mbW = mbT + 2;                                      // Vq, Pq MMAs
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(mbT + 3);
+  int *sRed = reinterpret_cast<int *>(tslot + 1);  // [5] maxima as float bits
+  int *sPend = sRed + 5;  // [6] thread 0's copies / MMAs in flight and their phases
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int q4 = warp & 3, g8 = warp >> 2;  // TMEM sub-partition, element group
+  const int q4 = warp & 3, g8 = warp >> 2;  // TMEM sub-partition, element group of 8
 
   // ---------------------------------------------------------------- setup
   if (tid == 0) {
-    tc::mbar_init(mbarT, 1);
-    tc::mbar_init(mbarM, 1);
+    tc::mbar_init(mbT, 1);
+    tc::mbar_init(mbM, 1);
+    tc::mbar_init(mbW, 1);
     tc::fence_mbar_init();
   }
   if (warp == 0) {
-    tc::tmem_alloc(tslot, 256);
+    tc::tmem_alloc(tslot, TC_COLS);
     tc::tmem_relinquish();
   }
   for (int i = tid; i < L.ops_halfs / 8; i += TC_T)
@@ -212,6 +269,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
   for (int i = tid; i < (L.raw - L.Bp) / 16; i += TC_T)  // B operands: zero padding
     reinterpret_cast<uint4 *>(smem + L.Bp)[i] = make_uint4(0, 0, 0, 0);
   for (int i = tid; i < TC_E * RS; i += TC_T) sRaw[i] = 0.f;  // absent elements stay finite
+  if (tid < 11) sRed[tid] = 0;
   tc::fence_proxy_async();
   tc::fence_before_sync();
   __syncthreads();
@@ -220,48 +278,48 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
   const int *sFmask = sTab;
   const int *sPat = sTab + P.pat_off;
   const int ntiles = cdv(P.K, TC_E);
-  // Failure path: a bounded wait that gives up sets `fail` (made warp
-  // uniform at once, so the warp-collective TMEM loads stay converged); the
-  // thread then skips every shared-memory, TMEM and global access that
-  // depends on the awaited data.  At the next CTA barrier the whole CTA
-  // votes, stops issuing copies and MMAs, and leaves the tile loop; thread 0
-  // then waits (bounded again) for the copies and MMAs it still has in
-  // flight before the TMEM is freed, and the error flag is raised.
-  bool fail = false;
-  bool tma_pend = false, mma_pend = false;  // thread 0: issued, completion not yet seen
-  uint32_t tma_par = 0, mma_par = 0;        // their mbarrier phases
+  const int nvt = P.S * ntiles;
+  const size_t sstride = (size_t)P.K * 4 * Np;  // floats per shot
+  // TMEM address of this warp's M = 64 rows (sub-partition q4) and elements
+  const uint32_t tsub = tbase + ((uint32_t)(32 * q4) << 16) + 8 * g8;
+  const int rowM = 16 * q4 + ep_row(lane);  // M = 64 accumulator row of this thread
+  const bool rowok = rowM < Np;
 
-  auto issue_tma = [&](int tile, int gb, uint32_t parity) {  // thread 0
-    const int k0 = tile * TC_E, ne = min(TC_E, P.K - k0);
-    tma_pend = true, tma_par = parity;
+  bool fail = false;
+  uint32_t tphase = 0, mphase = 0, wphase = 0;
+
+  // thread 0: bulk copies of a work item's inputs (state rows of its shot,
+  // geometry, neighbour codes) into the raw tile and geometry buffer gb
+  auto issue_tma = [&](int vt, int gb) {
+    const int shot = vt / ntiles, k0 = (vt - shot * ntiles) * TC_E, ne = min(TC_E, P.K - k0);
     const uint32_t bytes = (uint32_t)ne * (4 * Np * 4 + TC_GEO * 4 + 16);
-    tc::mbar_expect_tx(mbarT, bytes);
+    tc::mbar_expect_tx(mbT, bytes);
+    const float *q = P.Qin + shot * sstride + (size_t)k0 * 4 * Np;
     for (int e = 0; e < ne; ++e)
-      tc::bulk_g2s(sRaw + e * RS, P.Qin + (size_t)(k0 + e) * 4 * Np, 4 * Np * 4, mbarT);
-    tc::bulk_g2s(sGeoB + gb * TC_E * TC_GEO, P.geo + (size_t)k0 * TC_GEO, ne * TC_GEO * 4, mbarT);
-    tc::bulk_g2s(sNbr, P.nbr + (size_t)k0 * 4, ne * 16, mbarT);
+      tc::bulk_g2s(sRaw + e * RS, q + (size_t)e * 4 * Np, 4 * Np * 4, mbT);
+    tc::bulk_g2s(sGeoB + gb * TC_E * TC_GEO, P.geo + (size_t)k0 * TC_GEO, ne * TC_GEO * 4, mbT);
+    tc::bulk_g2s(sNbr, P.nbr + (size_t)k0 * 4, ne * 16, mbT);
+    sPend[0] = 1, sPend[1] = (int)tphase;  // in flight, awaited with this parity
   };
-  uint32_t tphase = 0, mphase = 0;
-  auto mma_commit = [&]() {  // thread 0
-    tc::mma_commit(mbarM);
-    mma_pend = true, mma_par = mphase;
-  };
-  auto mma_wait = [&]() {
-    const bool ok = tc::mbar_wait(mbarM, mphase, TC_WAIT);
-    if (ok && tid == 0) mma_pend = false;
+  // bounded wait; `pend` >= 0: the sPend slot thread 0 clears on success
+  auto wait_bar = [&](uint64_t *bar, uint32_t &ph, int pend) {
+    const bool ok = tc::mbar_wait(bar, ph, TC_WAIT);
+    if (ok && tid == 0 && pend >= 0) sPend[pend] = 0;
     fail = __any_sync(0xffffffffu, fail || !ok);
-    mphase ^= 1u;
+    ph ^= 1u;
     tc::fence_after_sync();
   };
-  auto sync_for_mma = [&]() {  // generic smem writes -> tensor core
+  // generic smem writes -> tensor core, with the CTA-wide failure vote
+  auto sync_for_mma = [&]() -> bool {
     tc::fence_proxy_async();
     tc::fence_before_sync();
-    __syncthreads();
+    const bool any = __syncthreads_or(fail);
     tc::fence_after_sync();
+    return any;
   };
-  // one operator/operand product chain: D (+)= A B^T over ksteps, 3 products
-  // descriptors of consecutive K steps differ only in the start-address field
-  // (+256 bytes = +16 in 16-byte units)
+  // one operator/operand product chain: D (+)= A B^T over ksteps, 3 products;
+  // descriptors of consecutive K steps differ only in the start-address
+  // field (+256 bytes = +16 in 16-byte units)
   auto chain = [&](uint32_t d, const E *Ahi, const E *Alo, int asbo, const E *Bhi,
                    const E *Blo, int bsbo, int ksteps, uint32_t idesc, bool acc) {
     uint64_t ah = tc::smem_desc(tc::smem_u32(Ahi), 128, asbo);
@@ -275,15 +333,33 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       ah += 16, al += 16, bh += 16, bl += 16;
     }
   };
+  // thread 0: gradient, divergence and lift products of the B1 operands,
+  // committed to mbM
+  auto issue_mma1 = [&]() {
+    const uint32_t id64 = tc::idesc_f16(64, TC_E, FMT);
+    const int sboV = (KV / 8) * 128, sboF = (KF / 8) * 128;
+    const int pD = MR * KV, pL = MR * KF;  // plane sizes (halves)
+    for (int d = 0; d < 3; ++d)
+      chain(tbase + cGrad + 32 * d, sOps + L.oD + 2 * d * pD, sOps + L.oD + (2 * d + 1) * pD,
+            sboV, sBp, sBp + TC_E * KV, sboV, KV / 16, id64, false);
+    for (int d = 0; d < 3; ++d)
+      chain(tbase + cDiv, sOps + L.oD + 2 * d * pD, sOps + L.oD + (2 * d + 1) * pD, sboV,
+            sBU + 2 * d * TC_E * KV, sBU + (2 * d + 1) * TC_E * KV, sboV, KV / 16, id64, d > 0);
+    for (int f = 0; f < 4; ++f)
+      chain(tbase + cLift + 32 * f, sOps + L.oL + 2 * f * pL, sOps + L.oL + (2 * f + 1) * pL,
+            sboF, sBF + 2 * f * TC_E * KF, sBF + (2 * f + 1) * TC_E * KF, sboF, KF / 16, id64,
+            false);
+    tc::mma_commit(mbM);
+    sPend[2] = 1, sPend[3] = (int)mphase;
+  };
 
-  // face traces of neighbours outside tile `tile` (whose inputs have landed)
-  // into registers.  Lane = face node, warp = (element, face) pairs: one load
-  // instruction reads the face of a single neighbour (a few sectors) instead
-  // of one node of 32 neighbours.  Traces inside the tile are read from
-  // shared memory in P1.
+  // neighbour face traces of the work item in the raw tile, outside the
+  // tile, into registers.  Lane = face node, warp = (element, face) pairs:
+  // one load instruction reads the face of a single neighbour.
   float nbv[FPW][4];
-  auto load_traces = [&](int tile) {
-    const int k0 = tile * TC_E, ne = min(TC_E, P.K - k0);
+  auto load_traces = [&](int vt) {
+    const int shot = vt / ntiles, k0 = (vt - shot * ntiles) * TC_E, ne = min(TC_E, P.K - k0);
+    const float *q = P.Qin + shot * sstride;
 #pragma unroll
     for (int j = 0; j < FPW; ++j) {
       nbv[j][0] = nbv[j][1] = nbv[j][2] = nbv[j][3] = 0.f;
@@ -294,99 +370,97 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       if (pat == 255) continue;
       const unsigned rel = (unsigned)((code >> 8) - k0);
       if (rel < (unsigned)ne) continue;
-      const float *o = P.Qin + (size_t)(code >> 8) * 4 * Np + sPat[pat * Nfp + lane];
+      const float *o = q + (size_t)(code >> 8) * 4 * Np + sPat[pat * Nfp + lane];
       nbv[j][0] = __ldg(o), nbv[j][1] = __ldg(o + Np), nbv[j][2] = __ldg(o + 2 * Np),
       nbv[j][3] = __ldg(o + 3 * Np);
     }
   };
 
-  if (blockIdx.x < ntiles && tid == 0) issue_tma(blockIdx.x, 0, tphase);
-  int it = 0;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
-    const int k0 = tile * TC_E, ne = min(TC_E, P.K - k0), gb = it & 1;
+  // producer: p, contravariant velocities and upwind flux of the work item
+  // in the raw tile -> B operands of the first MMA group; sets the scales;
+  // returns the CTA-wide failure vote
+  float sp = 1.f, sU = 1.f, sF = 1.f;
+  auto produce = [&](int vt, int gb) -> bool {
+    const int shot = vt / ntiles, k0 = (vt - shot * ntiles) * TC_E, ne = min(TC_E, P.K - k0);
+    (void)shot;
     const float *sGeo = sGeoB + gb * TC_E * TC_GEO;
-    const int next = tile + gridDim.x;
-
-    // ---- P0: tile inputs (issued during the previous tile's epilogues);
-    //          outside neighbour traces in flight through the first half of P1
-    {
-      const bool ok = tc::mbar_wait(mbarT, tphase, TC_WAIT);
-      if (ok && tid == 0) tma_pend = false;
-      fail = __any_sync(0xffffffffu, fail || !ok);
-    }
-    tphase ^= 1u;
-    if (!fail) load_traces(tile);
-    if (tid < 8) sRed[tid] = 0;
-    if (__syncthreads_or(fail)) {
-      fail = true;
-      break;
-    }
-
-    // ---- P1: p and contravariant velocities (4 nodes x 1 element per item),
-    //          then the upwind flux; maxima
-    constexpr int NC = KV / 4;  // node chunks incl. padding
+    constexpr int NC = KV / 4;               // node chunks incl. padding
     const int ce = tid & 31, cc = tid >> 5;  // item (chunk cc, element ce); TC_T = 16 * 32
-    float G[9];
-#pragma unroll
-    for (int i = 0; i < 9; ++i) G[i] = sGeo[ce * TC_GEO + i];
     float4 p4 = make_float4(0.f, 0.f, 0.f, 0.f), U4[3];
     U4[0] = U4[1] = U4[2] = p4;
-    float mp = 0.f, mU = 0.f;
-    if (cc < NC && 4 * cc < Np && ce < ne) {
-      const float *rr = sRaw + ce * RS + 4 * cc;
-      p4 = *reinterpret_cast<const float4 *>(rr);
-      const float4 u4 = *reinterpret_cast<const float4 *>(rr + Np);
-      const float4 v4 = *reinterpret_cast<const float4 *>(rr + 2 * Np);
-      const float4 w4 = *reinterpret_cast<const float4 *>(rr + 3 * Np);
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        U4[d].x = u4.x * G[3 * d] + v4.x * G[3 * d + 1] + w4.x * G[3 * d + 2];
-        U4[d].y = u4.y * G[3 * d] + v4.y * G[3 * d + 1] + w4.y * G[3 * d + 2];
-        U4[d].z = u4.z * G[3 * d] + v4.z * G[3 * d + 1] + w4.z * G[3 * d + 2];
-        U4[d].w = u4.w * G[3 * d] + v4.w * G[3 * d + 1] + w4.w * G[3 * d + 2];
-        mU = fmaxf(mU, fmaxf(fmaxf(fabsf(U4[d].x), fabsf(U4[d].y)),
-                             fmaxf(fabsf(U4[d].z), fabsf(U4[d].w))));
-      }
-      mp = fmaxf(fmaxf(fabsf(p4.x), fabsf(p4.y)), fmaxf(fabsf(p4.z), fabsf(p4.w)));
-    }
-    // upwind flux (Uflux = -pflux), lane = face node: last, its outside
-    // traces have had longest
+    float mp = 0.f, mU = 0.f, mF = 0.f;
     float pf[FPW];
-    float mF = 0.f;
 #pragma unroll
-    for (int j = 0; j < FPW; ++j) {
-      pf[j] = 0.f;
-      const int pp = warp * FPW + j, e = pp >> 2, f = pp & 3;
-      if (lane >= Nfp || e >= ne) continue;
-      const int m = f * Nfp + lane;
-      const int code = sNbr[e * 4 + f];
-      const int pat = code & 255;
-      const int vM = sFmask[m];
-      const float *own = sRaw + e * RS + vM;
-      const float pM = own[0], uM = own[Np], vvM = own[2 * Np], wM = own[3 * Np];
-      const float *fg = sGeo + e * TC_GEO + 9 + 4 * f;
-      const float Fscale = fg[0], nx = fg[1], ny = fg[2], nz = fg[3];
-      float pjump, Unjump;
-      if (pat == 255) {
-        if (P.bc == BBW_BC_PRESSURE_RELEASE) {
-          pjump = -2.f * pM;
-          Unjump = 0.f;
-        } else {
-          pjump = 0.f;
-          Unjump = -2.f * (uM * nx + vvM * ny + wM * nz);
+    for (int j = 0; j < FPW; ++j) pf[j] = 0.f;
+    if (!fail) {
+      if (cc < NC && 4 * cc < Np && ce < ne) {
+        float G[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) G[i] = sGeo[ce * TC_GEO + i];
+        const float *rr = sRaw + ce * RS + 4 * cc;
+        float4 u4, v4, w4;
+        if constexpr (C::V4) {
+          p4 = *reinterpret_cast<const float4 *>(rr);
+          u4 = *reinterpret_cast<const float4 *>(rr + Np);
+          v4 = *reinterpret_cast<const float4 *>(rr + 2 * Np);
+          w4 = *reinterpret_cast<const float4 *>(rr + 3 * Np);
+        } else {  // field rows not 16-byte aligned; nodes past Np read as zero
+          float a[4][4];
+#pragma unroll
+          for (int fl = 0; fl < 4; ++fl)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[fl][i] = (4 * cc + i < Np) ? rr[fl * Np + i] : 0.f;
+          p4 = make_float4(a[0][0], a[0][1], a[0][2], a[0][3]);
+          u4 = make_float4(a[1][0], a[1][1], a[1][2], a[1][3]);
+          v4 = make_float4(a[2][0], a[2][1], a[2][2], a[2][3]);
+          w4 = make_float4(a[3][0], a[3][1], a[3][2], a[3][3]);
         }
-      } else {
-        const unsigned rel = (unsigned)((code >> 8) - k0);
-        float pP = nbv[j][0], uP = nbv[j][1], vP_ = nbv[j][2], wP = nbv[j][3];
-        if (rel < (unsigned)ne) {  // neighbour inside the tile
-          const float *o = sRaw + rel * RS + sPat[pat * Nfp + lane];
-          pP = o[0], uP = o[Np], vP_ = o[2 * Np], wP = o[3 * Np];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          U4[d].x = u4.x * G[3 * d] + v4.x * G[3 * d + 1] + w4.x * G[3 * d + 2];
+          U4[d].y = u4.y * G[3 * d] + v4.y * G[3 * d + 1] + w4.y * G[3 * d + 2];
+          U4[d].z = u4.z * G[3 * d] + v4.z * G[3 * d + 1] + w4.z * G[3 * d + 2];
+          U4[d].w = u4.w * G[3 * d] + v4.w * G[3 * d + 1] + w4.w * G[3 * d + 2];
+          mU = fmaxf(mU, fmaxf(fmaxf(fabsf(U4[d].x), fabsf(U4[d].y)),
+                               fmaxf(fabsf(U4[d].z), fabsf(U4[d].w))));
         }
-        pjump = pP - pM;
-        Unjump = (uP - uM) * nx + (vP_ - vvM) * ny + (wP - wM) * nz;
+        mp = fmaxf(fmaxf(fabsf(p4.x), fabsf(p4.y)), fmaxf(fabsf(p4.z), fabsf(p4.w)));
       }
-      pf[j] = .5f * (pjump - Unjump) * Fscale;
-      mF = fmaxf(mF, fabsf(pf[j]));
+      // upwind flux (Uflux = -pflux), lane = face node
+#pragma unroll
+      for (int j = 0; j < FPW; ++j) {
+        const int pp = warp * FPW + j, e = pp >> 2, f = pp & 3;
+        if (lane >= Nfp || e >= ne) continue;
+        const int m = f * Nfp + lane;
+        const int code = sNbr[e * 4 + f];
+        const int pat = code & 255;
+        const int vM = sFmask[m];
+        const float *own = sRaw + e * RS + vM;
+        const float pM = own[0], uM = own[Np], vvM = own[2 * Np], wM = own[3 * Np];
+        const float *fg = sGeo + e * TC_GEO + 9 + 4 * f;
+        const float Fscale = fg[0], nx = fg[1], ny = fg[2], nz = fg[3];
+        float pjump, Unjump;
+        if (pat == 255) {
+          if (P.bc == BBW_BC_PRESSURE_RELEASE) {
+            pjump = -2.f * pM;
+            Unjump = 0.f;
+          } else {
+            pjump = 0.f;
+            Unjump = -2.f * (uM * nx + vvM * ny + wM * nz);
+          }
+        } else {
+          const unsigned rel = (unsigned)((code >> 8) - k0);
+          float pP = nbv[j][0], uP = nbv[j][1], vP_ = nbv[j][2], wP = nbv[j][3];
+          if (rel < (unsigned)ne) {  // neighbour inside the tile
+            const float *o = sRaw + rel * RS + sPat[pat * Nfp + lane];
+            pP = o[0], uP = o[Np], vP_ = o[2 * Np], wP = o[3 * Np];
+          }
+          pjump = pP - pM;
+          Unjump = (uP - uM) * nx + (vP_ - vvM) * ny + (wP - wM) * nz;
+        }
+        pf[j] = .5f * (pjump - Unjump) * Fscale;
+        mF = fmaxf(mF, fabsf(pf[j]));
+      }
     }
     mp = warp_max(mp);
     mU = warp_max(mU);
@@ -396,8 +470,8 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       atomicMax(&sRed[1], __float_as_int(mU));
       atomicMax(&sRed[2], __float_as_int(mF));
     }
-    __syncthreads();
-    const float sp = pow2_scale(sRed[0]), sU = pow2_scale(sRed[1]), sF = pow2_scale(sRed[2]);
+    __syncthreads();  // maxima complete
+    sp = pow2_scale(sRed[0]), sU = pow2_scale(sRed[1]), sF = pow2_scale(sRed[2]);
     // B operands (element rows, K-major): p, U_d, per-face pflux
     if (cc < NC) {
       const int o = tc::kmajor_offset_f16(ce, 4 * cc, KV);
@@ -413,51 +487,62 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       const int o = tc::kmajor_offset_f16(e, lane, KF);
       split_store1(sBF + 2 * f * TC_E * KF + o, sBF + (2 * f + 1) * TC_E * KF + o, pf[j] * sF);
     }
-    sync_for_mma();
+    return sync_for_mma();  // B1 written; the raw tile and codes no longer read
+  };
 
-    // ---- P2: gradient, divergence, lift MMAs; meanwhile every thread fetches
-    //          the old residual of u, v, w for its rows of epilogue 1
-    const int n = 16 * q4 + lane;  // M = 64 layout: lanes 0..15 of each sub-partition
-    const bool rowok = lane < 16 && n < Np;
-    if (tid == 0) {
-      const uint32_t id64 = tc::idesc_f16(64, TC_E, FMT);
-      const int sboV = (KV / 8) * 128, sboF = (KF / 8) * 128;
-      for (int d = 0; d < 3; ++d)
-        chain(tbase + 32 * d, sOps + L.oD + 2 * d * 64 * KV, sOps + L.oD + (2 * d + 1) * 64 * KV,
-              sboV, sBp, sBp + TC_E * KV, sboV, KV / 16, id64, false);
-      for (int d = 0; d < 3; ++d)
-        chain(tbase + 96, sOps + L.oD + 2 * d * 64 * KV, sOps + L.oD + (2 * d + 1) * 64 * KV, sboV,
-              sBU + 2 * d * TC_E * KV, sBU + (2 * d + 1) * TC_E * KV, sboV, KV / 16, id64, d > 0);
-      for (int f = 0; f < 4; ++f)
-        chain(tbase + 128 + 32 * f, sOps + L.oL + 2 * f * 64 * KF,
-              sOps + L.oL + (2 * f + 1) * 64 * KF, sboF, sBF + 2 * f * TC_E * KF,
-              sBF + (2 * f + 1) * TC_E * KF, sboF, KF / 16, id64, false);
-      mma_commit();
+  // ---------------------------------------------------------------- prologue
+  int vt = blockIdx.x, it = 0;
+  if (vt < nvt) {
+    if (tid == 0) issue_tma(vt, 0);
+    wait_bar(mbT, tphase, 0);
+    if (!fail) load_traces(vt);
+    fail = produce(vt, 0) || fail;
+    if (tid == 0 && !fail) {
+      issue_mma1();
+      if (vt + (int)gridDim.x < nvt) issue_tma(vt + gridDim.x, 1);
     }
-    float ro[8][3];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const int e = 8 * g8 + j;
-      const size_t id = (size_t)(k0 + e) * 4 * Np + n;
-#pragma unroll
-      for (int fl = 1; fl < 4; ++fl) ro[j][fl - 1] = rowok && e < ne ? P.res[id + fl * Np] : 0.f;
-    }
-    mma_wait();
+    if (tid < 3) sRed[tid] = 0;
+  }
+  float sp_cur = sp, sU_cur = sU, sF_cur = sF;  // scales of the item in acc1
 
-    // ---- P3: epilogue 1 (thread = node row n, 8 elements): rhs of p, u, v, w;
-    //          LSRK update of u, v, w (old state from the tile in shared
-    //          memory); rhs_p -> B operand of the Vq product
-    const uint32_t trow = tbase + ((uint32_t)(32 * q4) << 16) + 8 * g8;
-    float rp[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  // ------------------------------------------------------------- item loop
+  // (fail is CTA-uniform here; inside the loop a missed wait is acted on at
+  // the next CTA-wide vote, so every thread leaves at the same point)
+  if (!fail)
+  for (; vt < nvt; vt += gridDim.x, ++it) {
+    const int shot = vt / ntiles, k0 = (vt - shot * ntiles) * TC_E, ne = min(TC_E, P.K - k0);
+    const int gb = it & 1;
+    const int next = vt + gridDim.x, next2 = next + gridDim.x;
+    const size_t sbase = shot * sstride;
+    const float *sGeo = sGeoB + gb * TC_E * TC_GEO;
+
+    // ---- a. epilogue 1 (thread = node row, four elements): rhs of u, v, w;
+    //         LSRK update of u, v, w (old values from global memory, fetched
+    //         before the wait); rhs_p -> B operand of the Vq product
+    float ro[4][3], qo[4][3];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int e = 8 * g8 + ep_col(lane, j);
+      const bool ok = rowok && e < ne;
+      const size_t id = sbase + (size_t)(k0 + e) * 4 * Np + rowM;
+#pragma unroll
+      for (int fl = 1; fl < 4; ++fl) {
+        ro[j][fl - 1] = ok ? P.res[id + fl * Np] : 0.f;
+        qo[j][fl - 1] = ok ? __ldg(P.Qin + id + fl * Np) : 0.f;
+      }
+    }
+    wait_bar(mbM, mphase, 2);
+    float rp[4] = {0.f, 0.f, 0.f, 0.f};
     if (!fail) {
-      float gr[8], gs[8], gt[8], dv[8], lf[4][8];
-      tc::tmem_ld8x4(trow + 0, trow + 32, trow + 64, trow + 96, gr, gs, gt, dv);
-      tc::tmem_ld8x4(trow + 128, trow + 160, trow + 192, trow + 224, lf[0], lf[1], lf[2], lf[3]);
-      const float isp = 1.f / sp, isU = 1.f / sU, isF = 1.f / sF;
-      float mr = 0.f;
+      float gr[4], gs[4], gt[4], dv[4], lf[4][4];
+      tc::tmem_ld16x64b_x4x4(tsub + cGrad, tsub + cGrad + 32, tsub + cGrad + 64, tsub + cDiv, gr,
+                             gs, gt, dv);
+      tc::tmem_ld16x64b_x4x4(tsub + cLift, tsub + cLift + 32, tsub + cLift + 64,
+                             tsub + cLift + 96, lf[0], lf[1], lf[2], lf[3]);
+      const float isp = 1.f / sp_cur, isU = 1.f / sU_cur, isF = 1.f / sF_cur;
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int e = 8 * g8 + j;
+      for (int j = 0; j < 4; ++j) {
+        const int e = 8 * g8 + ep_col(lane, j);
         const float *Ge = sGeo + e * TC_GEO;
         const float dr = gr[j] * isp, ds = gs[j] * isp, dt = gt[j] * isp;
         float vp = -dv[j] * isU;
@@ -474,132 +559,183 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
         }
         const bool ok = rowok && e < ne;
         rp[j] = ok ? vp : 0.f;
-        mr = fmaxf(mr, fabsf(rp[j]));
         if (ok) {
-          const size_t id = (size_t)(k0 + e) * 4 * Np + n;
+          const size_t id = sbase + (size_t)(k0 + e) * 4 * Np + rowM;
           const float rv3[3] = {vu, vv, vw};
 #pragma unroll
           for (int fl = 1; fl < 4; ++fl) {
             const float r = P.fa * ro[j][fl - 1] + P.fdt * rv3[fl - 1];
             P.res[id + fl * Np] = r;
-            P.Qout[id + fl * Np] = sRaw[e * RS + fl * Np + n] + P.fb * r;
+            P.Qout[id + fl * Np] = qo[j][fl - 1] + P.fb * r;
           }
         }
       }
+    }
+    {
+      float mr = fmaxf(fmaxf(fabsf(rp[0]), fabsf(rp[1])), fmaxf(fabsf(rp[2]), fabsf(rp[3])));
       mr = warp_max(mr);
       if (lane == 0) atomicMax(&sRed[3], __float_as_int(mr));
     }
-    if (__syncthreads_or(fail)) {
+    tc::fence_before_sync();
+    __syncthreads();  // maxima of rhs_p; acc1 and this item's geometry no longer read
+    tc::fence_after_sync();
+    const float srp = pow2_scale(sRed[3]);
+    if (rowM < KV) {  // rows [Np, KV) store the zero K padding
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int o = tc::kmajor_offset_f16(8 * g8 + ep_col(lane, j), rowM, KV);
+        split_store1(sBW + o, sBW + TC_E * KV + o, rp[j] * srp);
+      }
+    }
+    if (tid == 0) sRed[4] = 0;
+    if (sync_for_mma()) {
       fail = true;
       break;
     }
-    // the state tile is dead: the next tile's copies overlap the rest
-    if (tid == 0 && next < ntiles) issue_tma(next, gb ^ 1, tphase);
-    const float srp = pow2_scale(sRed[3]);
-    if (lane < 16) {
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int e = 8 * g8 + j;
-        const int o = tc::kmajor_offset_f16(e, n, KV);
-        if (n < KV) split_store1(sBp + o, sBp + TC_E * KV + o, rp[j] * srp);
-      }
-    }
-    sync_for_mma();
-
-    // ---- P4: Vq product; meanwhile c2/J of this thread's cubature row
     if (tid == 0) {
-      chain(tbase + 0, sOps + L.oVq, sOps + L.oVq + MQ * KV, (KV / 8) * 128, sBp, sBp + TC_E * KV,
-            (KV / 8) * 128, KV / 16, tc::idesc_f16(MQ, TC_E, FMT), false);
-      mma_commit();
+      chain(tbase + cVq, sOps + L.oVq, sOps + L.oVq + MRQ * KV, (KV / 8) * 128, sBW,
+            sBW + TC_E * KV, (KV / 8) * 128, KV / 16, tc::idesc_f16(MQ, TC_E, FMT), false);
+      tc::mma_commit(mbW);
+      sPend[4] = 1, sPend[5] = (int)wphase;
     }
-    const int q = MQ == 128 ? 32 * q4 + lane : (lane < 16 ? 16 * q4 + lane : MQ);
-    float c2v[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const int e = 8 * g8 + j;
-      c2v[j] = q < Nq && e < ne ? __ldg(P.c2q + (size_t)(k0 + e) * Nq + q) : 0.f;
-    }
-    mma_wait();
 
-    // ---- P5: epilogue 2 (thread = cubature row q): c2/J * p_q -> B operand
-    {
-      float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-      if (!fail) tc::tmem_ld8(tbase + ((uint32_t)(32 * q4) << 16) + 8 * g8, v);
-      const float isr = 1.f / srp;
-      float mc = 0.f;
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        v[j] = v[j] * isr * c2v[j];
-        mc = fmaxf(mc, fabsf(v[j]));
-      }
-      mc = warp_max(mc);
-      if (lane == 0) atomicMax(&sRed[4], __float_as_int(mc));
-      if (__syncthreads_or(fail)) {
+    // ---- b. next item: its inputs landed during this item's first MMAs;
+    //         traces, flux and B operands of its first product group
+    if (next < nvt) {
+      wait_bar(mbT, tphase, 0);
+      if (!fail) load_traces(next);
+      if (produce(next, gb ^ 1)) {
         fail = true;
         break;
       }
-      const float sc = pow2_scale(sRed[4]);
-      if (q < KQ) {
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          const int e = 8 * g8 + j;
-          const int o = tc::kmajor_offset_f16(e, q, KQ);
-          split_store1(sBU + o, sBU + TC_E * KQ + o, v[j] * sc);
-        }
-      }
-      sync_for_mma();
+    }
 
-      // ---- P6: Pq product
-      if (tid == 0) {
-        chain(tbase + 32, sOps + L.oPq, sOps + L.oPq + 64 * KQ, (KQ / 8) * 128, sBU,
-              sBU + TC_E * KQ, (KQ / 8) * 128, KQ / 16, tc::idesc_f16(64, TC_E, FMT), false);
-        mma_commit();
-      }
-      float r7[8], q7[8];  // old residual and state of p, fetched during the MMAs
+    // ---- c. epilogue 2 (thread = cubature row q): c2/J * p_q -> B operand of Pq
+    const bool q128 = MQ == 128;
+    const int qrow = q128 ? 32 * q4 + lane : rowM;
+    const int nq = q128 ? 8 : 4;  // elements per thread
+    float c2v[8];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int e = 8 * g8 + j;
-        const size_t id = (size_t)(k0 + e) * 4 * Np + n;
-        r7[j] = rowok && e < ne ? P.res[id] : 0.f;
-        q7[j] = rowok && e < ne ? __ldg(P.Qin + id) : 0.f;
-      }
-      mma_wait();
-
-      // ---- P7: epilogue 3: rhs_p = Pq (c2 p_q); LSRK update of p
-      float w[8];
-      if (!fail) tc::tmem_ld8(tbase + ((uint32_t)(32 * q4) << 16) + 32 + 8 * g8, w);
-      const float isc = 1.f / sc;
-      if (rowok && !fail) {
-        const float *ro = r7, *qo = q7;
+    for (int j = 0; j < 8; ++j) {
+      const int e = 8 * g8 + (q128 ? j : ep_col(lane, j & 3));
+      c2v[j] = j < nq && qrow < Nq && e < ne ? __ldg(P.c2q + (size_t)(k0 + e) * Nq + qrow) : 0.f;
+    }
+    wait_bar(mbW, wphase, 4);
+    float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (!fail) {
+      if (q128) {
+        tc::tmem_ld8(tbase + ((uint32_t)(32 * q4) << 16) + cVq + 8 * g8, v);
+      } else {
+        float v4[4];
+        tc::tmem_ld16x64b_x4(tsub + cVq, v4);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          const int e = 8 * g8 + j;
-          if (e >= ne) continue;
-          const size_t id = (size_t)(k0 + e) * 4 * Np + n;
-          const float r = P.fa * ro[j] + P.fdt * (w[j] * isc);
-          P.res[id] = r;
-          P.Qout[id] = qo[j] + P.fb * r;
-        }
+        for (int j = 0; j < 4; ++j) v[j] = v4[j];
       }
     }
+    const float isr = 1.f / srp;
+    float mc = 0.f;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      v[j] = qrow < Nq ? v[j] * isr * c2v[j] : 0.f;  // rows past Nq: exact zeros
+      mc = fmaxf(mc, fabsf(v[j]));
+    }
+    mc = warp_max(mc);
+    if (lane == 0) atomicMax(&sRed[4], __float_as_int(mc));
     tc::fence_before_sync();
-    // TMEM, B operands and reduction slots free for the next tile
-    if (__syncthreads_or(fail)) {
+    __syncthreads();  // maxima; the Vq product has read its B operand in BW
+    tc::fence_after_sync();
+    const float sc = pow2_scale(sRed[4]);
+    if (qrow < KQ) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        if (j >= nq) break;
+        const int o = tc::kmajor_offset_f16(8 * g8 + (q128 ? j : ep_col(lane, j)), qrow, KQ);
+        split_store1(sBW + o, sBW + TC_E * KQ + o, v[j] * sc);
+      }
+    }
+    if (tid == 0) sRed[3] = 0;
+    if (sync_for_mma()) {
       fail = true;
       break;
     }
-    tc::fence_after_sync();
+    sp_cur = sp, sU_cur = sU, sF_cur = sF;  // scales of the next item's B1 operands
+    if (tid < 3) sRed[tid] = 0;
+    if (tid == 0) {
+      chain(tbase + cPq, sOps + L.oPq, sOps + L.oPq + MR * KQ, (KQ / 8) * 128, sBW,
+            sBW + TC_E * KQ, (KQ / 8) * 128, KQ / 16, tc::idesc_f16(64, TC_E, FMT), false);
+      tc::mma_commit(mbW);
+      sPend[4] = 1, sPend[5] = (int)wphase;
+      if (next < nvt) {
+        issue_mma1();                           // acc1 drained in a, B1 written in b
+        if (next2 < nvt) issue_tma(next2, gb);  // raw tile free after b, geometry gb after a
+      }
+    }
+
+    // ---- d. epilogue 3: rhs_p = Pq (c2 p_q) + sources; LSRK update of p
+    float r7[4], q7[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int e = 8 * g8 + ep_col(lane, j);
+      const bool ok = rowok && e < ne;
+      const size_t id = sbase + (size_t)(k0 + e) * 4 * Np + rowM;
+      r7[j] = ok ? P.res[id] : 0.f;
+      q7[j] = ok ? __ldg(P.Qin + id) : 0.f;
+    }
+    wait_bar(mbW, wphase, 4);
+    if (!fail) {
+      float w[4];
+      tc::tmem_ld16x64b_x4(tsub + cPq, w);
+      const float isc = 1.f / sc;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) w[j] *= isc;
+      if (P.src_off) {
+        // the entries of a shot are sorted by element: find the first one of
+        // this tile by bisection, then walk the tile's entries
+        const int j0 = __ldg(P.src_off + shot), j1 = __ldg(P.src_off + shot + 1);
+        int lo = j0, hi = j1;
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          if (__ldg(P.src_elem + mid) < k0) lo = mid + 1;
+          else hi = mid;
+        }
+        if (lo < j1 && __ldg(P.src_elem + lo) < k0 + ne) {
+          const float amp = tc_ricker((float)(*P.time) + P.cstage * P.fdt, P.f0, P.tR, P.samp);
+          for (int s = lo; s < j1; ++s) {
+            const int rel = __ldg(P.src_elem + s) - k0;
+            if (rel >= ne) break;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+              if (rowok && rel == 8 * g8 + ep_col(lane, j))
+                w[j] += amp * __ldg(P.src_vec + (size_t)s * Np + rowM);
+          }
+        }
+      }
+      if (rowok) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int e = 8 * g8 + ep_col(lane, j);
+          if (e >= ne) continue;
+          const size_t id = sbase + (size_t)(k0 + e) * 4 * Np + rowM;
+          const float r = P.fa * r7[j] + P.fdt * w[j];
+          P.res[id] = r;
+          P.Qout[id] = q7[j] + P.fb * r;
+        }
+      }
+    }
   }
-  if (fail && tid == 0) {
+  if (__syncthreads_or(fail) && tid == 0) {
     // drain this CTA's own copies and MMAs still in flight (bounded), so
-    // nothing lands in shared memory or TMEM after they are released
-    if (tma_pend) tc::mbar_wait(mbarT, tma_par, TC_WAIT);
-    if (mma_pend) tc::mbar_wait(mbarM, mma_par, TC_WAIT);
+    // nothing lands in shared memory or TMEM after they are released; a Vq
+    // or Pq product is awaited before the next one is issued, so at most
+    // the last of them can still be in flight
+    if (sPend[0]) tc::mbar_wait(mbT, (uint32_t)sPend[1], TC_WAIT);
+    if (sPend[2]) tc::mbar_wait(mbM, (uint32_t)sPend[3], TC_WAIT);
+    if (sPend[4]) tc::mbar_wait(mbW, (uint32_t)sPend[5], TC_WAIT);
     atomicAdd(P.err, 1);
   }
   tc::fence_before_sync();
   __syncthreads();
-  if (warp == 0) tc::tmem_dealloc(tbase, 256);
+  if (warp == 0) tc::tmem_dealloc(tbase, TC_COLS);
 }
 
 // --------------------------------------------------------------- host side
@@ -611,55 +747,71 @@ static bbw_status tc_prepare_n(TcPlan &pl) {
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (pl.L.total > maxsm)
     return set_error(BBW_ERR_UNSUPPORTED, "tensor-core stage: shared-memory footprint too large");
+  // the MMAs read up to 64 - MR (MQ - MRQ) rows past an operator plane: the
+  // buffers after the operators must cover the last plane's over-read
+  const TcLayout &L = pl.L;
+  const int over = std::max((64 - L.MR) * std::max(L.KV, std::max(L.KF, L.KQ)),
+                            (L.MQ - L.MRQ) * L.KV) * 2;
+  if (L.total - L.Bp < over)
+    return set_error(BBW_ERR_UNSUPPORTED, "tensor-core stage: operator layout");
   // the limit is per kernel and device while the footprint depends on the
   // mesh (face-permutation table): raise it to the device maximum once
   const bbw_status s = ensure_smem_limit(k_tc_stage<N, BF>, maxsm, "tensor-core stage attribute");
   if (s != BBW_OK) return s;
   pl.nsm = nsm > 0 ? nsm : 148;
-  pl.grid = std::min(cdv(pl.K, TC_E), pl.nsm);
   return BBW_OK;
 }
 
 template <int N, bool BF>
 static bbw_status tc_launch_n(const TcPlan &pl, const float *Qin, float *Qout, float *res, float fa,
-                              float fb, float fdt, cudaStream_t st) {
+                              float fb, float fdt, float cstage, cudaStream_t st) {
   TcParams P;
-  P.K = pl.K, P.Nq = pl.Nq, P.bc = pl.bc;
-  P.fa = fa, P.fb = fb, P.fdt = fdt;
+  P.K = pl.K, P.Nq = pl.Nq, P.bc = pl.bc, P.S = std::max(pl.S, 1);
+  P.fa = fa, P.fb = fb, P.fdt = fdt, P.cstage = cstage;
   P.Qin = Qin, P.Qout = Qout, P.res = res;
   P.geo = pl.geo, P.nbr = pl.nbr, P.c2q = pl.c2q;
   P.ops = pl.ops;
   P.tables = pl.tables, P.table_ints = pl.table_ints, P.pat_off = pl.pat_off;
   P.err = pl.err;
+  P.src_off = pl.src_off, P.src_elem = pl.src_elem, P.src_vec = pl.src_vec;
+  P.f0 = pl.f0, P.tR = pl.tR, P.samp = pl.samp, P.time = pl.time;
   P.L = pl.L;
-  const int grid = pl.max_ctas > 0 ? std::min(pl.grid, pl.max_ctas) : pl.grid;
+  const int items = cdv(pl.K, TC_E) * P.S;
+  int grid = std::min(items, pl.nsm);
+  if (pl.max_ctas > 0) grid = std::min(grid, pl.max_ctas);
   k_tc_stage<N, BF><<<grid, TC_T, pl.L.total, st>>>(P);
   return check_launch("tensor-core stage");
 }
 
-bool tc_supported(int N, int Nq) {
-  return (N == 3 || N == 5) && Nq >= 1 && Nq <= 128;
-}
+bool tc_supported(int N, int Nq) { return N >= 2 && N <= 5 && Nq >= 1 && Nq <= 128; }
 
 bbw_status tc_prepare(TcPlan &pl) {
   switch (pl.N * 2 + (pl.bf ? 1 : 0)) {
+    case 4: return tc_prepare_n<2, false>(pl);
+    case 5: return tc_prepare_n<2, true>(pl);
     case 6: return tc_prepare_n<3, false>(pl);
     case 7: return tc_prepare_n<3, true>(pl);
+    case 8: return tc_prepare_n<4, false>(pl);
+    case 9: return tc_prepare_n<4, true>(pl);
     case 10: return tc_prepare_n<5, false>(pl);
     case 11: return tc_prepare_n<5, true>(pl);
   }
-  return set_error(BBW_ERR_UNSUPPORTED, "tensor-core stage: N must be 3 or 5");
+  return set_error(BBW_ERR_UNSUPPORTED, "tensor-core stage: N must be in [2, 5]");
 }
 
 bbw_status tc_launch(const TcPlan &pl, const float *Qin, float *Qout, float *res, float fa,
-                     float fb, float fdt, cudaStream_t st) {
+                     float fb, float fdt, float cstage, cudaStream_t st) {
   switch (pl.N * 2 + (pl.bf ? 1 : 0)) {
-    case 6: return tc_launch_n<3, false>(pl, Qin, Qout, res, fa, fb, fdt, st);
-    case 7: return tc_launch_n<3, true>(pl, Qin, Qout, res, fa, fb, fdt, st);
-    case 10: return tc_launch_n<5, false>(pl, Qin, Qout, res, fa, fb, fdt, st);
-    case 11: return tc_launch_n<5, true>(pl, Qin, Qout, res, fa, fb, fdt, st);
+    case 4: return tc_launch_n<2, false>(pl, Qin, Qout, res, fa, fb, fdt, cstage, st);
+    case 5: return tc_launch_n<2, true>(pl, Qin, Qout, res, fa, fb, fdt, cstage, st);
+    case 6: return tc_launch_n<3, false>(pl, Qin, Qout, res, fa, fb, fdt, cstage, st);
+    case 7: return tc_launch_n<3, true>(pl, Qin, Qout, res, fa, fb, fdt, cstage, st);
+    case 8: return tc_launch_n<4, false>(pl, Qin, Qout, res, fa, fb, fdt, cstage, st);
+    case 9: return tc_launch_n<4, true>(pl, Qin, Qout, res, fa, fb, fdt, cstage, st);
+    case 10: return tc_launch_n<5, false>(pl, Qin, Qout, res, fa, fb, fdt, cstage, st);
+    case 11: return tc_launch_n<5, true>(pl, Qin, Qout, res, fa, fb, fdt, cstage, st);
   }
-  return set_error(BBW_ERR_UNSUPPORTED, "tensor-core stage: N must be 3 or 5");
+  return set_error(BBW_ERR_UNSUPPORTED, "tensor-core stage: N must be in [2, 5]");
 }
 
 // FP16 (or BF16, bf) hi/lo split of an FP32 operator into the canonical

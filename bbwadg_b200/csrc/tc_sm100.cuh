@@ -172,6 +172,45 @@ __device__ __forceinline__ void tmem_ld8x4(uint32_t a0, uint32_t a1, uint32_t a2
   }
 }
 
+// 16 lanes x 64 bits, 4 repetitions along the columns (8 consecutive
+// columns): the warp's 16 TMEM lanes spread over all 32 threads, 4 registers
+// per thread (the lane / column of each register: ep_row / ep_elem in
+// kernels_tc.cu); the wait is part of the statement
+__device__ __forceinline__ void tmem_ld16x64b_x4(uint32_t taddr, float (&v)[4]) {
+  uint32_t r[4];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.16x64b.x4.b32 {%0,%1,%2,%3}, [%4];\n\t"
+      "tcgen05.wait::ld.sync.aligned;\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 4; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// four such loads at column addresses a0..a3, then one wait
+__device__ __forceinline__ void tmem_ld16x64b_x4x4(uint32_t a0, uint32_t a1, uint32_t a2,
+                                                   uint32_t a3, float (&v0)[4], float (&v1)[4],
+                                                   float (&v2)[4], float (&v3)[4]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.16x64b.x4.b32 {%0,%1,%2,%3}, [%16];\n\t"
+      "tcgen05.ld.sync.aligned.16x64b.x4.b32 {%4,%5,%6,%7}, [%17];\n\t"
+      "tcgen05.ld.sync.aligned.16x64b.x4.b32 {%8,%9,%10,%11}, [%18];\n\t"
+      "tcgen05.ld.sync.aligned.16x64b.x4.b32 {%12,%13,%14,%15}, [%19];\n\t"
+      "tcgen05.wait::ld.sync.aligned;\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3));
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    v0[i] = __uint_as_float(r[i]);
+    v1[i] = __uint_as_float(r[4 + i]);
+    v2[i] = __uint_as_float(r[8 + i]);
+    v3[i] = __uint_as_float(r[12 + i]);
+  }
+}
+
 // ---- bulk (TMA, 1-D) copies global -> shared, completion on an mbarrier
 __device__ __forceinline__ void mbar_expect_tx(void *mbar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(mbar)),

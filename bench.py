@@ -245,12 +245,14 @@ def shots_workload(args, torch, dist, world):
     out = {"workload": "batched shots, N=4, %d^3x6 tets (K=%d), %d shots, Ricker f0=4, "
                        "c2 in [1,2] with 10 inclusions" % (nh, prob.K, S),
            "N": N, "K": prob.K, "shots": S}
-    for label, nshot in (("batched", S), ("one_shot", 1)):
-        s = WaveSolver(prob)
+    finals = {}
+    for label, nshot, prec in (("batched", S, "fp32"), ("one_shot", 1, "fp32"),
+                               ("batched_f16x3", S, "f16x3")):
+        s = WaveSolver(prob, precision=prec)
         s.set_shots(nshot)
         s.set_sources(*shot_sources(prob, nshot, 99), f0=4.0, amplitude=1e4, stage_times=True)
         s.set_time(0.0)
-        tuned = s.autotune(prob.dt, 5)
+        tuned = s.autotune(prob.dt, 5) if prec == "fp32" else None
         _, _, sp = s.device_state()
         stream = torch.cuda.ExternalStream(sp)
         s.steps(prob.dt, args.warmup)
@@ -269,11 +271,17 @@ def shots_workload(args, torch, dist, world):
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t.item())
         dofs = prob.K * prob.Np * 4 * 5 * args.shots_steps * nshot
+        q = s.get_data()
         out[label] = {"value": world * dofs / (ms / 1e3), "unit": "DOF-stage/s",
                       "ms_per_step": ms / args.shots_steps, "steps": args.shots_steps,
-                      "autotuned": tuned,
-                      "finite": bool(np.isfinite(s.get_data()).all())}
+                      "precision": prec, "autotuned": tuned,
+                      "finite": bool(np.isfinite(q).all())}
+        finals[label] = q
         s.close()
+    # the split-FP16 run against the FP32 run of the same shots (same inputs,
+    # warm-up + timed steps): relative L2 over all shots
+    a, b = finals["batched_f16x3"].astype(np.float64), finals["batched"].astype(np.float64)
+    out["batched_f16x3"]["rel_l2_vs_fp32"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
     return out
 
 

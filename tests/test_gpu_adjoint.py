@@ -177,3 +177,42 @@ def test_gradient_on_one_and_two_elements(cuda, n_elems, variant):
     tr64, grad64, _ = oracle_gradient(p, rec, dense, 0, nsteps, p.Q0)
     assert rel_l2(tr, tr64) < 1e-5
     assert rel_l2(grad, grad64) < TOL
+
+
+def test_gradient_at_size_matches_fp64_adjoint_and_finite_differences(cuda):
+    """A mid-size case: N = 4 with the reference's 57-point rule, 4^3 x 6
+    tets (K = 384), 2 shots, 16 seeded receivers, 100 LSRK45 steps,
+    checkpoints every 25.  The GPU gradient against the FP64 discrete
+    adjoint, and its directional derivatives along 5 seeded directions
+    against FP64 central finite differences of the misfit."""
+    from conftest import golden
+    g = golden("ops_N4.npz")
+    nfq = int(np.asarray(g["Nfq"]).ravel()[0])
+    rules = ((g["rq"], g["sq"], g["tq"], g["wq"]), (g["rfq"][:nfq], g["sfq"][:nfq], g["wfqFace"]))
+    p = make_problem(4, 4, variant="nodal", c2="sine", c2_jitter=0.3, seed=21, cubature=rules[0],
+                     tri_cubature=rules[1])
+    assert p.K == 384
+    rng = np.random.default_rng(64)
+    rec = receiver_weights(p, rng.uniform(-0.8, 0.8, (16, 3)))
+    dense = [gaussian_source(p, x0, a=3.0) for x0 in rng.uniform(-0.5, 0.5, (2, 3))]
+    nsteps, every = 100, 25
+    Q0 = np.zeros_like(p.Q0)
+    tr, grad, _ = gpu_gradient(p, rec, dense, 0, nsteps, every, Q0)
+    tr64, grad64, ad = oracle_gradient(p, rec, dense, 0, nsteps, Q0)
+    assert rel_l2(tr, tr64) < 1e-5
+    assert rel_l2(grad, grad64) < TOL
+    dt = float(np.float32(p.dt))
+    srcs = [dict(fsrc=f.astype(np.float64), f0=10.0, tR=0.1, amp=1e2, stage_times=True)
+            for f in dense]
+    c2 = ad.c2q.copy()
+
+    def loss(c):
+        ad.c2q = c
+        return sum(0.5 * float((ad.forward(Q0.astype(np.float64), dt, nsteps, rec, s)[1] ** 2).sum())
+                   for s in srcs)
+
+    for _ in range(5):
+        d = rng.standard_normal(c2.shape)
+        eps = 1e-4
+        fd = (loss(c2 + eps * d) - loss(c2 - eps * d)) / (2 * eps)
+        assert abs(float((grad * d).sum()) - fd) <= TOL * abs(fd)

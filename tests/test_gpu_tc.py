@@ -97,13 +97,37 @@ def test_tc_many_tiles_per_cta_and_tiny_tiles(cuda):
 
 
 def test_tc_rejects_unsupported(cuda):
+    """Np > 64 (N >= 6: operators beyond one M = 64 MMA and one SM's shared
+    memory) and the BB variant (sparse operators: the FP32 stage) are
+    refused."""
     from bbwadg_b200._lib import BBWError
-    p = make_problem(4, 2, variant="nodal")
+    p = make_problem(6, 1, variant="nodal")
     with pytest.raises(BBWError):
         WaveSolver(p, precision="f16x3")
     p = make_problem(3, 2, variant="bb")
     with pytest.raises(BBWError):
         WaveSolver(p, precision="f16x3")
+
+
+@pytest.mark.parametrize("prec", ["f16x3", "bf16x3"])
+@pytest.mark.parametrize("N,rule", [(2, "stroud"), (4, "reference"), (4, "stroud")])
+@pytest.mark.parametrize("bc", ["pressure_release", "rigid"])
+def test_tc_other_orders_match_oracle(cuda, prec, N, rule, bc):
+    """N = 2 (Np = 10) and N = 4 (Np = 35: field rows not 16-byte aligned in
+    the state tile) with the reference's rule or the Stroud rule, both walls,
+    a ragged last tile (3^3 x 6 = 162 elements)."""
+    from oracle import Oracle
+    cub, tri = ref_rule(N) if rule == "reference" else (None, None)
+    p = make_problem(N, 3, variant="nodal", c2="sine", c2_jitter=0.5, seed=7, cubature=cub,
+                     tri_cubature=tri)
+    q_ref, _ = Oracle(N, p.K, p.ops_dict(), p.geo_dict(), variant="nodal",
+                      bc=1 if bc == "rigid" else 0).run(p.Q0.copy(), p.dt, 25)
+    s = WaveSolver(p, bc=bc, precision=prec)
+    s.set_data(p.Q0)
+    s.steps(p.dt, 5)
+    s.check()
+    assert rel_l2(s.get_data(), q_ref) < TOL
+    s.close()
 
 
 # split-BF16: 16 significant bits per hi/lo pair, so each contraction is good
