@@ -165,13 +165,14 @@ __device__ __forceinline__ float pow2_scale(int bits_of_max) {
   // s = 2^-E with max = m 2^E, m in [0.5, 1): max * s < 1.  E is clamped to
   // [-100, 100] so that s and 1/s stay finite normal numbers (a tile whose
   // values are all below 2^-100 keeps them below 1 after scaling; they are
-  // far below the FP32 resolution of any tile that carries the solution)
+  // far below the FP32 resolution of any tile that carries the solution).
+  // From the exponent field: E = field - 126 for a normal max; a subnormal
+  // max has E <= -126, clamped to -100.
   const float mx = __int_as_float(bits_of_max);
-  if (!(mx > 0.f) || !isfinite(mx)) return 1.f;
-  int E;
-  frexpf(mx, &E);
-  E = max(-100, min(100, E));
-  return ldexpf(1.f, -E);
+  const int field = (bits_of_max >> 23) & 255;
+  if (!(mx > 0.f) || field == 255) return 1.f;
+  const int E = max(-100, min(100, field - 126));
+  return __int_as_float((127 - E) << 23);
 }
 
 // float -> the operand type and back (round to nearest)
@@ -251,11 +252,16 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
   int *sPend = sRed + 5;  // [6] thread 0's copies / MMAs in flight and their phases
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int q4 = warp & 3, g8 = warp >> 2;  // TMEM sub-partition, element group of 8
+  // single-thread issue work is spread over lane 0 of five warps, so that no
+  // warp carries all of it between two barriers: gradient / divergence /
+  // lift MMAs (each chain in issue order from one thread), Vq and Pq MMAs,
+  // bulk copies and L2 prefetches
+  constexpr int I_GRAD = 0, I_DIV = 32, I_LIFT = 64, I_WADG = 96, I_COPY = 128;
 
   // ---------------------------------------------------------------- setup
   if (tid == 0) {
     tc::mbar_init(mbT, 1);
-    tc::mbar_init(mbM, 1);
+    tc::mbar_init(mbM, 3);  // one commit from each of the three issuing threads
     tc::mbar_init(mbW, 1);
     tc::fence_mbar_init();
   }
@@ -288,7 +294,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
   bool fail = false;
   uint32_t tphase = 0, mphase = 0, wphase = 0;
 
-  // thread 0: bulk copies of a work item's inputs (state rows of its shot,
+  // I_COPY: bulk copies of a work item's inputs (state rows of its shot,
   // geometry, neighbour codes) into the raw tile and geometry buffer gb
   auto issue_tma = [&](int vt, int gb) {
     const int shot = vt / ntiles, k0 = (vt - shot * ntiles) * TC_E, ne = min(TC_E, P.K - k0);
@@ -301,10 +307,20 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
     tc::bulk_g2s(sNbr, P.nbr + (size_t)k0 * 4, ne * 16, mbT);
     sPend[0] = 1, sPend[1] = (int)tphase;  // in flight, awaited with this parity
   };
-  // bounded wait; `pend` >= 0: the sPend slot thread 0 clears on success
-  auto wait_bar = [&](uint64_t *bar, uint32_t &ph, int pend) {
+  // I_COPY: L2 prefetch of the blocks the epilogues of a work item read
+  // from global memory (old residual and state, c^2 at the cubature points)
+  auto prefetch_item = [&](int vt) {
+    const int shot = vt / ntiles, k0 = (vt - shot * ntiles) * TC_E, ne = min(TC_E, P.K - k0);
+    const size_t off = shot * sstride + (size_t)k0 * 4 * Np;
+    tc::prefetch_l2(P.res + off, ne * 4 * Np * 4);
+    tc::prefetch_l2(P.Qin + off, ne * 4 * Np * 4);
+    const uint32_t cb = (uint32_t)(ne * Nq * 4) & ~15u;
+    if (cb) tc::prefetch_l2(P.c2q + (size_t)k0 * Nq, cb);
+  };
+  // bounded wait; the thread `owner` clears sPend[pend] on success
+  auto wait_bar = [&](uint64_t *bar, uint32_t &ph, int pend, int owner) {
     const bool ok = tc::mbar_wait(bar, ph, TC_WAIT);
-    if (ok && tid == 0 && pend >= 0) sPend[pend] = 0;
+    if (ok && tid == owner) sPend[pend] = 0;
     fail = __any_sync(0xffffffffu, fail || !ok);
     ph ^= 1u;
     tc::fence_after_sync();
@@ -333,25 +349,30 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       ah += 16, al += 16, bh += 16, bl += 16;
     }
   };
-  // thread 0: gradient, divergence and lift products of the B1 operands,
-  // committed to mbM
+  // I_GRAD / I_DIV / I_LIFT: their part of the gradient, divergence and
+  // lift products of the B1 operands, each committed to mbM
   auto issue_mma1 = [&]() {
     const uint32_t id64 = tc::idesc_f16(64, TC_E, FMT);
     const int sboV = (KV / 8) * 128, sboF = (KF / 8) * 128;
     const int pD = MR * KV, pL = MR * KF;  // plane sizes (halves)
-    for (int d = 0; d < 3; ++d)
-      chain(tbase + cGrad + 32 * d, sOps + L.oD + 2 * d * pD, sOps + L.oD + (2 * d + 1) * pD,
-            sboV, sBp, sBp + TC_E * KV, sboV, KV / 16, id64, false);
-    for (int d = 0; d < 3; ++d)
-      chain(tbase + cDiv, sOps + L.oD + 2 * d * pD, sOps + L.oD + (2 * d + 1) * pD, sboV,
-            sBU + 2 * d * TC_E * KV, sBU + (2 * d + 1) * TC_E * KV, sboV, KV / 16, id64, d > 0);
-    for (int f = 0; f < 4; ++f)
-      chain(tbase + cLift + 32 * f, sOps + L.oL + 2 * f * pL, sOps + L.oL + (2 * f + 1) * pL,
-            sboF, sBF + 2 * f * TC_E * KF, sBF + (2 * f + 1) * TC_E * KF, sboF, KF / 16, id64,
-            false);
+    if (tid == I_GRAD) {
+      for (int d = 0; d < 3; ++d)
+        chain(tbase + cGrad + 32 * d, sOps + L.oD + 2 * d * pD, sOps + L.oD + (2 * d + 1) * pD,
+              sboV, sBp, sBp + TC_E * KV, sboV, KV / 16, id64, false);
+      sPend[2] = 1, sPend[3] = (int)mphase;
+    } else if (tid == I_DIV) {
+      for (int d = 0; d < 3; ++d)
+        chain(tbase + cDiv, sOps + L.oD + 2 * d * pD, sOps + L.oD + (2 * d + 1) * pD, sboV,
+              sBU + 2 * d * TC_E * KV, sBU + (2 * d + 1) * TC_E * KV, sboV, KV / 16, id64, d > 0);
+    } else {
+      for (int f = 0; f < 4; ++f)
+        chain(tbase + cLift + 32 * f, sOps + L.oL + 2 * f * pL, sOps + L.oL + (2 * f + 1) * pL,
+              sboF, sBF + 2 * f * TC_E * KF, sBF + (2 * f + 1) * TC_E * KF, sboF, KF / 16, id64,
+              false);
+    }
     tc::mma_commit(mbM);
-    sPend[2] = 1, sPend[3] = (int)mphase;
   };
+  auto mma1_issuer = [&]() { return tid == I_GRAD || tid == I_DIV || tid == I_LIFT; };
 
   // neighbour face traces of the work item in the raw tile, outside the
   // tile, into registers.  Lane = face node, warp = (element, face) pairs:
@@ -493,13 +514,16 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
   // ---------------------------------------------------------------- prologue
   int vt = blockIdx.x, it = 0;
   if (vt < nvt) {
-    if (tid == 0) issue_tma(vt, 0);
-    wait_bar(mbT, tphase, 0);
+    if (tid == I_COPY) issue_tma(vt, 0);
+    wait_bar(mbT, tphase, 0, I_COPY);
     if (!fail) load_traces(vt);
     fail = produce(vt, 0) || fail;
-    if (tid == 0 && !fail) {
-      issue_mma1();
-      if (vt + (int)gridDim.x < nvt) issue_tma(vt + gridDim.x, 1);
+    if (!fail) {
+      if (mma1_issuer()) issue_mma1();
+      if (tid == I_COPY) {
+        prefetch_item(vt);
+        if (vt + (int)gridDim.x < nvt) issue_tma(vt + gridDim.x, 1);
+      }
     }
     if (tid < 3) sRed[tid] = 0;
   }
@@ -531,7 +555,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
         qo[j][fl - 1] = ok ? __ldg(P.Qin + id + fl * Np) : 0.f;
       }
     }
-    wait_bar(mbM, mphase, 2);
+    wait_bar(mbM, mphase, 2, I_GRAD);
     float rp[4] = {0.f, 0.f, 0.f, 0.f};
     if (!fail) {
       float gr[4], gs[4], gt[4], dv[4], lf[4][4];
@@ -592,7 +616,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       fail = true;
       break;
     }
-    if (tid == 0) {
+    if (tid == I_WADG) {
       chain(tbase + cVq, sOps + L.oVq, sOps + L.oVq + MRQ * KV, (KV / 8) * 128, sBW,
             sBW + TC_E * KV, (KV / 8) * 128, KV / 16, tc::idesc_f16(MQ, TC_E, FMT), false);
       tc::mma_commit(mbW);
@@ -602,7 +626,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
     // ---- b. next item: its inputs landed during this item's first MMAs;
     //         traces, flux and B operands of its first product group
     if (next < nvt) {
-      wait_bar(mbT, tphase, 0);
+      wait_bar(mbT, tphase, 0, I_COPY);
       if (!fail) load_traces(next);
       if (produce(next, gb ^ 1)) {
         fail = true;
@@ -620,7 +644,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       const int e = 8 * g8 + (q128 ? j : ep_col(lane, j & 3));
       c2v[j] = j < nq && qrow < Nq && e < ne ? __ldg(P.c2q + (size_t)(k0 + e) * Nq + qrow) : 0.f;
     }
-    wait_bar(mbW, wphase, 4);
+    wait_bar(mbW, wphase, 4, I_WADG);
     float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (!fail) {
       if (q128) {
@@ -660,13 +684,16 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
     }
     sp_cur = sp, sU_cur = sU, sF_cur = sF;  // scales of the next item's B1 operands
     if (tid < 3) sRed[tid] = 0;
-    if (tid == 0) {
+    if (tid == I_WADG) {
       chain(tbase + cPq, sOps + L.oPq, sOps + L.oPq + MR * KQ, (KQ / 8) * 128, sBW,
             sBW + TC_E * KQ, (KQ / 8) * 128, KQ / 16, tc::idesc_f16(64, TC_E, FMT), false);
       tc::mma_commit(mbW);
       sPend[4] = 1, sPend[5] = (int)wphase;
-      if (next < nvt) {
-        issue_mma1();                           // acc1 drained in a, B1 written in b
+    }
+    if (next < nvt) {
+      if (mma1_issuer()) issue_mma1();  // acc1 drained in a, B1 written in b
+      if (tid == I_COPY) {
+        prefetch_item(next);
         if (next2 < nvt) issue_tma(next2, gb);  // raw tile free after b, geometry gb after a
       }
     }
@@ -681,7 +708,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       r7[j] = ok ? P.res[id] : 0.f;
       q7[j] = ok ? __ldg(P.Qin + id) : 0.f;
     }
-    wait_bar(mbW, wphase, 4);
+    wait_bar(mbW, wphase, 4, I_WADG);
     if (!fail) {
       float w[4];
       tc::tmem_ld16x64b_x4(tsub + cPq, w);
@@ -723,6 +750,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       }
     }
   }
+  // (sPend is written by the issuing threads and read after this barrier)
   if (__syncthreads_or(fail) && tid == 0) {
     // drain this CTA's own copies and MMAs still in flight (bounded), so
     // nothing lands in shared memory or TMEM after they are released; a Vq

@@ -217,6 +217,11 @@ __device__ __forceinline__ void mbar_expect_tx(void *mbar, uint32_t bytes) {
                "r"(bytes)
                : "memory");
 }
+// L2 prefetch of a global range (hint, no completion); src 16-byte aligned,
+// bytes a multiple of 16
+__device__ __forceinline__ void prefetch_l2(const void *src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(src), "r"(bytes) : "memory");
+}
 // dst, src 16-byte aligned, bytes a multiple of 16
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, void *mbar) {
   asm volatile(
