@@ -404,8 +404,8 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
     const TcLayout &TL = tp.L;
     std::vector<float> geo((size_t)K * TC_GEO, 0.f);
     for (int k = 0; k < K; ++k) {
-      std::memcpy(&geo[(size_t)k * TC_GEO], m->vgeo + (size_t)k * 9, 9 * sizeof(float));
-      std::memcpy(&geo[(size_t)k * TC_GEO + 9], m->fgeo + (size_t)k * 16, 16 * sizeof(float));
+      std::memcpy(&geo[(size_t)k * TC_GEO], m->fgeo + (size_t)k * 16, 16 * sizeof(float));
+      std::memcpy(&geo[(size_t)k * TC_GEO + 16], m->vgeo + (size_t)k * 9, 9 * sizeof(float));
     }
     // operator planes with MR (MRQ) stored rows, see tc_layout
     std::vector<uint16_t> h(TL.ops_halfs);

@@ -54,7 +54,7 @@ void pack_fused_ops(int N, int Nq, int W, bool bb, const float *Dr, const float 
                     FusedOps &out);
 
 // ---- tensor-core (tcgen05) stage, kernels_tc.cu
-constexpr int TC_GEO = 28;  // floats per element geometry record: vgeo 9 | fgeo 16 | pad 3
+constexpr int TC_GEO = 28;  // floats per element geometry record: fgeo 16 | vgeo 9 | pad 3
 
 struct TcLayout {
   int KV = 0, KF = 0, KQ = 0, MQ = 0;   // padded K extents, rows of the Vq MMA (64 or 128)

@@ -143,7 +143,7 @@ struct TcParams {
   const float *__restrict__ Qin;
   float *__restrict__ Qout;
   float *__restrict__ res;
-  const float *__restrict__ geo;  // [K][TC_GEO]: vgeo 9 | fgeo 16 | pad
+  const float *__restrict__ geo;  // [K][TC_GEO]: fgeo 16 | vgeo 9 | pad 3 (16-byte groups)
   const int *__restrict__ nbr;    // [K][4]
   const float *__restrict__ c2q;  // [K][Nq]
   const void *__restrict__ ops;   // split operators: __half, or __nv_bfloat16 (BF)
@@ -181,17 +181,30 @@ __device__ __forceinline__ void to_e(float x, __nv_bfloat16 &h) { h = __float2bf
 __device__ __forceinline__ float from_e(__half h) { return __half2float(h); }
 __device__ __forceinline__ float from_e(__nv_bfloat16 h) { return __bfloat162float(h); }
 
+// pairs: float -> two packed values of the operand type and back
+__device__ __forceinline__ uint32_t to_e2(float a, float b, __half) {
+  const __half2 h = __floats2half2_rn(a, b);
+  return *reinterpret_cast<const uint32_t *>(&h);
+}
+__device__ __forceinline__ uint32_t to_e2(float a, float b, __nv_bfloat16) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const uint32_t *>(&h);
+}
+__device__ __forceinline__ float2 from_e2(uint32_t v, __half) {
+  return __half22float2(*reinterpret_cast<const __half2 *>(&v));
+}
+__device__ __forceinline__ float2 from_e2(uint32_t v, __nv_bfloat16) {
+  return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&v));
+}
+
 template <class E>
 __device__ __forceinline__ void split_store4(E *hi, E *lo, float4 v, float s) {
-  const float x[4] = {v.x * s, v.y * s, v.z * s, v.w * s};
-  E h[4], l[4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    to_e(x[i], h[i]);
-    to_e(x[i] - from_e(h[i]), l[i]);
-  }
-  *reinterpret_cast<uint2 *>(hi) = *reinterpret_cast<uint2 *>(h);
-  *reinterpret_cast<uint2 *>(lo) = *reinterpret_cast<uint2 *>(l);
+  const float x0 = v.x * s, x1 = v.y * s, x2 = v.z * s, x3 = v.w * s;
+  const uint32_t h01 = to_e2(x0, x1, E()), h23 = to_e2(x2, x3, E());
+  const float2 f01 = from_e2(h01, E()), f23 = from_e2(h23, E());
+  const uint32_t l01 = to_e2(x0 - f01.x, x1 - f01.y, E()), l23 = to_e2(x2 - f23.x, x3 - f23.y, E());
+  *reinterpret_cast<uint2 *>(hi) = make_uint2(h01, h23);
+  *reinterpret_cast<uint2 *>(lo) = make_uint2(l01, l23);
 }
 
 template <class E>
@@ -415,9 +428,10 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
     for (int j = 0; j < FPW; ++j) pf[j] = 0.f;
     if (!fail) {
       if (cc < NC && 4 * cc < Np && ce < ne) {
-        float G[9];
-#pragma unroll
-        for (int i = 0; i < 9; ++i) G[i] = sGeo[ce * TC_GEO + i];
+        const float4 g0 = *reinterpret_cast<const float4 *>(sGeo + ce * TC_GEO + 16);
+        const float4 g1 = *reinterpret_cast<const float4 *>(sGeo + ce * TC_GEO + 20);
+        const float G[9] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w,
+                            sGeo[ce * TC_GEO + 24]};
         const float *rr = sRaw + ce * RS + 4 * cc;
         float4 u4, v4, w4;
         if constexpr (C::V4) {
@@ -458,8 +472,8 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
         const int vM = sFmask[m];
         const float *own = sRaw + e * RS + vM;
         const float pM = own[0], uM = own[Np], vvM = own[2 * Np], wM = own[3 * Np];
-        const float *fg = sGeo + e * TC_GEO + 9 + 4 * f;
-        const float Fscale = fg[0], nx = fg[1], ny = fg[2], nz = fg[3];
+        const float4 fg = *reinterpret_cast<const float4 *>(sGeo + e * TC_GEO + 4 * f);
+        const float Fscale = fg.x, nx = fg.y, ny = fg.z, nz = fg.w;
         float pjump, Unjump;
         if (pat == 255) {
           if (P.bc == BBW_BC_PRESSURE_RELEASE) {
@@ -568,18 +582,22 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       for (int j = 0; j < 4; ++j) {
         const int e = 8 * g8 + ep_col(lane, j);
         const float *Ge = sGeo + e * TC_GEO;
+        const float4 g0 = *reinterpret_cast<const float4 *>(Ge + 16);
+        const float4 g1 = *reinterpret_cast<const float4 *>(Ge + 20);
+        const float g8v = Ge[24];
         const float dr = gr[j] * isp, ds = gs[j] * isp, dt = gt[j] * isp;
         float vp = -dv[j] * isU;
-        float vu = -(Ge[0] * dr + Ge[3] * ds + Ge[6] * dt);
-        float vv = -(Ge[1] * dr + Ge[4] * ds + Ge[7] * dt);
-        float vw = -(Ge[2] * dr + Ge[5] * ds + Ge[8] * dt);
+        float vu = -(g0.x * dr + g0.w * ds + g1.z * dt);
+        float vv = -(g0.y * dr + g1.x * ds + g1.w * dt);
+        float vw = -(g0.z * dr + g1.y * ds + g8v * dt);
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
           const float a = lf[f][j] * isF;
+          const float4 fn = *reinterpret_cast<const float4 *>(Ge + 4 * f);  // Fscale nx ny nz
           vp += a;
-          vu -= Ge[9 + 4 * f + 1] * a;
-          vv -= Ge[9 + 4 * f + 2] * a;
-          vw -= Ge[9 + 4 * f + 3] * a;
+          vu -= fn.y * a;
+          vv -= fn.z * a;
+          vw -= fn.w * a;
         }
         const bool ok = rowok && e < ne;
         rp[j] = ok ? vp : 0.f;

@@ -12,6 +12,13 @@ rule), [-1,1]^3 split into 32^3 hexes x 6 tets, c^2 = 1 + 0.5 sin sin sin +
 The state (3 x 176 MB) exceeds the 126 MB L2, so no flush is needed between
 steps.
 
+The headline form is the tensor-core stage (nodal-f16x3): FP32 state, the
+dense contractions on tcgen05 as three FP16 products per split pair with
+FP32 accumulation.  Its error against the FP64 restatement is the FP32
+stage's (the line's `precision` object gives both, measured in the same
+run); the FP32 CUDA-core stage and the BB stage run beside it
+(`side_by_side`).
+
 * value      device-timed throughput of the fused stage kernels, inputs
              resident in HBM (CUDA events on the solver's stream, max over
              ranks, weak scaling: each rank advances its own copy of the
@@ -404,6 +411,23 @@ def precision_workload(args, torch):
             "rows": rows}
 
 
+def headline_precision(variant, prec_rows):
+    """Arithmetic of the headline form, with its error against the FP64
+    restatement and the FP32 stage's, from the precision study of the same
+    run (N = 5, 8^3 x 6, standing mode, 10 steps)."""
+    tc = variant.endswith("f16x3")
+    out = {"state": "fp32", "update": "fp32",
+           "contractions": "split-FP16, 3 products per pair on tcgen05, FP32 accumulation"
+           if tc else "FP32 CUDA cores"}
+    if prec_rows:
+        for r in prec_rows["rows"]:
+            if r["N"] == 5 and "rel_l2_vs_fp64_10_steps" in r:
+                key = {"f16x3": "f16x3", "fp32": "fp32"}.get(r["precision"])
+                if key:
+                    out["rel_l2_vs_fp64_%s" % key] = r["rel_l2_vs_fp64_10_steps"]
+    return out
+
+
 def curved_bytes_per_element(Np, Nq, Nfq, Nfp, curved):
     """Algorithmic bytes of one curvilinear stage per element: state and
     residual read + write (4 fields, FP32), J and c^2 at the update's
@@ -559,10 +583,10 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--variant", default="nodal", choices=["nodal", "bb", "nodal-f16x3"])
+    ap.add_argument("--variant", default="nodal-f16x3", choices=["nodal", "bb", "nodal-f16x3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--hex", type=int, default=N_HEX, help="hexes per direction (profiling cases)")
-    ap.add_argument("--variants", default="nodal,bb,nodal-f16x3",
+    ap.add_argument("--variants", default="nodal-f16x3,nodal,bb",
                     help="variants to run, comma separated (nodal, bb, nodal-f16x3)")
     ap.add_argument("--extra", default="shots,adjoint,precision,curved,kernel_level",
                     help="extra workloads reported beside the headline: shots, adjoint, "
@@ -707,6 +731,7 @@ def main():
                           "steps"},
         "gpu_launches": head["launches"],
         "clocks": head["clocks"],
+        "precision": headline_precision(args.variant, prec),
         "side_by_side": {v: {"value": world * r["dofs"] / (r["ms"] / 1e3),
                              "ms_per_step": r["ms"] / args.steps,
                              "hbm_frac": K * algorithmic_bytes_per_element(Np, Nq) /

@@ -63,3 +63,4 @@ def test_bench_line_on_the_gpu(cuda):
         assert k in d["roofline"], k
     assert d["e2e"]["h2d_bytes_per_step"] > 0 and d["e2e"]["d2h_bytes_per_step"] > 0
     assert "sm_mhz" in d["clocks"] and "reasons" in d["clocks"]
+    assert d["precision"]["state"] == "fp32" and "contractions" in d["precision"]
