@@ -229,14 +229,10 @@ extern "C" bbw_status bbw_backward(bbw_ctx *c, bbw_tape *t, const float *dL_dtra
   float *lamQ, *lamR, *z, *rhs, *sigma, *res, *g, *seg, *stq, *vq;
   double *grad, *tdev;
   const int seglen = std::min(every, nsteps);
-  // reverse stages in two kernels when the element-local tiles fit the
-  // shared memory (all orders with the reference's rules), else four
-  const bool local = adj_local_fits(N, Nq);
-  rhs = nullptr;
   if ((s = buf.get(&lamQ, t->state, "bbw_backward")) != BBW_OK ||
       (s = buf.get(&lamR, t->state, "bbw_backward")) != BBW_OK ||
       (s = buf.get(&z, t->state, "bbw_backward")) != BBW_OK ||
-      (!local && (s = buf.get(&rhs, t->state, "bbw_backward")) != BBW_OK) ||
+      (s = buf.get(&rhs, t->state, "bbw_backward")) != BBW_OK ||
       (s = buf.get(&sigma, (size_t)S * K * NF, "bbw_backward")) != BBW_OK ||
       (s = buf.get(&res, t->state, "bbw_backward")) != BBW_OK ||
       (s = buf.get(&g, (size_t)S * R * nsteps, "bbw_backward")) != BBW_OK ||
@@ -343,15 +339,6 @@ extern "C" bbw_status bbw_backward(bbw_ctx *c, bbw_tape *t, const float *dL_dtra
       }
       for (int i = 4; i >= 0; --i) {
         const float ai = (float)kRK4A[i], bi = (float)kRK4B[i];
-        if (local) {  // two passes: element-local part, then the face gather
-          if ((s = adj_local(N, S, K, Nq, a.PqT, a.VqT, a.LTp, a.DTp, pl.c2q, c->vgeo, c->fgeo,
-                             lamQ, lamR, ai, bi, dt, vqs + (size_t)i * vqn, sigma, grad, st)) !=
-                  BBW_OK ||
-              (s = adj_gather(N, S, K, c->bc, dt, c->fgeo, a.fidx, a.mapP, sigma, nullptr, lamQ,
-                              st)) != BBW_OK)
-            return s;
-          continue;
-        }
         if ((s = adj_wadg(N, S, K, Nq, a.PqT, a.VqT, pl.c2q, lamQ, lamR, ai, bi, dt,
                           vqs + (size_t)i * vqn, z, grad, st)) != BBW_OK ||
             (s = adj_volume(N, S, K, c->vgeo, a.DTp, z, rhs, st)) != BBW_OK ||

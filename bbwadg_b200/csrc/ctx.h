@@ -50,14 +50,6 @@ bbw_status adj_volume(int N, int S, int K, const float *vgeo, const float *DTp, 
 bbw_status adj_gather(int N, int S, int K, int bc, float dt, const float *fgeo, const int *fidx,
                       const int *mapP, const float *sigma, const float *vol, float *lamQ,
                       cudaStream_t st);
-// element-local part of a reverse stage in one kernel (WADG transpose,
-// gradient, face sigma, lamQ += dt volume^T z); then adj_gather with vol =
-// NULL.  adj_local_fits: its tiles fit the shared memory
-bbw_status adj_local(int N, int S, int K, int Nq, const float *PqT, const float *VqT,
-                     const float *LTp, const float *DTp, const float *c2q, const float *vgeo,
-                     const float *fgeo, float *lamQ, float *lamR, float a, float b, float dt,
-                     const float *vq, float *sigma, double *grad, cudaStream_t st);
-bool adj_local_fits(int N, int Nq);
 bbw_status adj_receivers(int S, int K, int Np, int R, const int *rec_elem, const float *rec_w,
                          const float *g, int nsteps, int n, float *lamQ, cudaStream_t st);
 bbw_status set_device_double(double *p, double v, cudaStream_t st);

@@ -21,8 +21,6 @@
 // k2, and -2 sigma (p = 0 wall) or 2 n sigma (rigid wall) on the boundary.
 #include <cuda_runtime.h>
 
-#include <algorithm>
-
 #include "bbwadg.h"
 #include "device_common.cuh"
 
@@ -270,174 +268,7 @@ __global__ void __launch_bounds__(AE * AW) k_adj_volume(int K, int Kg, int stage
   }
 }
 
-// The element-local part of one reverse stage in one pass, for a tile of AE
-// elements and every shot in turn (shot order, as k_adj_wadg, so each
-// gradient entry is accumulated by one thread in a fixed order):
-//   mu = lamR + b lamQ, lamR <- a mu, z = W^T mu, gradient   (k_adj_wadg)
-//   sigma of z -> global                                     (k_adj_sigma)
-//   lamQ += dt * (volume^T z)                                (k_adj_volume)
-// z stays in shared memory between the three; the neighbour part (face
-// gather of sigma) follows in k_adj_gather without a volume term.  Same
-// arithmetic per output as the three kernels; lamQ takes the volume term
-// and the surface term in two additions instead of one.
-template <int N>
-__global__ void __launch_bounds__(AE * AW) k_adj_local(
-    int S, int K, int Nq, int stage, const float *__restrict__ PqT, const float *__restrict__ VqT,
-    const float *__restrict__ LTp, const float *__restrict__ DTp, const float *__restrict__ c2q,
-    const float *__restrict__ vgeo, const float *__restrict__ fgeo, float *__restrict__ lamQ,
-    float *__restrict__ lamR, float a, float b, float dt, const float *__restrict__ vq,
-    float *__restrict__ sigma, double *__restrict__ grad) {
-  constexpr int Np = NP(N), Nfp = NFP(N), NF = 4 * NFP(N);
-  constexpr int ldp = (NP(N) + 3) & ~3, ldf = (NFP(N) + 3) & ~3;
-  constexpr int npq = (Np + 3) >> 2, nfq = (Nfp + 3) >> 2;
-  extern __shared__ float smem[];
-  const int ldq = pad4(Nq);
-  const int oV = Np * ldq, oL = oV + Nq * ldp, oD = oL + 4 * Np * ldf;
-  const int nops = stage ? oD + 3 * Np * ldp : 0;
-  float *sZ = smem + nops;                       // [4Np][AS] mu, then z
-  float *sC = sZ + 4 * Np * AS;                  // [Nq][AS] c2/J of the tile
-  float *sB = sC + Nq * AS;                      // [max(Nq, 4Np)][AS] T, then W, then vol
-  float *sO = sB + max(Nq, 4 * Np) * AS;         // [NF][AS] sigma
-  float *sG = sO + NF * AS;                      // [AE][16] fgeo of the tile
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int k0 = blockIdx.x * AE, ne = min(AE, K - k0);
-  const float *sPt = PqT, *sVt = VqT, *sL = LTp, *sD = DTp;
-  if (stage) {
-    const float *src[4] = {PqT, VqT, LTp, DTp};
-    const int off[5] = {0, oV, oL, oD, nops};
-    for (int o = 0; o < 4; ++o)
-      for (int i = tid; i < (off[o + 1] - off[o]) / 4; i += AE * AW)
-        reinterpret_cast<float4 *>(smem + off[o])[i] =
-            __ldg(reinterpret_cast<const float4 *>(src[o]) + i);
-    sPt = smem, sVt = smem + oV, sL = smem + oL, sD = smem + oD;
-  }
-  for (int i = tid; i < ne * Nq; i += AE * AW) sC[(i % Nq) * AS + i / Nq] = c2q[(size_t)k0 * Nq + i];
-  for (int i = tid; i < AE * 16; i += AE * AW)
-    sG[i] = i < ne * 16 ? fgeo[(size_t)k0 * 16 + i] : 0.f;
-  const int e = lane < ne ? lane : 0;
-  float G[9];
-#pragma unroll
-  for (int c = 0; c < 9; ++c) G[c] = __ldg(vgeo + (size_t)(k0 + e) * 9 + c);
-  const int nqq = (Nq + 3) >> 2;
-  for (int sh = 0; sh < S; ++sh) {
-    const size_t so = (size_t)sh * K * 4 * Np + (size_t)k0 * 4 * Np;
-    __syncthreads();  // the previous shot is done with sZ, sB, sO
-    for (int i = tid; i < AE * 4 * Np; i += AE * AW) {
-      const int el = i / (4 * Np), fn = i - el * 4 * Np;
-      float mu = 0.f;
-      if (el < ne) {
-        mu = lamR[so + i] + b * lamQ[so + i];
-        lamR[so + i] = a * mu;
-      }
-      sZ[fn * AS + el] = mu;  // velocity rows are z already: Pq Vq = I (J = 1)
-    }
-    __syncthreads();
-    for (int qq = warp; qq < nqq; qq += AW) {  // t = Pq^T mu_p, rows 4qq..4qq+3
-      float t[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll 5
-      for (int n = 0; n < Np; ++n)
-        fma4(t, reinterpret_cast<const float4 *>(sPt + n * ldq)[qq], sZ[n * AS + lane]);
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int q = 4 * qq + r;
-        if (q < Nq && lane < ne) {
-          if (vq)
-            grad[(size_t)q * K + k0 + lane] +=
-                (double)dt * (double)t[r] * (double)vq[((size_t)sh * Nq + q) * K + k0 + lane];
-          sB[q * AS + lane] = sC[q * AS + lane] * t[r];
-        } else if (q < Nq) {
-          sB[q * AS + lane] = 0.f;
-        }
-      }
-    }
-    __syncthreads();
-    for (int nq = warp; nq < npq; nq += AW) {  // z_p = Vq^T (c2 t), rows 4nq..4nq+3
-      float acc[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll 4
-      for (int q = 0; q < Nq; ++q)
-        fma4(acc, reinterpret_cast<const float4 *>(sVt + q * ldp)[nq], sB[q * AS + lane]);
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {  // mu_p is dead: its rows take z_p
-        const int n = 4 * nq + r;
-        if (n < Np) sZ[n * AS + lane] = acc[r];
-      }
-    }
-    __syncthreads();
-    for (int i = warp; i < 4 * Np; i += AW) {  // w_f[n] = z_p - n_f . z_U per lane
-      const int f = i / Np, n = i - f * Np;
-      const float nx = sG[e * 16 + 4 * f + 1], ny = sG[e * 16 + 4 * f + 2],
-                  nz = sG[e * 16 + 4 * f + 3];
-      sB[i * AS + lane] = lane < ne ? sZ[n * AS + lane] - (nx * sZ[(Np + n) * AS + lane] +
-                                                           ny * sZ[(2 * Np + n) * AS + lane] +
-                                                           nz * sZ[(3 * Np + n) * AS + lane])
-                                    : 0.f;
-    }
-    __syncthreads();
-    for (int u = warp; u < 4 * nfq; u += AW) {  // sigma = .5 Fscale LIFT_f^T w_f
-      const int f = u / nfq, jq = u - f * nfq;
-      float acc[4] = {0.f, 0.f, 0.f, 0.f};
-      const float *Lf = sL + f * Np * ldf;
-      const float *w = sB + f * Np * AS;
-#pragma unroll 5
-      for (int n = 0; n < Np; ++n)
-        fma4(acc, reinterpret_cast<const float4 *>(Lf + n * ldf)[jq], w[n * AS + lane]);
-      const float Fs = sG[e * 16 + 4 * f];
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int j = 4 * jq + r;
-        if (j < Nfp) sO[(f * Nfp + j) * AS + lane] = .5f * Fs * acc[r];
-      }
-    }
-    __syncthreads();
-    {
-      const size_t sg = ((size_t)sh * K + k0) * NF;
-      for (int i = tid; i < ne * NF; i += AE * AW) sigma[sg + i] = sO[(i % NF) * AS + i / NF];
-    }
-    for (int n = warp; n < Np; n += AW) {  // z_U -> contravariant components, in place
-      const float un = sZ[(Np + n) * AS + lane], vn = sZ[(2 * Np + n) * AS + lane],
-                  wn = sZ[(3 * Np + n) * AS + lane];
-      sZ[(Np + n) * AS + lane] = un * G[0] + vn * G[1] + wn * G[2];
-      sZ[(2 * Np + n) * AS + lane] = un * G[3] + vn * G[4] + wn * G[5];
-      sZ[(3 * Np + n) * AS + lane] = un * G[6] + vn * G[7] + wn * G[8];
-    }
-    __syncthreads();
-    for (int nq = warp; nq < npq; nq += AW) {  // volume^T z
-      float dr[4] = {0.f, 0.f, 0.f, 0.f}, ds[4] = {0.f, 0.f, 0.f, 0.f};
-      float dtt[4] = {0.f, 0.f, 0.f, 0.f}, dv[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll 5
-      for (int m = 0; m < Np; ++m) {
-        const float4 da = reinterpret_cast<const float4 *>(sD + m * ldp)[nq];
-        const float4 db = reinterpret_cast<const float4 *>(sD + (Np + m) * ldp)[nq];
-        const float4 dc = reinterpret_cast<const float4 *>(sD + (2 * Np + m) * ldp)[nq];
-        const float p = sZ[m * AS + lane], ur = sZ[(Np + m) * AS + lane],
-                    us = sZ[(2 * Np + m) * AS + lane], ut = sZ[(3 * Np + m) * AS + lane];
-        fma4(dr, da, p);
-        fma4(ds, db, p);
-        fma4(dtt, dc, p);
-        fma4(dv, da, ur);
-        fma4(dv, db, us);
-        fma4(dv, dc, ut);
-      }
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int n = 4 * nq + r;
-        if (n >= Np) continue;
-        sB[n * AS + lane] = -dv[r];
-        sB[(Np + n) * AS + lane] = -(G[0] * dr[r] + G[3] * ds[r] + G[6] * dtt[r]);
-        sB[(2 * Np + n) * AS + lane] = -(G[1] * dr[r] + G[4] * ds[r] + G[7] * dtt[r]);
-        sB[(3 * Np + n) * AS + lane] = -(G[2] * dr[r] + G[5] * ds[r] + G[8] * dtt[r]);
-      }
-    }
-    __syncthreads();
-    for (int i = tid; i < ne * 4 * Np; i += AE * AW) {
-      const int el = i / (4 * Np), j = i - el * 4 * Np;
-      lamQ[so + i] += dt * sB[j * AS + el];
-    }
-  }
-}
-
-// lamQ[k][.][n] += dt (vol[k][.][n] + surface adjoint at node n); vol may be
-// NULL when the volume term was added by k_adj_local
+// lamQ[k][.][n] += dt (vol[k][.][n] + surface adjoint at node n)
 template <int N>
 __global__ void __launch_bounds__(256) k_adj_gather(int K, int Kg, int bc, float dt,
                                                     const float *__restrict__ fgeo,
@@ -479,13 +310,10 @@ __global__ void __launch_bounds__(256) k_adj_gather(int K, int Kg, int bc, float
     }
   }
   const size_t id = (size_t)k * 4 * Np + n;
-  if (vol) {
-    dp += vol[id], du += vol[id + Np], dv += vol[id + 2 * Np], dw += vol[id + 3 * Np];
-  }
-  lamQ[id] += dt * dp;
-  lamQ[id + Np] += dt * du;
-  lamQ[id + 2 * Np] += dt * dv;
-  lamQ[id + 3 * Np] += dt * dw;
+  lamQ[id] += dt * (vol[id] + dp);
+  lamQ[id + Np] += dt * (vol[id + Np] + du);
+  lamQ[id + 2 * Np] += dt * (vol[id + 2 * Np] + dv);
+  lamQ[id + 3 * Np] += dt * (vol[id + 3 * Np] + dw);
 }
 
 // trace[s][r][n] = w_r . Q_p(elem_r) after step n  =>  lamQ_p(elem_r) += g w_r.
@@ -571,42 +399,6 @@ static bbw_status launch_gather_n(int S, int K, int bc, float dt, const float *f
   return check_launch("adjoint face gather");
 }
 
-template <int N>
-static size_t local_tiles_bytes(int Nq) {
-  constexpr int Np = NP(N), NF = 4 * NFP(N);
-  return sizeof(float) * ((size_t)AS * (4 * Np + Nq + std::max(Nq, 4 * Np) + NF) + AE * 16);
-}
-
-template <int N>
-static size_t local_ops_bytes(int Nq) {
-  constexpr int Np = NP(N), ldp = (NP(N) + 3) & ~3, ldf = (NFP(N) + 3) & ~3;
-  const int ldq = (Nq + 3) & ~3;
-  return sizeof(float) * ((size_t)Np * ldq + (size_t)Nq * ldp + 4 * (size_t)Np * ldf +
-                          3 * (size_t)Np * ldp);
-}
-
-template <int N>
-static bbw_status launch_local_n(int S, int K, int Nq, const float *PqT, const float *VqT,
-                                 const float *LTp, const float *DTp, const float *c2q,
-                                 const float *vgeo, const float *fgeo, float *lamQ, float *lamR,
-                                 float a, float b, float dt, const float *vq, float *sigma,
-                                 double *grad, cudaStream_t st) {
-  int stage = 0;
-  const size_t sm = stage_smem(local_tiles_bytes<N>(Nq), local_ops_bytes<N>(Nq), &stage);
-  if (sm > 200 * 1024) return set_error(BBW_ERR_UNSUPPORTED, "adjoint local stage: Nq too large");
-  bbw_status s = ensure_smem_limit(k_adj_local<N>, 200 * 1024, "adjoint local stage attribute");
-  if (s != BBW_OK) return s;
-  k_adj_local<N><<<(K + AE - 1) / AE, AE * AW, sm, st>>>(S, K, Nq, stage, PqT, VqT, LTp, DTp,
-                                                         c2q, vgeo, fgeo, lamQ, lamR, a, b, dt,
-                                                         vq, sigma, grad);
-  return check_launch("adjoint local stage");
-}
-
-template <int N>
-static bool local_fits_n(int Nq) {
-  return local_tiles_bytes<N>(Nq) <= 200 * 1024;
-}
-
 #define BBW_N_SWITCH(CALL)                    \
   switch (N) {                                \
     case 1: return CALL(1);                   \
@@ -648,31 +440,6 @@ bbw_status adj_gather(int N, int S, int K, int bc, float dt, const float *fgeo, 
 #define CALL(n) launch_gather_n<n>(S, K, bc, dt, fgeo, fidx, mapP, sigma, vol, lamQ, st)
   BBW_N_SWITCH(CALL)
 #undef CALL
-}
-
-bbw_status adj_local(int N, int S, int K, int Nq, const float *PqT, const float *VqT,
-                     const float *LTp, const float *DTp, const float *c2q, const float *vgeo,
-                     const float *fgeo, float *lamQ, float *lamR, float a, float b, float dt,
-                     const float *vq, float *sigma, double *grad, cudaStream_t st) {
-#define CALL(n)                                                                                \
-  launch_local_n<n>(S, K, Nq, PqT, VqT, LTp, DTp, c2q, vgeo, fgeo, lamQ, lamR, a, b, dt, vq, \
-                    sigma, grad, st)
-  BBW_N_SWITCH(CALL)
-#undef CALL
-}
-
-bool adj_local_fits(int N, int Nq) {
-  switch (N) {
-    case 1: return local_fits_n<1>(Nq);
-    case 2: return local_fits_n<2>(Nq);
-    case 3: return local_fits_n<3>(Nq);
-    case 4: return local_fits_n<4>(Nq);
-    case 5: return local_fits_n<5>(Nq);
-    case 6: return local_fits_n<6>(Nq);
-    case 7: return local_fits_n<7>(Nq);
-    case 8: return local_fits_n<8>(Nq);
-  }
-  return false;
 }
 
 bbw_status adj_receivers(int S, int K, int Np, int R, const int *rec_elem, const float *rec_w,
