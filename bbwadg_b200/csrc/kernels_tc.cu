@@ -641,6 +641,16 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       sPend[4] = 1, sPend[5] = (int)wphase;
     }
 
+    // c^2 of epilogue 2, fetched here so that its latency hides under b
+    const bool q128 = MQ == 128;
+    const int qrow = q128 ? 32 * q4 + lane : rowM;
+    const int nq = q128 ? 8 : 4;  // elements per thread in epilogue 2
+    float c2v[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int e = 8 * g8 + (q128 ? j : ep_col(lane, j & 3));
+      c2v[j] = j < nq && qrow < Nq && e < ne ? __ldg(P.c2q + (size_t)(k0 + e) * Nq + qrow) : 0.f;
+    }
     // ---- b. next item: its inputs landed during this item's first MMAs;
     //         traces, flux and B operands of its first product group
     if (next < nvt) {
@@ -653,15 +663,6 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
     }
 
     // ---- c. epilogue 2 (thread = cubature row q): c2/J * p_q -> B operand of Pq
-    const bool q128 = MQ == 128;
-    const int qrow = q128 ? 32 * q4 + lane : rowM;
-    const int nq = q128 ? 8 : 4;  // elements per thread
-    float c2v[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const int e = 8 * g8 + (q128 ? j : ep_col(lane, j & 3));
-      c2v[j] = j < nq && qrow < Nq && e < ne ? __ldg(P.c2q + (size_t)(k0 + e) * Nq + qrow) : 0.f;
-    }
     wait_bar(mbW, wphase, 4, I_WADG);
     float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (!fail) {
