@@ -245,10 +245,10 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
        precision != BBW_PREC_BF16X3))
     return set_error(BBW_ERR_ARG, "bbw_create: bad argument");
   const bool tcp = precision == BBW_PREC_F16X3 || precision == BBW_PREC_BF16X3;
-  if (tcp && (variant != BBW_NODAL || !tc_supported(m->N, m->Nq)))
+  if (tcp && !tc_supported(m->N, m->Nq))
     return set_error(BBW_ERR_UNSUPPORTED,
-                     "bbw_create: the split-FP16 tensor-core stage supports the nodal variant "
-                     "with N in [2, 5] and Nq <= 128");
+                     "bbw_create: the split-FP16 tensor-core stage supports N in [2, 5] and "
+                     "Nq <= 128");
   const int N = m->N, K = m->K, Nq = m->Nq;
   if (N < 1 || N > BBW_MAX_N) return set_error(BBW_ERR_UNSUPPORTED, "bbw_create: N out of range");
   if (K <= 0 || K >= (1 << 23) || Nq <= 0)
@@ -407,20 +407,24 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
       std::memcpy(&geo[(size_t)k * TC_GEO], m->fgeo + (size_t)k * 16, 16 * sizeof(float));
       std::memcpy(&geo[(size_t)k * TC_GEO + 16], m->vgeo + (size_t)k * 9, 9 * sizeof(float));
     }
-    // operator planes with MR (MRQ) stored rows, see tc_layout
+    // operator planes with MR (MRQ) stored rows, see tc_layout.  The dense
+    // operators of the context's basis: for BB the dense equivalents of the
+    // sparse derivative and of the L0 + degree-elevation lift
+    // (dense_operators), applied to BB coefficients as the reference's
+    // rk_volume_bern / rk_surface_bern do (cpp/okl/WaveKernels.okl:344-647)
     std::vector<uint16_t> h(TL.ops_halfs);
     const int MR = TL.MR, MRQ = TL.MRQ;
-    const float *Dd[3] = {o->Dr, o->Ds, o->Dt};
     for (int d = 0; d < 3; ++d)
-      tc_pack_operator(Dd[d], Np, Np, 1, Np, MR, TL.KV, &h[TL.oD + 2 * d * MR * TL.KV],
+      tc_pack_operator(c->hD[d].data(), Np, Np, 1, Np, MR, TL.KV, &h[TL.oD + 2 * d * MR * TL.KV],
                        &h[TL.oD + (2 * d + 1) * MR * TL.KV], tp.bf);
     for (int f = 0; f < 4; ++f)
-      tc_pack_operator(o->LIFT + (size_t)f * Nfp * Np, Np, Nfp, 1, Np, MR, TL.KF,
+      tc_pack_operator(c->hLIFT.data() + (size_t)f * Nfp * Np, Np, Nfp, 1, Np, MR, TL.KF,
                        &h[TL.oL + 2 * f * MR * TL.KF], &h[TL.oL + (2 * f + 1) * MR * TL.KF],
                        tp.bf);
-    tc_pack_operator(o->Pq, Np, Nq, 1, Np, MR, TL.KQ, &h[TL.oPq], &h[TL.oPq + MR * TL.KQ], tp.bf);
-    tc_pack_operator(o->Vq, Nq, Np, 1, Nq, MRQ, TL.KV, &h[TL.oVq], &h[TL.oVq + MRQ * TL.KV],
+    tc_pack_operator(c->hPq.data(), Np, Nq, 1, Np, MR, TL.KQ, &h[TL.oPq], &h[TL.oPq + MR * TL.KQ],
                      tp.bf);
+    tc_pack_operator(c->hVq.data(), Nq, Np, 1, Nq, MRQ, TL.KV, &h[TL.oVq],
+                     &h[TL.oVq + MRQ * TL.KV], tp.bf);
     uint16_t *dops = nullptr;
     if ((s = upload(&c->geo_tc, geo.data(), geo.size(), "bbw_create: geometry")) != BBW_OK ||
         (s = upload(&dops, h.data(), h.size(), "bbw_create: tensor-core operators")) != BBW_OK ||

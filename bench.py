@@ -583,11 +583,12 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--variant", default="nodal-f16x3", choices=["nodal", "bb", "nodal-f16x3"])
+    ap.add_argument("--variant", default="nodal-f16x3",
+                    choices=["nodal", "bb", "nodal-f16x3", "bb-f16x3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--hex", type=int, default=N_HEX, help="hexes per direction (profiling cases)")
-    ap.add_argument("--variants", default="nodal-f16x3,nodal,bb",
-                    help="variants to run, comma separated (nodal, bb, nodal-f16x3)")
+    ap.add_argument("--variants", default="nodal-f16x3,nodal,bb,bb-f16x3",
+                    help="variants to run, comma separated (nodal, bb, nodal-f16x3, bb-f16x3)")
     ap.add_argument("--extra", default="shots,adjoint,precision,curved,kernel_level",
                     help="extra workloads reported beside the headline: shots, adjoint, "
                          "precision, curved, kernel_level")

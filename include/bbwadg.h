@@ -243,9 +243,11 @@ typedef struct bbw_ops_desc {
  * per-tile power-of-two scaling, FP32 accumulation); state, fluxes and the
  * update stay FP32.  BF16X3: the same with BF16 pairs (16 significant bits
  * per pair instead of 22; the split-BF16 form of the precision study).  Both
- * support the nodal variant with N in [2, 5] (Np <= 64: each operator's rows
- * fit one M = 64 MMA and all operators one SM's shared memory), Nq <= 128,
- * batched shots and sources; not the adjoint (bbw_forward needs FP32). */
+ * run N in [2, 5] (Np <= 64: each operator's rows fit one M = 64 MMA and all
+ * operators one SM's shared memory), Nq <= 128, batched shots and sources,
+ * nodal or BB (BB: the dense equivalents of the sparse BB derivative and
+ * lift applied to BB coefficients); not the adjoint (bbw_forward needs
+ * FP32). */
 enum { BBW_PREC_FP32 = 0, BBW_PREC_F16X3 = 1, BBW_PREC_BF16X3 = 2 };
 
 /* Uploads mesh and operators (cpp/src/WaveOKL3d.cpp:1400-1615 and

@@ -206,7 +206,7 @@ def _tets(n_elems):
 
 @pytest.mark.parametrize("n_elems", [1, 2])
 @pytest.mark.parametrize("N", [3, 5])
-@pytest.mark.parametrize("form", ["nodal", "bb", "nodal-f16x3"])
+@pytest.mark.parametrize("form", ["nodal", "bb", "nodal-f16x3", "bb-f16x3"])
 def test_one_and_two_element_meshes_match_oracle(cuda, n_elems, N, form):
     """A tile holding one or two elements, every face but the shared one a
     wall: the stage (FP32 fused, or the split-FP16 tensor-core form) against

@@ -98,15 +98,13 @@ def test_tc_many_tiles_per_cta_and_tiny_tiles(cuda):
 
 def test_tc_rejects_unsupported(cuda):
     """Np > 64 (N >= 6: operators beyond one M = 64 MMA and one SM's shared
-    memory) and the BB variant (sparse operators: the FP32 stage) are
-    refused."""
+    memory) and N = 1 are refused, for both bases."""
     from bbwadg_b200._lib import BBWError
-    p = make_problem(6, 1, variant="nodal")
-    with pytest.raises(BBWError):
-        WaveSolver(p, precision="f16x3")
-    p = make_problem(3, 2, variant="bb")
-    with pytest.raises(BBWError):
-        WaveSolver(p, precision="f16x3")
+    for N, n in ((6, 1), (1, 2)):
+        for variant in ("nodal", "bb"):
+            p = make_problem(N, n, variant=variant)
+            with pytest.raises(BBWError):
+                WaveSolver(p, precision="f16x3")
 
 
 @pytest.mark.parametrize("prec", ["f16x3", "bf16x3"])
@@ -156,3 +154,42 @@ def test_bf16x3_matches_oracle(cuda, N, n):
     print("relative L2 vs FP32 restatement:", errs)
     assert errs["f16x3"] < TOL
     assert errs["bf16x3"] < BF16X3_TOL
+
+
+@pytest.mark.parametrize("prec", ["f16x3", "bf16x3"])
+@pytest.mark.parametrize("N", [3, 4, 5])
+@pytest.mark.parametrize("bc", ["pressure_release", "rigid"])
+def test_tc_bb_matches_oracle(cuda, prec, N, bc):
+    """The Bernstein-Bezier variant on the tensor cores: the dense
+    equivalents of the sparse BB derivative and of the L0 + degree-elevation
+    lift, applied to BB coefficients, against the restatement of the
+    reference's sparse BB kernels (cpp/okl/WaveKernels.okl:344-647); the
+    reference's rules, a ragged last tile."""
+    from oracle import Oracle
+    cub, tri = ref_rule(N)
+    p = make_problem(N, 3, variant="bb", c2="sine", c2_jitter=0.5, seed=17, cubature=cub,
+                     tri_cubature=tri)
+    q_ref, _ = Oracle(N, p.K, p.ops_dict(), p.geo_dict(), variant="bb",
+                      bc=1 if bc == "rigid" else 0).run(p.Q0.copy(), p.dt, 25)
+    s = WaveSolver(p, bc=bc, precision=prec)
+    s.set_data(p.Q0)
+    s.steps(p.dt, 5)
+    s.check()
+    assert rel_l2(s.get_data(), q_ref) < TOL
+    s.close()
+
+
+def test_tc_bb_over_many_tiles_matches_the_bb_reference_run(cuda):
+    """The BB tensor-core stage through the 100-step run of the reference's
+    own BB path (4^3 x 6, Gaussian pulse, sine c^2, p = 0 walls)."""
+    r = golden("run_N3_box4.npz")
+    ops = ref_ops(3, "bb")
+    m = connect_and_geometry(3, *kuhn_box(4), build_operators(3))
+    s = WaveSolver(N=3, K=384, Nq=int(ops["Nq"][0]), variant="bb", ops=ops, vgeo=m["vgeo"],
+                   fgeo=m["fgeo"], vmapP=m["vmapP"], c2q=r["c2q"], precision="f16x3")
+    s.set_grid_limit(2)
+    s.set_data(r["Q0_bb"])
+    s.steps(float(r["dt"][0]), 100)
+    s.check()
+    assert rel_l2(s.get_data(), r["Q100_bb"]) < TOL
+    s.close()
