@@ -168,8 +168,6 @@ extern "C" bbw_status bbw_forward(bbw_ctx *c, float dt, int nsteps, int checkpoi
   if (!c || !out || nsteps < 1 || checkpoint_every < 1 || !(dt > 0.f))
     return set_error(BBW_ERR_ARG, "bbw_forward: bad argument");
   *out = nullptr;
-  if (c->precision != BBW_PREC_FP32)
-    return set_error(BBW_ERR_UNSUPPORTED, "bbw_forward: the adjoint needs BBW_PREC_FP32");
   if (c->R <= 0) return set_error(BBW_ERR_STATE, "bbw_forward: no receivers set");
   if (c->plan.Kc > 0 && c->plan.Kc < c->K)
     return set_error(BBW_ERR_UNSUPPORTED, "bbw_forward: the adjoint needs the whole mesh (no halo)");
@@ -249,20 +247,30 @@ extern "C" bbw_status bbw_backward(bbw_ctx *c, bbw_tape *t, const float *dL_dtra
 
   FusedPlan pl = c->plan;
   pl.time = tdev;
+  TcPlan tpl = c->tc;
+  tpl.time = tdev;
+  // one forward stage of the recomputation in the context's own form (FP32
+  // fused or tensor-core stage, bit-identical to the forward pass),
+  // optionally storing Vq S(Q)_p at the cubature points
+  auto launch = [&](int i, const float *in, float *outq, float *vqo) {
+    const float cs = c->src_stage_times ? (float)kRK4C[i] : 0.f;
+    if (c->precision != BBW_PREC_FP32) {
+      TcPlan tp = tpl;
+      tp.vq_out = vqo;
+      return tc_launch(tp, in, outq, res, (float)kRK4A[i], (float)kRK4B[i], dt, cs, st);
+    }
+    FusedPlan p = pl;
+    p.vq_out = vqo;
+    return fused_launch(p, in, outq, res, (float)kRK4A[i], (float)kRK4B[i], dt, cs, st);
+  };
   // step-start times exactly as the device clock accumulated them
   std::vector<double> tn(nsteps + 1);
   tn[0] = t->t0;
   for (int n = 0; n < nsteps; ++n) tn[n + 1] = tn[n] + (double)dt;
-  FusedPlan pv = pl;  // same stage, also storing Vq S(Q)_p at the cubature points
-  auto stage = [&](int i, const float *in, float *outq) {
-    return fused_launch(pl, in, outq, res, (float)kRK4A[i], (float)kRK4B[i], dt,
-                        c->src_stage_times ? (float)kRK4C[i] : 0.f, st);
-  };
+  auto stage = [&](int i, const float *in, float *outq) { return launch(i, in, outq, nullptr); };
   const size_t vqn = (size_t)S * Nq * K;  // per stage
-  auto stage_v = [&](int i, const float *in, float *outq) {
-    pv.vq_out = vq + (size_t)i * vqn;
-    return fused_launch(pv, in, outq, res, (float)kRK4A[i], (float)kRK4B[i], dt,
-                        c->src_stage_times ? (float)kRK4C[i] : 0.f, st);
+  auto stage_v = [&](int i, const float *in, float *outq) {  // also storing Vq S(Q)_p
+    return launch(i, in, outq, vq + (size_t)i * vqn);
   };
   auto step_fwd = [&](int n, const float *in, float *outq) {  // stage outputs in stq[1..4]
     bbw_status r = set_device_double(tdev, tn[n], st);
@@ -300,10 +308,7 @@ extern "C" bbw_status bbw_backward(bbw_ctx *c, bbw_tape *t, const float *dL_dtra
         const float *qi = q;
         for (int i = 0; i < 5; ++i) {
           float *o = i < 4 ? stq + (size_t)(i + 1) * t->state : out;
-          pv.vq_out = vq_all + ((size_t)j * 5 + i) * vqn;
-          if ((s = fused_launch(pv, qi, o, res, (float)kRK4A[i], (float)kRK4B[i], dt,
-                                c->src_stage_times ? (float)kRK4C[i] : 0.f, st)) != BBW_OK)
-            return s;
+          if ((s = launch(i, qi, o, vq_all + ((size_t)j * 5 + i) * vqn)) != BBW_OK) return s;
           qi = o;
         }
         q = out;

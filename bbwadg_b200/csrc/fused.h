@@ -81,6 +81,7 @@ struct TcPlan {
   const float *src_vec = nullptr;
   float f0 = 0.f, tR = 0.f, samp = 0.f;
   const double *time = nullptr;
+  float *vq_out = nullptr;  // [S][Nq][K] pre-c2 cubature values of rhs_p (adjoint recomputation)
 };
 
 TcLayout tc_layout(int N, int Nq, int table_ints);

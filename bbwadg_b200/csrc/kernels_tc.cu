@@ -158,6 +158,9 @@ struct TcParams {
   const float *__restrict__ src_vec;
   float f0, tR, samp;
   const double *__restrict__ time;
+  // optional: Vq (raw rhs_p) at the cubature points, before c2/J, stored as
+  // [shot][Nq][K] (what the adjoint's gradient needs, as the FP32 stage)
+  float *__restrict__ vq_out;
   TcLayout L;
 };
 
@@ -679,7 +682,12 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
     float mc = 0.f;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-      v[j] = qrow < Nq ? v[j] * isr * c2v[j] : 0.f;  // rows past Nq: exact zeros
+      const float raw = v[j] * isr;
+      if (P.vq_out && j < nq && qrow < Nq) {
+        const int e = 8 * g8 + (q128 ? j : ep_col(lane, j));
+        if (e < ne) P.vq_out[((size_t)shot * Nq + qrow) * P.K + k0 + e] = raw;
+      }
+      v[j] = qrow < Nq ? raw * c2v[j] : 0.f;  // rows past Nq: exact zeros
       mc = fmaxf(mc, fabsf(v[j]));
     }
     mc = warp_max(mc);
@@ -822,6 +830,7 @@ static bbw_status tc_launch_n(const TcPlan &pl, const float *Qin, float *Qout, f
   P.err = pl.err;
   P.src_off = pl.src_off, P.src_elem = pl.src_elem, P.src_vec = pl.src_vec;
   P.f0 = pl.f0, P.tR = pl.tR, P.samp = pl.samp, P.time = pl.time;
+  P.vq_out = pl.vq_out;
   P.L = pl.L;
   const int items = cdv(pl.K, TC_E) * P.S;
   int grid = std::min(items, pl.nsm);

@@ -246,8 +246,8 @@ typedef struct bbw_ops_desc {
  * run N in [2, 5] (Np <= 64: each operator's rows fit one M = 64 MMA and all
  * operators one SM's shared memory), Nq <= 128, batched shots and sources,
  * nodal or BB (BB: the dense equivalents of the sparse BB derivative and
- * lift applied to BB coefficients); not the adjoint (bbw_forward needs
- * FP32). */
+ * lift applied to BB coefficients), and the adjoint (its forward and
+ * recomputation run the same stage). */
 enum { BBW_PREC_FP32 = 0, BBW_PREC_F16X3 = 1, BBW_PREC_BF16X3 = 2 };
 
 /* Uploads mesh and operators (cpp/src/WaveOKL3d.cpp:1400-1615 and
@@ -367,8 +367,10 @@ bbw_status bbw_get_time(bbw_ctx *ctx, double *t, int *step);
  * c^2 at the cubature points.  No reference counterpart: the adjoint
  * reverses the reference's stage (rk_volume + rk_surface + rk_update_WADG,
  * cpp/okl/WaveKernels.okl:44-260, cpp/okl/WaveKernelsWADG.okl:1760-1887)
- * and its LSRK45 loop (cpp/src/WaveOKL3d.cpp:2014-2109).  FP32 stage only;
- * both bases; any number of shots. */
+ * and its LSRK45 loop (cpp/src/WaveOKL3d.cpp:2014-2109).  Either stage form
+ * (FP32 or split-precision tensor-core: the forward pass and its
+ * recomputation run the context's stage, the reverse stages the FP32
+ * transposed operators); both bases; any number of shots. */
 /* ------------------------------------------------------------------
  * Curvilinear WADG path (cpp/src/WaveOKL3d.cpp:164-417 InitWADG_curved,
  * :2111-2185 RK_step_WADG).  Kernel-level entry points take device

@@ -27,9 +27,9 @@ def setup(variant, bc, S=2, N=3, n=2, seed=0, rules=(None, None)):
     return p, rec, dense
 
 
-def gpu_gradient(p, rec, dense, bc, nsteps, every, Q0, stage_times=True):
+def gpu_gradient(p, rec, dense, bc, nsteps, every, Q0, stage_times=True, precision="fp32"):
     S = len(dense)
-    s = WaveSolver(p, bc="rigid" if bc else "pressure_release")
+    s = WaveSolver(p, bc="rigid" if bc else "pressure_release", precision=precision)
     s.set_shots(S)
     ent = [source_entries(f, shot=i, rtol=0.0) for i, f in enumerate(dense)]
     s.set_sources(*(np.concatenate(x) for x in zip(*ent)), f0=10.0, amplitude=1e2,
@@ -151,11 +151,6 @@ def test_adjoint_errors(cuda):
     with pytest.raises(BBWError):  # capacity
         s.forward(p.dt, 4, 2)
     s.close()
-    t = WaveSolver(make_problem(3, 2), precision="f16x3")
-    t.set_receivers(*rec, 8)
-    with pytest.raises(BBWError):
-        t.forward(p.dt, 4, 2)
-    t.close()
 
 
 @pytest.mark.parametrize("n_elems", [1, 2])
@@ -216,3 +211,39 @@ def test_gradient_at_size_matches_fp64_adjoint_and_finite_differences(cuda):
         eps = 1e-4
         fd = (loss(c2 + eps * d) - loss(c2 - eps * d)) / (2 * eps)
         assert abs(float((grad * d).sum()) - fd) <= TOL * abs(fd)
+
+
+@pytest.mark.parametrize("variant", ["nodal", "bb"])
+@pytest.mark.parametrize("N", [3, 5])
+def test_gradient_with_the_tensor_core_forward(cuda, variant, N):
+    """The forward pass and its recomputation on the split-FP16 tensor-core
+    stage (the reverse stages use the FP32 transposed operators): the
+    gradient against the FP64 discrete adjoint, and a directional derivative
+    against FP64 central finite differences; checkpoint intervals agree bit
+    for bit."""
+    from conftest import golden
+    g = golden("ops_N%d.npz" % N)
+    nfq = int(np.asarray(g["Nfq"]).ravel()[0])
+    rules = ((g["rq"], g["sq"], g["tq"], g["wq"]), (g["rfq"][:nfq], g["sfq"][:nfq], g["wfqFace"]))
+    p, rec, dense = setup(variant, 0, S=2, N=N, rules=rules)
+    nsteps = 10
+    tr, grad, _ = gpu_gradient(p, rec, dense, 0, nsteps, 3, p.Q0, precision="f16x3")
+    tr64, grad64, ad = oracle_gradient(p, rec, dense, 0, nsteps, p.Q0)
+    assert rel_l2(tr, tr64) < 1e-5
+    assert rel_l2(grad, grad64) < TOL
+    assert np.array_equal(gpu_gradient(p, rec, dense, 0, nsteps, 10, p.Q0, precision="f16x3")[1],
+                          grad)
+    dt = float(np.float32(p.dt))
+    srcs = [dict(fsrc=f.astype(np.float64), f0=10.0, tR=0.1, amp=1e2, stage_times=True)
+            for f in dense]
+    c2 = ad.c2q.copy()
+
+    def loss(c):
+        ad.c2q = c
+        return sum(0.5 * float((ad.forward(p.Q0.astype(np.float64), dt, nsteps, rec, s)[1] ** 2)
+                               .sum()) for s in srcs)
+
+    d = np.random.default_rng(5).standard_normal(c2.shape)
+    eps = 1e-4
+    fd = (loss(c2 + eps * d) - loss(c2 - eps * d)) / (2 * eps)
+    assert abs(float((grad * d).sum()) - fd) <= TOL * abs(fd)
