@@ -312,51 +312,63 @@ def adjoint_workload(args, torch, dist, rank, world):
     c2_back = np.ascontiguousarray(base(xq, yq, zq), np.float32)
     rng = np.random.default_rng(64)
     el, w = receiver_weights(prob, rng.uniform(-0.8, 0.8, (R, 3)))
-    s = WaveSolver(prob)
-    s.set_shots(S)
-    s.set_sources(*shot_sources(prob, S, 8, first=lo), f0=4.0, amplitude=1e4, stage_times=True)
-    s.set_receivers(el, w, steps)
-    zero = np.zeros(s.state_size, np.float32)
+    def one(prec):
+        """Forward + backward with the stage form `prec`; times, misfit, gradient."""
+        s = WaveSolver(prob, precision=prec)
+        s.set_shots(S)
+        s.set_sources(*shot_sources(prob, S, 8, first=lo), f0=4.0, amplitude=1e4,
+                      stage_times=True)
+        s.set_receivers(el, w, steps)
+        zero = np.zeros(s.state_size, np.float32)
 
-    def run(c2, tape):
-        s.set_c2q(c2)
-        s.set_data(zero)
-        s.set_residual(zero)
-        s.set_time(0.0)
-        if tape:
-            return s.forward(prob.dt, steps, every)
-        s.steps(prob.dt, steps)
+        def run(c2, tape):
+            s.set_c2q(c2)
+            s.set_data(zero)
+            s.set_residual(zero)
+            s.set_time(0.0)
+            if tape:
+                return s.forward(prob.dt, steps, every)
+            s.steps(prob.dt, steps)
+            s.sync()
+            return None
+
+        run(c2_target, False)
+        obs = s.get_traces().copy()
         s.sync()
-        return None
+        t0 = time.perf_counter()
+        tape = run(c2_back, True)
+        s.sync()
+        t1 = time.perf_counter()
+        tr = s.get_traces()
+        misfit = 0.5 * float(((tr - obs).astype(np.float64) ** 2).sum())
+        t2 = time.perf_counter()
+        grad = s.backward(tape, tr - obs)
+        if world > 1:
+            grad = allreduce_gradient(grad, device="cuda")
+            misfit = allreduce_gradient(np.array([misfit]), device="cuda")[0]
+        t3 = time.perf_counter()
+        tape.free()
+        s.close()
+        tf, tb = t1 - t0, t3 - t2
+        if world > 1:
+            t = torch.tensor([tf, tb], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            tf, tb = float(t[0]), float(t[1])
+        return tf, tb, misfit, grad
 
-    run(c2_target, False)
-    obs = s.get_traces().copy()
-    s.sync()
-    t0 = time.perf_counter()
-    tape = run(c2_back, True)
-    s.sync()
-    t1 = time.perf_counter()
-    tr = s.get_traces()
-    misfit = 0.5 * float(((tr - obs).astype(np.float64) ** 2).sum())
-    t2 = time.perf_counter()
-    grad = s.backward(tape, tr - obs)
-    if world > 1:
-        grad = allreduce_gradient(grad, device="cuda")
-        misfit = allreduce_gradient(np.array([misfit]), device="cuda")[0]
-    t3 = time.perf_counter()
-    tape.free()
-    s.close()
-    tf, tb = t1 - t0, t3 - t2
-    if world > 1:
-        t = torch.tensor([tf, tb], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tf, tb = float(t[0]), float(t[1])
+    tf, tb, misfit, grad = one("fp32")
+    tf2, tb2, misfit2, grad2 = one("f16x3")
     return {"workload": "forward + adjoint c2 gradient, N=4, 16^3x6 tets (K=%d), %d shots per "
                         "GPU, %d receivers, %d steps, checkpoints every %d" % (prob.K, S, R, steps,
                                                                                every),
             "forward_s": tf, "backward_s": tb, "total_s": tf + tb, "shots_total": 8 * world,
             "misfit": misfit, "grad_norm": float(np.linalg.norm(grad)),
-            "grad_finite": bool(np.isfinite(grad).all())}
+            "grad_finite": bool(np.isfinite(grad).all()),
+            "f16x3": {"forward_s": tf2, "backward_s": tb2, "total_s": tf2 + tb2,
+                      "misfit": misfit2,
+                      "grad_rel_l2_vs_fp32": float(np.linalg.norm(grad2 - grad) /
+                                                   np.linalg.norm(grad)),
+                      "note": "forward and recomputation on the split-FP16 tensor-core stage"}}
 
 
 def precision_workload(args, torch):
