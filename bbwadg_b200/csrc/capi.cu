@@ -80,7 +80,8 @@ void release(bbw_ctx *c) {
 
 namespace bbw {
 
-// Operators packed per warp for the fused kernel with W warps per CTA:
+// Operators packed per thread group for the fused kernel with W thread
+// groups (row blocks) per CTA:
 //   vol  [W][Np(m)][P3R]  rows in pairs p = i/2: Dr, Ds, Dt of row r0+i at
 //                         6p + (i%2) + {0, 2, 4}                      (nodal)
 //   lift [W][NF(m)][PR]   LIFT[r0+i][m]                           (nodal)
@@ -283,9 +284,9 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
   for (int i = 0; i < NF; ++i)
     if (m->Fmask[i] < 0 || m->Fmask[i] >= Np)
       return set_error(BBW_ERR_ARG, "bbw_create: Fmask entry out of range");
-  const int W = fused_default_warps(N);
+  const int W = fused_default_warps(N), E = fused_default_tile(N);
   FusedOps fo;
-  pack_fused_ops(N, Nq, W, bb, o->Dr, o->Ds, o->Dt, o->LIFT, o->Vq, o->Pq, fo);
+  pack_fused_ops(N, Nq, fused_groups(W, E), bb, o->Dr, o->Ds, o->Dt, o->LIFT, o->Vq, o->Pq, fo);
   const std::vector<float> &ops = fo.ops;
   const int off_lift = fo.off_lift, off_pq = fo.off_pq, off_vq = fo.off_vq;
   const int RQ = fo.RQ, PRQ = fo.PRQ;
@@ -309,8 +310,7 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
       std::memcpy(&bits, &o->Dvals4[i], 4);
       tab.push_back(bits);
     }
-    // header, L0 and EEL as (shared-memory offset, value bits) pairs; the
-    // offsets are pre-multiplied by the kernel's element row stride
+    // header, L0 and EEL as (face-node row, value bits) pairs
     const int L0 = o->L0_nnz;
     auto bits = [](float v) {
       int b;
@@ -327,7 +327,7 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
           const int c = o->EEL_ids[n + j * Np];
           const float v = o->EEL_vals[n + j * Np];
           if (c < 0 || c >= NF) return set_error(BBW_ERR_ARG, "bbw_create: EEL id out of range");
-          if (v != 0.f && c / Nfp == f) pairs.push_back(c * kFusedRowStride), pairs.push_back(bits(v));
+          if (v != 0.f && c / Nfp == f) pairs.push_back(c), pairs.push_back(bits(v));
         }
         if (f == 3) ptr[(size_t)n * 5 + 4] = (int)pairs.size() / 2;
       }
@@ -337,7 +337,7 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
     tab.push_back(0);
     for (int nt = 0; nt < Nfp; ++nt)
       for (int j = 0; j < L0; ++j) {
-        tab.push_back(o->L0_ids[nt + j * Nfp] * kFusedRowStride);
+        tab.push_back(o->L0_ids[nt + j * Nfp]);
         tab.push_back(bits(o->L0_vals[nt + j * Nfp]));
       }
     tab.insert(tab.end(), ptr.begin(), ptr.end());
@@ -388,7 +388,7 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
   pl.ops = c->ops, pl.ops_floats = (int)ops.size();
   pl.off_lift = off_lift, pl.off_pq = off_pq, pl.off_vq = off_vq;
   pl.tables = c->tables, pl.table_ints = (int)tab.size(), pl.pat_off = pat_off, pl.bb_off = bb_off;
-  pl.S = 1, pl.time = c->d_time, pl.W = W;
+  pl.S = 1, pl.time = c->d_time, pl.W = W, pl.E = E;
   if ((s = fused_prepare(pl)) != BBW_OK) {
     release(c);
     return s;
@@ -564,17 +564,18 @@ extern "C" bbw_status bbw_steps(bbw_ctx *c, float dt, int nsteps) {
   return BBW_OK;
 }
 
-// plan of the fused stage with W warps and the requested placement; the
-// packed operators are uploaded to *ops_buf (owned by the caller)
-static bbw_status make_variant(bbw_ctx *c, int W, int want_ops, int want_pipe, FusedPlan &p,
-                               float **ops_buf) {
+// plan of the fused stage with W warps, E-element tiles and the requested
+// placement; the packed operators are uploaded to *ops_buf (owned by the
+// caller)
+static bbw_status make_variant(bbw_ctx *c, int W, int E, int want_ops, int want_pipe,
+                               FusedPlan &p, float **ops_buf) {
   FusedOps fo;
-  pack_fused_ops(c->N, c->Nq, W, c->variant == BBW_BB, c->hD[0].data(), c->hD[1].data(),
+  pack_fused_ops(c->N, c->Nq, fused_groups(W, E), c->variant == BBW_BB, c->hD[0].data(), c->hD[1].data(),
                  c->hD[2].data(), c->hLIFT.data(), c->hVq.data(), c->hPq.data(), fo);
   bbw_status s = upload(ops_buf, fo.ops.data(), fo.ops.size(), "fused stage: operators");
   if (s != BBW_OK) return s;
   p = c->plan;
-  p.W = W;
+  p.W = W, p.E = E;
   p.ops = *ops_buf, p.ops_floats = (int)fo.ops.size();
   p.off_lift = fo.off_lift, p.off_pq = fo.off_pq, p.off_vq = fo.off_vq;
   p.RQ = fo.RQ, p.PRQ = fo.PRQ;
@@ -583,21 +584,22 @@ static bbw_status make_variant(bbw_ctx *c, int W, int want_ops, int want_pipe, F
 }
 
 static int config_code(const FusedPlan &p) {
-  return p.W | (p.ops_smem > 0 ? 1 << 8 : 0) | (p.pipe ? 1 << 9 : 0);
+  return p.W | (p.ops_smem > 0 ? 1 << 8 : 0) | (p.pipe ? 1 << 9 : 0) | (p.E == 16 ? 1 << 10 : 0);
 }
 
 extern "C" bbw_status bbw_set_config(bbw_ctx *c, int config) {
   DeviceGuard dg(c ? c->device : -1);
   if (!c) return set_error(BBW_ERR_ARG, "bbw_set_config: ctx is NULL");
   const int W = config & 255;
-  if ((W != 8 && W != 16) || (config >> 10) != 0)
-    return set_error(BBW_ERR_ARG, "bbw_set_config: W must be 8 or 16, flags bits 8-9");
+  if ((W != 8 && W != 16) || (config >> 11) != 0)
+    return set_error(BBW_ERR_ARG, "bbw_set_config: W must be 8 or 16, flags bits 8-10");
   if (c->precision != BBW_PREC_FP32) return BBW_OK;
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return set_cuda_error(e, "bbw_set_config");
   FusedPlan p;
   float *buf = nullptr;
-  bbw_status s = make_variant(c, W, config >> 8 & 1, config >> 9 & 1, p, &buf);
+  bbw_status s = make_variant(c, W, (config >> 10 & 1) ? 16 : 32, config >> 8 & 1, config >> 9 & 1, p,
+                              &buf);
   if (s != BBW_OK) {
     cudaFree(buf);
     return s;
@@ -636,14 +638,15 @@ extern "C" bbw_status bbw_autotune(bbw_ctx *c, float dt, int stages, int *config
   cudaMemcpy(q[0], c->Q[c->cur], n * sizeof(float), cudaMemcpyDeviceToDevice);
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  const int Ws[2] = {8, 16};
+  const int Ws[2] = {8, 16}, Es[2] = {32, 16};
   float best_ms = 0.f;
   int best = -1;
+  for (int ei = 0; ei < 2; ++ei)
   for (int wi = 0; wi < 2; ++wi)
     for (int v = 0; v < 4; ++v) {
       FusedPlan p;
       float *buf = nullptr;
-      if (make_variant(c, Ws[wi], v < 2 ? 1 : 0, v % 2 == 0 ? 1 : 0, p, &buf) != BBW_OK) {
+      if (make_variant(c, Ws[wi], Es[ei], v < 2 ? 1 : 0, v % 2 == 0 ? 1 : 0, p, &buf) != BBW_OK) {
         cudaFree(buf);  // does not fit
         continue;
       }

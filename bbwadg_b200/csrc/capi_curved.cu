@@ -373,9 +373,10 @@ extern "C" bbw_status bbw_curved_autotune(bbw_curved *h, float dt, int stages, i
   float best_ms = 0.f;
   int best = -1;
   bbw_status s = BBW_OK;
+  for (int e16 = 0; e16 < 2 && s == BBW_OK; ++e16)
   for (int W = 8; W <= 16 && s == BBW_OK; W += 8)
     for (int v = 0; v < 4 && s == BBW_OK; ++v) {
-      const int code = W | (v < 2 ? 1 << 8 : 0) | (v % 2 == 0 ? 1 << 9 : 0);
+      const int code = W | (v < 2 ? 1 << 8 : 0) | (v % 2 == 0 ? 1 << 9 : 0) | e16 << 10;
       if (bbw_set_config(h->aff, code) != BBW_OK) continue;  // does not fit
       for (int i = 0; i < 2 && s == BBW_OK; ++i) s = stage(h, 0.f, (float)kRK4B[0], dt);
       if (s == BBW_OK) e = cudaEventRecord(e0, h->stream);

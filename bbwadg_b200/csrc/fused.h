@@ -12,12 +12,10 @@
 
 namespace bbw {
 
-// element-tile row stride (floats) of the fused kernel's shared-memory arrays
-constexpr int kFusedRowStride = 33;
-
 struct FusedPlan {
   int N = 0, K = 0, Nq = 0, RQ = 0, PRQ = 0, bc = 0, npat = 0;
   int W = 0;                            // warps per CTA (8 or 16; 0 = default for N)
+  int E = 0;                            // elements per tile (16 or 32; 0 = default for N)
   int Kc = 0;                           // elements advanced (0 = all K; rest are halo copies)
   int K0 = 0;                           // first element advanced (a launch covers [K0, Kc))
   int want_ops = -1, want_pipe = -1;    // requested placement (-1: first that fits)
@@ -41,15 +39,20 @@ struct FusedPlan {
 };
 
 int fused_default_warps(int N);
-// cubature rows per accumulator block of the fused kernel's Vq product
-__host__ __device__ constexpr int fused_vq_block(int W) { return W == 8 ? 12 : 8; }
+int fused_default_tile(int N);
+// cubature rows per accumulator block of the fused kernel's Vq product, by
+// the number of thread groups (row blocks) per CTA
+__host__ __device__ constexpr int fused_vq_block(int groups) { return groups == 8 ? 12 : 8; }
+// thread groups of a fused-stage CTA: W warps, one thread per element of an
+// E-element tile
+constexpr int fused_groups(int W, int E) { return 32 * W / E; }
 
-// operators packed per warp for a W-warp fused kernel (capi.cu)
+// operators packed per thread group for a fused kernel with G groups (capi.cu)
 struct FusedOps {
   std::vector<float> ops;
   int off_lift = 0, off_pq = 0, off_vq = 0, RQ = 0, PRQ = 0;
 };
-void pack_fused_ops(int N, int Nq, int W, bool bb, const float *Dr, const float *Ds,
+void pack_fused_ops(int N, int Nq, int G, bool bb, const float *Dr, const float *Ds,
                     const float *Dt, const float *LIFT, const float *Vq, const float *Pq,
                     FusedOps &out);
 

@@ -10,14 +10,17 @@
 // applies the LSRK45 stage update, reading each element's state once from
 // HBM and writing the new state and residual once.
 //
-// Work decomposition: a persistent CTA owns a tile of E = 32 consecutive
-// elements at a time; lane l of every warp works on element l of the tile,
-// warp w owns a block of R output rows (nodes) or RQ cubature points.  The
-// reference-element operators are staged in shared memory once per CTA in a
-// per-warp packed layout, so every operator read is a warp-uniform broadcast
-// (float4) while the element data is read conflict-free with lane = element.
-// State tiles are moved between HBM and shared memory with coalesced float4
-// traffic and transposed to [row][element] (stride 33) on the way.
+// Work decomposition: a persistent CTA owns a tile of E consecutive elements
+// at a time (E = 32, or 16 where a 32-element tile's arrays do not fit in
+// shared memory); the CTA's threads form groups of E, thread l of a group
+// works on element l of the tile and group g owns a block of R output rows
+// (nodes) or RQ cubature points.  With E = 32 a group is a warp; with E = 16
+// a warp holds two groups.  The reference-element operators are staged in
+// shared memory once per CTA in a per-group packed layout, so every operator
+// read is a (half-)warp-uniform broadcast (float4) while the element data is
+// read conflict-free with thread = element.  State tiles are moved between
+// HBM and shared memory with coalesced traffic and transposed to
+// [row][element] (row stride E + 1) on the way.
 //
 // Double-buffered state: the stage reads Qin (this element and its
 // neighbours' face traces) and writes Qout, so neighbour gathers never race
@@ -45,22 +48,22 @@
 
 namespace bbw {
 
-constexpr int TILE_E = 32;
-constexpr int ES = kFusedRowStride;  // shared-memory row stride (floats), TILE_E + 1
-static_assert(ES == TILE_E + 1, "row stride");
-
 __host__ __device__ constexpr int round4(int x) { return (x + 3) & ~3; }
 __host__ __device__ constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }
 
 // warps per CTA: 8 or 16 (run-time choice, see fused_prepare / bbw_autotune)
 __host__ __device__ constexpr int fused_default_warps_c(int N) { return N <= 3 ? 8 : 16; }
 
-template <int N, int W_>
+template <int N, int W_, int E_ = 32>
 struct FusedCfg {
+  static_assert(E_ == 16 || E_ == 32, "element tile of 16 or 32");
   static constexpr int Np = NP(N), Nfp = NFP(N), NF = 4 * NFP(N);
   static constexpr int W = W_;  // warps per CTA
   static constexpr int T = 32 * W;
-  static constexpr int R = cdiv(Np, W);     // node rows per warp
+  static constexpr int E = E_;        // elements per tile
+  static constexpr int ES = E_ + 1;   // shared-memory row stride (floats)
+  static constexpr int NG = T / E_;   // thread groups (one element each) per CTA
+  static constexpr int R = cdiv(Np, NG);    // node rows per group
   static constexpr int R2 = cdiv(R, 2);     // row pairs (packed FP32 FMAs)
   static constexpr int PR = round4(R);
   static constexpr int P3R = round4(6 * R2);
@@ -73,13 +76,13 @@ __device__ __forceinline__ float2 pair(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float pick(const float2 *v, int i) { return (i & 1) ? v[i >> 1].y : v[i >> 1].x; }
 
 // ------------------------------------------------------------------ layouts
-// Operators, packed per warp so that warp w reads one contiguous, 16-byte
-// aligned block per reduction index:
-//   vol  [W][Np(m)][P3R]  rows in pairs p = i/2: (Dr, Ds, Dt)[r0+i][m] at
-//                         6p + (i%2) + {0, 2, 4}
-//   lift [W][NF(m)][PR]   LIFT[r0+i][m]
-//   pq   [W][Nq(q)][PR]   Pq[r0+i][q]
-//   vq   [W][Np(n)][PRQ]  Vq[q0+i][n]
+// Operators, packed per thread group so that group g reads one contiguous,
+// 16-byte aligned block per reduction index (NG groups):
+//   vol  [NG][Np(m)][P3R]  rows in pairs p = i/2: (Dr, Ds, Dt)[r0+i][m] at
+//                          6p + (i%2) + {0, 2, 4}
+//   lift [NG][NF(m)][PR]   LIFT[r0+i][m]
+//   pq   [NG][Nq(q)][PR]   Pq[r0+i][q]
+//   vq   [NG][Np(n)][PRQ]  Vq[q0+i][n]
 // plus, for BB, the sparse tables.  Built on the host (fused_host.cu).
 struct FusedParams {
   int K, Nq, RQ, PRQ, bc, npat;
@@ -123,13 +126,14 @@ __device__ __forceinline__ float ricker(float t, float f0, float tR, float amp) 
 // Shared-memory map (floats, rows of stride ES).  Input tiles are double
 // buffered when they fit (PIPE): the next tile's copies are in flight while
 // the current one is computed.
-template <int N, bool BB>
+template <int N, bool BB, int E_>
 struct FusedSmem {
-  using C = FusedCfg<N, 8>;  // row counts only; independent of the warp count
+  using C = FusedCfg<N, 8, E_>;  // row counts only; independent of the warp count
+  static constexpr int ES = C::ES;
   static constexpr int inQ = 0;                               // [4Np][ES] state tile
   static constexpr int inGeo = 4 * C::Np * ES;                // [E][25]  vgeo + fgeo
-  static constexpr int inNbr = inGeo + TILE_E * 25;           // [E][4]   neighbour codes
-  static constexpr int inC2 = inNbr + TILE_E * 4;             // [Nq][ES] c2 (runtime Nq)
+  static constexpr int inNbr = inGeo + E_ * 25;               // [E][4]   neighbour codes
+  static constexpr int inC2 = inNbr + E_ * 4;                 // [Nq][ES] c2 (runtime Nq)
   __host__ __device__ static int in_size(int Nq) { return inC2 + round4(Nq * ES); }
   static constexpr int sR = 0;                                // [4Np][ES] rhs / U scratch
   static constexpr int sF = sR + 4 * C::Np * ES;              // [NF][ES]  pflux
@@ -160,14 +164,15 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // WIN: the advanced elements start at P.K0 (a window of a split stage);
 // without it they start at 0, a constant, which keeps the window arithmetic
 // out of the whole-mesh stage.
-template <int N, bool BB, bool OPS_SMEM, bool PIPE, int W_, bool WIN = false>
-__global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedParams P) {
-  using C = FusedCfg<N, W_>;
+template <int N, bool BB, bool OPS_SMEM, bool PIPE, int W_, int E_ = 32, bool WIN = false>
+__global__ void __launch_bounds__(FusedCfg<N, W_, E_>::T, 1) k_fused_stage(FusedParams P) {
+  using C = FusedCfg<N, W_, E_>;
   const int K0 = WIN ? P.K0 : 0;  // first element advanced
-  using L = FusedSmem<N, BB>;
-  constexpr int Np = C::Np, Nfp = C::Nfp, NF = C::NF, W = C::W, T = C::T, R = C::R;
-  constexpr int FIT = cdiv(TILE_E * NF, T);        // flux items per thread
-  constexpr int QIT = cdiv(TILE_E * 4 * Np, T);    // state-tile floats per thread
+  using L = FusedSmem<N, BB, E_>;
+  constexpr int Np = C::Np, Nfp = C::Nfp, NF = C::NF, T = C::T, R = C::R;
+  constexpr int E = C::E, ES = C::ES, NG = C::NG;
+  constexpr int FIT = cdiv(E * NF, T);        // flux items per thread
+  constexpr int QIT = cdiv(E * 4 * Np, T);    // state-tile floats per thread
   extern __shared__ __align__(16) float sm[];
   const int Nq = P.Nq, RQ = P.RQ, PRQ = P.PRQ;
   const int inSize = L::in_size(Nq);
@@ -180,8 +185,9 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
   const int tabSmem = OPS_SMEM ? P.table_ints : P.bb_off;
   int *sTab = (int *)(sW + L::work_size(Nq));
   float *sOps = (float *)(sTab + tabSmem);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int r0 = warp * R;
+  // el: element of the tile this thread works on; grp: its row block
+  const int tid = threadIdx.x, el = tid & (E - 1), grp = tid / E;
+  const int r0 = grp * R;
 
   // stage operators (when they fit) and tables once per CTA
   if (OPS_SMEM)
@@ -192,32 +198,32 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
   const int *sPat = sTab + P.pat_off;
 
   const float *opBase = OPS_SMEM ? (const float *)sOps : P.ops;
-  const float *wVol = opBase + warp * Np * C::P3R;              // [W][Np][P3R]
-  const float *wLift = opBase + P.off_lift + warp * NF * C::PR;  // [W][NF][PR]
-  const float *wPq = opBase + P.off_pq + warp * Nq * C::PR;      // [W][Nq][PR]
-  const float *wVq = opBase + P.off_vq + warp * Np * PRQ;        // [W][Np][PRQ]
+  const float *wVol = opBase + grp * Np * C::P3R;              // [NG][Np][P3R]
+  const float *wLift = opBase + P.off_lift + grp * NF * C::PR;  // [NG][NF][PR]
+  const float *wPq = opBase + P.off_pq + grp * Nq * C::PR;      // [NG][Nq][PR]
+  const float *wVq = opBase + P.off_vq + grp * Np * PRQ;        // [NG][Np][PRQ]
   // BB tables: D ids int4 [4][Np], Dvals float4 [Np], then the lift tables
   const int *bbTab = OPS_SMEM ? sTab + P.bb_off : P.tables + P.bb_off;
 
   // asynchronous copies of one tile's inputs into buffer `buf`
-  const int ntiles = cdiv(P.Kc - K0, TILE_E);
+  const int ntiles = cdiv(P.Kc - K0, E);
   const size_t sstride = (size_t)P.K * 4 * Np;  // floats per shot
   // parts of a tile's inputs: geometry + neighbour codes, state, c2
   constexpr int IN_GEO = 1, IN_Q = 2, IN_C2 = 4, IN_ALL = 7;
   auto issue_tile = [&](int vt, float *buf, int parts) {
     const int shot = vt / ntiles, tile = vt - shot * ntiles;
-    const int k0 = K0 + tile * TILE_E, ne = min(TILE_E, P.Kc - k0);
+    const int k0 = K0 + tile * E, ne = min(E, P.Kc - k0);
     float *bQ = buf + L::inQ, *bGeo = buf + L::inGeo, *bC2 = buf + L::inC2;
     int *bNbr = (int *)(buf + L::inNbr);
     if (parts & IN_GEO) {
-    for (int i = tid; i < TILE_E * 9; i += T)
+    for (int i = tid; i < E * 9; i += T)
       cp_async4(&bGeo[(i / 9) * 25 + i % 9], P.vgeo + (size_t)k0 * 9 + (i < ne * 9 ? i : 0), i < ne * 9);
-    for (int i = tid; i < TILE_E * 16; i += T)
+    for (int i = tid; i < E * 16; i += T)
       cp_async4(&bGeo[(i / 16) * 25 + 9 + i % 16], P.fgeo + (size_t)k0 * 16 + (i < ne * 16 ? i : 0),
                 i < ne * 16);
     // zero codes of absent elements: element 0, permutation 0 (the host
     // always provides that table row); their fluxes are never used
-    for (int i = tid; i < TILE_E * 4; i += T)
+    for (int i = tid; i < E * 4; i += T)
       cp_async4(&bNbr[i], P.nbr + (size_t)k0 * 4 + (i < ne * 4 ? i : 0), i < ne * 4);
     }
     if (parts & IN_Q) {
@@ -225,7 +231,7 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
 #pragma unroll 4
     for (int j = 0; j < QIT; ++j) {
       const int i = tid + j * T;
-      if (i < TILE_E * 4 * Np) {
+      if (i < E * 4 * Np) {
         const int e = i / (4 * Np), fn = i - e * (4 * Np);
         const bool ok = e < ne;
         cp_async4(&bQ[fn * ES + e], ok ? Qg + i : P.Qin, ok);
@@ -234,7 +240,7 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
     }
     if (parts & IN_C2) {
     const float *cg = P.c2q + (size_t)k0 * Nq;
-    for (int i = tid; i < TILE_E * Nq; i += T) {
+    for (int i = tid; i < E * Nq; i += T) {
       const int e = i / Nq, q = i - e * Nq;
       const bool ok = e < ne;
       cp_async4(&bC2[q * ES + e], ok ? cg + i : P.c2q, ok);
@@ -245,15 +251,15 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
   // neighbour face traces of the tile in `buf` into registers
   auto load_traces = [&](const float *buf, int vt, float (&nb)[FIT][4]) {
     const int shot = vt / ntiles, tile_of_buf = vt - shot * ntiles;
-    const int kb = K0 + tile_of_buf * TILE_E;  // first element of the tile
-    const int ne_b = min(TILE_E, P.Kc - kb);
+    const int kb = K0 + tile_of_buf * E;  // first element of the tile
+    const int ne_b = min(E, P.Kc - kb);
     const int *bNbr = (const int *)(buf + L::inNbr);
 #pragma unroll
     for (int j = 0; j < FIT; ++j) {
       const int i = tid + j * T;
       nb[j][0] = nb[j][1] = nb[j][2] = nb[j][3] = 0.f;
-      if (i < TILE_E * NF && (i & 31) < ne_b) {  // absent elements have no codes
-        const int e = i & 31, m = i >> 5, f = m / Nfp;
+      if (i < E * NF && (i & (E - 1)) < ne_b) {  // absent elements have no codes
+        const int e = i & (E - 1), m = i / E, f = m / Nfp;
         const int code = bNbr[e * 4 + f];
         const int pat = code & 255;
         const unsigned rel = (unsigned)((code >> 8) - kb);
@@ -281,8 +287,8 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
   }
   for (; vt < nvt; vt += gridDim.x) {
     const int shot = vt / ntiles, tile = vt - shot * ntiles;
-    const int k0 = K0 + tile * TILE_E;
-    const int ne = min(TILE_E, P.Kc - k0);
+    const int k0 = K0 + tile * E;
+    const int ne = min(E, P.Kc - k0);
     const int next = vt + gridDim.x;
     const size_t sbase = shot * sstride;
     float *cur = sIn + b * inSize;
@@ -299,8 +305,8 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
 #pragma unroll
     for (int j = 0; j < FIT; ++j) {
       const int i = tid + j * T;
-      if (i >= TILE_E * NF) continue;
-      const int e = i & 31, m = i >> 5, f = m / Nfp;
+      if (i >= E * NF) continue;
+      const int e = i & (E - 1), m = i / E, f = m / Nfp;
       const int code = sNbr[e * 4 + f];
       const int pat = code & 255;
       const unsigned rel = (unsigned)((code >> 8) - k0);
@@ -333,8 +339,8 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
     }
 
     // ---- 2. contravariant velocities Ur, Us, Ut into sR rows [Np, 4Np)
-    for (int i = tid; i < TILE_E * Np; i += T) {
-      const int e = i & 31, n = i >> 5;
+    for (int i = tid; i < E * Np; i += T) {
+      const int e = i & (E - 1), n = i / E;
       const float *G = sGeo + e * 25;
       const float u = sQ[(Np + n) * ES + e], v = sQ[(2 * Np + n) * ES + e],
                   w = sQ[(3 * Np + n) * ES + e];
@@ -344,10 +350,10 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
     }
     __syncthreads();
 
-    // ---- 3. volume term (registers: rows r0..r0+R of this warp, lane = element)
+    // ---- 3. volume term (registers: rows r0..r0+R of this group, thread = element)
     float rp[R], ru[R], rv[R], rw[R];
     {
-      const float *G = sGeo + lane * 25;
+      const float *G = sGeo + el * 25;
       if constexpr (!BB) {
         // rows in pairs: per pair the operator block is
         // (Dr, Dr', Ds, Ds', Dt, Dt') of rows (i, i+1)
@@ -357,9 +363,9 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
         for (int i = 0; i < R2; ++i) dr[i] = ds[i] = dt[i] = dv[i] = pair(0.f);
 #pragma unroll 2
         for (int m = 0; m < Np; ++m) {
-          const float2 pm = pair(sQ[m * ES + lane]);
-          const float2 ur = pair(sR[(Np + m) * ES + lane]), us = pair(sR[(2 * Np + m) * ES + lane]),
-                       ut = pair(sR[(3 * Np + m) * ES + lane]);
+          const float2 pm = pair(sQ[m * ES + el]);
+          const float2 ur = pair(sR[(Np + m) * ES + el]), us = pair(sR[(2 * Np + m) * ES + el]),
+                       ut = pair(sR[(3 * Np + m) * ES + el]);
           const float4 *op = reinterpret_cast<const float4 *>(wVol + m * C::P3R);
           float o[C::P3R];
 #pragma unroll
@@ -391,8 +397,8 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
         // sparse Bernstein derivative, cpp/okl/WaveKernels.okl:428-467
         const int4 *Dids = reinterpret_cast<const int4 *>(bbTab);          // [4][Np]
         const float4 *Dv = reinterpret_cast<const float4 *>(bbTab + 16 * Np);  // [Np]
-        const float *p = sQ + lane, *ur = sR + Np * ES + lane, *us = sR + 2 * Np * ES + lane,
-                    *ut = sR + 3 * Np * ES + lane;
+        const float *p = sQ + el, *ur = sR + Np * ES + el, *us = sR + 2 * Np * ES + el,
+                    *ut = sR + 3 * Np * ES + el;
 #pragma unroll
         for (int i = 0; i < R; ++i) {
           const int n = r0 + i;
@@ -427,7 +433,7 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
 
     // ---- 4. lift of the face fluxes
     {
-      const float *fgl = sGeo + lane * 25 + 9;
+      const float *fgl = sGeo + el * 25 + 9;
       if constexpr (!BB) {
 #pragma unroll 1
         for (int f = 0; f < 4; ++f) {
@@ -437,7 +443,7 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
 #pragma unroll 3
           for (int j = 0; j < Nfp; ++j) {
             const int m = f * Nfp + j;
-            const float2 pf = pair(sF[m * ES + lane]);
+            const float2 pf = pair(sF[m * ES + el]);
             const float4 *op = reinterpret_cast<const float4 *>(wLift + m * C::PR);
 #pragma unroll
             for (int q = 0; q < C::PR / 4; ++q) {
@@ -467,19 +473,19 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
         const int2 *L0p = reinterpret_cast<const int2 *>(bbTab + 20 * Np + 4);
         const int *eelPtr = bbTab + 20 * Np + 4 + 2 * Nfp * L0nnz;
         const int2 *eelP = reinterpret_cast<const int2 *>(eelPtr + ((5 * Np + 1) & ~1));
-        for (int m = warp; m < NF; m += W) {
+        for (int m = grp; m < NF; m += NG) {
           const int f = m / Nfp, nt = m - f * Nfp;
-          const float *src = sF + f * Nfp * ES + lane;
+          const float *src = sF + f * Nfp * ES + el;
           const int2 *row = L0p + nt * L0nnz;
           float v0 = 0.f, v1 = 0.f;
           int j = 0;
           for (; j + 1 < L0nnz; j += 2) {
             const int2 t0 = row[j], t1 = row[j + 1];
-            v0 += __int_as_float(t0.y) * src[t0.x];
-            v1 += __int_as_float(t1.y) * src[t1.x];
+            v0 += __int_as_float(t0.y) * src[t0.x * ES];
+            v1 += __int_as_float(t1.y) * src[t1.x * ES];
           }
-          if (j < L0nnz) v0 += __int_as_float(row[j].y) * src[row[j].x];
-          sF2[m * ES + lane] = v0 + v1;
+          if (j < L0nnz) v0 += __int_as_float(row[j].y) * src[row[j].x * ES];
+          sF2[m * ES + el] = v0 + v1;
         }
         __syncthreads();
 #pragma unroll
@@ -494,12 +500,12 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
             const int end = ptr[f + 1];
             for (; j + 3 < end; j += 4) {
               const int2 t0 = eelP[j], t1 = eelP[j + 1], t2 = eelP[j + 2], t3 = eelP[j + 3];
-              a0 += __int_as_float(t0.y) * sF2[t0.x + lane];
-              a1 += __int_as_float(t1.y) * sF2[t1.x + lane];
-              a2 += __int_as_float(t2.y) * sF2[t2.x + lane];
-              a3 += __int_as_float(t3.y) * sF2[t3.x + lane];
+              a0 += __int_as_float(t0.y) * sF2[t0.x * ES + el];
+              a1 += __int_as_float(t1.y) * sF2[t1.x * ES + el];
+              a2 += __int_as_float(t2.y) * sF2[t2.x * ES + el];
+              a3 += __int_as_float(t3.y) * sF2[t3.x * ES + el];
             }
-            for (; j < end; ++j) a0 += __int_as_float(eelP[j].y) * sF2[eelP[j].x + lane];
+            for (; j < end; ++j) a0 += __int_as_float(eelP[j].y) * sF2[eelP[j].x * ES + el];
             const float acc = (a0 + a1) + (a2 + a3);
             rp[i] += acc;
             ru[i] -= fgl[4 * f + 1] * acc;
@@ -514,10 +520,10 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
     for (int i = 0; i < R; ++i) {
       const int n = r0 + i;
       if (n < Np) {
-        sR[n * ES + lane] = rp[i];
-        sR[(Np + n) * ES + lane] = ru[i];
-        sR[(2 * Np + n) * ES + lane] = rv[i];
-        sR[(3 * Np + n) * ES + lane] = rw[i];
+        sR[n * ES + el] = rp[i];
+        sR[(Np + n) * ES + el] = ru[i];
+        sR[(2 * Np + n) * ES + el] = rv[i];
+        sR[(3 * Np + n) * ES + el] = rw[i];
       }
     }
     if (!PIPE && next < nvt) issue_tile(next, sIn, IN_GEO | IN_Q);  // sQ, sGeo, sNbr are dead
@@ -529,15 +535,15 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
     {
       // blocks of QB cubature rows: QB independent accumulators per thread,
       // one state value and QB/4 operator broadcasts per node
-      constexpr int QB = fused_vq_block(W_);
-      const int q0 = warp * RQ;
+      constexpr int QB = fused_vq_block(NG);
+      const int q0 = grp * RQ;
       for (int qb = 0; qb < RQ; qb += QB) {
         float2 acc[QB / 2];
 #pragma unroll
         for (int j = 0; j < QB / 2; ++j) acc[j] = pair(0.f);
 #pragma unroll 2
         for (int n = 0; n < Np; ++n) {
-          const float2 x = pair(sR[n * ES + lane]);
+          const float2 x = pair(sR[n * ES + el]);
           const float4 *v = reinterpret_cast<const float4 *>(wVq + n * PRQ + qb);
 #pragma unroll
           for (int j = 0; j < QB / 4; ++j) {
@@ -550,9 +556,9 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
         for (int j = 0; j < QB; ++j) {
           const int q = q0 + qb + j;
           if (qb + j < RQ && q < Nq) {
-            sQuad[q * ES + lane] = pick(acc, j) * sC2[q * ES + lane];
-            if (P.vq_out && lane < ne)
-              P.vq_out[((size_t)shot * Nq + q) * P.K + k0 + lane] = pick(acc, j);
+            sQuad[q * ES + el] = pick(acc, j) * sC2[q * ES + el];
+            if (P.vq_out && el < ne)
+              P.vq_out[((size_t)shot * Nq + q) * P.K + k0 + el] = pick(acc, j);
           }
         }
       }
@@ -562,7 +568,7 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
 
     // ---- 6. project back: rhs_p = Pq * (c2 p_q); the residual tile is
     //         fetched meanwhile for the stage update (scalar, coalesced)
-    constexpr int UIT = cdiv(TILE_E * 4 * Np, T);
+    constexpr int UIT = cdiv(E * 4 * Np, T);
     const float *resg = P.res + sbase + (size_t)k0 * 4 * Np;
     float rpre[UIT];
 #pragma unroll
@@ -576,7 +582,7 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
       for (int i = 0; i < C::PR / 2; ++i) acc2[i] = pair(0.f);
 #pragma unroll 2
       for (int q = 0; q < Nq; ++q) {
-        const float2 x = pair(sQuad[q * ES + lane]);
+        const float2 x = pair(sQuad[q * ES + el]);
         const float4 *op = reinterpret_cast<const float4 *>(wPq + q * C::PR);
 #pragma unroll
         for (int j = 0; j < C::PR / 4; ++j) {
@@ -606,7 +612,7 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
             for (int j = lo; j < j1; ++j) {
               const int rel = __ldg(P.src_elem + j) - k0;
               if (rel >= ne) break;
-              if (lane == rel) {
+              if (el == rel) {
 #pragma unroll
                 for (int i = 0; i < R; ++i)
                   if (r0 + i < Np) acc[i] += amp * __ldg(P.src_vec + (size_t)j * Np + r0 + i);
@@ -618,7 +624,7 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
       __syncthreads();  // everyone has read sR rows [0, Np) in step 5
 #pragma unroll
       for (int i = 0; i < R; ++i)
-        if (r0 + i < Np) sR[(r0 + i) * ES + lane] = acc[i];
+        if (r0 + i < Np) sR[(r0 + i) * ES + el] = acc[i];
     }
     __syncthreads();
 
@@ -657,17 +663,17 @@ __global__ void __launch_bounds__(FusedCfg<N, W_>::T, 1) k_fused_stage(FusedPara
 }
 
 // --------------------------------------------------------------- host side
-template <int N, bool BB>
+template <int N, bool BB, int E>
 static size_t smem_bytes(int Nq, bool pipe, bool ops_smem, int ops_floats, int table_ints,
                          int bb_off) {
   if (!ops_smem) table_ints = bb_off;
-  using L = FusedSmem<N, BB>;
+  using L = FusedSmem<N, BB, E>;
   return sizeof(float) * ((size_t)(pipe ? 2 : 1) * L::in_size(Nq) + L::work_size(Nq) +
                           (ops_smem ? ops_floats : 0)) +
          sizeof(int) * (size_t)table_ints;
 }
 
-template <int N, bool BB>
+template <int N, bool BB, int E>
 static bbw_status launch_fused(const FusedPlan &pl, const float *Qin, float *Qout, float *res,
                                float fa, float fb, float fdt, float cstage, cudaStream_t st) {
   FusedParams P;
@@ -690,30 +696,30 @@ static bbw_status launch_fused(const FusedPlan &pl, const float *Qin, float *Qou
   size_t sm = pl.smem;
   const int ctas = pl.max_ctas > 0 ? std::min(pl.max_ctas, pl.nsm) : pl.nsm;
   const int grid =
-      std::min(cdiv((pl.Kc > 0 ? pl.Kc : pl.K) - pl.K0, TILE_E) * std::max(pl.S, 1), ctas);
+      std::min(cdiv((pl.Kc > 0 ? pl.Kc : pl.K) - pl.K0, E) * std::max(pl.S, 1), ctas);
   if (pl.K0 > 0) {  // a window of a split stage: the single-buffered WIN variants
-    sm = smem_bytes<N, BB>(pl.Nq, false, os, pl.ops_floats, pl.table_ints, pl.bb_off);
+    sm = smem_bytes<N, BB, E>(pl.Nq, false, os, pl.ops_floats, pl.table_ints, pl.bb_off);
     if (pl.W == 8) {
-      if (os) k_fused_stage<N, BB, true, false, 8, true><<<grid, 256, sm, st>>>(P);
-      else k_fused_stage<N, BB, false, false, 8, true><<<grid, 256, sm, st>>>(P);
+      if (os) k_fused_stage<N, BB, true, false, 8, E, true><<<grid, 256, sm, st>>>(P);
+      else k_fused_stage<N, BB, false, false, 8, E, true><<<grid, 256, sm, st>>>(P);
     } else {
-      if (os) k_fused_stage<N, BB, true, false, 16, true><<<grid, 512, sm, st>>>(P);
-      else k_fused_stage<N, BB, false, false, 16, true><<<grid, 512, sm, st>>>(P);
+      if (os) k_fused_stage<N, BB, true, false, 16, E, true><<<grid, 512, sm, st>>>(P);
+      else k_fused_stage<N, BB, false, false, 16, E, true><<<grid, 512, sm, st>>>(P);
     }
     return check_launch("fused stage (window)");
   }
   if (pl.W == 8) {
     constexpr int T = 256;
-    if (os && pl.pipe) k_fused_stage<N, BB, true, true, 8><<<grid, T, sm, st>>>(P);
-    else if (os) k_fused_stage<N, BB, true, false, 8><<<grid, T, sm, st>>>(P);
-    else if (pl.pipe) k_fused_stage<N, BB, false, true, 8><<<grid, T, sm, st>>>(P);
-    else k_fused_stage<N, BB, false, false, 8><<<grid, T, sm, st>>>(P);
+    if (os && pl.pipe) k_fused_stage<N, BB, true, true, 8, E><<<grid, T, sm, st>>>(P);
+    else if (os) k_fused_stage<N, BB, true, false, 8, E><<<grid, T, sm, st>>>(P);
+    else if (pl.pipe) k_fused_stage<N, BB, false, true, 8, E><<<grid, T, sm, st>>>(P);
+    else k_fused_stage<N, BB, false, false, 8, E><<<grid, T, sm, st>>>(P);
   } else {
     constexpr int T = 512;
-    if (os && pl.pipe) k_fused_stage<N, BB, true, true, 16><<<grid, T, sm, st>>>(P);
-    else if (os) k_fused_stage<N, BB, true, false, 16><<<grid, T, sm, st>>>(P);
-    else if (pl.pipe) k_fused_stage<N, BB, false, true, 16><<<grid, T, sm, st>>>(P);
-    else k_fused_stage<N, BB, false, false, 16><<<grid, T, sm, st>>>(P);
+    if (os && pl.pipe) k_fused_stage<N, BB, true, true, 16, E><<<grid, T, sm, st>>>(P);
+    else if (os) k_fused_stage<N, BB, true, false, 16, E><<<grid, T, sm, st>>>(P);
+    else if (pl.pipe) k_fused_stage<N, BB, false, true, 16, E><<<grid, T, sm, st>>>(P);
+    else k_fused_stage<N, BB, false, false, 16, E><<<grid, T, sm, st>>>(P);
   }
   return check_launch("fused stage");
 }
@@ -722,14 +728,14 @@ static bbw_status launch_fused(const FusedPlan &pl, const float *Qin, float *Qou
 // while a plan's size depends on its mesh (the face-permutation table), so
 // every variant's limit is raised to the device maximum once: contexts on
 // different meshes then never undercut each other's launches.
-template <int N, bool BB, int W>
+template <int N, bool BB, int E, int W>
 static bbw_status set_smem_attr(int bytes) {
-  const void *fn[6] = {(const void *)k_fused_stage<N, BB, true, true, W>,
-                       (const void *)k_fused_stage<N, BB, true, false, W>,
-                       (const void *)k_fused_stage<N, BB, false, true, W>,
-                       (const void *)k_fused_stage<N, BB, false, false, W>,
-                       (const void *)k_fused_stage<N, BB, true, false, W, true>,
-                       (const void *)k_fused_stage<N, BB, false, false, W, true>};
+  const void *fn[6] = {(const void *)k_fused_stage<N, BB, true, true, W, E>,
+                       (const void *)k_fused_stage<N, BB, true, false, W, E>,
+                       (const void *)k_fused_stage<N, BB, false, true, W, E>,
+                       (const void *)k_fused_stage<N, BB, false, false, W, E>,
+                       (const void *)k_fused_stage<N, BB, true, false, W, E, true>,
+                       (const void *)k_fused_stage<N, BB, false, false, W, E, true>};
   for (const void *f : fn) {
     const bbw_status s = ensure_smem_limit(f, bytes, "fused stage attribute");
     if (s != BBW_OK) return s;
@@ -737,7 +743,7 @@ static bbw_status set_smem_attr(int bytes) {
   return BBW_OK;
 }
 
-template <int N, bool BB>
+template <int N, bool BB, int E>
 static bbw_status prepare(FusedPlan &pl) {
   int dev = 0, maxsm = 0, nsm = 0;
   cudaGetDevice(&dev);
@@ -751,21 +757,21 @@ static bbw_status prepare(FusedPlan &pl) {
   for (int c = 0; c < 4 && pick < 0; ++c) {
     if (pl.want_ops >= 0 && cand[c][0] != (pl.want_ops > 0)) continue;
     if (pl.want_pipe >= 0 && cand[c][1] != (pl.want_pipe > 0)) continue;
-    if (smem_bytes<N, BB>(pl.Nq, cand[c][1], cand[c][0], pl.ops_floats, pl.table_ints,
-                          pl.bb_off) <=
-        (size_t)maxsm)
+    if (smem_bytes<N, BB, E>(pl.Nq, cand[c][1], cand[c][0], pl.ops_floats, pl.table_ints,
+                             pl.bb_off) <= (size_t)maxsm)
       pick = c;
   }
   if (pick < 0)
     return set_error(BBW_ERR_UNSUPPORTED, "fused stage: element tile does not fit in shared memory");
   pl.ops_smem = cand[pick][0] ? pl.ops_floats : 0;
   pl.pipe = cand[pick][1];
-  pl.smem = smem_bytes<N, BB>(pl.Nq, pl.pipe, pl.ops_smem > 0, pl.ops_floats, pl.table_ints,
-                              pl.bb_off);
-  bbw_status st = pl.W == 8 ? set_smem_attr<N, BB, 8>(maxsm) : set_smem_attr<N, BB, 16>(maxsm);
+  pl.smem = smem_bytes<N, BB, E>(pl.Nq, pl.pipe, pl.ops_smem > 0, pl.ops_floats, pl.table_ints,
+                                 pl.bb_off);
+  bbw_status st =
+      pl.W == 8 ? set_smem_attr<N, BB, E, 8>(maxsm) : set_smem_attr<N, BB, E, 16>(maxsm);
   if (st != BBW_OK) return st;
   pl.nsm = nsm > 0 ? nsm : 148;
-  pl.grid = std::min(cdiv(pl.Kc > 0 ? pl.Kc : pl.K, TILE_E) * std::max(pl.S, 1), pl.nsm);
+  pl.grid = std::min(cdiv(pl.Kc > 0 ? pl.Kc : pl.K, E) * std::max(pl.S, 1), pl.nsm);
   return BBW_OK;
 }
 

@@ -8,44 +8,44 @@
 
 namespace bbw {
 
-#define BBW_DECL(n)                                                                         \
-  bbw_status fused_prepare_n##n(FusedPlan &pl);                                             \
-  bbw_status fused_launch_n##n(const FusedPlan &pl, const float *Qin, float *Qout, float *res, \
-                               float fa, float fb, float fdt, float cstage, cudaStream_t st);
+#define BBW_DECL1(n, e)                                                                     \
+  bbw_status fused_prepare_n##n##_e##e(FusedPlan &pl);                                      \
+  bbw_status fused_launch_n##n##_e##e(const FusedPlan &pl, const float *Qin, float *Qout,   \
+                                      float *res, float fa, float fb, float fdt, float cstage, \
+                                      cudaStream_t st);
+#define BBW_DECL(n) BBW_DECL1(n, 32) BBW_DECL1(n, 16)
 BBW_DECL(1) BBW_DECL(2) BBW_DECL(3) BBW_DECL(4) BBW_DECL(5) BBW_DECL(6) BBW_DECL(7) BBW_DECL(8)
 #undef BBW_DECL
+#undef BBW_DECL1
 
 int fused_default_warps(int N) { return N <= 3 ? 8 : 16; }
+// 32-element tiles up to N = 7; at N = 8 (Np = 165 and 729 cubature points
+// with the Stroud rule) the arrays of a 32-element tile exceed one SM's
+// shared memory, those of a 16-element tile fit
+int fused_default_tile(int N) { return N <= 7 ? 32 : 16; }
 
 bbw_status fused_prepare(FusedPlan &pl) {
   if (pl.W == 0) pl.W = fused_default_warps(pl.N);
-  switch (pl.N) {
-    case 1: return fused_prepare_n1(pl);
-    case 2: return fused_prepare_n2(pl);
-    case 3: return fused_prepare_n3(pl);
-    case 4: return fused_prepare_n4(pl);
-    case 5: return fused_prepare_n5(pl);
-    case 6: return fused_prepare_n6(pl);
-    case 7: return fused_prepare_n7(pl);
-    case 8: return fused_prepare_n8(pl);
-  }
+  if (pl.E == 0) pl.E = fused_default_tile(pl.N);
+  if (pl.E != 16 && pl.E != 32)
+    return set_error(BBW_ERR_ARG, "fused stage: element tile must be 16 or 32");
+  const bool e16 = pl.E == 16;
+#define CASE(n) \
+  case n: return e16 ? fused_prepare_n##n##_e16(pl) : fused_prepare_n##n##_e32(pl);
+  switch (pl.N) { CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) }
+#undef CASE
   return set_error(BBW_ERR_UNSUPPORTED, "fused stage: N out of range");
 }
 
 bbw_status fused_launch(const FusedPlan &pl, const float *Qin, float *Qout, float *res, float fa,
                         float fb, float fdt, float cstage, cudaStream_t st) {
-#define CALL(n) fused_launch_n##n(pl, Qin, Qout, res, fa, fb, fdt, cstage, st)
-  switch (pl.N) {
-    case 1: return CALL(1);
-    case 2: return CALL(2);
-    case 3: return CALL(3);
-    case 4: return CALL(4);
-    case 5: return CALL(5);
-    case 6: return CALL(6);
-    case 7: return CALL(7);
-    case 8: return CALL(8);
-  }
-#undef CALL
+  const bool e16 = pl.E == 16;
+#define CASE(n)                                                               \
+  case n:                                                                     \
+    return e16 ? fused_launch_n##n##_e16(pl, Qin, Qout, res, fa, fb, fdt, cstage, st) \
+               : fused_launch_n##n##_e32(pl, Qin, Qout, res, fa, fb, fdt, cstage, st);
+  switch (pl.N) { CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) }
+#undef CASE
   return set_error(BBW_ERR_UNSUPPORTED, "fused stage: N out of range");
 }
 

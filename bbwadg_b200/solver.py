@@ -47,6 +47,20 @@ def _i32(a):
     return np.ascontiguousarray(a, np.int32)
 
 
+def encode_config(warps, ops_in_smem, pipelined, tile=32):
+    """Configuration code of a fused-stage variant (bbw_set_config)."""
+    if tile not in (16, 32):
+        raise ValueError("tile must be 16 or 32")
+    return (int(warps) | (int(bool(ops_in_smem)) << 8) | (int(bool(pipelined)) << 9)
+            | (int(tile == 16) << 10))
+
+
+def decode_config(code):
+    """Fields of a configuration code as bbw_autotune returns it."""
+    return dict(warps=code & 255, ops_in_smem=bool(code >> 8 & 1),
+                pipelined=bool(code >> 9 & 1), tile=16 if code >> 10 & 1 else 32, code=code)
+
+
 class WaveSolver:
     """Fused-stage solver context for one mesh / operator set on the current GPU."""
 
@@ -174,17 +188,15 @@ class WaveSolver:
 
     def autotune(self, dt, stages=10):
         """Pick the fastest fused-stage variant for this mesh and batch;
-        returns dict(warps, ops_in_smem, pipelined)."""
+        returns dict(warps, ops_in_smem, pipelined, tile, code)."""
         cfg = ctypes.c_int(0)
         _lib.call("bbw_autotune", self._h, float(dt), int(stages), ctypes.byref(cfg))
-        v = cfg.value
-        return dict(warps=v & 255, ops_in_smem=bool(v >> 8 & 1), pipelined=bool(v >> 9 & 1),
-                    code=v)
+        return decode_config(cfg.value)
 
-    def set_config(self, warps, ops_in_smem, pipelined):
-        """Pin a fused-stage variant (as returned by autotune)."""
-        _lib.call("bbw_set_config", self._h,
-                  int(warps) | (int(bool(ops_in_smem)) << 8) | (int(bool(pipelined)) << 9))
+    def set_config(self, warps, ops_in_smem, pipelined, tile=32):
+        """Pin a fused-stage variant (as returned by autotune); tile is the
+        elements per tile, 32 or 16."""
+        _lib.call("bbw_set_config", self._h, encode_config(warps, ops_in_smem, pipelined, tile))
 
     def set_grid_limit(self, max_ctas):
         """Cap the persistent stage kernels at max_ctas CTAs (0: one per SM)."""

@@ -628,6 +628,7 @@ def main():
     import torch
     import torch.distributed as dist
     from bbwadg_b200 import WaveSolver, make_problem
+    from bbwadg_b200.solver import decode_config
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
@@ -649,10 +650,8 @@ def main():
         s.set_data(prob.Q0)
         tuned = None
         if prec == "fp32" and args.config:  # a pinned configuration (profiling runs)
-            c = args.config
-            s.set_config(c & 255, c >> 8 & 1, c >> 9 & 1)
-            tuned = {"warps": c & 255, "ops_in_smem": bool(c >> 8 & 1),
-                     "pipelined": bool(c >> 9 & 1), "code": c, "pinned": True}
+            tuned = dict(decode_config(args.config), pinned=True)
+            s.set_config(tuned["warps"], tuned["ops_in_smem"], tuned["pipelined"], tuned["tile"])
         elif prec == "fp32":
             tuned = s.autotune(prob.dt, 10)
         qptr, rptr, stream_ptr = s.device_state()

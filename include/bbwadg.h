@@ -285,10 +285,11 @@ bbw_status bbw_steps(bbw_ctx *ctx, float dt, int nsteps);
 bbw_status bbw_run(bbw_ctx *ctx, double final_time, float dt);
 
 /* Times every variant of the FP32 fused stage on this context's mesh, shots
- * and state (8 or 16 warps per CTA, i.e. rows per warp ceil(Np/W);
- * operators in shared or global memory; single or double-buffered input
- * tiles), `stages` launches each on scratch copies of the state, and keeps
- * the fastest.  *config (may be NULL) = W | ops_in_smem << 8 | pipelined << 9.
+ * and state (8 or 16 warps per CTA; element tiles of 32 or 16 elements, i.e.
+ * rows per thread group ceil(Np / (32 W / E)); operators in shared or global
+ * memory; single or double-buffered input tiles), `stages` launches each on
+ * scratch copies of the state, and keeps the fastest.  *config (may be NULL)
+ * = W | ops_in_smem << 8 | pipelined << 9 | (E == 16) << 10.
  * The state is not modified.  No-op for the tensor-core stage.  The
  * reference's counterpart is its hand-swept KblkV/KblkS/KblkU block sizes
  * (cpp/src/WaveOKL3d.cpp:1618-1650, cpp/profileKernels). */

@@ -99,21 +99,22 @@ def test_compute_range_is_validated(cuda):
 @pytest.mark.parametrize("variant", ["nodal", "bb"])
 @pytest.mark.parametrize("N", [3, 5])
 def test_windows_equal_whole_stage(cuda, variant, N):
-    """Element windows that start inside a 32-element tile ([0,37), [37,200),
+    """Element windows that start inside an element tile ([0,37), [37,200),
     [200,K)) advance the same elements as one whole-mesh stage, bit for bit,
-    for every fused-stage variant (warps, operators in shared memory, double
-    buffering) the device holds."""
+    for every fused-stage variant (element tile, warps, operators in shared
+    memory, double buffering) the device holds."""
     from bbwadg_b200 import RK4A, RK4B
     from bbwadg_b200._lib import BBWError
     p = make_problem(N, 4, variant=variant, c2="sine", c2_jitter=0.5, seed=11)
     ran = 0
-    for warps in (8, 16):
+    for tile in (32, 16):
+      for warps in (8, 16):
         for ops in (True, False):
             for pipe in (True, False):
                 a, b = WaveSolver(p), WaveSolver(p)
                 try:
-                    a.set_config(warps, ops, pipe)
-                    b.set_config(warps, ops, pipe)
+                    a.set_config(warps, ops, pipe, tile)
+                    b.set_config(warps, ops, pipe, tile)
                 except BBWError:  # this variant does not fit in shared memory
                     a.close(), b.close()
                     continue
@@ -123,8 +124,9 @@ def test_windows_equal_whole_stage(cuda, variant, N):
                     for k0, k1 in ((0, 37), (37, 200), (200, p.K)):
                         b.stage_part(fa, fb, p.dt, k0, k1)
                     b.stage_commit()
-                assert np.array_equal(a.get_data(), b.get_data()), (warps, ops, pipe)
-                assert np.array_equal(a.get_residual(), b.get_residual()), (warps, ops, pipe)
+                cfg = (warps, ops, pipe, tile)
+                assert np.array_equal(a.get_data(), b.get_data()), cfg
+                assert np.array_equal(a.get_residual(), b.get_residual()), cfg
                 a.close(), b.close()
                 ran += 1
-    assert ran >= 2
+    assert ran >= 4

@@ -118,33 +118,34 @@ def test_nodal_and_bb_agree(cuda):
 @pytest.mark.parametrize("N", [3, 5])
 @pytest.mark.parametrize("variant", ["nodal", "bb"])
 def test_every_stage_configuration_matches_oracle(cuda, N, variant):
-    """All warps-per-CTA / operator-placement / pipelining variants the
-    autotuner chooses from give the restatement's result; the autotuner
-    keeps one of them and leaves the state untouched."""
+    """All element-tile / warps-per-CTA / operator-placement / pipelining
+    variants the autotuner chooses from give the restatement's result; the
+    autotuner keeps one of them and leaves the state untouched."""
     from oracle import Oracle
     from bbwadg_b200._lib import BBWError
     p = make_problem(N, 3, variant=variant, c2="sine", c2_jitter=0.5, seed=3)
     q_ref, _ = Oracle(N, p.K, p.ops_dict(), p.geo_dict(), variant=variant).run(p.Q0.copy(), p.dt, 10)
     ran = 0
-    for warps in (8, 16):
+    for tile in (32, 16):
+      for warps in (8, 16):
         for ops in (True, False):
             for pipe in (True, False):
                 s = WaveSolver(p)
                 try:
-                    s.set_config(warps, ops, pipe)
+                    s.set_config(warps, ops, pipe, tile)
                 except BBWError:
                     s.close()
                     continue
                 s.set_data(p.Q0)
                 s.steps(p.dt, 2)
-                assert rel_l2(s.get_data(), q_ref) < TOL, (warps, ops, pipe)
+                assert rel_l2(s.get_data(), q_ref) < TOL, (warps, ops, pipe, tile)
                 s.close()
                 ran += 1
-    assert ran >= 4
+    assert ran >= 8
     s = WaveSolver(p)
     s.set_data(p.Q0)
     cfg = s.autotune(p.dt, 5)
-    assert cfg["warps"] in (8, 16)
+    assert cfg["warps"] in (8, 16) and cfg["tile"] in (16, 32)
     assert np.array_equal(s.get_data(), p.Q0.astype(np.float32))
     s.steps(p.dt, 2)
     assert rel_l2(s.get_data(), q_ref) < TOL
@@ -255,16 +256,34 @@ def test_fused_n6_matches_oracle(cuda, variant, rule):
     assert rel_l2(q, q_ref) < TOL
 
 
-def test_fused_n8_with_729_point_rule_is_refused(cuda):
+@pytest.mark.parametrize("variant", ["nodal", "bb"])
+def test_fused_n8_on_16_element_tiles(cuda, variant):
     """N = 8 with the 729-point Stroud rule: a 32-element tile's cubature
-    arrays alone exceed one SM's shared memory, so the context is refused
-    (BBW_ERR_UNSUPPORTED) rather than run out of bounds; the kernel-level
-    entry points still take it."""
+    arrays alone exceed one SM's shared memory, so the context runs 16-element
+    tiles (operators read through the cache).  2^3 x 6 tets = 3 tiles, on the
+    full grid and on one CTA walking all three; the 32-element variants are
+    refused rather than run out of bounds, and the autotuner keeps a
+    16-element one."""
+    from oracle import Oracle
     from bbwadg_b200._lib import BBWError
-    p = make_problem(8, 2, variant="nodal", c2="sine", seed=3)
-    assert p.Nq == 729
-    with pytest.raises(BBWError, match="shared memory"):
-        WaveSolver(p)
+    p = make_problem(8, 2, variant=variant, c2="sine", c2_jitter=0.5, seed=3)
+    assert p.Nq == 729 and p.K == 48
+    q_ref, _ = Oracle(8, p.K, p.ops_dict(), p.geo_dict(), variant=variant).run(p.Q0.copy(), p.dt, 10)
+    s = WaveSolver(p)
+    for limit in (0, 1):
+        s.set_grid_limit(limit)
+        s.set_data(p.Q0)
+        s.steps(p.dt, 2)
+        assert rel_l2(s.get_data(), q_ref) < TOL, limit
+    for warps in (8, 16):
+        with pytest.raises(BBWError, match="shared memory"):
+            s.set_config(warps, False, False, 32)
+    s.set_data(p.Q0)
+    cfg = s.autotune(p.dt, 3)
+    assert cfg["tile"] == 16
+    s.steps(p.dt, 2)
+    assert rel_l2(s.get_data(), q_ref) < TOL
+    s.close()
 
 
 @pytest.mark.parametrize("form", ["fp32", "f16x3"])

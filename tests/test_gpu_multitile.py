@@ -37,27 +37,29 @@ def oracle_run(p, stages, Q0=None):
     return [orc.run(q.copy(), p.dt, stages)[0] for q in Q0]
 
 
-CONFIGS = [(w, ops, pipe) for w in (8, 16) for ops in (True, False) for pipe in (True, False)]
+CONFIGS = [(w, ops, pipe, tile) for tile in (32, 16) for w in (8, 16) for ops in (True, False)
+           for pipe in (True, False)]
 
 
 @pytest.mark.parametrize("N", [3, 5])
 @pytest.mark.parametrize("variant", ["nodal", "bb"])
 def test_every_configuration_over_many_tiles(cuda, N, variant):
-    """10^3 x 6 tets (K = 6000, 188 tiles on 148 CTAs) with the full grid,
-    and the same mesh on 7 CTAs (27 tiles each), for every warps /
-    operator-placement / buffering variant the autotuner can pick
-    (including the single-buffered form the N = 5 headline runs)."""
+    """10^3 x 6 tets (K = 6000: 188 tiles of 32 or 375 tiles of 16 elements
+    on 148 CTAs) with the full grid, and the same mesh on 7 CTAs (27 or 54
+    tiles each), for every element-tile / warps / operator-placement /
+    buffering variant the autotuner can pick (including the single-buffered
+    form the N = 5 headline runs)."""
     cub, tri = ref_rule(N)
     p = make_problem(N, 10, variant=variant, c2="sine", c2_jitter=0.5, seed=11, cubature=cub,
                      tri_cubature=tri)
     assert p.K == 6000
     q_ref = oracle_run(p, 10)
     ran = []
-    for warps, ops, pipe in CONFIGS:
+    for warps, ops, pipe, tile in CONFIGS:
         for limit in (0, 7):
             s = WaveSolver(p)
             try:
-                s.set_config(warps, ops, pipe)
+                s.set_config(warps, ops, pipe, tile)
             except BBWError:  # does not fit in shared memory
                 s.close()
                 break
@@ -66,17 +68,18 @@ def test_every_configuration_over_many_tiles(cuda, N, variant):
             s.steps(p.dt, 2)
             err = rel_l2(s.get_data(), q_ref)
             s.close()
-            assert err < TOL, (warps, ops, pipe, limit, err)
-            ran.append((warps, ops, pipe, limit))
-    assert len(ran) >= 8, ran
-    if N == 5:  # the headline form: 8 warps, operators in shared memory, one buffer
-        assert (8, True, False, 0) in ran
+            assert err < TOL, (warps, ops, pipe, tile, limit, err)
+            ran.append((warps, ops, pipe, tile, limit))
+    assert len(ran) >= 16, ran
+    if N == 5:  # the FP32 autotuned form: 8 warps, operators in shared memory, one buffer
+        assert (8, True, False, 32, 0) in ran
 
 
 @pytest.mark.parametrize("variant", ["nodal", "bb"])
 def test_shots_over_many_tiles_on_a_capped_grid(cuda, variant):
-    """Three shots of a 6^3 x 6 mesh (41 tiles each, 123 work items) on 5
-    CTAs: every CTA's loop crosses shot boundaries and ragged last tiles."""
+    """Three shots of a 6^3 x 6 mesh (41 tiles of 32 or 81 of 16 elements
+    each) on 5 CTAs: every CTA's loop crosses shot boundaries and ragged
+    last tiles."""
     N = 4
     cub, tri = ref_rule(N)
     p = make_problem(N, 6, variant=variant, c2="sine", c2_jitter=0.5, seed=4, cubature=cub,
@@ -86,10 +89,10 @@ def test_shots_over_many_tiles_on_a_capped_grid(cuda, variant):
     Q0 = np.stack([p.Q0 * (1.0 - 0.3 * i) + 0.01 * rng.standard_normal(p.Q0.size)
                    for i in range(S)]).astype(np.float32)
     refs = oracle_run(p, 10, Q0=Q0)
-    for warps, ops, pipe in CONFIGS:
+    for warps, ops, pipe, tile in CONFIGS:
         s = WaveSolver(p)
         try:
-            s.set_config(warps, ops, pipe)
+            s.set_config(warps, ops, pipe, tile)
         except BBWError:
             s.close()
             continue
@@ -100,7 +103,7 @@ def test_shots_over_many_tiles_on_a_capped_grid(cuda, variant):
         out = s.get_data().reshape(S, -1)
         s.close()
         for i in range(S):
-            assert rel_l2(out[i], refs[i]) < TOL, (warps, ops, pipe, i)
+            assert rel_l2(out[i], refs[i]) < TOL, (warps, ops, pipe, tile, i)
 
 
 @pytest.mark.parametrize("prec,tol", [("f16x3", TOL), ("bf16x3", BF16X3_TOL)])
