@@ -25,33 +25,40 @@
 // padding of the element operands (B) in exact zero products.
 //
 // Work items are (shot, tile of 32 elements); a persistent CTA walks them
-// with a grid stride and keeps two in flight in one instruction stream:
+// with a grid stride.  Its 16 warps form two groups that work on different
+// items at the same time and meet only through mbarriers:
 //
-//   a. epilogue 1 of tile T: rhs of u, v, w and the LSRK update of u, v, w
-//      from the gradient / divergence / lift accumulators; rhs_p split into
-//      the B operand of Vq; issue the Vq MMAs
-//   b. while they run: tile T+1 (its bulk copies were issued one tile
-//      earlier) - neighbour traces, upwind flux, B operands of its first
-//      MMA group
-//   c. epilogue 2 of T: c^2 / J at the cubature points -> B operand of Pq;
-//      issue the Pq MMAs of T, the first MMA group of T+1, the bulk copies
-//      of T+2
-//   d. epilogue 3 of T: rhs_p, sources, LSRK update of p, while T+1's MMAs
-//      run.
+//   producer (warps 8-15), item T+1: neighbour traces, upwind flux, p and
+//     the contravariant velocities -> split B operands of the first MMA
+//     group (gradient, divergence, lift); then the bulk copies of item T+2
+//     and the first MMA group of T+1, issued from lane 0 of four warps
+//   epilogue (warps 0-7), item T: first-group accumulators -> rhs and LSRK
+//     update of u, v, w; rhs_p split -> Vq MMAs; c^2 / J at the cubature
+//     points split -> Pq MMAs; rhs_p, sources, LSRK update of p
+//
+// Handshakes: copies landed (mbT), first group done (mbM), Vq / Pq done
+// (mbW), first-group accumulators read out (mbF) and geometry buffer read
+// out (mbG); the producer passes each item's B1 scales through a tagged
+// shared-memory slot.  Within a group, named barriers (1: epilogue, 2:
+// producer) carry the per-tile maxima of the power-of-two scaling.
 //
 // TMEM (512 columns): [0,96) gradient r,s,t, [96,128) divergence,
 // [128,256) lift per face, [256,288) Vq, [288,320) Pq.  For M = 64 an
-// accumulator row m lives in lane (m % 16) + 32 (m / 16); the epilogues read
+// accumulator row m lives in lane (m % 16) + 32 (m / 16); the epilogue reads
 // those with the 16x64b shape, so all 32 threads of a warp hold a (row,
-// element) pair.  The LSRK update reads the old state and residual from
-// global memory (L2), so the state tile in shared memory is free for the
-// next copies as soon as the tile's B operands are built.
+// element) pair; epilogue warp w reads sub-partition w % 4 and elements
+// 16 (w / 4) .. 16 (w / 4) + 15.  The LSRK update reads the old state and
+// residual from global memory (L2, prefetched one item ahead), so the state
+// tile in shared memory is free for the next copies as soon as the
+// producer has built its B operands.
 //
-// Every mbarrier wait is bounded.  A wait that gives up sets a warp-uniform
-// failure flag; the thread then skips every access that depends on the
-// awaited data, the CTA votes at its next barrier, issues no further copy or
-// MMA and leaves the loop; thread 0 waits (bounded) for what it still has
-// in flight before the TMEM is freed and the error flag is raised.
+// Every mbarrier wait is bounded.  A wait that gives up records the failure
+// (per thread, warp-uniform where warp-collective TMEM loads follow, and in
+// a shared flag); the thread skips every access that depends on the awaited
+// data, its group leaves the loop at its next named-barrier vote, a waiting
+// partner group runs out of its own bounded waits, and thread 0 waits
+// (bounded) for the copies and MMAs still in flight before the TMEM is
+// freed and the error flag is raised.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -87,9 +94,10 @@ struct TcCfg {
   // lane-per-element reads of one node hit distinct bank groups
   static constexpr int RS = (Np % 2) ? 4 * Np : 4 * Np + 4;
   static constexpr bool V4 = Np % 4 == 0;  // field rows 16-byte aligned in the raw tile
-  // flux items with lane = face node: (element, face) pairs per warp
-  static constexpr int FPW = (4 * TC_E) / (TC_T / 32);
-  static_assert((4 * TC_E) % (TC_T / 32) == 0, "face pairs per warp");
+  // flux items with lane = face node: the 4 TC_E (element, face) pairs of
+  // a tile over the 8 producer warps, in two halves of FPW pairs each
+  static constexpr int FPW = (4 * TC_E) / 16;
+  static_assert((4 * TC_E) % 16 == 0, "face pairs per producer warp and half");
   static_assert(NFP(N) <= 32, "one face per warp pass");
   static_assert(Np <= 64, "tensor-core stage: Np <= 64 (operator rows of one M = 64 MMA)");
 };
@@ -132,7 +140,7 @@ TcLayout tc_layout(int N, int Nq, int table_ints) {
   L.tab = o;
   o = al(o + 4 * table_ints);
   L.misc = o;
-  o = al(o + 128);
+  o = al(o + 256);
   L.total = o;
   return L;
 }
@@ -239,6 +247,28 @@ __device__ __forceinline__ float tc_ricker(float t, float f0, float tR, float am
 __device__ __forceinline__ int ep_row(int lane) { return (lane >> 2) + 8 * (lane & 1); }
 __device__ __forceinline__ int ep_col(int lane, int j) { return 2 * j + ((lane >> 1) & 1); }
 
+__device__ __forceinline__ void mbar_arrive1(uint64_t *mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(tc::smem_u32(mbar)) : "memory");
+}
+// group barriers: the epilogue warps (0-7) use named barrier 1, the
+// producer warps (8-15) barrier 2; __syncthreads keeps barrier 0
+__device__ __forceinline__ void group_sync(int id) {
+  asm volatile("bar.sync %0, 256;\n" ::"r"(id) : "memory");
+}
+// group barrier with an OR vote over the group's threads
+__device__ __forceinline__ bool group_sync_or(int id, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 q, %1, 0;\n\t"
+      "bar.red.or.pred p, %2, 256, q;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(id)
+      : "memory");
+  return r != 0;
+}
+
 template <int N, bool BF>
 __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
   // operand type; A and B of every MMA share it (the instruction descriptor
@@ -247,7 +277,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
   constexpr int FMT = BF ? 1 : 0;
   using C = TcCfg<N>;
   constexpr int Np = C::Np, Nfp = C::Nfp, KV = C::KV, KF = C::KF, RS = C::RS;
-  constexpr int FPW = C::FPW;
+  constexpr int FPW = C::FPW;  // flux items per producer warp and half
   extern __shared__ __align__(1024) unsigned char smem[];
   const TcLayout &L = P.L;
   const int KQ = L.KQ, MQ = L.MQ, MR = L.MR, MRQ = L.MRQ, Nq = P.Nq;
@@ -260,25 +290,33 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
   float *sGeoB = reinterpret_cast<float *>(smem + L.geo);
   int *sNbr = reinterpret_cast<int *>(smem + L.nbr);
   int *sTab = reinterpret_cast<int *>(smem + L.tab);
-  uint64_t *mbT = reinterpret_cast<uint64_t *>(smem + L.misc);  // tile copies
-  uint64_t *mbM = mbT + 1;                                      // gradient/divergence/lift MMAs
-  uint64_t *mbW = mbT + 2;                                      // Vq, Pq MMAs
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(mbT + 3);
-  int *sRed = reinterpret_cast<int *>(tslot + 1);  // [5] maxima as float bits
-  int *sPend = sRed + 5;  // [6] thread 0's copies / MMAs in flight and their phases
+  uint64_t *mbT = reinterpret_cast<uint64_t *>(smem + L.misc);  // tile copies landed
+  uint64_t *mbM = mbT + 1;  // gradient/divergence/lift MMAs done (3 commits)
+  uint64_t *mbW = mbT + 2;  // Vq / Pq MMAs done
+  uint64_t *mbF = mbT + 3;  // first-group accumulators read out (8 epilogue warps)
+  uint64_t *mbG = mbT + 4;  // geometry buffer read out (8 epilogue warps)
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(mbT + 5);
+  int *sRed = reinterpret_cast<int *>(tslot + 1);  // [10] maxima as float bits
+  int *sPend = sRed + 10;                          // [6] copies / MMAs in flight, phases
+  volatile int *sFail = sPend + 6;                 // any wait gave up
+  volatile int *sTag = sFail + 1;                  // [2] tile of the scales in slot
+  float *sScale = reinterpret_cast<float *>(sPend + 9);  // [2][3] B1 scales per slot
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int q4 = warp & 3, g8 = warp >> 2;  // TMEM sub-partition, element group of 8
-  // single-thread issue work is spread over lane 0 of five warps, so that no
-  // warp carries all of it between two barriers: gradient / divergence /
-  // lift MMAs (each chain in issue order from one thread), Vq and Pq MMAs,
-  // bulk copies and L2 prefetches
-  constexpr int I_GRAD = 0, I_DIV = 32, I_LIFT = 64, I_WADG = 96, I_COPY = 128;
+  const bool isEpi = warp < 8;
+  // epilogue warps: TMEM sub-partition q4, element half eh (columns 16 eh ..)
+  const int q4 = warp & 3, eh = (warp >> 2) & 1;
+  const int ptid = tid - 256;  // producer thread index (0..255)
+  // single-thread issuers: first-group MMA chains on lane 0 of producer
+  // warps 8, 9, 10, bulk copies on warp 11; Vq / Pq on epilogue warp 0
+  constexpr int I_GRAD = 256, I_DIV = 288, I_LIFT = 320, I_COPY = 352, I_WADG = 0;
 
   // ---------------------------------------------------------------- setup
   if (tid == 0) {
     tc::mbar_init(mbT, 1);
-    tc::mbar_init(mbM, 3);  // one commit from each of the three issuing threads
+    tc::mbar_init(mbM, 3);
     tc::mbar_init(mbW, 1);
+    tc::mbar_init(mbF, 8);
+    tc::mbar_init(mbG, 8);
     tc::fence_mbar_init();
   }
   if (warp == 0) {
@@ -291,7 +329,9 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
   for (int i = tid; i < (L.raw - L.Bp) / 16; i += TC_T)  // B operands: zero padding
     reinterpret_cast<uint4 *>(smem + L.Bp)[i] = make_uint4(0, 0, 0, 0);
   for (int i = tid; i < TC_E * RS; i += TC_T) sRaw[i] = 0.f;  // absent elements stay finite
-  if (tid < 11) sRed[tid] = 0;
+  if (tid < 10) sRed[tid] = 0;
+  if (tid < 6) sPend[tid] = 0;
+  if (tid == 0) *sFail = 0, sTag[0] = sTag[1] = -1;
   tc::fence_proxy_async();
   tc::fence_before_sync();
   __syncthreads();
@@ -302,56 +342,15 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
   const int ntiles = cdv(P.K, TC_E);
   const int nvt = P.S * ntiles;
   const size_t sstride = (size_t)P.K * 4 * Np;  // floats per shot
-  // TMEM address of this warp's M = 64 rows (sub-partition q4) and elements
-  const uint32_t tsub = tbase + ((uint32_t)(32 * q4) << 16) + 8 * g8;
-  const int rowM = 16 * q4 + ep_row(lane);  // M = 64 accumulator row of this thread
-  const bool rowok = rowM < Np;
-
   bool fail = false;
-  uint32_t tphase = 0, mphase = 0, wphase = 0;
 
-  // I_COPY: bulk copies of a work item's inputs (state rows of its shot,
-  // geometry, neighbour codes) into the raw tile and geometry buffer gb
-  auto issue_tma = [&](int vt, int gb) {
-    const int shot = vt / ntiles, k0 = (vt - shot * ntiles) * TC_E, ne = min(TC_E, P.K - k0);
-    const uint32_t bytes = (uint32_t)ne * (4 * Np * 4 + TC_GEO * 4 + 16);
-    tc::mbar_expect_tx(mbT, bytes);
-    const float *q = P.Qin + shot * sstride + (size_t)k0 * 4 * Np;
-    for (int e = 0; e < ne; ++e)
-      tc::bulk_g2s(sRaw + e * RS, q + (size_t)e * 4 * Np, 4 * Np * 4, mbT);
-    tc::bulk_g2s(sGeoB + gb * TC_E * TC_GEO, P.geo + (size_t)k0 * TC_GEO, ne * TC_GEO * 4, mbT);
-    tc::bulk_g2s(sNbr, P.nbr + (size_t)k0 * 4, ne * 16, mbT);
-    sPend[0] = 1, sPend[1] = (int)tphase;  // in flight, awaited with this parity
-  };
-  // I_COPY: L2 prefetch of the blocks the epilogues of a work item read
-  // from global memory (old residual and state, c^2 at the cubature points)
-  auto prefetch_item = [&](int vt) {
-    const int shot = vt / ntiles, k0 = (vt - shot * ntiles) * TC_E, ne = min(TC_E, P.K - k0);
-    const size_t off = shot * sstride + (size_t)k0 * 4 * Np;
-    tc::prefetch_l2(P.res + off, ne * 4 * Np * 4);
-    tc::prefetch_l2(P.Qin + off, ne * 4 * Np * 4);
-    const uint32_t cb = (uint32_t)(ne * Nq * 4) & ~15u;
-    if (cb) tc::prefetch_l2(P.c2q + (size_t)k0 * Nq, cb);
-  };
-  // bounded wait; the thread `owner` clears sPend[pend] on success
-  auto wait_bar = [&](uint64_t *bar, uint32_t &ph, int pend, int owner) {
-    const bool ok = tc::mbar_wait(bar, ph, TC_WAIT);
-    if (ok && tid == owner) sPend[pend] = 0;
-    fail = __any_sync(0xffffffffu, fail || !ok);
-    ph ^= 1u;
+  // bounded wait of one thread; a miss is recorded for the group votes
+  auto wait1 = [&](uint64_t *bar, uint32_t parity) -> bool {
+    const bool ok = tc::mbar_wait(bar, parity, TC_WAIT);
+    if (!ok) fail = true, *sFail = 1;
     tc::fence_after_sync();
+    return ok;
   };
-  // generic smem writes -> tensor core, with the CTA-wide failure vote
-  auto sync_for_mma = [&]() -> bool {
-    tc::fence_proxy_async();
-    tc::fence_before_sync();
-    const bool any = __syncthreads_or(fail);
-    tc::fence_after_sync();
-    return any;
-  };
-  // one operator/operand product chain: D (+)= A B^T over ksteps, 3 products;
-  // descriptors of consecutive K steps differ only in the start-address
-  // field (+256 bytes = +16 in 16-byte units)
   auto chain = [&](uint32_t d, const E *Ahi, const E *Alo, int asbo, const E *Bhi,
                    const E *Blo, int bsbo, int ksteps, uint32_t idesc, bool acc) {
     uint64_t ah = tc::smem_desc(tc::smem_u32(Ahi), 128, asbo);
@@ -365,395 +364,525 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       ah += 16, al += 16, bh += 16, bl += 16;
     }
   };
-  // I_GRAD / I_DIV / I_LIFT: their part of the gradient, divergence and
-  // lift products of the B1 operands, each committed to mbM
-  auto issue_mma1 = [&]() {
-    const uint32_t id64 = tc::idesc_f16(64, TC_E, FMT);
-    const int sboV = (KV / 8) * 128, sboF = (KF / 8) * 128;
-    const int pD = MR * KV, pL = MR * KF;  // plane sizes (halves)
-    if (tid == I_GRAD) {
-      for (int d = 0; d < 3; ++d)
-        chain(tbase + cGrad + 32 * d, sOps + L.oD + 2 * d * pD, sOps + L.oD + (2 * d + 1) * pD,
-              sboV, sBp, sBp + TC_E * KV, sboV, KV / 16, id64, false);
-      sPend[2] = 1, sPend[3] = (int)mphase;
-    } else if (tid == I_DIV) {
-      for (int d = 0; d < 3; ++d)
-        chain(tbase + cDiv, sOps + L.oD + 2 * d * pD, sOps + L.oD + (2 * d + 1) * pD, sboV,
-              sBU + 2 * d * TC_E * KV, sBU + (2 * d + 1) * TC_E * KV, sboV, KV / 16, id64, d > 0);
-    } else {
-      for (int f = 0; f < 4; ++f)
-        chain(tbase + cLift + 32 * f, sOps + L.oL + 2 * f * pL, sOps + L.oL + (2 * f + 1) * pL,
-              sboF, sBF + 2 * f * TC_E * KF, sBF + (2 * f + 1) * TC_E * KF, sboF, KF / 16, id64,
-              false);
-    }
-    tc::mma_commit(mbM);
-  };
-  auto mma1_issuer = [&]() { return tid == I_GRAD || tid == I_DIV || tid == I_LIFT; };
 
-  // neighbour face traces of the work item in the raw tile, outside the
-  // tile, into registers.  Lane = face node, warp = (element, face) pairs:
-  // one load instruction reads the face of a single neighbour.
-  float nbv[FPW][4];
-  auto load_traces = [&](int vt) {
-    const int shot = vt / ntiles, k0 = (vt - shot * ntiles) * TC_E, ne = min(TC_E, P.K - k0);
-    const float *q = P.Qin + shot * sstride;
-#pragma unroll
-    for (int j = 0; j < FPW; ++j) {
-      nbv[j][0] = nbv[j][1] = nbv[j][2] = nbv[j][3] = 0.f;
-      const int pp = warp * FPW + j, e = pp >> 2, f = pp & 3;
-      if (lane >= Nfp || e >= ne) continue;
-      const int code = sNbr[e * 4 + f];
-      const int pat = code & 255;
-      if (pat == 255) continue;
-      const unsigned rel = (unsigned)((code >> 8) - k0);
-      if (rel < (unsigned)ne) continue;
-      const float *o = q + (size_t)(code >> 8) * 4 * Np + sPat[pat * Nfp + lane];
-      nbv[j][0] = __ldg(o), nbv[j][1] = __ldg(o + Np), nbv[j][2] = __ldg(o + 2 * Np),
-      nbv[j][3] = __ldg(o + 3 * Np);
+  if (!isEpi) {
+    // ============================================================ producer
+    // per work item: neighbour traces, upwind flux, p and contravariant
+    // velocities -> split B operands of the first MMA group; then the bulk
+    // copies of the next item and the first MMA group of this one
+    const int pw = warp - 8;
+    auto issue_tma = [&](int vt, int gb, uint32_t ph) {
+      const int shot = vt / ntiles, k0 = (vt - shot * ntiles) * TC_E, ne = min(TC_E, P.K - k0);
+      const uint32_t bytes = (uint32_t)ne * (4 * Np * 4 + TC_GEO * 4 + 16);
+      tc::mbar_expect_tx(mbT, bytes);
+      const float *q = P.Qin + shot * sstride + (size_t)k0 * 4 * Np;
+      for (int e = 0; e < ne; ++e)
+        tc::bulk_g2s(sRaw + e * RS, q + (size_t)e * 4 * Np, 4 * Np * 4, mbT);
+      tc::bulk_g2s(sGeoB + gb * TC_E * TC_GEO, P.geo + (size_t)k0 * TC_GEO, ne * TC_GEO * 4, mbT);
+      tc::bulk_g2s(sNbr, P.nbr + (size_t)k0 * 4, ne * 16, mbT);
+      sPend[0] = 1, sPend[1] = (int)ph;
+    };
+    auto prefetch_item = [&](int vt) {
+      const int shot = vt / ntiles, k0 = (vt - shot * ntiles) * TC_E, ne = min(TC_E, P.K - k0);
+      const size_t off = shot * sstride + (size_t)k0 * 4 * Np;
+      tc::prefetch_l2(P.res + off, ne * 4 * Np * 4);
+      tc::prefetch_l2(P.Qin + off, ne * 4 * Np * 4);
+      const uint32_t cb = (uint32_t)(ne * Nq * 4) & ~15u;
+      if (cb) tc::prefetch_l2(P.c2q + (size_t)k0 * Nq, cb);
+    };
+    // L2 prefetch of the blocks a later item's bulk copies read, one item
+    // ahead of them (the copies of an item are issued only once the raw
+    // tile is free, just before the item is needed)
+    auto prefetch_copies = [&](int vt) {
+      const int shot = vt / ntiles, k0 = (vt - shot * ntiles) * TC_E, ne = min(TC_E, P.K - k0);
+      tc::prefetch_l2(P.Qin + shot * sstride + (size_t)k0 * 4 * Np, ne * 4 * Np * 4);
+      tc::prefetch_l2(P.geo + (size_t)k0 * TC_GEO, ne * TC_GEO * 4);
+      tc::prefetch_l2(P.nbr + (size_t)k0 * 4, ne * 16);
+    };
+    if (ptid == I_COPY - 256 && (int)blockIdx.x < nvt) {
+      issue_tma(blockIdx.x, 0, 0);
+      prefetch_item(blockIdx.x);
+      if ((int)(blockIdx.x + gridDim.x) < nvt) prefetch_copies(blockIdx.x + gridDim.x);
     }
-  };
-
-  // producer: p, contravariant velocities and upwind flux of the work item
-  // in the raw tile -> B operands of the first MMA group; sets the scales;
-  // returns the CTA-wide failure vote
-  float sp = 1.f, sU = 1.f, sF = 1.f;
-  auto produce = [&](int vt, int gb) -> bool {
-    const int shot = vt / ntiles, k0 = (vt - shot * ntiles) * TC_E, ne = min(TC_E, P.K - k0);
-    (void)shot;
-    const float *sGeo = sGeoB + gb * TC_E * TC_GEO;
-    constexpr int NC = KV / 4;               // node chunks incl. padding
-    const int ce = tid & 31, cc = tid >> 5;  // item (chunk cc, element ce); TC_T = 16 * 32
-    float4 p4 = make_float4(0.f, 0.f, 0.f, 0.f), U4[3];
-    U4[0] = U4[1] = U4[2] = p4;
-    float mp = 0.f, mU = 0.f, mF = 0.f;
-    float pf[FPW];
-#pragma unroll
-    for (int j = 0; j < FPW; ++j) pf[j] = 0.f;
-    if (!fail) {
-      if (cc < NC && 4 * cc < Np && ce < ne) {
-        const float4 g0 = *reinterpret_cast<const float4 *>(sGeo + ce * TC_GEO + 16);
-        const float4 g1 = *reinterpret_cast<const float4 *>(sGeo + ce * TC_GEO + 20);
-        const float G[9] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w,
-                            sGeo[ce * TC_GEO + 24]};
-        const float *rr = sRaw + ce * RS + 4 * cc;
-        float4 u4, v4, w4;
-        if constexpr (C::V4) {
-          p4 = *reinterpret_cast<const float4 *>(rr);
-          u4 = *reinterpret_cast<const float4 *>(rr + Np);
-          v4 = *reinterpret_cast<const float4 *>(rr + 2 * Np);
-          w4 = *reinterpret_cast<const float4 *>(rr + 3 * Np);
-        } else {  // field rows not 16-byte aligned; nodes past Np read as zero
-          float a[4][4];
-#pragma unroll
-          for (int fl = 0; fl < 4; ++fl)
-#pragma unroll
-            for (int i = 0; i < 4; ++i) a[fl][i] = (4 * cc + i < Np) ? rr[fl * Np + i] : 0.f;
-          p4 = make_float4(a[0][0], a[0][1], a[0][2], a[0][3]);
-          u4 = make_float4(a[1][0], a[1][1], a[1][2], a[1][3]);
-          v4 = make_float4(a[2][0], a[2][1], a[2][2], a[2][3]);
-          w4 = make_float4(a[3][0], a[3][1], a[3][2], a[3][3]);
-        }
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          U4[d].x = u4.x * G[3 * d] + v4.x * G[3 * d + 1] + w4.x * G[3 * d + 2];
-          U4[d].y = u4.y * G[3 * d] + v4.y * G[3 * d + 1] + w4.y * G[3 * d + 2];
-          U4[d].z = u4.z * G[3 * d] + v4.z * G[3 * d + 1] + w4.z * G[3 * d + 2];
-          U4[d].w = u4.w * G[3 * d] + v4.w * G[3 * d + 1] + w4.w * G[3 * d + 2];
-          mU = fmaxf(mU, fmaxf(fmaxf(fabsf(U4[d].x), fabsf(U4[d].y)),
-                               fmaxf(fabsf(U4[d].z), fabsf(U4[d].w))));
-        }
-        mp = fmaxf(fmaxf(fabsf(p4.x), fabsf(p4.y)), fmaxf(fabsf(p4.z), fabsf(p4.w)));
+    int it = 0;
+    for (int vt = blockIdx.x; vt < nvt; vt += gridDim.x, ++it) {
+      const int shot = vt / ntiles, k0 = (vt - shot * ntiles) * TC_E, ne = min(TC_E, P.K - k0);
+      const int gb = it & 1, next = vt + gridDim.x;
+      const float *sGeo = sGeoB + gb * TC_E * TC_GEO;
+      const float *qs = P.Qin + shot * sstride;
+      // the item's copies
+      {
+        const bool ok = tc::mbar_wait(mbT, (uint32_t)(it & 1), TC_WAIT);
+        if (!ok) fail = true, *sFail = 1;
+        else if (ptid == I_COPY - 256) sPend[0] = 0;
+        tc::fence_after_sync();
       }
-      // upwind flux (Uflux = -pflux), lane = face node
+      // state part: item (chunk cc, element ce), two per thread
+      constexpr int NC = KV / 4;
+      float4 p4[2], U4[2][3];
+      float mp = 0.f, mU = 0.f, mF = 0.f;
+      float pf[2 * FPW];
 #pragma unroll
-      for (int j = 0; j < FPW; ++j) {
-        const int pp = warp * FPW + j, e = pp >> 2, f = pp & 3;
-        if (lane >= Nfp || e >= ne) continue;
-        const int m = f * Nfp + lane;
-        const int code = sNbr[e * 4 + f];
-        const int pat = code & 255;
-        const int vM = sFmask[m];
-        const float *own = sRaw + e * RS + vM;
-        const float pM = own[0], uM = own[Np], vvM = own[2 * Np], wM = own[3 * Np];
-        const float4 fg = *reinterpret_cast<const float4 *>(sGeo + e * TC_GEO + 4 * f);
-        const float Fscale = fg.x, nx = fg.y, ny = fg.z, nz = fg.w;
-        float pjump, Unjump;
-        if (pat == 255) {
-          if (P.bc == BBW_BC_PRESSURE_RELEASE) {
-            pjump = -2.f * pM;
-            Unjump = 0.f;
-          } else {
-            pjump = 0.f;
-            Unjump = -2.f * (uM * nx + vvM * ny + wM * nz);
+      for (int j = 0; j < 2 * FPW; ++j) pf[j] = 0.f;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        p4[h] = make_float4(0.f, 0.f, 0.f, 0.f);
+        U4[h][0] = U4[h][1] = U4[h][2] = p4[h];
+      }
+      if (!fail) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int item = ptid + 256 * h, ce = item & 31, cc = item >> 5;
+          if (cc < NC && 4 * cc < Np && ce < ne) {
+            const float4 g0 = *reinterpret_cast<const float4 *>(sGeo + ce * TC_GEO + 16);
+            const float4 g1 = *reinterpret_cast<const float4 *>(sGeo + ce * TC_GEO + 20);
+            const float G[9] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w,
+                                sGeo[ce * TC_GEO + 24]};
+            const float *rr = sRaw + ce * RS + 4 * cc;
+            float4 u4, v4, w4;
+            if constexpr (C::V4) {
+              p4[h] = *reinterpret_cast<const float4 *>(rr);
+              u4 = *reinterpret_cast<const float4 *>(rr + Np);
+              v4 = *reinterpret_cast<const float4 *>(rr + 2 * Np);
+              w4 = *reinterpret_cast<const float4 *>(rr + 3 * Np);
+            } else {
+              float a[4][4];
+#pragma unroll
+              for (int fl = 0; fl < 4; ++fl)
+#pragma unroll
+                for (int i = 0; i < 4; ++i) a[fl][i] = (4 * cc + i < Np) ? rr[fl * Np + i] : 0.f;
+              p4[h] = make_float4(a[0][0], a[0][1], a[0][2], a[0][3]);
+              u4 = make_float4(a[1][0], a[1][1], a[1][2], a[1][3]);
+              v4 = make_float4(a[2][0], a[2][1], a[2][2], a[2][3]);
+              w4 = make_float4(a[3][0], a[3][1], a[3][2], a[3][3]);
+            }
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              float4 &U = U4[h][d];
+              U.x = u4.x * G[3 * d] + v4.x * G[3 * d + 1] + w4.x * G[3 * d + 2];
+              U.y = u4.y * G[3 * d] + v4.y * G[3 * d + 1] + w4.y * G[3 * d + 2];
+              U.z = u4.z * G[3 * d] + v4.z * G[3 * d + 1] + w4.z * G[3 * d + 2];
+              U.w = u4.w * G[3 * d] + v4.w * G[3 * d + 1] + w4.w * G[3 * d + 2];
+              mU = fmaxf(mU, fmaxf(fmaxf(fabsf(U.x), fabsf(U.y)), fmaxf(fabsf(U.z), fabsf(U.w))));
+            }
+            mp = fmaxf(mp, fmaxf(fmaxf(fabsf(p4[h].x), fabsf(p4[h].y)),
+                                 fmaxf(fabsf(p4[h].z), fabsf(p4[h].w))));
           }
-        } else {
-          const unsigned rel = (unsigned)((code >> 8) - k0);
-          float pP = nbv[j][0], uP = nbv[j][1], vP_ = nbv[j][2], wP = nbv[j][3];
-          if (rel < (unsigned)ne) {  // neighbour inside the tile
-            const float *o = sRaw + rel * RS + sPat[pat * Nfp + lane];
-            pP = o[0], uP = o[Np], vP_ = o[2 * Np], wP = o[3 * Np];
+        }
+        // upwind flux (Uflux = -pflux), lane = face node; warp pw owns the
+        // (element, face) pairs 16 pw .. 16 pw + 15, in two halves whose
+        // outside-tile neighbour traces are fetched together
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          float nbv[FPW][4];
+#pragma unroll
+          for (int j = 0; j < FPW; ++j) {
+            nbv[j][0] = nbv[j][1] = nbv[j][2] = nbv[j][3] = 0.f;
+            const int pp = pw * 2 * FPW + h * FPW + j, e = pp >> 2, f = pp & 3;
+            if (lane >= Nfp || e >= ne) continue;
+            const int code = sNbr[e * 4 + f];
+            const int pat = code & 255;
+            if (pat == 255) continue;
+            const unsigned rel = (unsigned)((code >> 8) - k0);
+            if (rel < (unsigned)ne) continue;
+            const float *o = qs + (size_t)(code >> 8) * 4 * Np + sPat[pat * Nfp + lane];
+            nbv[j][0] = __ldg(o), nbv[j][1] = __ldg(o + Np), nbv[j][2] = __ldg(o + 2 * Np),
+            nbv[j][3] = __ldg(o + 3 * Np);
           }
-          pjump = pP - pM;
-          Unjump = (uP - uM) * nx + (vP_ - vvM) * ny + (wP - wM) * nz;
+#pragma unroll
+          for (int j = 0; j < FPW; ++j) {
+            const int pp = pw * 2 * FPW + h * FPW + j, e = pp >> 2, f = pp & 3;
+            if (lane >= Nfp || e >= ne) continue;
+            const int m = f * Nfp + lane;
+            const int code = sNbr[e * 4 + f];
+            const int pat = code & 255;
+            const int vM = sFmask[m];
+            const float *own = sRaw + e * RS + vM;
+            const float pM = own[0], uM = own[Np], vvM = own[2 * Np], wM = own[3 * Np];
+            const float4 fg = *reinterpret_cast<const float4 *>(sGeo + e * TC_GEO + 4 * f);
+            const float Fscale = fg.x, nx = fg.y, ny = fg.z, nz = fg.w;
+            float pjump, Unjump;
+            if (pat == 255) {
+              if (P.bc == BBW_BC_PRESSURE_RELEASE) {
+                pjump = -2.f * pM;
+                Unjump = 0.f;
+              } else {
+                pjump = 0.f;
+                Unjump = -2.f * (uM * nx + vvM * ny + wM * nz);
+              }
+            } else {
+              const unsigned rel = (unsigned)((code >> 8) - k0);
+              float pP = nbv[j][0], uP = nbv[j][1], vP_ = nbv[j][2], wP = nbv[j][3];
+              if (rel < (unsigned)ne) {
+                const float *o = sRaw + rel * RS + sPat[pat * Nfp + lane];
+                pP = o[0], uP = o[Np], vP_ = o[2 * Np], wP = o[3 * Np];
+              }
+              pjump = pP - pM;
+              Unjump = (uP - uM) * nx + (vP_ - vvM) * ny + (wP - wM) * nz;
+            }
+            pf[h * FPW + j] = .5f * (pjump - Unjump) * Fscale;
+            mF = fmaxf(mF, fabsf(pf[h * FPW + j]));
+          }
         }
-        pf[j] = .5f * (pjump - Unjump) * Fscale;
-        mF = fmaxf(mF, fabsf(pf[j]));
       }
-    }
-    mp = warp_max(mp);
-    mU = warp_max(mU);
-    mF = warp_max(mF);
-    if (lane == 0) {
-      atomicMax(&sRed[0], __float_as_int(mp));
-      atomicMax(&sRed[1], __float_as_int(mU));
-      atomicMax(&sRed[2], __float_as_int(mF));
-    }
-    __syncthreads();  // maxima complete
-    sp = pow2_scale(sRed[0]), sU = pow2_scale(sRed[1]), sF = pow2_scale(sRed[2]);
-    // B operands (element rows, K-major): p, U_d, per-face pflux
-    if (cc < NC) {
-      const int o = tc::kmajor_offset_f16(ce, 4 * cc, KV);
-      split_store4(sBp + o, sBp + TC_E * KV + o, p4, sp);
-#pragma unroll
-      for (int d = 0; d < 3; ++d)
-        split_store4(sBU + 2 * d * TC_E * KV + o, sBU + (2 * d + 1) * TC_E * KV + o, U4[d], sU);
-    }
-#pragma unroll
-    for (int j = 0; j < FPW; ++j) {
-      const int pp = warp * FPW + j, e = pp >> 2, f = pp & 3;
-      if (lane >= Nfp) continue;  // absent elements store zeros (pf = 0)
-      const int o = tc::kmajor_offset_f16(e, lane, KF);
-      split_store1(sBF + 2 * f * TC_E * KF + o, sBF + (2 * f + 1) * TC_E * KF + o, pf[j] * sF);
-    }
-    return sync_for_mma();  // B1 written; the raw tile and codes no longer read
-  };
-
-  // ---------------------------------------------------------------- prologue
-  int vt = blockIdx.x, it = 0;
-  if (vt < nvt) {
-    if (tid == I_COPY) issue_tma(vt, 0);
-    wait_bar(mbT, tphase, 0, I_COPY);
-    if (!fail) load_traces(vt);
-    fail = produce(vt, 0) || fail;
-    if (!fail) {
-      if (mma1_issuer()) issue_mma1();
-      if (tid == I_COPY) {
-        prefetch_item(vt);
-        if (vt + (int)gridDim.x < nvt) issue_tma(vt + gridDim.x, 1);
+      const int rs = 3 * (it & 1);  // maxima slot set of this item
+      mp = warp_max(mp);
+      mU = warp_max(mU);
+      mF = warp_max(mF);
+      if (lane == 0) {
+        atomicMax(&sRed[rs], __float_as_int(mp));
+        atomicMax(&sRed[rs + 1], __float_as_int(mU));
+        atomicMax(&sRed[rs + 2], __float_as_int(mF));
       }
-    }
-    if (tid < 3) sRed[tid] = 0;
-  }
-  float sp_cur = sp, sU_cur = sU, sF_cur = sF;  // scales of the item in acc1
-
-  // ------------------------------------------------------------- item loop
-  // (fail is CTA-uniform here; inside the loop a missed wait is acted on at
-  // the next CTA-wide vote, so every thread leaves at the same point)
-  if (!fail)
-  for (; vt < nvt; vt += gridDim.x, ++it) {
-    const int shot = vt / ntiles, k0 = (vt - shot * ntiles) * TC_E, ne = min(TC_E, P.K - k0);
-    const int gb = it & 1;
-    const int next = vt + gridDim.x, next2 = next + gridDim.x;
-    const size_t sbase = shot * sstride;
-    const float *sGeo = sGeoB + gb * TC_E * TC_GEO;
-
-    // ---- a. epilogue 1 (thread = node row, four elements): rhs of u, v, w;
-    //         LSRK update of u, v, w (old values from global memory, fetched
-    //         before the wait); rhs_p -> B operand of the Vq product
-    float ro[4][3], qo[4][3];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int e = 8 * g8 + ep_col(lane, j);
-      const bool ok = rowok && e < ne;
-      const size_t id = sbase + (size_t)(k0 + e) * 4 * Np + rowM;
-#pragma unroll
-      for (int fl = 1; fl < 4; ++fl) {
-        ro[j][fl - 1] = ok ? P.res[id + fl * Np] : 0.f;
-        qo[j][fl - 1] = ok ? __ldg(P.Qin + id + fl * Np) : 0.f;
+      if (group_sync_or(2, fail || *sFail)) break;  // maxima complete
+      const float sp = pow2_scale(sRed[rs]), sU = pow2_scale(sRed[rs + 1]),
+                  sF = pow2_scale(sRed[rs + 2]);
+      if (ptid < 3) sRed[3 - rs + ptid] = 0;  // the other set: read one item ago
+      if (ptid == 0) {  // scales of this item's B1 for the epilogue warps
+        float *sc = sScale + 3 * (it & 1);
+        sc[0] = sp, sc[1] = sU, sc[2] = sF;
+        __threadfence_block();
+        sTag[it & 1] = it;
       }
-    }
-    wait_bar(mbM, mphase, 2, I_GRAD);
-    float rp[4] = {0.f, 0.f, 0.f, 0.f};
-    if (!fail) {
-      float gr[4], gs[4], gt[4], dv[4], lf[4][4];
-      tc::tmem_ld16x64b_x4x4(tsub + cGrad, tsub + cGrad + 32, tsub + cGrad + 64, tsub + cDiv, gr,
-                             gs, gt, dv);
-      tc::tmem_ld16x64b_x4x4(tsub + cLift, tsub + cLift + 32, tsub + cLift + 64,
-                             tsub + cLift + 96, lf[0], lf[1], lf[2], lf[3]);
-      const float isp = 1.f / sp_cur, isU = 1.f / sU_cur, isF = 1.f / sF_cur;
+      // B1 is free once the previous item's first MMA group has read it
+      if (it > 0) {
+        const bool ok = tc::mbar_wait(mbM, (uint32_t)((it - 1) & 1), TC_WAIT);
+        if (!ok) fail = true, *sFail = 1;
+      }
+      if (!fail) {
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int e = 8 * g8 + ep_col(lane, j);
-        const float *Ge = sGeo + e * TC_GEO;
-        const float4 g0 = *reinterpret_cast<const float4 *>(Ge + 16);
-        const float4 g1 = *reinterpret_cast<const float4 *>(Ge + 20);
-        const float g8v = Ge[24];
-        const float dr = gr[j] * isp, ds = gs[j] * isp, dt = gt[j] * isp;
-        float vp = -dv[j] * isU;
-        float vu = -(g0.x * dr + g0.w * ds + g1.z * dt);
-        float vv = -(g0.y * dr + g1.x * ds + g1.w * dt);
-        float vw = -(g0.z * dr + g1.y * ds + g8v * dt);
+        for (int h = 0; h < 2; ++h) {
+          const int item = ptid + 256 * h, ce = item & 31, cc = item >> 5;
+          if (cc < NC) {
+            const int o = tc::kmajor_offset_f16(ce, 4 * cc, KV);
+            split_store4(sBp + o, sBp + TC_E * KV + o, p4[h], sp);
 #pragma unroll
-        for (int f = 0; f < 4; ++f) {
-          const float a = lf[f][j] * isF;
-          const float4 fn = *reinterpret_cast<const float4 *>(Ge + 4 * f);  // Fscale nx ny nz
-          vp += a;
-          vu -= fn.y * a;
-          vv -= fn.z * a;
-          vw -= fn.w * a;
+            for (int d = 0; d < 3; ++d)
+              split_store4(sBU + 2 * d * TC_E * KV + o, sBU + (2 * d + 1) * TC_E * KV + o,
+                           U4[h][d], sU);
+          }
         }
-        const bool ok = rowok && e < ne;
-        rp[j] = ok ? vp : 0.f;
+#pragma unroll
+        for (int j = 0; j < 2 * FPW; ++j) {
+          const int pp = pw * 2 * FPW + j, e = pp >> 2, f = pp & 3;
+          if (lane >= Nfp) continue;  // absent elements store zeros (pf = 0)
+          const int o = tc::kmajor_offset_f16(e, lane, KF);
+          split_store1(sBF + 2 * f * TC_E * KF + o, sBF + (2 * f + 1) * TC_E * KF + o,
+                       pf[j] * sF);
+        }
+      }
+      tc::fence_proxy_async();
+      tc::fence_before_sync();
+      if (group_sync_or(2, fail || *sFail)) break;  // B1 written; raw tile and codes free
+      tc::fence_after_sync();
+      if (ptid == I_COPY - 256) {
+        if (next < nvt) {
+          // the geometry buffer of the next item was read by the epilogue
+          // of the item before this one
+          const bool ok = it == 0 || wait1(mbG, (uint32_t)((it - 1) & 1));
+          if (ok) {
+            issue_tma(next, gb ^ 1, (uint32_t)((it + 1) & 1));
+            prefetch_item(next);
+            if (next + (int)gridDim.x < nvt) prefetch_copies(next + gridDim.x);
+          }
+        }
+      } else if (ptid == I_GRAD - 256 || ptid == I_DIV - 256 || ptid == I_LIFT - 256) {
+        // the accumulators of the previous item have been read out
+        const bool ok = it == 0 || wait1(mbF, (uint32_t)((it - 1) & 1));
         if (ok) {
-          const size_t id = sbase + (size_t)(k0 + e) * 4 * Np + rowM;
-          const float rv3[3] = {vu, vv, vw};
-#pragma unroll
-          for (int fl = 1; fl < 4; ++fl) {
-            const float r = P.fa * ro[j][fl - 1] + P.fdt * rv3[fl - 1];
-            P.res[id + fl * Np] = r;
-            P.Qout[id + fl * Np] = qo[j][fl - 1] + P.fb * r;
+          const uint32_t id64 = tc::idesc_f16(64, TC_E, FMT);
+          const int sboV = (KV / 8) * 128, sboF = (KF / 8) * 128;
+          const int pD = MR * KV, pL = MR * KF;
+          if (ptid == I_GRAD - 256) {
+            for (int d = 0; d < 3; ++d)
+              chain(tbase + cGrad + 32 * d, sOps + L.oD + 2 * d * pD,
+                    sOps + L.oD + (2 * d + 1) * pD, sboV, sBp, sBp + TC_E * KV, sboV, KV / 16,
+                    id64, false);
+            sPend[2] = 1, sPend[3] = it & 1;
+          } else if (ptid == I_DIV - 256) {
+            for (int d = 0; d < 3; ++d)
+              chain(tbase + cDiv, sOps + L.oD + 2 * d * pD, sOps + L.oD + (2 * d + 1) * pD, sboV,
+                    sBU + 2 * d * TC_E * KV, sBU + (2 * d + 1) * TC_E * KV, sboV, KV / 16, id64,
+                    d > 0);
+          } else {
+            for (int f = 0; f < 4; ++f)
+              chain(tbase + cLift + 32 * f, sOps + L.oL + 2 * f * pL,
+                    sOps + L.oL + (2 * f + 1) * pL, sboF, sBF + 2 * f * TC_E * KF,
+                    sBF + (2 * f + 1) * TC_E * KF, sboF, KF / 16, id64, false);
           }
+          tc::mma_commit(mbM);
         }
       }
     }
-    {
-      float mr = fmaxf(fmaxf(fabsf(rp[0]), fabsf(rp[1])), fmaxf(fabsf(rp[2]), fabsf(rp[3])));
-      mr = warp_max(mr);
-      if (lane == 0) atomicMax(&sRed[3], __float_as_int(mr));
-    }
-    tc::fence_before_sync();
-    __syncthreads();  // maxima of rhs_p; acc1 and this item's geometry no longer read
-    tc::fence_after_sync();
-    const float srp = pow2_scale(sRed[3]);
-    if (rowM < KV) {  // rows [Np, KV) store the zero K padding
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int o = tc::kmajor_offset_f16(8 * g8 + ep_col(lane, j), rowM, KV);
-        split_store1(sBW + o, sBW + TC_E * KV + o, rp[j] * srp);
-      }
-    }
-    if (tid == 0) sRed[4] = 0;
-    if (sync_for_mma()) {
-      fail = true;
-      break;
-    }
-    if (tid == I_WADG) {
-      chain(tbase + cVq, sOps + L.oVq, sOps + L.oVq + MRQ * KV, (KV / 8) * 128, sBW,
-            sBW + TC_E * KV, (KV / 8) * 128, KV / 16, tc::idesc_f16(MQ, TC_E, FMT), false);
-      tc::mma_commit(mbW);
-      sPend[4] = 1, sPend[5] = (int)wphase;
-    }
-
-    // c^2 of epilogue 2, fetched here so that its latency hides under b
+  } else {
+    // ============================================================ epilogue
+    // per work item, thread = node row x 8 elements (two groups of four):
+    //   1. first-group accumulators -> rhs of u, v, w, their LSRK update;
+    //      rhs_p split -> Vq MMAs
+    //   2. c^2 / J * (Vq rhs_p) split -> Pq MMAs
+    //   3. rhs_p = Pq (...) + sources, LSRK update of p
+    const uint32_t tq = tbase + ((uint32_t)(32 * q4) << 16);
+    const int rowM = 16 * q4 + ep_row(lane);
+    const bool rowok = rowM < Np;
     const bool q128 = MQ == 128;
     const int qrow = q128 ? 32 * q4 + lane : rowM;
-    const int nq = q128 ? 8 : 4;  // elements per thread in epilogue 2
-    float c2v[8];
+    uint32_t wphase = 0;
+    int it = 0;
+    for (int vt = blockIdx.x; vt < nvt; vt += gridDim.x, ++it) {
+      const int shot = vt / ntiles, k0 = (vt - shot * ntiles) * TC_E, ne = min(TC_E, P.K - k0);
+      const int gb = it & 1;
+      const size_t sbase = shot * sstride;
+      const float *sGeo = sGeoB + gb * TC_E * TC_GEO;
+      const int rs = 6 + 2 * (it & 1);  // maxima slot set of this item
+      // ---- 1. first group
+      float rp[2][4];
+      // old u, v, w and their residual, fetched before the wait
+      float ro[2][4][3], qo[2][4][3];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const int e = 8 * g8 + (q128 ? j : ep_col(lane, j & 3));
-      c2v[j] = j < nq && qrow < Nq && e < ne ? __ldg(P.c2q + (size_t)(k0 + e) * Nq + qrow) : 0.f;
-    }
-    // ---- b. next item: its inputs landed during this item's first MMAs;
-    //         traces, flux and B operands of its first product group
-    if (next < nvt) {
-      wait_bar(mbT, tphase, 0, I_COPY);
-      if (!fail) load_traces(next);
-      if (produce(next, gb ^ 1)) {
-        fail = true;
-        break;
-      }
-    }
-
-    // ---- c. epilogue 2 (thread = cubature row q): c2/J * p_q -> B operand of Pq
-    wait_bar(mbW, wphase, 4, I_WADG);
-    float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    if (!fail) {
-      if (q128) {
-        tc::tmem_ld8(tbase + ((uint32_t)(32 * q4) << 16) + cVq + 8 * g8, v);
-      } else {
-        float v4[4];
-        tc::tmem_ld16x64b_x4(tsub + cVq, v4);
+      for (int hh = 0; hh < 2; ++hh)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) v[j] = v4[j];
-      }
-    }
-    const float isr = 1.f / srp;
-    float mc = 0.f;
+        for (int j = 0; j < 4; ++j) {
+          const int e = 8 * (2 * eh + hh) + ep_col(lane, j);
+          const bool ok = rowok && e < ne && !fail;
+          const size_t id = sbase + (size_t)(k0 + e) * 4 * Np + rowM;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const float raw = v[j] * isr;
-      if (P.vq_out && j < nq && qrow < Nq) {
-        const int e = 8 * g8 + (q128 ? j : ep_col(lane, j));
-        if (e < ne) P.vq_out[((size_t)shot * Nq + qrow) * P.K + k0 + e] = raw;
-      }
-      v[j] = qrow < Nq ? raw * c2v[j] : 0.f;  // rows past Nq: exact zeros
-      mc = fmaxf(mc, fabsf(v[j]));
-    }
-    mc = warp_max(mc);
-    if (lane == 0) atomicMax(&sRed[4], __float_as_int(mc));
-    tc::fence_before_sync();
-    __syncthreads();  // maxima; the Vq product has read its B operand in BW
-    tc::fence_after_sync();
-    const float sc = pow2_scale(sRed[4]);
-    if (qrow < KQ) {
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        if (j >= nq) break;
-        const int o = tc::kmajor_offset_f16(8 * g8 + (q128 ? j : ep_col(lane, j)), qrow, KQ);
-        split_store1(sBW + o, sBW + TC_E * KQ + o, v[j] * sc);
-      }
-    }
-    if (tid == 0) sRed[3] = 0;
-    if (sync_for_mma()) {
-      fail = true;
-      break;
-    }
-    sp_cur = sp, sU_cur = sU, sF_cur = sF;  // scales of the next item's B1 operands
-    if (tid < 3) sRed[tid] = 0;
-    if (tid == I_WADG) {
-      chain(tbase + cPq, sOps + L.oPq, sOps + L.oPq + MR * KQ, (KQ / 8) * 128, sBW,
-            sBW + TC_E * KQ, (KQ / 8) * 128, KQ / 16, tc::idesc_f16(64, TC_E, FMT), false);
-      tc::mma_commit(mbW);
-      sPend[4] = 1, sPend[5] = (int)wphase;
-    }
-    if (next < nvt) {
-      if (mma1_issuer()) issue_mma1();  // acc1 drained in a, B1 written in b
-      if (tid == I_COPY) {
-        prefetch_item(next);
-        if (next2 < nvt) issue_tma(next2, gb);  // raw tile free after b, geometry gb after a
-      }
-    }
-
-    // ---- d. epilogue 3: rhs_p = Pq (c2 p_q) + sources; LSRK update of p
-    float r7[4], q7[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int e = 8 * g8 + ep_col(lane, j);
-      const bool ok = rowok && e < ne;
-      const size_t id = sbase + (size_t)(k0 + e) * 4 * Np + rowM;
-      r7[j] = ok ? P.res[id] : 0.f;
-      q7[j] = ok ? __ldg(P.Qin + id) : 0.f;
-    }
-    wait_bar(mbW, wphase, 4, I_WADG);
-    if (!fail) {
-      float w[4];
-      tc::tmem_ld16x64b_x4(tsub + cPq, w);
-      const float isc = 1.f / sc;
-#pragma unroll
-      for (int j = 0; j < 4; ++j) w[j] *= isc;
-      if (P.src_off) {
-        // the entries of a shot are sorted by element: find the first one of
-        // this tile by bisection, then walk the tile's entries
-        const int j0 = __ldg(P.src_off + shot), j1 = __ldg(P.src_off + shot + 1);
-        int lo = j0, hi = j1;
-        while (lo < hi) {
-          const int mid = (lo + hi) >> 1;
-          if (__ldg(P.src_elem + mid) < k0) lo = mid + 1;
-          else hi = mid;
+          for (int fl = 1; fl < 4; ++fl) {
+            ro[hh][j][fl - 1] = ok ? P.res[id + fl * Np] : 0.f;
+            qo[hh][j][fl - 1] = ok ? __ldg(P.Qin + id + fl * Np) : 0.f;
+          }
         }
-        if (lo < j1 && __ldg(P.src_elem + lo) < k0 + ne) {
-          const float amp = tc_ricker((float)(*P.time) + P.cstage * P.fdt, P.f0, P.tR, P.samp);
+      {
+        const bool ok = tc::mbar_wait(mbM, (uint32_t)(it & 1), TC_WAIT);
+        if (!ok) fail = true, *sFail = 1;
+        else if (tid == 0) sPend[2] = 0;
+        fail = __any_sync(0xffffffffu, fail);  // the TMEM loads are warp-collective
+        tc::fence_after_sync();
+      }
+      float isp = 1.f, isU = 1.f, isF = 1.f;
+      if (!fail) {
+        // the producer wrote this item's scales before its MMAs were issued
+        uint32_t n = 0;
+        while (sTag[it & 1] != it && ++n < TC_WAIT) {
+        }
+        if (sTag[it & 1] != it) fail = true, *sFail = 1;
+        __threadfence_block();
+      }
+      fail = __any_sync(0xffffffffu, fail);
+      if (!fail) {
+        const float *sc = sScale + 3 * (it & 1);
+        isp = 1.f / sc[0], isU = 1.f / sc[1], isF = 1.f / sc[2];
+      }
+#pragma unroll
+      for (int hh = 0; hh < 2; ++hh) {
+        const int g8 = 2 * eh + hh;
+        const uint32_t tsub = tq + 8 * g8;
+        float gr[4], gs[4], gt[4], dv[4], lf[4][4];
+        if (!fail) {
+          tc::tmem_ld16x64b_x4x4(tsub + cGrad, tsub + cGrad + 32, tsub + cGrad + 64, tsub + cDiv,
+                                 gr, gs, gt, dv);
+          tc::tmem_ld16x64b_x4x4(tsub + cLift, tsub + cLift + 32, tsub + cLift + 64,
+                                 tsub + cLift + 96, lf[0], lf[1], lf[2], lf[3]);
+        }
+        if (hh == 1) {  // both halves read: the first group's accumulators are free
+          tc::fence_before_sync();
+          __syncwarp();
+          if (lane == 0) mbar_arrive1(mbF);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          rp[hh][j] = 0.f;
+          if (fail) continue;
+          const int e = 8 * g8 + ep_col(lane, j);
+          const float *Ge = sGeo + e * TC_GEO;
+          const float4 g0 = *reinterpret_cast<const float4 *>(Ge + 16);
+          const float4 g1 = *reinterpret_cast<const float4 *>(Ge + 20);
+          const float g8v = Ge[24];
+          const float dr = gr[j] * isp, ds = gs[j] * isp, dt = gt[j] * isp;
+          float vp = -dv[j] * isU;
+          float vu = -(g0.x * dr + g0.w * ds + g1.z * dt);
+          float vv = -(g0.y * dr + g1.x * ds + g1.w * dt);
+          float vw = -(g0.z * dr + g1.y * ds + g8v * dt);
+#pragma unroll
+          for (int f = 0; f < 4; ++f) {
+            const float a = lf[f][j] * isF;
+            const float4 fn = *reinterpret_cast<const float4 *>(Ge + 4 * f);
+            vp += a;
+            vu -= fn.y * a;
+            vv -= fn.z * a;
+            vw -= fn.w * a;
+          }
+          const bool ok = rowok && e < ne;
+          rp[hh][j] = ok ? vp : 0.f;
+          if (ok) {
+            const size_t id = sbase + (size_t)(k0 + e) * 4 * Np + rowM;
+            const float rv3[3] = {vu, vv, vw};
+#pragma unroll
+            for (int fl = 1; fl < 4; ++fl) {
+              const float r = P.fa * ro[hh][j][fl - 1] + P.fdt * rv3[fl - 1];
+              P.res[id + fl * Np] = r;
+              P.Qout[id + fl * Np] = qo[hh][j][fl - 1] + P.fb * r;
+            }
+          }
+        }
+      }
+      // this item's geometry has been read
+      __syncwarp();
+      if (lane == 0) mbar_arrive1(mbG);
+      {
+        float mr = 0.f;
+#pragma unroll
+        for (int hh = 0; hh < 2; ++hh)
+          mr = fmaxf(mr, fmaxf(fmaxf(fabsf(rp[hh][0]), fabsf(rp[hh][1])),
+                               fmaxf(fabsf(rp[hh][2]), fabsf(rp[hh][3]))));
+        mr = warp_max(mr);
+        if (lane == 0) atomicMax(&sRed[rs], __float_as_int(mr));
+      }
+      if (group_sync_or(1, fail || *sFail)) break;  // maxima of rhs_p
+      const float srp = pow2_scale(sRed[rs]);
+      if (tid < 2) sRed[14 - rs + tid] = 0;  // the other set: read one item ago
+      if (rowM < KV) {  // rows [Np, KV) store the zero K padding
+#pragma unroll
+        for (int hh = 0; hh < 2; ++hh)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int o = tc::kmajor_offset_f16(8 * (2 * eh + hh) + ep_col(lane, j), rowM, KV);
+            split_store1(sBW + o, sBW + TC_E * KV + o, rp[hh][j] * srp);
+          }
+      }
+      tc::fence_proxy_async();
+      tc::fence_before_sync();
+      if (group_sync_or(1, fail || *sFail)) break;
+      tc::fence_after_sync();
+      if (tid == I_WADG) {
+        chain(tbase + cVq, sOps + L.oVq, sOps + L.oVq + MRQ * KV, (KV / 8) * 128, sBW,
+              sBW + TC_E * KV, (KV / 8) * 128, KV / 16, tc::idesc_f16(MQ, TC_E, FMT), false);
+        tc::mma_commit(mbW);
+        sPend[4] = 1, sPend[5] = (int)wphase;
+      }
+      // ---- 2. c^2 / J at the cubature points; c2 fetched under the Vq MMAs
+      const int nq = q128 ? 8 : 4;  // elements per thread and group of eight
+      float v[2][8];
+#pragma unroll
+      for (int hh = 0; hh < 2; ++hh) {
+        const int g8 = 2 * eh + hh;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int e = 8 * g8 + (q128 ? j : ep_col(lane, j & 3));
+          v[hh][j] = j < nq && qrow < Nq && e < ne ? __ldg(P.c2q + (size_t)(k0 + e) * Nq + qrow)
+                                                   : 0.f;
+        }
+      }
+      {
+        const bool ok = tc::mbar_wait(mbW, wphase, TC_WAIT);
+        if (!ok) fail = true, *sFail = 1;
+        else if (tid == I_WADG) sPend[4] = 0;
+        wphase ^= 1u;
+        fail = __any_sync(0xffffffffu, fail);
+        tc::fence_after_sync();
+      }
+      const float isr = 1.f / srp;
+      float mc = 0.f;
+#pragma unroll
+      for (int hh = 0; hh < 2; ++hh) {
+        const int g8 = 2 * eh + hh;
+        float a[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (!fail) {
+          if (q128) {
+            tc::tmem_ld8(tq + cVq + 8 * g8, a);
+          } else {
+            float a4[4];
+            tc::tmem_ld16x64b_x4(tq + 8 * g8 + cVq, a4);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) a[j] = a4[j];
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const float raw = a[j] * isr;
+          if (P.vq_out && j < nq && qrow < Nq && !fail) {
+            const int e = 8 * g8 + (q128 ? j : ep_col(lane, j));
+            if (e < ne) P.vq_out[((size_t)shot * Nq + qrow) * P.K + k0 + e] = raw;
+          }
+          v[hh][j] = qrow < Nq ? raw * v[hh][j] : 0.f;  // rows past Nq: exact zeros
+          mc = fmaxf(mc, fabsf(v[hh][j]));
+        }
+      }
+      mc = warp_max(mc);
+      if (lane == 0) atomicMax(&sRed[rs + 1], __float_as_int(mc));
+      // the residual and state of p, fetched under the Pq MMAs
+      float r7[2][4], q7[2][4];
+      tc::fence_before_sync();
+      if (group_sync_or(1, fail || *sFail)) break;  // maxima; Vq has read BW
+      tc::fence_after_sync();
+      const float sc = pow2_scale(sRed[rs + 1]);
+      if (qrow < KQ) {
+#pragma unroll
+        for (int hh = 0; hh < 2; ++hh)
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            if (j >= nq) break;
+            const int o = tc::kmajor_offset_f16(8 * (2 * eh + hh) + (q128 ? j : ep_col(lane, j)),
+                                                qrow, KQ);
+            split_store1(sBW + o, sBW + TC_E * KQ + o, v[hh][j] * sc);
+          }
+      }
+      tc::fence_proxy_async();
+      tc::fence_before_sync();
+      if (group_sync_or(1, fail || *sFail)) break;
+      tc::fence_after_sync();
+      if (tid == I_WADG) {
+        chain(tbase + cPq, sOps + L.oPq, sOps + L.oPq + MR * KQ, (KQ / 8) * 128, sBW,
+              sBW + TC_E * KQ, (KQ / 8) * 128, KQ / 16, tc::idesc_f16(64, TC_E, FMT), false);
+        tc::mma_commit(mbW);
+        sPend[4] = 1, sPend[5] = (int)wphase;
+      }
+      // ---- 3. rhs_p = Pq (c2 p_q) + sources; LSRK update of p
+#pragma unroll
+      for (int hh = 0; hh < 2; ++hh)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int e = 8 * (2 * eh + hh) + ep_col(lane, j);
+          const bool ok = rowok && e < ne;
+          const size_t id = sbase + (size_t)(k0 + e) * 4 * Np + rowM;
+          r7[hh][j] = ok ? P.res[id] : 0.f;
+          q7[hh][j] = ok ? __ldg(P.Qin + id) : 0.f;
+        }
+      {
+        const bool ok = tc::mbar_wait(mbW, wphase, TC_WAIT);
+        if (!ok) fail = true, *sFail = 1;
+        else if (tid == I_WADG) sPend[4] = 0;
+        wphase ^= 1u;
+        fail = __any_sync(0xffffffffu, fail);
+        tc::fence_after_sync();
+      }
+      if (!fail) {
+        const float isc = 1.f / sc;
+        float amp = 0.f;
+        int lo = 0, j1 = 0;
+        if (P.src_off) {
+          // the entries of a shot are sorted by element: find the first one
+          // of this tile by bisection, then walk the tile's entries
+          const int j0 = __ldg(P.src_off + shot);
+          j1 = __ldg(P.src_off + shot + 1);
+          lo = j0;
+          int hi = j1;
+          while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (__ldg(P.src_elem + mid) < k0) lo = mid + 1;
+            else hi = mid;
+          }
+          if (lo < j1 && __ldg(P.src_elem + lo) < k0 + ne)
+            amp = tc_ricker((float)(*P.time) + P.cstage * P.fdt, P.f0, P.tR, P.samp);
+          else
+            lo = j1;
+        }
+#pragma unroll
+        for (int hh = 0; hh < 2; ++hh) {
+          const int g8 = 2 * eh + hh;
+          float w[4];
+          tc::tmem_ld16x64b_x4(tq + 8 * g8 + cPq, w);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) w[j] *= isc;
           for (int s = lo; s < j1; ++s) {
             const int rel = __ldg(P.src_elem + s) - k0;
             if (rel >= ne) break;
@@ -762,27 +891,25 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
               if (rowok && rel == 8 * g8 + ep_col(lane, j))
                 w[j] += amp * __ldg(P.src_vec + (size_t)s * Np + rowM);
           }
-        }
-      }
-      if (rowok) {
+          if (rowok) {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int e = 8 * g8 + ep_col(lane, j);
-          if (e >= ne) continue;
-          const size_t id = sbase + (size_t)(k0 + e) * 4 * Np + rowM;
-          const float r = P.fa * r7[j] + P.fdt * w[j];
-          P.res[id] = r;
-          P.Qout[id] = q7[j] + P.fb * r;
+            for (int j = 0; j < 4; ++j) {
+              const int e = 8 * g8 + ep_col(lane, j);
+              if (e >= ne) continue;
+              const size_t id = sbase + (size_t)(k0 + e) * 4 * Np + rowM;
+              const float r = P.fa * r7[hh][j] + P.fdt * w[j];
+              P.res[id] = r;
+              P.Qout[id] = q7[hh][j] + P.fb * r;
+            }
+          }
         }
       }
     }
   }
   // (sPend is written by the issuing threads and read after this barrier)
-  if (__syncthreads_or(fail) && tid == 0) {
+  if (__syncthreads_or(fail || *sFail) && tid == 0) {
     // drain this CTA's own copies and MMAs still in flight (bounded), so
-    // nothing lands in shared memory or TMEM after they are released; a Vq
-    // or Pq product is awaited before the next one is issued, so at most
-    // the last of them can still be in flight
+    // nothing lands in shared memory or TMEM after they are released
     if (sPend[0]) tc::mbar_wait(mbT, (uint32_t)sPend[1], TC_WAIT);
     if (sPend[2]) tc::mbar_wait(mbM, (uint32_t)sPend[3], TC_WAIT);
     if (sPend[4]) tc::mbar_wait(mbW, (uint32_t)sPend[5], TC_WAIT);
