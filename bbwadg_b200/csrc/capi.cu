@@ -64,6 +64,7 @@ void release(bbw_ctx *c) {
   cudaFree(c->d_step);
   cudaFree(c->src_off);
   cudaFree(c->src_elem);
+  cudaFree(c->src_tile);
   cudaFree(c->src_vec);
   cudaFree(c->rec_elem);
   cudaFree(c->rec_w);
@@ -775,10 +776,10 @@ extern "C" bbw_status bbw_set_shots(bbw_ctx *c, int S) {
   c->plan.S = S;
   c->tc.S = S;
   if (c->src_off) {  // source table is per shot: drop it
-    cudaFree(c->src_off), cudaFree(c->src_elem), cudaFree(c->src_vec);
-    c->src_off = c->src_elem = nullptr, c->src_vec = nullptr;
+    cudaFree(c->src_off), cudaFree(c->src_elem), cudaFree(c->src_vec), cudaFree(c->src_tile);
+    c->src_off = c->src_elem = c->src_tile = nullptr, c->src_vec = nullptr;
     c->plan.src_off = c->plan.src_elem = nullptr, c->plan.src_vec = nullptr;
-    c->tc.src_off = c->tc.src_elem = nullptr, c->tc.src_vec = nullptr;
+    c->tc.src_tile = c->tc.src_elem = nullptr, c->tc.src_vec = nullptr;
   }
   if (c->traces) {
     cudaFree(c->traces);
@@ -799,10 +800,10 @@ extern "C" bbw_status bbw_set_sources(bbw_ctx *c, int nent, const int *shot, con
   if (!c || nent < 0 || (nent > 0 && (!shot || !elem || !vec)))
     return set_error(BBW_ERR_ARG, "bbw_set_sources: bad argument");
   cudaStreamSynchronize(c->stream);
-  cudaFree(c->src_off), cudaFree(c->src_elem), cudaFree(c->src_vec);
-  c->src_off = c->src_elem = nullptr, c->src_vec = nullptr;
+  cudaFree(c->src_off), cudaFree(c->src_elem), cudaFree(c->src_vec), cudaFree(c->src_tile);
+  c->src_off = c->src_elem = c->src_tile = nullptr, c->src_vec = nullptr;
   c->plan.src_off = c->plan.src_elem = nullptr, c->plan.src_vec = nullptr;
-  c->tc.src_off = c->tc.src_elem = nullptr, c->tc.src_vec = nullptr;
+  c->tc.src_tile = c->tc.src_elem = nullptr, c->tc.src_vec = nullptr;
   drop_graphs(c);
   if (nent == 0) return BBW_OK;
   const int Np = c->Np;
@@ -819,19 +820,26 @@ extern "C" bbw_status bbw_set_sources(bbw_ctx *c, int nent, const int *shot, con
     return shot[a] != shot[b] ? shot[a] < shot[b] : elem[a] < elem[b];
   });
   std::vector<float> v((size_t)nent * Np);
+  // the tensor-core stage's table: entries of work item (shot, 32-element
+  // tile) vt are [tile[vt], tile[vt + 1]) in the sorted order
+  const int ntiles = (c->K + 31) / 32;
+  std::vector<int> tile((size_t)c->S * ntiles + 1, 0);
   for (int at = 0; at < nent; ++at) {
     const int j = order[at];
     el[at] = elem[j];
     std::memcpy(&v[(size_t)at * Np], vec + (size_t)j * Np, Np * sizeof(float));
+    tile[(size_t)shot[j] * ntiles + elem[j] / 32 + 1] += 1;
   }
+  for (size_t i = 1; i < tile.size(); ++i) tile[i] += tile[i - 1];
   bbw_status s;
   if ((s = upload(&c->src_off, off.data(), off.size(), "bbw_set_sources")) != BBW_OK ||
       (s = upload(&c->src_elem, el.data(), el.size(), "bbw_set_sources")) != BBW_OK ||
-      (s = upload(&c->src_vec, v.data(), v.size(), "bbw_set_sources")) != BBW_OK)
+      (s = upload(&c->src_vec, v.data(), v.size(), "bbw_set_sources")) != BBW_OK ||
+      (s = upload(&c->src_tile, tile.data(), tile.size(), "bbw_set_sources")) != BBW_OK)
     return s;
   c->plan.src_off = c->src_off, c->plan.src_elem = c->src_elem, c->plan.src_vec = c->src_vec;
   c->plan.f0 = f0, c->plan.tR = t_delay, c->plan.samp = amplitude;
-  c->tc.src_off = c->src_off, c->tc.src_elem = c->src_elem, c->tc.src_vec = c->src_vec;
+  c->tc.src_tile = c->src_tile, c->tc.src_elem = c->src_elem, c->tc.src_vec = c->src_vec;
   c->tc.f0 = f0, c->tc.tR = t_delay, c->tc.samp = amplitude;
   c->src_stage_times = stage_times != 0;
   return BBW_OK;

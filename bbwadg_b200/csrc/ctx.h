@@ -70,6 +70,7 @@ struct bbw_ctx {
   double *d_time = nullptr;
   int *d_step = nullptr;
   int *src_off = nullptr, *src_elem = nullptr;
+  int *src_tile = nullptr;  // [S * ceil(K / 32) + 1] entry offsets per (shot, 32-element tile)
   float *src_vec = nullptr;
   int src_stage_times = 0;
   int R = 0, max_steps = 0;

@@ -80,7 +80,7 @@ struct TcPlan {
   int table_ints = 0, pat_off = 0;
   int *err = nullptr;
   // sources, as FusedPlan (null: none)
-  const int *src_off = nullptr, *src_elem = nullptr;
+  const int *src_tile = nullptr, *src_elem = nullptr;  // [S * ntiles + 1] entries per item
   const float *src_vec = nullptr;
   float f0 = 0.f, tR = 0.f, samp = 0.f;
   const double *time = nullptr;

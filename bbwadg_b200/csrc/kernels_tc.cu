@@ -158,10 +158,11 @@ struct TcParams {
   const int *__restrict__ tables;
   int table_ints, pat_off;
   int *err;
-  // sources: entries [src_off[s], src_off[s+1]) of shot s, sorted by element,
-  // add ricker(t) * src_vec[j][:] to the projected rhs_p of element
-  // src_elem[j], t = *time + cstage * fdt (as the FP32 fused stage)
-  const int *__restrict__ src_off;
+  // sources: entries j in [src_tile[vt], src_tile[vt+1]) of work item vt
+  // (entries sorted by shot and element) add ricker(t) * src_vec[j][:] to
+  // the projected rhs_p of element src_elem[j], t = *time + cstage * fdt (as
+  // the FP32 fused stage)
+  const int *__restrict__ src_tile;
   const int *__restrict__ src_elem;
   const float *__restrict__ src_vec;
   float f0, tR, samp;
@@ -626,6 +627,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
     const bool rowok = rowM < Np;
     const bool q128 = MQ == 128;
     const int qrow = q128 ? 32 * q4 + lane : rowM;
+    float *sVo = reinterpret_cast<float *>(sBW);  // vq_out staging, [Nq][TC_E]
     uint32_t wphase = 0;
     int it = 0;
     for (int vt = blockIdx.x; vt < nvt; vt += gridDim.x, ++it) {
@@ -634,6 +636,10 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       const size_t sbase = shot * sstride;
       const float *sGeo = sGeoB + gb * TC_E * TC_GEO;
       const int rs = 6 + 2 * (it & 1);  // maxima slot set of this item
+      // the item's source entries [src_lo, src_hi), fetched here and used
+      // in epilogue 3
+      int src_lo = 0, src_hi = 0;
+      if (P.src_tile) src_lo = __ldg(P.src_tile + vt), src_hi = __ldg(P.src_tile + vt + 1);
       // ---- 1. first group
       float rp[2][4];
       // old u, v, w and their residual, fetched before the wait
@@ -800,8 +806,10 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
         for (int j = 0; j < 8; ++j) {
           const float raw = a[j] * isr;
           if (P.vq_out && j < nq && qrow < Nq && !fail) {
+            // staged in BW (the Vq product has read it) as [q][element],
+            // elements XOR-swizzled by the row against bank conflicts
             const int e = 8 * g8 + (q128 ? j : ep_col(lane, j));
-            if (e < ne) P.vq_out[((size_t)shot * Nq + qrow) * P.K + k0 + e] = raw;
+            sVo[qrow * TC_E + (e ^ (qrow & 31))] = raw;
           }
           v[hh][j] = qrow < Nq ? raw * v[hh][j] : 0.f;  // rows past Nq: exact zeros
           mc = fmaxf(mc, fabsf(v[hh][j]));
@@ -814,6 +822,15 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       tc::fence_before_sync();
       if (group_sync_or(1, fail || *sFail)) break;  // maxima; Vq has read BW
       tc::fence_after_sync();
+      if (P.vq_out) {
+        // the staged pre-c2 cubature values, one row of the tile's elements
+        // per warp store
+        if (!fail)
+          for (int q = warp; q < Nq; q += 8)
+            if (lane < ne) P.vq_out[((size_t)shot * Nq + q) * P.K + k0 + lane] =
+                sVo[q * TC_E + (lane ^ (q & 31))];
+        if (group_sync_or(1, fail || *sFail)) break;  // staging read before BW is rewritten
+      }
       const float sc = pow2_scale(sRed[rs + 1]);
       if (qrow < KQ) {
 #pragma unroll
@@ -857,25 +874,9 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
       }
       if (!fail) {
         const float isc = 1.f / sc;
-        float amp = 0.f;
-        int lo = 0, j1 = 0;
-        if (P.src_off) {
-          // the entries of a shot are sorted by element: find the first one
-          // of this tile by bisection, then walk the tile's entries
-          const int j0 = __ldg(P.src_off + shot);
-          j1 = __ldg(P.src_off + shot + 1);
-          lo = j0;
-          int hi = j1;
-          while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (__ldg(P.src_elem + mid) < k0) lo = mid + 1;
-            else hi = mid;
-          }
-          if (lo < j1 && __ldg(P.src_elem + lo) < k0 + ne)
-            amp = tc_ricker((float)(*P.time) + P.cstage * P.fdt, P.f0, P.tR, P.samp);
-          else
-            lo = j1;
-        }
+        const float amp = src_lo < src_hi
+                              ? tc_ricker((float)(*P.time) + P.cstage * P.fdt, P.f0, P.tR, P.samp)
+                              : 0.f;
 #pragma unroll
         for (int hh = 0; hh < 2; ++hh) {
           const int g8 = 2 * eh + hh;
@@ -883,7 +884,7 @@ __global__ void __launch_bounds__(TC_T, 1) k_tc_stage(TcParams P) {
           tc::tmem_ld16x64b_x4(tq + 8 * g8 + cPq, w);
 #pragma unroll
           for (int j = 0; j < 4; ++j) w[j] *= isc;
-          for (int s = lo; s < j1; ++s) {
+          for (int s = src_lo; s < src_hi; ++s) {
             const int rel = __ldg(P.src_elem + s) - k0;
             if (rel >= ne) break;
 #pragma unroll
@@ -955,7 +956,7 @@ static bbw_status tc_launch_n(const TcPlan &pl, const float *Qin, float *Qout, f
   P.ops = pl.ops;
   P.tables = pl.tables, P.table_ints = pl.table_ints, P.pat_off = pl.pat_off;
   P.err = pl.err;
-  P.src_off = pl.src_off, P.src_elem = pl.src_elem, P.src_vec = pl.src_vec;
+  P.src_tile = pl.src_tile, P.src_elem = pl.src_elem, P.src_vec = pl.src_vec;
   P.f0 = pl.f0, P.tR = pl.tR, P.samp = pl.samp, P.time = pl.time;
   P.vq_out = pl.vq_out;
   P.L = pl.L;
