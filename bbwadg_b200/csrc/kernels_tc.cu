@@ -252,11 +252,8 @@ __device__ __forceinline__ void mbar_arrive1(uint64_t *mbar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(tc::smem_u32(mbar)) : "memory");
 }
 // group barriers: the epilogue warps (0-7) use named barrier 1, the
-// producer warps (8-15) barrier 2; __syncthreads keeps barrier 0
-__device__ __forceinline__ void group_sync(int id) {
-  asm volatile("bar.sync %0, 256;\n" ::"r"(id) : "memory");
-}
-// group barrier with an OR vote over the group's threads
+// producer warps (8-15) barrier 2 (__syncthreads keeps barrier 0); each
+// is a barrier with an OR vote over the group's 256 threads
 __device__ __forceinline__ bool group_sync_or(int id, bool v) {
   uint32_t r;
   asm volatile(
