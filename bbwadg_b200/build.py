@@ -60,7 +60,7 @@ def build(force=False, verbose=False):
     objs = [o for o, _ in results]
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(map(os.path.getmtime, objs)):
         cmd = [NVCC] + ARCH + ["-shared", "-ccbin", HOSTCXX, "-o", LIB] + objs + \
-              ["-Xcompiler", "-fopenmp", "-lgomp"]
+              ["-Xcompiler", "-fopenmp", "-lgomp", "-lcublas"]
         if verbose:
             print(" ".join(cmd), flush=True)
         p = subprocess.run(cmd, capture_output=True, text=True)

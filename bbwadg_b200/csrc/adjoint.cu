@@ -169,6 +169,8 @@ extern "C" bbw_status bbw_forward(bbw_ctx *c, float dt, int nsteps, int checkpoi
     return set_error(BBW_ERR_ARG, "bbw_forward: bad argument");
   *out = nullptr;
   if (c->R <= 0) return set_error(BBW_ERR_STATE, "bbw_forward: no receivers set");
+  if (c->gs)
+    return set_error(BBW_ERR_UNSUPPORTED, "bbw_forward: no adjoint in the GEMM precision form");
   if (c->plan.Kc > 0 && c->plan.Kc < c->K)
     return set_error(BBW_ERR_UNSUPPORTED, "bbw_forward: the adjoint needs the whole mesh (no halo)");
   bbw_status s = adj_setup(c);

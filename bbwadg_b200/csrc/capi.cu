@@ -49,6 +49,11 @@ namespace {
 
 void release(bbw_ctx *c) {
   if (!c) return;
+  if (c->gs) {
+    gemm_stage_release(*c->gs);
+    delete c->gs;
+    c->gs = nullptr;
+  }
   for (int i = 0; i < 2; ++i)
     if (c->step_graph[i]) cudaGraphExecDestroy(c->step_graph[i]);
   cudaFree(c->Q[0]);
@@ -244,13 +249,13 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
   *out = nullptr;
   if (!m || !o || (variant != BBW_NODAL && variant != BBW_BB) || (bc != 0 && bc != 1) ||
       (precision != BBW_PREC_FP32 && precision != BBW_PREC_F16X3 &&
-       precision != BBW_PREC_BF16X3))
+       precision != BBW_PREC_BF16X3 && precision != BBW_PREC_TF32))
     return set_error(BBW_ERR_ARG, "bbw_create: bad argument");
-  const bool tcp = precision == BBW_PREC_F16X3 || precision == BBW_PREC_BF16X3;
-  if (tcp && !tc_supported(m->N, m->Nq))
-    return set_error(BBW_ERR_UNSUPPORTED,
-                     "bbw_create: the split-FP16 tensor-core stage supports N in [2, 5] and "
-                     "Nq <= 128");
+  // split pairs on the fused tensor-core stage where it fits; TF32, and
+  // split pairs beyond it, on the GEMM form (gemm_stage.cu)
+  const bool split = precision == BBW_PREC_F16X3 || precision == BBW_PREC_BF16X3;
+  const bool gemm = precision == BBW_PREC_TF32 || (split && !tc_supported(m->N, m->Nq));
+  const bool tcp = split && !gemm;
   const int N = m->N, K = m->K, Nq = m->Nq;
   if (N < 1 || N > BBW_MAX_N) return set_error(BBW_ERR_UNSUPPORTED, "bbw_create: N out of range");
   if (K <= 0 || K >= (1 << 23) || Nq <= 0)
@@ -395,6 +400,14 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
     return s;
   }
   c->precision = precision;
+  if (gemm) {
+    c->gs = new GemmStage;
+    if ((s = gemm_stage_create(*c->gs, N, K, Nq, bc, precision, c->hD, c->hLIFT, c->hVq,
+                               c->hPq)) != BBW_OK) {
+      release(c);
+      return s;
+    }
+  }
   if (tcp) {
     // geometry records, split-FP16 / split-BF16 operators in the canonical
     // K-major layout
@@ -508,12 +521,18 @@ static void drop_graphs(bbw_ctx *c) {
 extern "C" bbw_status bbw_stage_ex(bbw_ctx *c, float fa, float fb, float fdt, float cstage) {
   DeviceGuard dg(c ? c->device : -1);
   if (!c) return set_error(BBW_ERR_ARG, "bbw_stage: ctx is NULL");
-  bbw_status s =
-      c->precision != BBW_PREC_FP32
-          ? tc_launch(c->tc, c->Q[c->cur], c->Q[c->cur ^ 1], c->res, fa, fb, fdt, cstage,
-                      c->stream)
-          : fused_launch(c->plan, c->Q[c->cur], c->Q[c->cur ^ 1], c->res, fa, fb, fdt, cstage,
-                         c->stream);
+  bbw_status s;
+  if (c->gs) {
+    const GemmInputs in = {c->vgeo, c->fgeo, c->c2q, c->nbr, c->tables, c->plan.pat_off};
+    s = gemm_stage_launch(*c->gs, in, c->Q[c->cur], c->Q[c->cur ^ 1], c->res, fa, fb, fdt,
+                          c->stream);
+  } else {
+    s = c->precision != BBW_PREC_FP32
+            ? tc_launch(c->tc, c->Q[c->cur], c->Q[c->cur ^ 1], c->res, fa, fb, fdt, cstage,
+                        c->stream)
+            : fused_launch(c->plan, c->Q[c->cur], c->Q[c->cur ^ 1], c->res, fa, fb, fdt, cstage,
+                           c->stream);
+  }
   if (s == BBW_OK) c->cur ^= 1;
   return s;
 }
@@ -754,6 +773,8 @@ extern "C" bbw_status bbw_scatter_elements(bbw_ctx *c, int n, const int *idx, co
 extern "C" bbw_status bbw_set_shots(bbw_ctx *c, int S) {
   DeviceGuard dg(c ? c->device : -1);
   if (!c || S < 1) return set_error(BBW_ERR_ARG, "bbw_set_shots: bad argument");
+  if (c->gs && S != 1)
+    return set_error(BBW_ERR_UNSUPPORTED, "bbw_set_shots: one shot in the GEMM precision form");
   cudaStreamSynchronize(c->stream);
   const size_t n = (size_t)S * c->K * 4 * c->Np;
   if ((size_t)S * c->K * 4 * c->Np > ((size_t)1 << 40))
@@ -799,6 +820,8 @@ extern "C" bbw_status bbw_set_sources(bbw_ctx *c, int nent, const int *shot, con
   DeviceGuard dg(c ? c->device : -1);
   if (!c || nent < 0 || (nent > 0 && (!shot || !elem || !vec)))
     return set_error(BBW_ERR_ARG, "bbw_set_sources: bad argument");
+  if (c->gs && nent > 0)
+    return set_error(BBW_ERR_UNSUPPORTED, "bbw_set_sources: no sources in the GEMM precision form");
   cudaStreamSynchronize(c->stream);
   cudaFree(c->src_off), cudaFree(c->src_elem), cudaFree(c->src_vec), cudaFree(c->src_tile);
   c->src_off = c->src_elem = c->src_tile = nullptr, c->src_vec = nullptr;

@@ -9,6 +9,7 @@
 #include "bbwadg.h"
 #include "device_common.cuh"
 #include "fused.h"
+#include "gemm_stage.h"
 
 namespace bbw {
 
@@ -77,6 +78,7 @@ struct bbw_ctx {
   int *rec_elem = nullptr;
   float *rec_w = nullptr, *traces = nullptr;
   bbw::TcPlan tc;
+  bbw::GemmStage *gs = nullptr;  // precision-study GEMM form (null: fused or tensor-core stage)
   float *geo_tc = nullptr;
   void *ops_tc = nullptr;
   int *err = nullptr;

@@ -35,7 +35,7 @@ RK4C = (0.0,
         1.0)
 
 VARIANTS = {"nodal": 0, "bb": 1}
-PRECISIONS = {"fp32": 0, "f16x3": 1, "bf16x3": 2}
+PRECISIONS = {"fp32": 0, "f16x3": 1, "bf16x3": 2, "tf32": 3}
 BCS = {"pressure_release": 0, "rigid": 1}
 
 

@@ -374,18 +374,21 @@ def adjoint_workload(args, torch, dist, rank, world):
 def precision_workload(args, torch):
     """Error study on the standing mode p = cos(pi x)cos(pi y)cos(pi z)
     cos(sqrt(3) pi t), c^2 = 1, p = 0 walls on [-1/2, 1/2]^3 (exact for the
-    reference's boundary condition), h-refinement 8/16/24: FP32 stage at
-    N = 7 (the tensor-core forms need Np <= 64, Nq <= 128: N in {3, 5}), and
-    FP32 against the split-FP16 and split-BF16 tensor-core forms at N = 5.  Errors: relative
-    L2 against the exact solution at T (FP64 quadrature), and against the
-    FP64 C restatement over the first 10 steps on the 8^3 mesh."""
+    reference's boundary condition), h-refinement 8/16/24: at N = 7 the FP32
+    fused stage against the GEMM precision form (split FP16, split BF16, TF32
+    contractions as cuBLAS GEMMs; the fused tensor-core stage needs
+    Np <= 64), at N = 5 the FP32 stage against the split-FP16 and split-BF16
+    tensor-core stage and TF32 on the GEMM form.  Errors: relative L2
+    against the exact solution at T (FP64 quadrature), and against the FP64
+    C restatement over the first 10 steps on the 8^3 mesh."""
     import math
     from oracle import Oracle
     from bbwadg_b200 import WaveSolver, make_problem
     from bbwadg_b200.problem import cavity_mode
     T = args.prec_time
     rows = []
-    for N, precs in ((7, ("fp32",)), (5, ("fp32", "f16x3", "bf16x3"))):
+    for N, precs in ((7, ("fp32", "f16x3", "bf16x3", "tf32")),
+                     (5, ("fp32", "f16x3", "bf16x3", "tf32"))):
         cub, tri = reference_rule(N)
         for nh in (8, 16, 24):
             p = make_problem(N, nh, c2="one", ic="cavity", lo=-0.5, hi=0.5, cubature=cub,
@@ -393,6 +396,7 @@ def precision_workload(args, torch):
             nsteps = int(math.ceil(T / p.dt))
             dt = float(np.float32(T / nsteps))
             zero = np.zeros(p.K * 4 * p.Np, np.float32)
+            q64 = None
             for prec in precs:
                 s = WaveSolver(p, precision=prec)
                 s.set_data(p.Q0)
@@ -407,14 +411,18 @@ def precision_workload(args, torch):
                 Q = s.get_data()
                 err, rel = p.l2_error(Q, nsteps * dt, cavity_mode)
                 row = {"N": N, "n": nh, "K": p.K, "precision": prec, "steps": nsteps,
+                       "form": ("fused FP32" if prec == "fp32" else
+                                "tensor-core stage" if (N <= 5 and prec != "tf32") else
+                                "GEMM precision form"),
                        "rel_l2_vs_exact": rel, "ms_per_step": 1e3 * el / nsteps}
                 if nh == 8:
                     s.set_data(p.Q0)
                     s.set_residual(zero)
                     s.steps(dt, 10)
                     q10 = s.get_data()
-                    q64, _ = Oracle(N, p.K, p.ops_dict(), p.geo_dict(), dtype=np.float64).run(
-                        p.Q0.astype(np.float64), dt, 50)
+                    if q64 is None:  # once per mesh
+                        q64, _ = Oracle(N, p.K, p.ops_dict(), p.geo_dict(),
+                                        dtype=np.float64).run(p.Q0.astype(np.float64), dt, 50)
                     row["rel_l2_vs_fp64_10_steps"] = float(
                         np.linalg.norm(q10 - q64) / np.linalg.norm(q64))
                 rows.append(row)

@@ -248,7 +248,14 @@ typedef struct bbw_ops_desc {
  * nodal or BB (BB: the dense equivalents of the sparse BB derivative and
  * lift applied to BB coefficients), and the adjoint (its forward and
  * recomputation run the same stage). */
-enum { BBW_PREC_FP32 = 0, BBW_PREC_F16X3 = 1, BBW_PREC_BF16X3 = 2 };
+enum { BBW_PREC_FP32 = 0, BBW_PREC_F16X3 = 1, BBW_PREC_BF16X3 = 2, BBW_PREC_TF32 = 3 };
+/* Precision-study form: F16X3 and BF16X3 at orders the fused tensor-core
+ * stage does not take (N >= 6, or Nq > 128), and TF32 at every order, run
+ * the same contractions as GEMMs over all elements (cuBLAS; split pairs as
+ * three GEMMs with per-element power-of-two scaling, TF32 as one GEMM with
+ * TF32 inputs and FP32 accumulation) around this library's flux, split and
+ * update kernels: one shot, no sources, no adjoint (BBW_ERR_UNSUPPORTED);
+ * its speed is that of separate launches over HBM intermediates. */
 
 /* Uploads mesh and operators (cpp/src/WaveOKL3d.cpp:1400-1615 and
  * :894-909) to the current CUDA device; state and residual start at zero.
