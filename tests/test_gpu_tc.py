@@ -96,15 +96,27 @@ def test_tc_many_tiles_per_cta_and_tiny_tiles(cuda):
     s.close()
 
 
-def test_tc_rejects_unsupported(cuda):
-    """Np > 64 (N >= 6: operators beyond one M = 64 MMA and one SM's shared
-    memory) and N = 1 are refused, for both bases."""
+def test_tc_other_orders_take_the_gemm_form(cuda):
+    """N >= 6 (Np > 64: operators beyond one M = 64 MMA and one SM's shared
+    memory) and N = 1 do not fit the fused tensor-core stage; a split-FP16
+    context there runs the GEMM form instead (one shot only, so set_shots(2)
+    is refused), for both bases, within the FP32 bar of the FP64
+    restatement after 2 LSRK45 steps."""
     from bbwadg_b200._lib import BBWError
+    from oracle import Oracle
     for N, n in ((6, 1), (1, 2)):
         for variant in ("nodal", "bb"):
-            p = make_problem(N, n, variant=variant)
+            p = make_problem(N, n, variant=variant, c2="sine")
+            q64, _ = Oracle(N, p.K, p.ops_dict(), p.geo_dict(), variant=variant,
+                            dtype=np.float64).run(p.Q0.astype(np.float64), p.dt, 10)
+            s = WaveSolver(p, precision="f16x3")
             with pytest.raises(BBWError):
-                WaveSolver(p, precision="f16x3")
+                s.set_shots(2)
+            s.set_data(p.Q0)
+            s.steps(p.dt, 2)
+            err = rel_l2(s.get_data(), q64)
+            s.close()
+            assert err < TOL, (N, variant, err)
 
 
 @pytest.mark.parametrize("prec", ["f16x3", "bf16x3"])
