@@ -413,7 +413,9 @@ extern "C" bbw_status bbw_create_ex(const bbw_mesh_desc *m, const bbw_ops_desc *
     // K-major layout
     TcPlan &tp = c->tc;
     tp.N = N, tp.K = K, tp.Nq = Nq, tp.bc = bc, tp.bf = precision == BBW_PREC_BF16X3;
-    tp.table_ints = (int)tab.size(), tp.pat_off = pat_off;
+    // Fmask and the face permutations only: the BB tables after them serve
+    // the FP32 stage (the tensor-core stage applies dense BB operators)
+    tp.table_ints = bb_off, tp.pat_off = pat_off;
     tp.L = tc_layout(N, Nq, tp.table_ints);
     const TcLayout &TL = tp.L;
     std::vector<float> geo((size_t)K * TC_GEO, 0.f);
