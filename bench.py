@@ -254,7 +254,7 @@ def shots_workload(args, torch, dist, world):
            "N": N, "K": prob.K, "shots": S}
     finals = {}
     for label, nshot, prec in (("batched", S, "fp32"), ("one_shot", 1, "fp32"),
-                               ("batched_f16x3", S, "f16x3")):
+                               ("batched_f16x3", S, "f16x3"), ("one_shot_f16x3", 1, "f16x3")):
         s = WaveSolver(prob, precision=prec)
         s.set_shots(nshot)
         s.set_sources(*shot_sources(prob, nshot, 99), f0=4.0, amplitude=1e4, stage_times=True)
