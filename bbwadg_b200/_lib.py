@@ -107,6 +107,8 @@ SIGNATURES = {
     "bbw_forward": (c_int, [c_void_p, c_float, c_int, c_int, ctypes.POINTER(c_void_p)]),
     "bbw_backward": (c_int, [c_void_p, c_void_p, P, P, P]),
     "bbw_tape_free": (c_int, [c_void_p]),
+    "bbw_forward_ex": (c_int, [c_void_p, c_float, c_int, c_int, c_int, ctypes.POINTER(c_void_p)]),
+    "bbw_tape_kind": (c_int, [c_void_p]),
     "bbw_device_state": (c_int, [c_void_p, ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p),
                                  ctypes.POINTER(c_void_p)]),
     "bbw_gordon_hall_sphere": (c_int, [c_int, c_int, P, P, P, P, P]),

@@ -1,13 +1,14 @@
 // Forward / backward pair of the discrete adjoint (receiver-misfit
 // gradient with respect to c^2 at the cubature points).
 //
-// bbw_forward advances the context like bbw_steps (same fused stage, same
-// CUDA graph, traces recorded by the receivers) and keeps the state at
-// every `checkpoint_every`-th step start.  bbw_backward sweeps the steps in
-// reverse: each checkpoint segment is recomputed forward once (step-start
-// states kept), each step's five stage inputs are recomputed from its start
-// state with the same fused kernel, and the stages are reversed with the
-// adjoint kernels of kernels_adj.cu.  The c^2 gradient is accumulated in
+// bbw_forward advances the context like bbw_steps (same fused stage, traces
+// recorded by the receivers).  Its tape keeps either the pre-c^2 cubature
+// values of every stage (when the device has room: on a B200 the 400-step,
+// 8-shot N = 4 workload on 24 576 elements takes 90 GB), which is all the
+// reverse sweep needs, or the state at every `checkpoint_every`-th step
+// start, from which bbw_backward recomputes each segment forward once with
+// the same stage kernel.  The stages are reversed with the adjoint kernels
+// of kernels_adj.cu.  The c^2 gradient is accumulated in
 // FP64.  There is no reference counterpart; the forward operators are the
 // reference's rk_volume / rk_surface / rk_update_WADG
 // (cpp/okl/WaveKernels.okl:44-260, cpp/okl/WaveKernelsWADG.okl:1760-1887).
@@ -29,6 +30,7 @@ struct bbw_tape {
   double t0 = 0.0;
   size_t state = 0;           // floats per state (all shots)
   std::vector<float *> ck;    // step-start states at steps 0, every, 2 every, ...
+  float *vq_all = nullptr;    // or: cubature values of every stage, [step][stage][S][Nq][K]
 };
 
 namespace bbw {
@@ -158,14 +160,23 @@ extern "C" bbw_status bbw_set_c2q(bbw_ctx *c, const float *c2q) {
 extern "C" bbw_status bbw_tape_free(bbw_tape *t) {
   if (!t) return BBW_OK;
   for (float *p : t->ck) cudaFree(p);
+  cudaFree(t->vq_all);
   delete t;
   return BBW_OK;
 }
 
+extern "C" int bbw_tape_kind(const bbw_tape *t) { return t && t->vq_all ? 1 : 0; }
+
 extern "C" bbw_status bbw_forward(bbw_ctx *c, float dt, int nsteps, int checkpoint_every,
                                   bbw_tape **out) {
+  return bbw_forward_ex(c, dt, nsteps, checkpoint_every, BBW_TAPE_CUBATURE, out);
+}
+
+extern "C" bbw_status bbw_forward_ex(bbw_ctx *c, float dt, int nsteps, int checkpoint_every,
+                                     int keep, bbw_tape **out) {
   DeviceGuard dg(c ? c->device : -1);
-  if (!c || !out || nsteps < 1 || checkpoint_every < 1 || !(dt > 0.f))
+  if (!c || !out || nsteps < 1 || checkpoint_every < 1 || !(dt > 0.f) ||
+      (keep != BBW_TAPE_CHECKPOINTS && keep != BBW_TAPE_CUBATURE))
     return set_error(BBW_ERR_ARG, "bbw_forward: bad argument");
   *out = nullptr;
   if (c->R <= 0) return set_error(BBW_ERR_STATE, "bbw_forward: no receivers set");
@@ -183,6 +194,25 @@ extern "C" bbw_status bbw_forward(bbw_ctx *c, float dt, int nsteps, int checkpoi
   bbw_tape *t = new bbw_tape;
   t->nsteps = nsteps, t->every = checkpoint_every, t->step0 = st0, t->dt = dt, t->t0 = t0;
   t->state = (size_t)c->S * c->K * 4 * c->Np;
+  const size_t vqn = (size_t)c->S * c->Nq * c->K;  // cubature values per stage
+  if (keep == BBW_TAPE_CUBATURE) {
+    size_t fr = 0, tot = 0;
+    const size_t need = (size_t)nsteps * 5 * vqn * sizeof(float);
+    void *p = nullptr;
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && need + ((size_t)4 << 30) < fr &&
+        cudaMalloc(&p, need) == cudaSuccess)
+      t->vq_all = static_cast<float *>(p);  // every entry is written by the forward stages
+    cudaGetLastError();  // no room after all: checkpoints
+  }
+  if (t->vq_all) {
+    for (int n = 0; n < nsteps; ++n)
+      if ((s = step_storing_cubature(c, dt, t->vq_all + (size_t)n * 5 * vqn, vqn)) != BBW_OK) {
+        bbw_tape_free(t);
+        return s;
+      }
+    *out = t;
+    return BBW_OK;
+  }
   const int nck = (nsteps + checkpoint_every - 1) / checkpoint_every;
   for (int i = 0; i < nck; ++i) {
     float *p = nullptr;
@@ -226,9 +256,10 @@ extern "C" bbw_status bbw_backward(bbw_ctx *c, bbw_tape *t, const float *dL_dtra
   cudaStream_t st = c->stream;
   const AdjOps &a = c->adj;
   DevBuf buf;
-  float *lamQ, *lamR, *z, *rhs, *sigma, *res, *g, *seg, *stq, *vq;
+  float *lamQ, *lamR, *z, *rhs, *sigma, *res, *g, *seg = nullptr, *stq = nullptr, *vq = nullptr;
   double *grad, *tdev;
   const int seglen = std::min(every, nsteps);
+  const bool full = t->vq_all != nullptr;  // the tape holds every stage's cubature values
   if ((s = buf.get(&lamQ, t->state, "bbw_backward")) != BBW_OK ||
       (s = buf.get(&lamR, t->state, "bbw_backward")) != BBW_OK ||
       (s = buf.get(&z, t->state, "bbw_backward")) != BBW_OK ||
@@ -236,11 +267,13 @@ extern "C" bbw_status bbw_backward(bbw_ctx *c, bbw_tape *t, const float *dL_dtra
       (s = buf.get(&sigma, (size_t)S * K * NF, "bbw_backward")) != BBW_OK ||
       (s = buf.get(&res, t->state, "bbw_backward")) != BBW_OK ||
       (s = buf.get(&g, (size_t)S * R * nsteps, "bbw_backward")) != BBW_OK ||
-      (s = buf.get(&seg, (size_t)seglen * t->state, "bbw_backward: segment states")) != BBW_OK ||
-      (s = buf.get(&stq, (size_t)5 * t->state, "bbw_backward: stage states")) != BBW_OK ||
-      (s = buf.get(&vq, (size_t)5 * S * Nq * K, "bbw_backward: cubature values")) != BBW_OK ||
       (s = buf.get(&grad, (size_t)K * Nq, "bbw_backward")) != BBW_OK ||
       (s = buf.get(&tdev, 1, "bbw_backward")) != BBW_OK)
+    return s;
+  if (!full &&
+      ((s = buf.get(&seg, (size_t)seglen * t->state, "bbw_backward: segment states")) != BBW_OK ||
+       (s = buf.get(&stq, (size_t)5 * t->state, "bbw_backward: stage states")) != BBW_OK ||
+       (s = buf.get(&vq, (size_t)5 * S * Nq * K, "bbw_backward: cubature values")) != BBW_OK))
     return s;
   cudaError_t e = cudaStreamSynchronize(st);
   if (e == cudaSuccess)
@@ -290,7 +323,7 @@ extern "C" bbw_status bbw_backward(bbw_ctx *c, bbw_tape *t, const float *dL_dtra
   // reverse sweep needs no second recomputation (the adjoint stages need only
   // those values, not the forward states).
   float *vq_all = nullptr;
-  {
+  if (!full) {
     size_t fr = 0, tot = 0;
     const size_t need = (size_t)seglen * 5 * vqn * sizeof(float);
     if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && need + ((size_t)2 << 30) < fr &&
@@ -300,7 +333,9 @@ extern "C" bbw_status bbw_backward(bbw_ctx *c, bbw_tape *t, const float *dL_dtra
   const int nseg = (nsteps + every - 1) / every;
   for (int sg = nseg - 1; sg >= 0; --sg) {
     const int n0 = sg * every, len = std::min(every, nsteps - n0);
-    if (vq_all) {
+    if (full) {
+      // nothing to recompute
+    } else if (vq_all) {
       // forward over the segment; stage outputs chain through stq[1..4] and
       // the step outputs alternate between z and seg
       const float *q = t->ck[sg];
@@ -329,7 +364,9 @@ extern "C" bbw_status bbw_backward(bbw_ctx *c, bbw_tape *t, const float *dL_dtra
           BBW_OK)
         return s;
       const float *vqs = vq;
-      if (vq_all) {
+      if (full) {
+        vqs = t->vq_all + (size_t)n * 5 * vqn;
+      } else if (vq_all) {
         vqs = vq_all + (size_t)j * 5 * vqn;
       } else {
         // the step's five stages again from its start state (bit-identical

@@ -556,6 +556,22 @@ static bbw_status one_step(bbw_ctx *c, float dt) {
                             c->traces, c->max_steps, c->d_time, c->d_step, dt, c->stream);
 }
 
+// one LSRK45 step launched stage by stage (no graph), as one_step, storing
+// each stage's pre-c^2 cubature values at vq + i * vqn (the adjoint tape)
+bbw_status step_storing_cubature(bbw_ctx *c, float dt, float *vq, size_t vqn) {
+  float *keep_f = c->plan.vq_out, *keep_t = c->tc.vq_out;
+  bbw_status s = BBW_OK;
+  for (int i = 0; i < 5 && s == BBW_OK; ++i) {
+    c->plan.vq_out = c->tc.vq_out = vq + (size_t)i * vqn;
+    s = bbw_stage_ex(c, (float)kRK4A[i], (float)kRK4B[i], dt,
+                     c->src_stage_times ? (float)kRK4C[i] : 0.f);
+  }
+  c->plan.vq_out = keep_f, c->tc.vq_out = keep_t;
+  if (s != BBW_OK) return s;
+  return record_and_advance(c->N, c->K, c->S, c->Q[c->cur], c->R, c->rec_elem, c->rec_w,
+                            c->traces, c->max_steps, c->d_time, c->d_step, dt, c->stream);
+}
+
 extern "C" bbw_status bbw_steps(bbw_ctx *c, float dt, int nsteps) {
   DeviceGuard dg(c ? c->device : -1);
   if (!c || nsteps < 0) return set_error(BBW_ERR_ARG, "bbw_steps: bad argument");

@@ -93,6 +93,10 @@ struct bbw_ctx {
 };
 
 
+// one LSRK45 step launched stage by stage that also stores each stage's
+// pre-c^2 cubature values at vq + i * vqn (capi.cu)
+bbw_status step_storing_cubature(bbw_ctx *c, float dt, float *vq, size_t vqn);
+
 namespace bbw {
 void adj_release(bbw_ctx *c);
 

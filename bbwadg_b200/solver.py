@@ -257,11 +257,17 @@ class WaveSolver:
             raise ValueError("c2q must have K*Nq values")
         _lib.call("bbw_set_c2q", self._h, c2q.ctypes.data)
 
-    def forward(self, dt, nsteps, checkpoint_every=50):
-        """nsteps steps as steps() does, keeping checkpoints; returns a Tape."""
+    def forward(self, dt, nsteps, checkpoint_every=50, keep="cubature"):
+        """nsteps steps as steps() does; returns a Tape.  keep="cubature"
+        stores every stage's cubature values when the device has room (the
+        backward pass then recomputes nothing), else checkpoints every
+        checkpoint_every steps; keep="checkpoints" always checkpoints."""
+        modes = {"checkpoints": 0, "cubature": 1}
+        if keep not in modes:
+            raise ValueError("keep must be 'checkpoints' or 'cubature'")
         t = ctypes.c_void_p()
-        _lib.call("bbw_forward", self._h, float(dt), int(nsteps), int(checkpoint_every),
-                  ctypes.byref(t))
+        _lib.call("bbw_forward_ex", self._h, float(dt), int(nsteps), int(checkpoint_every),
+                  modes[keep], ctypes.byref(t))
         return Tape(t, int(nsteps))
 
     def backward(self, tape, dL_dtraces, want_state=False):
@@ -307,10 +313,12 @@ class WaveSolver:
 
 
 class Tape:
-    """Checkpoints of one bbw_forward call (freed with the object)."""
+    """What one bbw_forward call kept (freed with the object): every stage's
+    cubature values (kind "cubature") or checkpoints ("checkpoints")."""
 
     def __init__(self, handle, nsteps):
         self.handle, self.nsteps = handle, nsteps
+        self.kind = "cubature" if _lib.lib().bbw_tape_kind(handle) else "checkpoints"
 
     def free(self):
         if getattr(self, "handle", None):

@@ -340,6 +340,7 @@ def adjoint_workload(args, torch, dist, rank, world):
         tape = run(c2_back, True)
         s.sync()
         t1 = time.perf_counter()
+        kind = tape.kind
         tr = s.get_traces()
         misfit = 0.5 * float(((tr - obs).astype(np.float64) ** 2).sum())
         t2 = time.perf_counter()
@@ -355,21 +356,23 @@ def adjoint_workload(args, torch, dist, rank, world):
             t = torch.tensor([tf, tb], device="cuda", dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             tf, tb = float(t[0]), float(t[1])
-        return tf, tb, misfit, grad
+        return tf, tb, misfit, grad, kind
 
-    tf, tb, misfit, grad = one("fp32")
-    tf2, tb2, misfit2, grad2 = one("f16x3")
+    tf, tb, misfit, grad, kind = one("fp32")
+    tf2, tb2, misfit2, grad2, kind2 = one("f16x3")
     return {"workload": "forward + adjoint c2 gradient, N=4, 16^3x6 tets (K=%d), %d shots per "
                         "GPU, %d receivers, %d steps, checkpoints every %d" % (prob.K, S, R, steps,
                                                                                every),
+            "tape": kind,  # cubature: every stage's Vq S(Q)_p kept, no recomputation
             "forward_s": tf, "backward_s": tb, "total_s": tf + tb, "shots_total": 8 * world,
             "misfit": misfit, "grad_norm": float(np.linalg.norm(grad)),
             "grad_finite": bool(np.isfinite(grad).all()),
-            "f16x3": {"forward_s": tf2, "backward_s": tb2, "total_s": tf2 + tb2,
+            "f16x3": {"tape": kind2, "forward_s": tf2, "backward_s": tb2, "total_s": tf2 + tb2,
                       "misfit": misfit2,
                       "grad_rel_l2_vs_fp32": float(np.linalg.norm(grad2 - grad) /
                                                    np.linalg.norm(grad)),
-                      "note": "forward and recomputation on the split-FP16 tensor-core stage"}}
+                      "note": "forward (and any recomputation) on the split-FP16 tensor-core "
+                              "stage"}}
 
 
 def precision_workload(args, torch):

@@ -481,11 +481,25 @@ bbw_status bbw_set_c2q(bbw_ctx *ctx, const float *c2q);
 bbw_status bbw_forward(bbw_ctx *ctx, float dt, int nsteps, int checkpoint_every,
                        bbw_tape **tape);
 
+/* What a tape keeps (bbw_forward_ex).  CHECKPOINTS: the state every
+ * checkpoint_every steps; bbw_backward recomputes each segment once.
+ * CUBATURE: every stage's pre-c^2 cubature values Vq S(Q)_p ([S][Nq][K]
+ * floats per stage, 5 stages per step), which is all the reverse sweep
+ * needs, so bbw_backward recomputes nothing; taken only when the device has
+ * room for them with 4 GiB to spare, else the tape falls back to
+ * checkpoints.  bbw_forward keeps CUBATURE when it fits. */
+#define BBW_TAPE_CHECKPOINTS 0
+#define BBW_TAPE_CUBATURE 1
+bbw_status bbw_forward_ex(bbw_ctx *ctx, float dt, int nsteps, int checkpoint_every, int keep,
+                          bbw_tape **tape);
+/* 1 if the tape holds every stage's cubature values, 0 if checkpoints. */
+int bbw_tape_kind(const bbw_tape *tape);
+
 /* Given dL/dtraces [S][R][nsteps] (host, for the tape's steps), writes
  * dL/d(c2q) [K][Nq] (host, FP64, summed over shots) and, if dL_dQ0 is not
- * NULL, dL/d(state at the tape's first step) [S][K][4][Np].  Recomputes the
- * forward states from the checkpoints; the context's own state is left as
- * bbw_forward left it. */
+ * NULL, dL/d(state at the tape's first step) [S][K][4][Np].  From a
+ * checkpoint tape it recomputes the forward stages of each segment; the
+ * context's own state is left as bbw_forward left it. */
 bbw_status bbw_backward(bbw_ctx *ctx, bbw_tape *tape, const float *dL_dtraces, double *dL_dc2q,
                         float *dL_dQ0);
 bbw_status bbw_tape_free(bbw_tape *tape);

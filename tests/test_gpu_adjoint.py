@@ -27,7 +27,8 @@ def setup(variant, bc, S=2, N=3, n=2, seed=0, rules=(None, None)):
     return p, rec, dense
 
 
-def gpu_gradient(p, rec, dense, bc, nsteps, every, Q0, stage_times=True, precision="fp32"):
+def gpu_gradient(p, rec, dense, bc, nsteps, every, Q0, stage_times=True, precision="fp32",
+                 keep="cubature"):
     S = len(dense)
     s = WaveSolver(p, bc="rigid" if bc else "pressure_release", precision=precision)
     s.set_shots(S)
@@ -37,7 +38,8 @@ def gpu_gradient(p, rec, dense, bc, nsteps, every, Q0, stage_times=True, precisi
     s.set_receivers(*rec, nsteps)
     s.set_data(np.tile(Q0, S))
     s.set_time(0.0)
-    tape = s.forward(p.dt, nsteps, every)
+    tape = s.forward(p.dt, nsteps, every, keep=keep)
+    assert tape.kind == keep  # small meshes: the cubature tape always fits
     tr = s.get_traces()
     grad, dq = s.backward(tape, tr, want_state=True)
     tape.free()
@@ -110,9 +112,24 @@ def test_directional_derivatives_match_finite_differences(cuda):
 
 def test_checkpoint_interval_does_not_change_the_gradient(cuda):
     p, rec, dense = setup("nodal", 0, S=1)
-    ref = gpu_gradient(p, rec, dense, 0, 10, 1, p.Q0)[1]
+    ref = gpu_gradient(p, rec, dense, 0, 10, 1, p.Q0, keep="checkpoints")[1]
     for every in (3, 10, 64):
-        assert np.array_equal(gpu_gradient(p, rec, dense, 0, 10, every, p.Q0)[1], ref)
+        assert np.array_equal(
+            gpu_gradient(p, rec, dense, 0, 10, every, p.Q0, keep="checkpoints")[1], ref)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "f16x3"])
+@pytest.mark.parametrize("variant", ["nodal", "bb"])
+def test_cubature_tape_equals_checkpoint_tape(cuda, variant, precision):
+    """A tape of every stage's cubature values (no recomputation in the
+    backward pass) and a checkpoint tape (each segment recomputed) give the
+    same traces, c^2 gradient and state gradient bit for bit: the forward
+    stages are the same kernels on the same inputs."""
+    p, rec, dense = setup(variant, 0, S=2)
+    a = gpu_gradient(p, rec, dense, 0, 12, 5, p.Q0, precision=precision, keep="cubature")
+    b = gpu_gradient(p, rec, dense, 0, 12, 5, p.Q0, precision=precision, keep="checkpoints")
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
 
 
 def test_state_gradient_matches_fp64_adjoint(cuda):
