@@ -477,7 +477,9 @@ bbw_status bbw_set_c2q(bbw_ctx *ctx, const float *c2q);
 
 /* Advances nsteps steps of dt exactly as bbw_steps does (receivers must be
  * set; traces land at the current step count onwards) and returns a tape
- * holding the state at every checkpoint_every-th step start. */
+ * for bbw_backward: bbw_forward_ex with BBW_TAPE_CUBATURE (every stage's
+ * cubature values when they fit, else the state at every
+ * checkpoint_every-th step start).  No counterpart in the reference. */
 bbw_status bbw_forward(bbw_ctx *ctx, float dt, int nsteps, int checkpoint_every,
                        bbw_tape **tape);
 
