@@ -361,8 +361,8 @@ def adjoint_workload(args, torch, dist, rank, world):
     tf, tb, misfit, grad, kind = one("fp32")
     tf2, tb2, misfit2, grad2, kind2 = one("f16x3")
     return {"workload": "forward + adjoint c2 gradient, N=4, 16^3x6 tets (K=%d), %d shots per "
-                        "GPU, %d receivers, %d steps, checkpoints every %d" % (prob.K, S, R, steps,
-                                                                               every),
+                        "GPU, %d receivers, %d steps; tape: every stage's cubature values, or "
+                        "checkpoints every %d where they do not fit" % (prob.K, S, R, steps, every),
             "tape": kind,  # cubature: every stage's Vq S(Q)_p kept, no recomputation
             "forward_s": tf, "backward_s": tb, "total_s": tf + tb, "shots_total": 8 * world,
             "misfit": misfit, "grad_norm": float(np.linalg.norm(grad)),
